@@ -1,0 +1,1095 @@
+// dda_oracle.cpp -- CPU restatement of the reference DDA hot path.
+//
+// TEST INFRASTRUCTURE ONLY.  This library is the checker for the CUDA path in
+// dda_b200: only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline /
+// reference arm may load it.  The product never links or calls it.
+//
+// Parity status: UNPINNED against outputs of the reference itself.  The
+// reference (steffen-kiess/dda) cannot be built in this environment (it needs
+// Boost, FFTW3, HDF5 and omake, none of which are present) and its own tests
+// compare against a live ADDA binary (DDA/test-adda.sh, DDA/compare-adda.sh)
+// that is absent too, so no reference output exists to pin against.  The
+// restatement is pinned instead by independent checks kept in tests/:
+//   * the FFT against numpy.fft and a naive DFT,
+//   * the FFT matvec against a brute-force O(nv^2) direct sum of the same
+//     Green's tensor (pins the D-matrix sign, layout and 1/N normalisation),
+//   * voxelisation counts against the reference fixture DDA/box_10_8_6.geom
+//     and the dipole counts quoted for the reference's README workloads,
+//   * DDA cross sections of spheres against the Mie series (EMSim/Mie.cpp).
+//
+// Every function cites the reference file:line it follows.  Third-party
+// arithmetic: the reference computes FFTs with FFTW3 (un-vendored, README asks
+// for ">= 3.2.2", no pinned version; call sites LinAlg/FFTWPlan.cpp:82,113).
+// This file restates the published DFT definition FFTW implements
+// (unnormalised, forward kernel exp(-2 pi i jk/n), backward exp(+2 pi i jk/n))
+// with a recursive mixed-radix Cooley-Tukey decomposition.
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+typedef long double ldouble;
+typedef std::complex<double> cd;
+typedef std::complex<ldouble> cld;
+
+namespace {
+
+// Constants of DDA/FPConst.hpp:36-50 (ldr_b* from doi:10.1086/172396).
+const ldouble kPi = 3.1415926535897932384626433832795028L;
+const ldouble kTwoPi = 6.2831853071795864769252867665590056L;
+const ldouble kFourPi = 12.5663706143591729538505735331180112L;
+const double kLdrB1 = 1.8915316;
+const double kLdrB2 = -0.1648469;
+const double kLdrB3 = 1.7700004;
+
+std::string g_error;
+
+// ---------------------------------------------------------------- FFT ----
+// Restatement of the DFT that FFTW computes (LinAlg/FFTWPlan.cpp:82,113):
+// y_k = sum_j x_j exp(-/+ 2 pi i jk/n), unnormalised both ways.
+struct FftPlan {
+  size_t n;
+  std::vector<int> factors;
+  std::vector<cd> tw;  // exp(-2 pi i k / n), k = 0..n-1, from long double
+
+  explicit FftPlan(size_t n_) : n(n_), tw(n_) {
+    size_t m = n;
+    for (int p : {4, 2, 3, 5, 7}) {
+      while (m % p == 0) {
+        factors.push_back(p);
+        m /= p;
+      }
+    }
+    for (size_t p = 11; m > 1; p += 2) {
+      while (m % p == 0) {
+        factors.push_back((int)p);
+        m /= p;
+      }
+    }
+    for (size_t k = 0; k < n; k++) {
+      ldouble a = -kTwoPi * (ldouble)k / (ldouble)n;
+      tw[k] = cd((double)cosl(a), (double)sinl(a));
+    }
+  }
+
+  // Recursive decimation in time: out[0..len) = DFT of in[0], in[s], ...
+  void rec(const cd* in, size_t stride, cd* out, size_t len, size_t fi,
+           bool inv, std::vector<cd>& t) const {
+    if (len == 1) {
+      out[0] = in[0];
+      return;
+    }
+    int p = factors[fi];
+    size_t m = len / p;
+    for (int q = 0; q < p; q++)
+      rec(in + q * stride, stride * p, out + q * m, m, fi + 1, inv, t);
+    size_t step = n / len;  // table index scale: w_len^j = w_n^(j*step)
+    for (size_t k = 0; k < m; k++) {
+      for (int q = 0; q < p; q++) {
+        cd w = tw[(q * k * step) % n];
+        if (inv) w = std::conj(w);
+        t[q] = out[q * m + k] * w;
+      }
+      for (int s = 0; s < p; s++) {
+        cd acc = 0;
+        for (int q = 0; q < p; q++) {
+          cd w = tw[((size_t)q * s * m * step) % n];
+          if (inv) w = std::conj(w);
+          acc += t[q] * w;
+        }
+        out[k + m * s] = acc;
+      }
+    }
+  }
+
+  // In-place transform of `count` lines: line b starts at data + b*dist,
+  // elements are `stride` apart.
+  void exec(cd* data, size_t count, size_t stride, size_t dist, bool inv) const {
+    std::vector<cd> a(n), b(n), t(16);
+    if (factors.size() && *std::max_element(factors.begin(), factors.end()) > 16)
+      t.resize(*std::max_element(factors.begin(), factors.end()));
+    for (size_t c = 0; c < count; c++) {
+      cd* d = data + c * dist;
+      for (size_t i = 0; i < n; i++) a[i] = d[i * stride];
+      rec(a.data(), 1, b.data(), n, 0, inv, t);
+      for (size_t i = 0; i < n; i++) d[i * stride] = b[i];
+    }
+  }
+};
+
+std::mutex g_plan_mutex;
+std::map<size_t, std::shared_ptr<FftPlan>> g_plans;
+
+std::shared_ptr<FftPlan> plan(size_t n) {
+  std::lock_guard<std::mutex> lock(g_plan_mutex);
+  auto it = g_plans.find(n);
+  if (it != g_plans.end()) return it->second;
+  auto p = std::make_shared<FftPlan>(n);
+  g_plans[n] = p;
+  return p;
+}
+
+// ------------------------------------------------------------ fftFit ----
+// DDA/DDAParams.cpp:45-90.
+uint32_t fftFit(uint32_t x, uint32_t override, bool supportNonPot) {
+  if (override != 0) return override;
+  if (x == 0) return 0;
+  if (!supportNonPot) {
+    uint32_t ret = 1;
+    while (x > 1) {
+      ret *= 2;
+      x = (x + 1) / 2;
+    }
+    return ret;
+  }
+  uint32_t ret = x;
+  if (ret % 2 == 1) ret++;
+  for (;;) {
+    uint32_t y = ret;
+    while (y % 2 == 0) y /= 2;
+    while (y % 3 == 0) y /= 3;
+    while (y % 5 == 0) y /= 5;
+    while (y % 7 == 0) y /= 7;
+    if (y == 1) return ret;
+    ret += 2;
+  }
+}
+
+uint32_t roundUp(uint32_t v, uint32_t d) { return ((v + d - 1) / d) * d; }
+
+}  // namespace
+
+// ============================================================ geometry ====
+// DipoleGeometry (DDA/DipoleGeometry.hpp:49-156): positions (x,y,z) as u32,
+// 0-based material index per dipole, bounding box, ldouble grid unit.
+struct orc_geom {
+  ldouble gridUnit = 0;
+  uint32_t box[3] = {0, 0, 0};
+  uint32_t matCount = 0;
+  std::vector<uint32_t> pos;  // nv*3 interleaved x,y,z
+  std::vector<uint8_t> mat;
+  bool ok = true;
+
+  // DDA/DipoleGeometry.cpp:90-107
+  void addDipole(uint32_t x, uint32_t y, uint32_t z, uint8_t m) {
+    if (!(box[2] <= z + 1)) {  // positions must be sorted by z
+      ok = false;
+      g_error = "dipoles not sorted by z";
+    }
+    pos.push_back(x);
+    pos.push_back(y);
+    pos.push_back(z);
+    mat.push_back(m);
+    if (x >= box[0]) box[0] = x + 1;
+    if (y >= box[1]) box[1] = y + 1;
+    if (z >= box[2]) box[2] = z + 1;
+    if (m >= matCount) matCount = m + 1u;
+  }
+};
+
+extern "C" {
+
+const char* orc_last_error() { return g_error.c_str(); }
+
+// EMSim/Length.cpp:30-67: a number parsed as long double, times a unit
+// factor in long double.  Returns 0 on success.
+int orc_parse_number(const char* s, ldouble* out) {
+  std::istringstream in(s);
+  ldouble value;
+  in >> value;
+  if (in.fail()) return -1;
+  *out = value;
+  return 0;
+}
+
+int orc_parse_length(const char* s, ldouble* out) {
+  std::istringstream in(s);
+  ldouble value;
+  in >> value;
+  if (in.fail()) return -1;
+  std::string unit;
+  std::getline(in, unit);
+  ldouble factor;
+  if (unit.empty() && value == 0) {
+    *out = 0;
+    return 0;
+  } else if (unit == "um" || unit == "\xc2\xb5m") {
+    factor = 1e-6L;
+  } else if (unit == "nm") {
+    factor = 1e-9L;
+  } else if (unit == "mm") {
+    factor = 1e-3L;
+  } else if (unit == "m") {
+    factor = 1e+0L;
+  } else {
+    return -1;
+  }
+  *out = value * factor;
+  return 0;
+}
+
+// Unnormalised in-place DFT of `count` contiguous lines of length n
+// (complex interleaved), the transform the reference gets from FFTW.
+void orc_fft(double* data, uint32_t n, uint32_t count, int inverse) {
+  plan(n)->exec(reinterpret_cast<cd*>(data), count, 1, n, inverse != 0);
+}
+
+uint32_t orc_fft_fit(uint32_t x, uint32_t override, int supportNonPot) {
+  return fftFit(x, override, supportNonPot != 0);
+}
+
+// DDA/Shapes.cpp:53-73 (sphere): radius in grid units as double, dipole at
+// cell centre (x - r + 0.5) kept when inside r^2; loops z, y, x.
+orc_geom* orc_geom_sphere(ldouble radius, ldouble gridUnit) {
+  orc_geom* g = new orc_geom;
+  g->gridUnit = gridUnit;
+  double r = static_cast<double>(radius / gridUnit);
+  double diameter = r * 2;
+  double r2 = r * r;
+  for (uint32_t z = 0; z < diameter; z++)
+    for (uint32_t y = 0; y < diameter; y++)
+      for (uint32_t x = 0; x < diameter; x++) {
+        double xd = x - r + 0.5;
+        double yd = y - r + 0.5;
+        double zd = z - r + 0.5;
+        if (xd * xd + yd * yd + zd * zd <= r2) g->addDipole(x, y, z, 0);
+      }
+  return g;
+}
+
+// DDA/Shapes.cpp:91-111 (cylinder along x).
+orc_geom* orc_geom_cylinder(ldouble length, ldouble radius, ldouble gridUnit) {
+  orc_geom* g = new orc_geom;
+  g->gridUnit = gridUnit;
+  double len = static_cast<double>(length / gridUnit);
+  double r = static_cast<double>(radius / gridUnit);
+  double diameter = r * 2;
+  double r2 = r * r;
+  for (uint32_t z = 0; z < diameter; z++)
+    for (uint32_t y = 0; y < diameter; y++) {
+      double yd = y - r + 0.5;
+      double zd = z - r + 0.5;
+      if (yd * yd + zd * zd <= r2)
+        for (uint32_t x = 0; x < len; x++) g->addDipole(x, y, z, 0);
+    }
+  return g;
+}
+
+// DDA/Shapes.cpp:130-143 (box): extent / grid unit in long double.
+orc_geom* orc_geom_box(ldouble sx, ldouble sy, ldouble sz, ldouble gridUnit) {
+  orc_geom* g = new orc_geom;
+  g->gridUnit = gridUnit;
+  ldouble s[3] = {sx / gridUnit, sy / gridUnit, sz / gridUnit};
+  for (uint32_t z = 0; z < s[2]; z++)
+    for (uint32_t y = 0; y < s[1]; y++)
+      for (uint32_t x = 0; x < s[0]; x++) g->addDipole(x, y, z, 0);
+  return g;
+}
+
+// DDA/Load.cpp:37-69: "x y z [m]" lines, '#' and 'N' lines skipped,
+// materials 1-based in the file (default 1).
+orc_geom* orc_geom_load_text(const char* path, ldouble gridUnit) {
+  std::ifstream in(path);
+  if (!in) {
+    g_error = std::string("cannot open ") + path;
+    return nullptr;
+  }
+  orc_geom* g = new orc_geom;
+  g->gridUnit = gridUnit;
+  std::string line;
+  while (std::getline(in, line)) {
+    if (line.empty() || line[0] == '#' || line[0] == 'N') continue;
+    std::istringstream ls(line);
+    long long x, y, z, m = 1;
+    if (!(ls >> x)) continue;
+    if (!(ls >> y >> z)) {
+      g_error = "malformed dipole line";
+      delete g;
+      return nullptr;
+    }
+    if (!(ls >> m)) m = 1;
+    if (!(m > 0 && m <= 256) || x < 0 || y < 0 || z < 0) {
+      g_error = "bad material index or coordinate";
+      delete g;
+      return nullptr;
+    }
+    g->addDipole((uint32_t)x, (uint32_t)y, (uint32_t)z, (uint8_t)(m - 1));
+  }
+  if (!g->ok) {
+    delete g;
+    return nullptr;
+  }
+  return g;
+}
+
+orc_geom* orc_geom_from_arrays(const uint32_t* pos, const uint8_t* mat,
+                               uint32_t nv, ldouble gridUnit) {
+  orc_geom* g = new orc_geom;
+  g->gridUnit = gridUnit;
+  for (uint32_t i = 0; i < nv; i++)
+    g->addDipole(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], mat ? mat[i] : 0);
+  if (!g->ok) {
+    delete g;
+    return nullptr;
+  }
+  return g;
+}
+
+uint32_t orc_geom_nv(const orc_geom* g) { return (uint32_t)g->mat.size(); }
+void orc_geom_box_size(const orc_geom* g, uint32_t* out) {
+  for (int i = 0; i < 3; i++) out[i] = g->box[i];
+}
+uint32_t orc_geom_matcount(const orc_geom* g) { return g->matCount; }
+void orc_geom_positions(const orc_geom* g, uint32_t* out) {
+  std::copy(g->pos.begin(), g->pos.end(), out);
+}
+void orc_geom_materials(const orc_geom* g, uint8_t* out) {
+  std::copy(g->mat.begin(), g->mat.end(), out);
+}
+void orc_geom_free(orc_geom* g) { delete g; }
+
+}  // extern "C"
+
+// ============================================================ problem =====
+// DDAParams (DDA/DDAParams.cpp:93-214) + CoupleConstants
+// (DDA/DDAParams.cpp:315-331) + D matrix + matvec + solvers, all in double.
+struct orc_problem {
+  // geometry
+  uint32_t nv = 0, nvs = 0, box[3] = {0, 0, 0}, grid[3] = {0, 0, 0};
+  std::vector<uint32_t> pos;
+  std::vector<uint8_t> mat;
+  uint32_t nmat = 0;
+  std::vector<cld> materials;  // nmat*3 refractive index (DiagMatrix3)
+  ldouble gridUnitL = 0;
+  double gridUnit = 0, gridUnitVol = 0, lambda = 0, waveNum = 0, kd = 0;
+  ldouble origin[3] = {0, 0, 0};  // DDA/DipoleGeometry.cpp:75-80
+
+  // D matrix, reference layout: [Gx][Gz][Gy][6] complex (offset
+  // comp + 6*(j + Gy*(k + Gz*i)), DDA/GpuMatVecInst.cl:114)
+  std::vector<cd> D;
+  // couple constants per material: cc, cc_sqrt, chi_inv (3 each)
+  std::vector<cd> cc, ccSqrt, chiInv;
+
+  // matvec scratch (DDA/MatVecCpu.cpp:48-50)
+  std::vector<cd> X;  // Xmatrix [3][bz][by][Gx] (x fastest)
+
+  size_t vecSize() const { return 3 * (size_t)nvs; }
+  size_t N() const { return (size_t)grid[0] * grid[1] * grid[2]; }
+};
+
+namespace {
+
+// DDA/DMatrixCpu.cpp:49-63.
+cd singleInteractionTerm(const orc_problem& p, double rx, double ry, double rz,
+                         int mu, int nu) {
+  double r[3] = {rx, ry, rz};
+  double rr = std::sqrt(rx * rx + ry * ry + rz * rz);
+  double q[3] = {rx / rr, ry / rr, rz / rr};
+  double kr = p.waveNum * rr;
+  double kr2 = kr * kr;
+  double qmunu = q[mu] * q[nu];
+  (void)r;
+  cd expval = std::exp(cd(0, kr)) / cd(std::pow(rr, 3.0));
+  cd br = cd(3 - kr2, -3 * kr) * qmunu;
+  if (mu == nu) br += cd(kr2 - 1, kr);
+  return expval * br;
+}
+
+// DDA/DMatrixCpu.cpp:65-74 (periodicity dimension 0).
+cd interactionTerm(const orc_problem& p, int i, int j, int k, int mu, int nu) {
+  if (!i && !j && !k) return cd(0);
+  return singleInteractionTerm(p, (double)i * p.gridUnit, (double)j * p.gridUnit,
+                               (double)k * p.gridUnit, mu, nu);
+}
+
+uint32_t clip(int32_t n, uint32_t M) {  // DDA/DMatrixCpu.cpp:124-131
+  if (n < 0) return n + M;
+  if ((uint32_t)n >= M) return n - M;
+  return n;
+}
+
+inline cd maybeConj(cd f, bool c) { return c ? std::conj(f) : f; }
+
+}  // namespace
+
+extern "C" {
+
+// DDAParams ctor (DDA/DDAParams.cpp:93-214), single process.
+// materials: nmat*3 complex refractive indices as (re, im) long double pairs.
+// grid_override: three values, 0 = automatic (fftFit).
+orc_problem* orc_problem_create(const orc_geom* g, const ldouble* materials,
+                                uint32_t nmat, ldouble lambda,
+                                const uint32_t* grid_override, int supportNonPot) {
+  if (!g || g->mat.empty()) {
+    g_error = "empty geometry";
+    return nullptr;
+  }
+  if (nmat < g->matCount) {
+    g_error = "fewer materials than material indices";
+    return nullptr;
+  }
+  orc_problem* p = new orc_problem;
+  p->nv = (uint32_t)g->mat.size();
+  p->nvs = roundUp(p->nv, 16);
+  for (int i = 0; i < 3; i++) {
+    p->box[i] = g->box[i];
+    p->grid[i] = fftFit(g->box[i] * 2, grid_override ? grid_override[i] : 0,
+                        supportNonPot != 0);
+    if (p->grid[i] % 2 != 0 || p->grid[i] < 2 * p->box[i]) {
+      g_error = "bad FFT grid";
+      delete p;
+      return nullptr;
+    }
+    // DipoleGeometry::moveToCenter, DDA/DipoleGeometry.cpp:75-80
+    p->origin[i] = -((ldouble)(g->box[i]) - 1.0L) / 2 * g->gridUnit;
+  }
+  p->pos = g->pos;
+  p->mat = g->mat;
+  p->nmat = nmat;
+  p->materials.resize(nmat * 3);
+  for (uint32_t i = 0; i < nmat * 3; i++)
+    p->materials[i] = cld(materials[2 * i], materials[2 * i + 1]);
+  p->gridUnitL = g->gridUnit;
+  p->gridUnit = (double)g->gridUnit;
+  p->gridUnitVol = (double)(g->gridUnit * g->gridUnit * g->gridUnit);
+  p->lambda = (double)lambda;
+  p->waveNum = (double)kTwoPi / p->lambda;  // DDA/DDAParams.cpp:212-213
+  p->kd = p->waveNum * p->gridUnit;
+  return p;
+}
+
+void orc_problem_free(orc_problem* p) { delete p; }
+
+void orc_problem_info(const orc_problem* p, uint32_t* out /*9*/, double* dout /*4*/) {
+  out[0] = p->nv;
+  out[1] = p->nvs;
+  for (int i = 0; i < 3; i++) {
+    out[2 + i] = p->box[i];
+    out[5 + i] = p->grid[i];
+  }
+  out[8] = p->nmat;
+  dout[0] = p->gridUnit;
+  dout[1] = p->waveNum;
+  dout[2] = p->kd;
+  dout[3] = p->gridUnitVol;
+}
+
+void orc_set_threads(int n) {
+#ifdef _OPENMP
+  omp_set_num_threads(n);
+#else
+  (void)n;
+#endif
+}
+
+int orc_max_threads() {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+// Beam polarisation convention of DDA/Beam.cpp:33-51 (ADDA's): pol 1 is the
+// "y polarisation" incPolY, pol 2 the "x polarisation" incPolX.
+void orc_beam_pol(const double* propIn, int pol, double* out3, double* prop3) {
+  ldouble pr[3] = {propIn[0], propIn[1], propIn[2]};
+  ldouble nrm = sqrtl(pr[0] * pr[0] + pr[1] * pr[1] + pr[2] * pr[2]);
+  for (int i = 0; i < 3; i++) pr[i] /= nrm;
+  ldouble px[3], py[3];
+  if (fabsl(pr[2]) >= (1 - 1e-6)) {
+    px[0] = pr[2]; px[1] = 0; px[2] = 0;
+    py[0] = 0; py[1] = 1; py[2] = 0;
+  } else {
+    ldouble t = sqrtl(1 - pr[2] * pr[2]);
+    px[0] = pr[0] * pr[2] / t; px[1] = pr[1] * pr[2] / t; px[2] = -t;
+    py[0] = -pr[1] / t; py[1] = pr[0] / t; py[2] = 0;
+  }
+  for (int i = 0; i < 3; i++) {
+    out3[i] = (double)(pol == 1 ? py[i] : px[i]);
+    if (prop3) prop3[i] = (double)pr[i];
+  }
+}
+
+// CoupleConstants (DDA/DDAParams.cpp:315-331) with the CM / LDR
+// polarisability of DDA/PolarizabilityDescription.cpp:65-110.
+// kind: 0 = cm, 1 = ldr, 2 = ldr-avgpol.  pol: 1 or 2.
+void orc_set_cc(orc_problem* p, int kind, const double* propIn, int pol) {
+  p->cc.assign(p->nmat * 3, 0);
+  p->ccSqrt.assign(p->nmat * 3, 0);
+  p->chiInv.assign(p->nmat * 3, 0);
+  double incPol[3], prop[3];
+  orc_beam_pol(propIn, pol, incPol, prop);
+  double temp = p->gridUnitVol / (double)kFourPi;
+  for (uint32_t i = 0; i < p->nmat; i++) {
+    for (int j = 0; j < 3; j++) {
+      cd m = cd((double)p->materials[i * 3 + j].real(), (double)p->materials[i * 3 + j].imag());
+      cd m2 = m * m;
+      cd uncorrected = 3.0 * temp * (m2 - cd(1)) / (m2 + cd(2));
+      cd c = uncorrected;
+      if (kind != 0) {
+        cd t1 = cd(0, 2.0 / 3 * p->kd * p->kd * p->kd);
+        double prop2[3] = {prop[0] * prop[0], prop[1] * prop[1], prop[2] * prop[2]};
+        double inc2[3] = {incPol[0] * incPol[0], incPol[1] * incPol[1], incPol[2] * incPol[2]};
+        double S;
+        if (kind == 2)
+          S = 0.5f * (1 - (prop2[0] * prop2[0] + prop2[1] * prop2[1] + prop2[2] * prop2[2]));
+        else
+          S = prop2[0] * inc2[0] + prop2[1] * inc2[1] + prop2[2] * inc2[2];
+        t1 += (kLdrB1 + (kLdrB2 + kLdrB3 * S) * m2) * p->kd * p->kd;
+        c = uncorrected / (cd(1) - (uncorrected / p->gridUnitVol) * t1);
+      }
+      p->cc[i * 3 + j] = c;
+      p->ccSqrt[i * 3 + j] = std::sqrt(c);
+      p->chiInv[i * 3 + j] = 1.0 / (temp * (m2 - cd(1)));
+    }
+  }
+}
+
+void orc_get_cc(const orc_problem* p, double* cc, double* ccSqrt, double* chiInv) {
+  for (size_t i = 0; i < p->cc.size(); i++) {
+    if (cc) { cc[2 * i] = p->cc[i].real(); cc[2 * i + 1] = p->cc[i].imag(); }
+    if (ccSqrt) { ccSqrt[2 * i] = p->ccSqrt[i].real(); ccSqrt[2 * i + 1] = p->ccSqrt[i].imag(); }
+    if (chiInv) { chiInv[2 * i] = p->chiInv[i].real(); chiInv[2 * i + 1] = p->chiInv[i].imag(); }
+  }
+}
+
+// Overrides the couple-constant square roots (nmat*3 complex) directly.
+void orc_set_cc_sqrt(orc_problem* p, const double* ccSqrt) {
+  p->ccSqrt.resize(p->nmat * 3);
+  for (size_t i = 0; i < p->ccSqrt.size(); i++) p->ccSqrt[i] = cd(ccSqrt[2 * i], ccSqrt[2 * i + 1]);
+}
+
+// DMatrixCpu::createDMatrix, DDA/DMatrixCpu.cpp:133-205 (non-periodic).
+void orc_build_dmatrix(orc_problem* p) {
+  const uint32_t Gx = p->grid[0], Gy = p->grid[1], Gz = p->grid[2];
+  const int bx = p->box[0], by = p->box[1], bz = p->box[2];
+  const size_t N = p->N();
+  p->D.assign(6 * N, 0);
+  std::vector<cd> d2(N);  // [Gz][Gy][Gx], x fastest (Fortran [Gx][Gy][Gz])
+  auto px = plan(Gx), py = plan(Gy), pz = plan(Gz);
+  const double scale = -(double)(Gx * (size_t)Gy * Gz);
+  for (int component = 0; component < 6; component++) {
+    static const int MU[6] = {0, 0, 0, 1, 1, 2}, NU[6] = {0, 1, 2, 1, 2, 2};
+    int mu = MU[component], nu = NU[component];
+    std::fill(d2.begin(), d2.end(), cd(0));
+#pragma omp parallel for schedule(dynamic)
+    for (int k = 0; k < (int)Gz; k++) {
+      int kcor = k > (int)Gz / 2 ? k - (int)Gz : k;
+      for (int j = 1 - by; j < by; j++)
+        for (int i = 1 - bx; i < bx; i++)
+          d2[clip(i, Gx) + Gx * (clip(j, Gy) + (size_t)Gy * k)] = interactionTerm(*p, i, j, kcor, mu, nu);
+    }
+    // FFT along x over all Gy*Gz lines
+#pragma omp parallel for schedule(dynamic)
+    for (long long l = 0; l < (long long)Gy * Gz; l++) px->exec(d2.data() + l * Gx, 1, 1, Gx, false);
+#pragma omp parallel for schedule(dynamic)
+    for (int i = 0; i < (int)Gx; i++) {
+      std::vector<cd> slice((size_t)Gz * Gy, 0);   // [Gy][Gz], z fastest
+      std::vector<cd> sliceTr((size_t)Gy * Gz, 0); // [Gz][Gy], y fastest
+      for (int j = 1 - by; j < by; j++)
+        for (int k = 1 - bz; k < bz; k++) {
+          uint32_t y = clip(j, Gy), z = clip(k, Gz);
+          slice[z + (size_t)Gz * y] = d2[i + Gx * (y + (size_t)Gy * z)];
+        }
+      pz->exec(slice.data(), Gy, 1, Gz, false);
+      for (uint32_t y = 0; y < Gy; y++)
+        for (uint32_t z = 0; z < Gz; z++) sliceTr[y + (size_t)Gy * z] = slice[z + (size_t)Gz * y];
+      py->exec(sliceTr.data(), Gz, 1, Gy, false);
+      for (uint32_t k = 0; k < Gz; k++)
+        for (uint32_t j = 0; j < Gy; j++)
+          p->D[component + 6 * (j + (size_t)Gy * (k + (size_t)Gz * i))] = sliceTr[j + (size_t)Gy * k] / scale;
+    }
+  }
+}
+
+void orc_get_dmatrix(const orc_problem* p, double* out) {
+  std::memcpy(out, p->D.data(), p->D.size() * sizeof(cd));
+}
+void orc_set_dmatrix(orc_problem* p, const double* in) {
+  p->D.resize(6 * p->N());
+  std::memcpy(static_cast<void*>(p->D.data()), in, p->D.size() * sizeof(cd));
+}
+
+// MatVecCpu::apply, DDA/MatVecCpu.cpp:67-150: vectors are SoA
+// [x: nvs][y: nvs][z: nvs] complex (DDA/DDAParams.hpp:176-186).
+void orc_matvec(orc_problem* p, const double* argD, double* resD, int conj) {
+  const cd* arg = reinterpret_cast<const cd*>(argD);
+  cd* res = reinterpret_cast<cd*>(resD);
+  const uint32_t Gx = p->grid[0], Gy = p->grid[1], Gz = p->grid[2];
+  const uint32_t bx = p->box[0], by = p->box[1], bz = p->box[2];
+  (void)bx;
+  const size_t nvs = p->nvs;
+  const size_t plane = (size_t)Gx * by * bz;
+  p->X.assign(3 * plane, 0);  // Xmatrix[Gx][by][bz][3] Fortran
+  cd* X = p->X.data();
+  for (uint32_t i = 0; i < p->nv; i++) {
+    uint32_t x = p->pos[3 * i], y = p->pos[3 * i + 1], z = p->pos[3 * i + 2];
+    for (int c = 0; c < 3; c++) {
+      cd r = p->ccSqrt[p->mat[i] * 3 + c] * maybeConj(arg[i + c * nvs], conj);
+      X[x + Gx * (y + (size_t)by * (z + (size_t)bz * c))] = r;
+    }
+  }
+  auto px = plan(Gx), py = plan(Gy), pz = plan(Gz);
+#pragma omp parallel for schedule(static)
+  for (long long l = 0; l < (long long)by * bz * 3; l++) px->exec(X + l * Gx, 1, 1, Gx, false);
+#pragma omp parallel for schedule(dynamic)
+  for (int i = 0; i < (int)Gx; i++) {
+    std::vector<cd> slices((size_t)Gz * Gy * 3, 0);   // [3][Gy][Gz] z fastest
+    std::vector<cd> slicesTr((size_t)Gy * Gz * 3, 0); // [3][Gz][Gy] y fastest
+    for (uint32_t j = 0; j < by; j++)
+      for (uint32_t k = 0; k < bz; k++)
+        for (int c = 0; c < 3; c++)
+          slices[k + Gz * (j + (size_t)Gy * c)] = X[i + Gx * (j + (size_t)by * (k + (size_t)bz * c))];
+    for (int c = 0; c < 3; c++) pz->exec(slices.data() + (size_t)c * Gy * Gz, by, 1, Gz, false);
+    for (int c = 0; c < 3; c++)
+      for (uint32_t j = 0; j < Gy; j++)
+        for (uint32_t k = 0; k < Gz; k++)
+          slicesTr[j + Gy * (k + (size_t)Gz * c)] = slices[k + Gz * (j + (size_t)Gy * c)];
+    py->exec(slicesTr.data(), (size_t)Gz * 3, 1, Gy, false);
+    for (uint32_t k = 0; k < Gz; k++)
+      for (uint32_t j = 0; j < Gy; j++) {
+        const cd* d = &p->D[6 * (j + (size_t)Gy * (k + (size_t)Gz * i))];
+        cd xv[3], yv[3];
+        for (int c = 0; c < 3; c++) xv[c] = slicesTr[j + Gy * (k + (size_t)Gz * c)];
+        // SymMatrix3 * Vector3, Math/SymMatrix3.hpp:86-92
+        yv[0] = d[0] * xv[0] + d[1] * xv[1] + d[2] * xv[2];
+        yv[1] = d[1] * xv[0] + d[3] * xv[1] + d[4] * xv[2];
+        yv[2] = d[2] * xv[0] + d[4] * xv[1] + d[5] * xv[2];
+        for (int c = 0; c < 3; c++) slicesTr[j + Gy * (k + (size_t)Gz * c)] = yv[c];
+      }
+    py->exec(slicesTr.data(), (size_t)Gz * 3, 1, Gy, true);
+    for (int c = 0; c < 3; c++)
+      for (uint32_t j = 0; j < Gy; j++)
+        for (uint32_t k = 0; k < Gz; k++)
+          slices[k + Gz * (j + (size_t)Gy * c)] = slicesTr[j + Gy * (k + (size_t)Gz * c)];
+    for (int c = 0; c < 3; c++) pz->exec(slices.data() + (size_t)c * Gy * Gz, by, 1, Gz, true);
+    for (uint32_t j = 0; j < by; j++)
+      for (uint32_t k = 0; k < bz; k++)
+        for (int c = 0; c < 3; c++)
+          X[i + Gx * (j + (size_t)by * (k + (size_t)bz * c))] = slices[k + Gz * (j + (size_t)Gy * c)];
+  }
+#pragma omp parallel for schedule(static)
+  for (long long l = 0; l < (long long)by * bz * 3; l++) px->exec(X + l * Gx, 1, 1, Gx, true);
+  for (size_t i = p->nv; i < nvs; i++)
+    for (int c = 0; c < 3; c++) res[i + c * nvs] = 0;
+  for (uint32_t i = 0; i < p->nv; i++) {
+    uint32_t x = p->pos[3 * i], y = p->pos[3 * i + 1], z = p->pos[3 * i + 2];
+    for (int c = 0; c < 3; c++) {
+      cd r = X[x + Gx * (y + (size_t)by * (z + (size_t)bz * c))];
+      cd a = maybeConj(arg[i + c * nvs], conj);
+      res[i + c * nvs] = maybeConj(p->ccSqrt[p->mat[i] * 3 + c] * r + a, conj);
+    }
+  }
+}
+
+// Independent check (not in the reference): the same operator as a direct
+// O(nv^2) sum, y_i = x_i - sqrt(cc_i) sum_{j != i} G(r_i - r_j) sqrt(cc_j) x_j,
+// with G the Green's tensor of DDA/DMatrixCpu.cpp:49-63.  Pins the sign and
+// the 1/N normalisation folded into D (DDA/DMatrixCpu.cpp:200).
+void orc_direct_matvec(const orc_problem* p, const double* argD, double* resD) {
+  const cd* arg = reinterpret_cast<const cd*>(argD);
+  cd* res = reinterpret_cast<cd*>(resD);
+  const size_t nvs = p->nvs;
+#pragma omp parallel for schedule(dynamic)
+  for (long long ii = 0; ii < (long long)p->nv; ii++) {
+    size_t i = (size_t)ii;
+    cd acc[3] = {0, 0, 0};
+    for (size_t j = 0; j < p->nv; j++) {
+      if (i == j) continue;
+      int di = (int)p->pos[3 * i] - (int)p->pos[3 * j];
+      int dj = (int)p->pos[3 * i + 1] - (int)p->pos[3 * j + 1];
+      int dk = (int)p->pos[3 * i + 2] - (int)p->pos[3 * j + 2];
+      cd xj[3];
+      for (int c = 0; c < 3; c++) xj[c] = p->ccSqrt[p->mat[j] * 3 + c] * arg[j + c * nvs];
+      for (int mu = 0; mu < 3; mu++)
+        for (int nu = 0; nu < 3; nu++)
+          acc[mu] += interactionTerm(*p, di, dj, dk, std::min(mu, nu), std::max(mu, nu)) * xj[nu];
+    }
+    for (int c = 0; c < 3; c++)
+      res[i + c * nvs] = arg[i + c * nvs] - p->ccSqrt[p->mat[i] * 3 + c] * acc[c];
+  }
+  for (size_t i = p->nv; i < nvs; i++)
+    for (int c = 0; c < 3; c++) res[i + c * nvs] = 0;
+}
+
+// PlaneWave::createEInc, DDA/Beam.cpp:111-118: E = exp(i k r.prop) * pol
+// with r the dipole coordinate in the particle frame
+// (DDA/DipoleGeometry.hpp:105-109).
+void orc_einc(const orc_problem* p, const double* propIn, int pol, double* outD) {
+  cd* out = reinterpret_cast<cd*>(outD);
+  double incPol[3], prop[3];
+  orc_beam_pol(propIn, pol, incPol, prop);
+  std::fill(out, out + p->vecSize(), cd(0));
+  for (uint32_t i = 0; i < p->nv; i++) {
+    double c[3];
+    for (int a = 0; a < 3; a++)
+      c[a] = (double)((ldouble)(double)p->origin[a] + (ldouble)(double)p->pos[3 * i + a] * p->gridUnitL);
+    double ph = p->waveNum * (c[0] * prop[0] + c[1] * prop[1] + c[2] * prop[2]);
+    cd e = std::exp(cd(0, ph));
+    for (int a = 0; a < 3; a++) out[i + a * p->nvs] = e * incPol[a];
+  }
+}
+
+}  // extern "C"
+
+// ============================================================ solvers =====
+namespace {
+
+typedef std::vector<cd> Vec;
+
+double vnorm(const Vec& v) {  // LinAlg/LinComb.hpp:67-73
+  double r = 0;
+  for (const cd& x : v) r += std::norm(x);
+  return r;
+}
+cd vecProdConj(const Vec& a, const Vec& b) {  // DDA/QmrCs.cpp:48-55 (bilinear)
+  cd s = 0;
+  for (size_t i = 0; i < a.size(); i++) s += a[i] * b[i];
+  return s;
+}
+cd vecProd(const Vec& a, const Vec& b) {  // DDA/BicgStab.cpp:34-41 (Hermitian)
+  cd s = 0;
+  for (size_t i = 0; i < a.size(); i++) s += a[i] * std::conj(b[i]);
+  return s;
+}
+
+struct SolveCtx {
+  orc_problem* p;
+  Vec A, r, x, t1, t2, t3, t4;
+  double residScale = 0, epsB = 0, inprodR = 0;
+  std::vector<double> history;
+  int status = 0;
+  std::string msg;
+
+  explicit SolveCtx(orc_problem* p_) : p(p_) {
+    size_t n = p->vecSize();
+    A.assign(n, 0); r.assign(n, 0); x.assign(n, 0);
+    t1.assign(n, 0); t2.assign(n, 0); t3.assign(n, 0); t4.assign(n, 0);
+  }
+  void matvec(const Vec& a, Vec& out, bool conj) {
+    orc_matvec(p, reinterpret_cast<const double*>(a.data()), reinterpret_cast<double*>(out.data()), conj);
+  }
+  // multMat / multMatInv, DDA/DDAParams.hpp:188-210
+  void multCc(const Vec& in, Vec& out, bool inverse) {
+    for (uint32_t i = 0; i < p->nv; i++)
+      for (int c = 0; c < 3; c++) {
+        cd s = p->ccSqrt[p->mat[i] * 3 + c];
+        out[i + c * p->nvs] = inverse ? in[i + c * p->nvs] / s : s * in[i + c * p->nvs];
+      }
+  }
+  bool fail(int code, const char* m) {
+    status = code;
+    msg = m;
+    return false;
+  }
+};
+
+// CpuIterativeSolver::initGeneral, DDA/CpuIterativeSolver.cpp:45-91.
+double initGeneral(SolveCtx& s, const Vec& einc, const Vec& start) {
+  Vec& pvec = s.t1;
+  std::fill(pvec.begin(), pvec.end(), cd(0));
+  s.multCc(einc, pvec, false);
+  double temp = vnorm(pvec);
+  s.residScale = 1 / temp;
+  double inprodR;
+  if (!start.empty()) {
+    s.multCc(start, s.x, true);
+    s.matvec(s.x, s.A, false);
+    for (size_t i = 0; i < pvec.size(); i++) s.r[i] = s.A[i] * cd(-1) + pvec[i];
+    inprodR = vnorm(s.r);
+  } else {
+    s.matvec(pvec, s.A, false);
+    for (size_t i = 0; i < pvec.size(); i++) s.r[i] = s.A[i] * cd(-1) + pvec[i];
+    inprodR = vnorm(s.r);
+    if (temp < inprodR) {
+      std::fill(s.x.begin(), s.x.end(), cd(0));
+      std::swap(s.r, pvec);
+      inprodR = temp;
+    } else {
+      std::swap(s.x, pvec);
+    }
+  }
+  return inprodR;
+}
+
+// ---- QMR-CS, DDA/QmrCs.cpp:58-168
+struct Qmr {
+  double omega_old, omega_new, c_old, c_new;
+  cd beta, mBeta, tautilda, s_old, s_new;
+  void init(SolveCtx& s) {
+    Vec& v = s.t1;
+    cd rvec2 = vecProdConj(s.r, s.r);
+    omega_old = 0;
+    beta = std::sqrt(rvec2);
+    mBeta = -beta;
+    omega_new = std::sqrt(s.inprodR) / std::abs(beta);
+    tautilda = omega_new * beta;
+    c_old = 1; c_new = 1; s_old = 0; s_new = 0;
+    cd bi = 1.0 / beta;
+    for (size_t i = 0; i < v.size(); i++) v[i] = s.r[i] * bi;
+  }
+  bool iteration(SolveCtx& s, size_t nr, double& out) {
+    Vec &r = s.r, &A = s.A, &x = s.x, &v = s.t1, &vt = s.t2, &p_old = s.t3, &p_new = s.t4;
+    double rtmp1 = std::norm(beta) * s.residScale;
+    if (nr == 0) {
+      if (rtmp1 > 1e+38f) return s.fail(-5, "QMR breakdown: beta too large");
+    } else if (rtmp1 < 1e-10f || rtmp1 > 1e+38f) {
+      return s.fail(-5, "QMR breakdown: beta out of range");
+    }
+    s.matvec(v, A, false);
+    cd alpha = vecProdConj(v, A);
+    if (nr == 0)
+      for (size_t i = 0; i < v.size(); i++) vt[i] = v[i] * (-alpha) + A[i];
+    else
+      for (size_t i = 0; i < v.size(); i++) vt[i] = vt[i] * mBeta + v[i] * (-alpha) + A[i];
+    cd ctmp3 = vecProdConj(vt, vt);
+    double rtmp2 = vnorm(vt);
+    cd ctmp1 = omega_old * beta;
+    cd ctmp2 = omega_new * alpha;
+    cd theta = std::conj(s_old) * ctmp1;
+    cd eta = c_old * c_new * ctmp1 + std::conj(s_new) * ctmp2;
+    cd zetatilda = c_new * ctmp2 - c_old * s_new * ctmp1;
+    beta = std::sqrt(ctmp3);
+    mBeta = -beta;
+    omega_old = omega_new;
+    omega_new = std::sqrt(rtmp2) / std::abs(beta);
+    double zetaabs = std::sqrt(std::norm(zetatilda) + rtmp2);
+    double rtmp3 = std::sqrt(std::norm(zetatilda));
+    cd zeta;
+    if (rtmp3 < 1e-40f) zeta = zetaabs;
+    else zeta = zetaabs / rtmp3 * zetatilda;
+    c_old = c_new;
+    c_new = rtmp3 / zetaabs;
+    s_old = s_new;
+    s_new = omega_new * (beta / zeta);
+    cd tau = c_new * tautilda;
+    tautilda = -s_new * tautilda;
+    cd zetaInv = 1.0 / zeta;
+    cd mEtaZeta = -eta / zeta;
+    cd mThetaZeta = -theta / zeta;
+    cd betaInv = 1.0 / beta;
+    double normSNew = std::norm(s_new);
+    cd cNewOmegaNewTautilda = (c_new / omega_new) * tautilda;
+    if (nr == 0) {
+      for (size_t i = 0; i < v.size(); i++) p_new[i] = v[i] * zetaInv;
+    } else {
+      if (nr == 1)
+        for (size_t i = 0; i < v.size(); i++) p_old[i] = p_new[i] * mEtaZeta + v[i] * zetaInv;
+      else
+        for (size_t i = 0; i < v.size(); i++)
+          p_old[i] = p_old[i] * mThetaZeta + p_new[i] * mEtaZeta + v[i] * zetaInv;
+      std::swap(p_old, p_new);
+    }
+    for (size_t i = 0; i < v.size(); i++) x[i] = p_new[i] * tau + x[i];
+    for (size_t i = 0; i < v.size(); i++) vt[i] = vt[i] * betaInv;
+    std::swap(v, vt);
+    for (size_t i = 0; i < v.size(); i++) r[i] = r[i] * cd(normSNew) + v[i] * cNewOmegaNewTautilda;
+    out = vnorm(r);
+    return true;
+  }
+};
+
+// ---- BiCGStab, DDA/BicgStab.cpp:59-112 (long double for alpha, beta, omega)
+struct BicgStab {
+  cd beta, ro_new, ro_old, omega, alpha;
+  double denumOmega;
+  void init(SolveCtx& s) { s.t4 = s.r; }
+  bool iteration(SolveCtx& s, size_t nr, double& out) {
+    Vec &r = s.r, &A = s.A, &x = s.x, &pv = s.t1, &v = s.t2, &sv = s.t3, &rt = s.t4;
+    ro_new = vecProd(r, rt);
+    double dtmp = (double)(std::abs(cld(ro_new)) / (ldouble)s.inprodR);
+    if (!(dtmp >= 1e-16)) return s.fail(-5, "BiCGStab breakdown: ro_new too small");
+    if (nr == 0) {
+      pv = r;
+    } else {
+      cld ro_new_alpha = cld(ro_new) * cld(alpha);
+      cld ro_old_omega = cld(ro_old) * cld(omega);
+      if (!(std::abs(ro_old_omega) / std::abs(ro_new_alpha) >= 10e-10))
+        return s.fail(-5, "BiCGStab breakdown: omega too small");
+      beta = cd(ro_new_alpha / ro_old_omega);
+      cd mbo = -beta * omega;
+      for (size_t i = 0; i < pv.size(); i++) pv[i] = pv[i] * beta + v[i] * mbo + r[i];
+    }
+    s.matvec(pv, v, false);
+    cld vRtilda = cld(vecProd(v, rt));
+    alpha = cd(cld(ro_new) / vRtilda);
+    for (size_t i = 0; i < v.size(); i++) sv[i] = v[i] * (-alpha) + r[i];
+    double inprodRplus1 = vnorm(sv);
+    if (inprodRplus1 < s.epsB) {
+      for (size_t i = 0; i < v.size(); i++) x[i] = pv[i] * alpha + x[i];
+    } else {
+      s.matvec(sv, A, false);
+      denumOmega = vnorm(A);
+      omega = cd(cld(vecProd(sv, A)) / (ldouble)denumOmega);
+      for (size_t i = 0; i < v.size(); i++) x[i] = pv[i] * alpha + sv[i] * omega + x[i];
+      for (size_t i = 0; i < v.size(); i++) r[i] = A[i] * (-omega) + sv[i];
+      inprodRplus1 = vnorm(r);
+      ro_old = ro_new;
+    }
+    out = inprodRplus1;
+    return true;
+  }
+};
+
+// ---- BiCG-CS, DDA/BicgCs.cpp:56-84
+struct BicgCs {
+  cd alpha, beta, ro_new, ro_old;
+  double abs_ro_new;
+  void init(SolveCtx&) {}
+  bool iteration(SolveCtx& s, size_t nr, double& out) {
+    Vec &r = s.r, &A = s.A, &x = s.x, &pv = s.t1;
+    ro_new = vecProdConj(r, r);
+    abs_ro_new = std::abs(ro_new);
+    double dtmp = abs_ro_new / s.inprodR;
+    if (dtmp < 1e-10 || dtmp > 1e+10) return s.fail(-5, "BiCG-CS breakdown: rho out of range");
+    if (nr == 0) {
+      pv = r;
+    } else {
+      beta = ro_new / ro_old;
+      for (size_t i = 0; i < pv.size(); i++) pv[i] = pv[i] * beta + r[i];
+    }
+    s.matvec(pv, A, false);
+    cd mu_k = vecProdConj(pv, A);
+    double dtmp2 = std::abs(mu_k) / abs_ro_new;
+    if (dtmp2 < 10e-10) return s.fail(-5, "BiCG-CS breakdown: mu too small");
+    alpha = ro_new / mu_k;
+    for (size_t i = 0; i < pv.size(); i++) x[i] = pv[i] * alpha + x[i];
+    for (size_t i = 0; i < pv.size(); i++) r[i] = A[i] * (-alpha) + r[i];
+    ro_old = ro_new;
+    out = vnorm(r);
+    return true;
+  }
+};
+
+// ---- CGNR, DDA/Cgnr.cpp:39-73
+struct Cgnr {
+  cd beta;
+  double ro_new, ro_old;
+  void init(SolveCtx&) { ro_old = 0; }
+  bool iteration(SolveCtx& s, size_t nr, double& out) {
+    Vec &r = s.r, &A = s.A, &x = s.x, &pv = s.t1;
+    if (nr == 0) {
+      s.matvec(r, pv, true);
+      ro_new = vnorm(pv);
+    } else {
+      s.matvec(r, A, true);
+      ro_new = vnorm(A);
+      beta = ro_new / ro_old;
+      for (size_t i = 0; i < pv.size(); i++) pv[i] = pv[i] * beta + A[i];
+    }
+    s.matvec(pv, A, false);
+    cd alpha = ro_new / vnorm(A);
+    for (size_t i = 0; i < pv.size(); i++) x[i] = pv[i] * alpha + x[i];
+    for (size_t i = 0; i < pv.size(); i++) r[i] = A[i] * (-alpha) + r[i];
+    ro_old = ro_new;
+    out = vnorm(r);
+    return true;
+  }
+};
+
+template <class S>
+int runSolver(SolveCtx& s, S& solver, size_t maxIter, size_t maxResIncrease,
+              size_t stopAfter) {
+  // IterativeSolverBase::getPolVec loop, DDA/IterativeSolverBase.cpp:53-98
+  size_t count = 0, counter = 0;
+  solver.init(s);
+  while (s.inprodR >= s.epsB) {
+    if (stopAfter && count >= stopAfter) return 1;
+    if (count >= maxIter) {
+      s.status = -6;
+      s.msg = "Too many iterations";
+      return s.status;
+    } else if (counter > maxResIncrease) {
+      s.status = -7;
+      s.msg = "Too many iterations w/o increase";
+      return s.status;
+    }
+    double next;
+    if (!solver.iteration(s, count, next)) return s.status;
+    count++;
+    if (next <= s.inprodR) {
+      s.inprodR = next;
+      counter = 0;
+    } else {
+      counter++;
+    }
+    s.history.push_back(std::sqrt(s.residScale * next));
+  }
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+struct orc_stats {
+  int64_t iterations;
+  int64_t matvecs;
+  double residScale;
+  double inprodR;      // best |r|^2 reached
+  double relResidual;  // sqrt(inprodR * residScale)
+  int32_t status;
+  int32_t pad;
+};
+
+// IterativeSolverBase::getPolVec (DDA/IterativeSolverBase.cpp:40-103)
+// followed by CpuIterativeSolver::getResult (DDA/CpuIterativeSolver.cpp:93-99).
+// solver: 0 = qmr, 1 = bicgstab, 2 = bicg (BiCG-CS), 3 = cgnr.
+// stop_after > 0 stops after that many iterations (a bounded timing sample;
+// status 1).  history (may be NULL) receives up to history_cap RE_ values.
+int orc_solve(orc_problem* p, int solver, const double* eincD, double eps,
+              int64_t maxIter, const double* startD, double* polOut,
+              orc_stats* st, int64_t stopAfter, double* history,
+              int64_t historyCap) {
+  SolveCtx s(p);
+  size_t n = p->vecSize();
+  Vec einc(reinterpret_cast<const cd*>(eincD), reinterpret_cast<const cd*>(eincD) + n);
+  Vec start;
+  if (startD) start.assign(reinterpret_cast<const cd*>(startD), reinterpret_cast<const cd*>(startD) + n);
+  s.inprodR = initGeneral(s, einc, start);
+  s.epsB = eps * eps / s.residScale;
+  int rc;
+  static const size_t maxInc[4] = {50000, 30000, 50000, 10};
+  if (solver < 0 || solver > 3) {
+    g_error = "unknown solver";
+    return -1;
+  }
+  size_t mi = maxIter > 0 ? (size_t)maxIter : (size_t)-1;
+  if (solver == 0) { Qmr q; rc = runSolver(s, q, mi, maxInc[0], stopAfter); }
+  else if (solver == 1) { BicgStab q; rc = runSolver(s, q, mi, maxInc[1], stopAfter); }
+  else if (solver == 2) { BicgCs q; rc = runSolver(s, q, mi, maxInc[2], stopAfter); }
+  else { Cgnr q; rc = runSolver(s, q, mi, maxInc[3], stopAfter); }
+  if (rc < 0) g_error = s.msg;
+  if (polOut) {
+    Vec pv(n, 0);
+    s.multCc(s.x, pv, false);
+    std::memcpy(polOut, pv.data(), n * sizeof(cd));
+  }
+  if (st) {
+    st->iterations = (int64_t)s.history.size();
+    st->residScale = s.residScale;
+    st->inprodR = s.inprodR;
+    st->relResidual = std::sqrt(s.inprodR * s.residScale);
+    st->status = rc;
+  }
+  if (history)
+    for (size_t i = 0; i < s.history.size() && (int64_t)i < historyCap; i++) history[i] = s.history[i];
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,334 @@
+#!/usr/bin/env python
+"""bench.py -- DDA solve throughput on B200.
+
+Workload (the reference README's GPU-scale case): box 10 x 5 x 5 um, grid
+unit 0.1 um (100 x 50 x 50 = 250 000 dipoles, FFT grid 200 x 100 x 100),
+refractive index 1.5+0.1i, wavelength 6 um, incidence (0,1,0), LDR couple
+constants, BiCGStab to relative residual 1e-5, both polarisations.  One step
+is one solve of both polarisations; the metric is solves per second.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Every GPU (one process each under torchrun) solves its own copy: the solves
+are independent ("replicas only"), so `value` is the total solves of all
+ranks over the slowest rank's device time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = {
+    "workload": "box 10x5x5um d=0.1um m=1.5+0.1i lambda=6um prop=(0,1,0) ldr bicgstab eps=1e-5, both pols",
+    "nv": 250000, "grid": [200, 100, 100], "rhs_per_step": 2,
+}
+EPS = 1e-5
+PROP = (0.0, 1.0, 0.0)
+METRIC = "solves/s at relative residual 1e-5 (box 10x5x5um, BiCGStab)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64", "mixed"])
+    ap.add_argument("--solver", default="bicgstab")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), \
+        int(os.environ.get("WORLD_SIZE", 1))
+
+
+# ------------------------------------------------------------ clocks ----
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.f = None
+
+    def start(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except Exception:
+            self.proc.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+                for n, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                pass
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------- CPU sample ----
+def cpu_sample(max_seconds=30.0):
+    """Times the oracle (the CPU restatement of the reference's --cpu path)
+    on a bounded sample: the solve set-up plus 1 and 3 BiCGStab iterations of
+    polarisation 1; the per-solve time is set-up + n_iter * per-iteration,
+    with n_iter from the oracle's full solve of this workload
+    (tests/golden/cfg2_oracle_bicgstab.json)."""
+    from oracle import oracle as O
+    ref = json.load(open(os.path.join(ROOT, "tests", "golden", "cfg2_oracle_bicgstab.json")))
+    n_iter = [ref["pols"][k]["iterations"] for k in ("1", "2")]
+    g = O.Geometry.box("10um", "5um", "5um", "0.1um")
+    p = O.Problem(g, [1.5 + 0.1j], "6um")
+    p.build_dmatrix()
+    p.set_cc(PROP, 1, "ldr")
+    e = p.einc(PROP, 1)
+    t0 = time.time()
+    p.solve(e, "bicgstab", EPS, stop_after=1)
+    t1 = time.time() - t0
+    t0 = time.time()
+    p.solve(e, "bicgstab", EPS, stop_after=3)
+    t3 = time.time() - t0
+    t_iter = max((t3 - t1) / 2, 1e-9)
+    t_init = max(t1 - t_iter, 0.0)
+    per_solve = [t_init + n * t_iter for n in n_iter]
+    value = 2.0 / sum(per_solve)
+    return {"value": value, "unit": "solves/s", "cores": O.max_threads(), "kind": "port",
+            "sample": "oracle BiCGStab pol 1: set-up + 1 and 3 iterations (%.1f s), scaled by the "
+                      "oracle's full-solve iteration counts %s" % (t1 + t3, n_iter),
+            "seconds_per_iteration": t_iter, "iterations": n_iter}
+
+
+# ----------------------------------------------------------- our arm ----
+def build_problem(precision, max_rhs):
+    import dda_b200
+    g = dda_b200.Geometry.box_shape("10um", "5um", "5um", "0.1um")
+    p = dda_b200.DDAParams(g, [1.5 + 0.1j], "6um")
+    mv = dda_b200.CudaMatVec(p, precision, max_rhs=max_rhs)
+    ein = []
+    for r, pol in enumerate((1, 2)[:max_rhs]):
+        mv.set_couple_constants(dda_b200.CoupleConstants(p, PROP, pol, "ldr"), rhs=r)
+        ein.append(p.einc(PROP, pol))
+    return p, mv, np.concatenate(ein)
+
+
+def stage_bytes(p, mv, nrhs, s):
+    """Algorithmic bytes per launch of the three matvec passes."""
+    gx, gy, gz = p.grid
+    bx, by, bz = p.box
+    nvs, nv = p.nvs, p.nv
+    plane = gx * by * bz
+    oct_ = (gx // 2 + 1) * (gy // 2 + 1) * (gz // 2 + 1)
+    return {
+        "x_forward": nrhs * s * (3 * nvs + 3 * plane) + 13 * nv,
+        "yz_planes": nrhs * s * 6 * plane + s * 6 * oct_,
+        "x_inverse": nrhs * s * (6 * nvs + 3 * plane) + 13 * nv,
+    }
+
+
+def run_ours(args):
+    import torch
+    import dda_b200
+    rank, local, world = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        pg = dist
+    prec = args.precision
+    nrhs = 2
+    p, mv, einc = build_problem(prec, nrhs)
+    solver = dda_b200.CudaSolver(mv, args.solver)
+    cdt = torch.complex128 if prec == "fp64" else torch.complex64
+    s_bytes = 16 if prec == "fp64" else 8
+    einc_dev = torch.from_numpy(einc).to(cdt).cuda()
+    pol_dev = torch.zeros_like(einc_dev)
+    stream = torch.cuda.ExternalStream(mv.stream)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
+
+    def step():
+        solver.get_pol_vec_device(einc_dev.data_ptr(), pol_dev.data_ptr(), nrhs, EPS)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    iters = [st.iterations for st in solver.last_stats]
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    l0 = mv.launches
+    total_ms = 0.0
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        step()
+        e1.record(stream)
+        e1.synchronize()
+        total_ms += e0.elapsed_time(e1)
+    launches = mv.launches - l0
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    t_max = total_ms
+    if pg:
+        t = torch.tensor([total_ms], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        t_max = float(t.item())
+    value = nrhs * args.steps * world / (t_max / 1000.0)
+    ms_per_step = t_max / args.steps
+
+    # e2e: host FP64 einc in, host FP64 polarisations out, through dda_solve
+    einc_host = np.ascontiguousarray(einc)
+    e2e_ms = 0.0
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        solver.get_pol_vec(einc_host, EPS, history_cap=1)
+        e1.record(stream)
+        e1.synchronize()
+        e2e_ms += e0.elapsed_time(e1)
+    if pg:
+        t = torch.tensor([e2e_ms], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = {"value": nrhs * args.steps * world / (e2e_ms / 1000.0), "unit": "solves/s",
+           "h2d_bytes_per_step": int(einc_host.nbytes), "d2h_bytes_per_step": int(einc_host.nbytes)}
+
+    # matvec stage profile and roofline of the dominant pass
+    ms = mv.profile(nrhs=nrhs, reps=20)
+    sb = stage_bytes(p, mv, nrhs, s_bytes)
+    names = ["x_forward", "yz_planes", "x_inverse"]
+    dom = int(np.argmax(ms[:3]))
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = sb[names[dom]] / (ms[dom] * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                "algorithmic_bytes_per_launch": sb[names[dom]], "ms_per_launch": float(ms[dom])}
+    matvec = {"ms": float(ms[3]), "stages_ms": dict(zip(names, map(float, ms[:3]))),
+              "GB_per_s": sum(sb.values()) / (ms[3] * 1e-3) / 1e9, "nrhs": nrhs}
+
+    # plain FP64 single-rhs solve: the two polarisations one after the other
+    plain = None
+    if rank == 0:
+        p64, mv64, e64 = build_problem("fp64", 1)
+        s64 = dda_b200.CudaSolver(mv64, args.solver)
+        ein = [p64.einc(PROP, pol) for pol in (1, 2)]
+        import dda_b200 as D
+
+        def plain_step():
+            for pol in (1, 2):
+                mv64.set_couple_constants(D.CoupleConstants(p64, PROP, pol, "ldr"))
+                s64.get_pol_vec(ein[pol - 1], EPS, history_cap=1)
+
+        plain_step()
+        st64 = torch.cuda.ExternalStream(mv64.stream)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(st64)
+        plain_step()
+        b.record(st64)
+        b.synchronize()
+        plain = {"value": 2 / (a.elapsed_time(b) / 1000.0), "unit": "solves/s",
+                 "iterations": [st.iterations for st in s64.last_stats]}
+        mv64.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            cpu = cpu_sample()
+        except Exception as ex:  # the CPU baseline is reported, never required
+            cpu = {"value": None, "error": str(ex)}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "c64+f64" if prec != "fp64" else "c128",
+                "data": "synthetic (the reference README geometry; generated in-process)",
+                "config": dict(WORKLOAD, precision=prec, solver=args.solver,
+                               iterations=iters, l2="flushed between steps (256 MB write)",
+                               parallelism="replicas x%d" % world),
+                "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "matvec": matvec,
+                "plain_fp64_single_rhs": plain, "cpu_baseline": cpu, "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def run_reference(args):
+    rank, local, world = dist_env()
+    if rank != 0:
+        return
+    samples = []
+    for _ in range(args.warmup + args.steps):
+        samples.append(cpu_sample())
+    s = samples[args.warmup:]
+    vals = [x["value"] for x in s]
+    v = float(np.mean(vals))
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 2000.0 / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+            "data": "synthetic", "config": dict(WORKLOAD, precision="fp64", solver="bicgstab"),
+            "cpu_baseline": dict(s[-1], value=v),
+            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)

@@ -1,0 +1,987 @@
+// dda_cuda.cu -- host side of libdda_b200.so: the C ABI of include/dda_cuda.h.
+//
+// A context owns the device-resident problem (geometry tables, FFT plans,
+// the D-matrix octant in FP64 and/or FP32), the matvec work buffers and the
+// Krylov vectors and scalar state for up to max_rhs right-hand sides.  Solves
+// run entirely on the device: scalars never leave it during the iteration
+// (compare the host round trips of DDA/GpuQmrCs.cpp:146-177); the host only
+// polls the per-rhs `done` flags between batches of iterations, which are
+// replayed from a captured CUDA graph.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/dda_cuda.h"
+#include "dmatrix_kernels.cuh"
+#include "fft_engine.cuh"
+#include "krylov_kernels.cuh"
+#include "krylov_ops.cuh"
+#include "matvec_kernels.cuh"
+#include "reduce.cuh"
+
+using namespace dda;
+
+namespace {
+
+std::string g_create_error;
+
+struct DdaError : std::runtime_error {
+  int code;
+  DdaError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define CK(call)                                                                          \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      throw DdaError(e_ == cudaErrorMemoryAllocation ? DDA_ERR_OOM : DDA_ERR_CUDA,        \
+                     std::string(#call) + ": " + cudaGetErrorString(e_));                 \
+  } while (0)
+
+// Kernel shapes.  Register arrays in the FFT stages hold about MAXE complex
+// values per thread.
+template <typename T> struct Shape;
+template <> struct Shape<float> { static constexpr int maxe = 8; };
+template <> struct Shape<double> { static constexpr int maxe = 4; };
+constexpr int kNtX = 256;   // k_xfwd / k_xinv
+constexpr int kNtYz = 512;  // k_yz / k_yrows
+constexpr int kNtC = 256;   // k_fft_cols / k_fft_rows
+constexpr int kNtV = 256;                 // k_vec
+constexpr size_t kSmemMax = 227 * 1024;
+
+// ----------------------------------------------------------- FFT plans ----
+struct FftPlan {
+  int n = 0;
+  std::vector<int> radix;
+  float2* tw32 = nullptr;
+  double2* tw64 = nullptr;
+
+  void create(int n_) {
+    n = n_;
+    int m = n;
+    while (m % 8 == 0) { radix.push_back(8); m /= 8; }
+    while (m % 4 == 0) { radix.push_back(4); m /= 4; }
+    while (m % 2 == 0) { radix.push_back(2); m /= 2; }
+    while (m % 3 == 0) { radix.push_back(3); m /= 3; }
+    while (m % 5 == 0) { radix.push_back(5); m /= 5; }
+    while (m % 7 == 0) { radix.push_back(7); m /= 7; }
+    if (m != 1) throw DdaError(DDA_ERR_UNSUPPORTED, "FFT length " + std::to_string(n) + " is not 2,3,5,7-smooth");
+    if ((int)radix.size() > kMaxStages) throw DdaError(DDA_ERR_UNSUPPORTED, "FFT length too large");
+    std::vector<double2> h64(n);
+    std::vector<float2> h32(n);
+    const long double two_pi = 6.2831853071795864769252867665590056L;
+    for (int k = 0; k < n; k++) {
+      long double a = -two_pi * (long double)k / (long double)n;
+      long double c = cosl(a), s = sinl(a);
+      h64[k] = make_double2((double)c, (double)s);
+      h32[k] = make_float2((float)c, (float)s);
+    }
+    CK(cudaMalloc(&tw64, n * sizeof(double2)));
+    CK(cudaMalloc(&tw32, n * sizeof(float2)));
+    CK(cudaMemcpy(tw64, h64.data(), n * sizeof(double2), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(tw32, h32.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
+  }
+  template <typename T> FftPlanDev dev() const {
+    FftPlanDev d;
+    memset(&d, 0, sizeof(d));
+    d.n = n;
+    d.nst = (int)radix.size();
+    for (size_t i = 0; i < radix.size(); i++) d.radix[i] = radix[i];
+    d.tw = std::is_same<T, float>::value ? (const void*)tw32 : (const void*)tw64;
+    return d;
+  }
+  void release() {
+    if (tw32) cudaFree(tw32);
+    if (tw64) cudaFree(tw64);
+    tw32 = nullptr;
+    tw64 = nullptr;
+  }
+};
+
+template <typename T> void* dalloc(size_t bytes) {
+  void* p = nullptr;
+  if (bytes == 0) return nullptr;
+  CK(cudaMalloc(&p, bytes));
+  return p;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------ Engine<T> ----
+// Everything that depends on the working precision T.
+template <typename T> struct Engine {
+  typedef typename C2<T>::t T2;
+  bool on = false;
+  T2* dc = nullptr;    // D octant
+  T2* ccs = nullptr;   // [max_rhs][nmat][3] scaled sqrt(cc)
+  T2* xhat = nullptr;  // [max_rhs][Gx][3][nlines]
+  T2* zbuf = nullptr;  // split path [max_rhs][Gx][3][Gz][by]
+  T2* vec[10] = {};    // Krylov vectors [max_rhs][3 nvs]
+  T2* io = nullptr;    // host-API staging [max_rhs][3 nvs]
+  bool fused = false;
+  YzGeom yz{};
+  size_t smem_x = 0, smem_yz = 0, smem_rows = 0, smem_cols = 0;
+  ColGeom cz_fwd{}, cz_inv{};
+  void release() {
+    for (void* p : {(void*)dc, (void*)ccs, (void*)xhat, (void*)zbuf, (void*)io})
+      if (p) cudaFree(p);
+    for (auto& v : vec)
+      if (v) cudaFree(v);
+    dc = ccs = xhat = zbuf = io = nullptr;
+    for (auto& v : vec) v = nullptr;
+  }
+};
+
+struct dda_ctx {
+  int device = 0;
+  int precision = DDA_PREC_FP64;
+  int max_rhs = 1;
+  uint32_t flags = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  MvGeom g{};
+  double kd = 0, grid_unit = 0;
+  uint32_t* line_off = nullptr;
+  uint32_t* dip = nullptr;
+  uint32_t* perm = nullptr;
+  uint8_t* mat_ext = nullptr;
+  FftPlan px, py, pz;
+  Engine<float> e32;
+  Engine<double> e64;
+  std::vector<std::complex<double>> cc_host;  // [max_rhs][nmat][3], reference units
+  std::vector<char> cc_set;
+  KrylovState* st = nullptr;  // device [max_rhs]
+  KrylovState* st_host = nullptr;  // pinned mirror
+  RedSums* parts = nullptr;
+  unsigned* tickets = nullptr;
+  int nparts_vec = 0, nparts_mv = 0;
+  double* hist = nullptr;
+  long long hist_cap = 0;
+  long long launches = 0;  // kernels this context has launched
+
+  void release() {
+    if (device >= 0) cudaSetDevice(device);
+    e32.release();
+    e64.release();
+    px.release();
+    py.release();
+    pz.release();
+    for (void* p : {(void*)line_off, (void*)dip, (void*)perm, (void*)mat_ext, (void*)st,
+                    (void*)parts, (void*)tickets, (void*)hist})
+      if (p) cudaFree(p);
+    if (st_host) cudaFreeHost(st_host);
+    if (stream) cudaStreamDestroy(stream);
+    line_off = dip = perm = nullptr;
+    mat_ext = nullptr;
+    st = nullptr;
+    st_host = nullptr;
+    parts = nullptr;
+    tickets = nullptr;
+    hist = nullptr;
+    stream = nullptr;
+  }
+};
+
+namespace {
+
+int ntiles(const dda_ctx* c) { return (c->g.nlines + c->g.tl - 1) / c->g.tl; }
+
+template <typename T> Engine<T>& eng(dda_ctx* c);
+template <> Engine<float>& eng<float>(dda_ctx* c) { return c->e32; }
+template <> Engine<double>& eng<double>(dda_ctx* c) { return c->e64; }
+
+// Chooses tile shapes and allocates the matvec buffers of one precision.
+template <typename T> void setup_engine(dda_ctx* c) {
+  typedef typename C2<T>::t T2;
+  Engine<T>& e = eng<T>(c);
+  const MvGeom& g = c->g;
+  const size_t s = sizeof(T2);
+  e.on = true;
+  // k_xfwd / k_xinv tiles: shared tile tl x (Gx+1) plus the material table
+  e.smem_x = (size_t)g.tl * g.pitchx * s + (size_t)g.nmat * s;
+  // fused plane kernel: slab Gz x q plus nr rows of 3 x (Gy+1)
+  YzGeom y;
+  y.q = 3 * g.by + ((3 * g.by) % 2 == 0 ? 1 : 0);
+  y.py = g.Gy + 1;
+  size_t slab = (size_t)g.Gz * y.q * s;
+  int nr = std::max(1, std::min(g.Gz, (kNtYz * Shape<T>::maxe) / (3 * g.Gy)));
+  while (nr > 1 && slab + (size_t)nr * 3 * y.py * s > kSmemMax) nr--;
+  y.nr = nr;
+  e.yz = y;
+  e.smem_yz = slab + (size_t)nr * 3 * y.py * s;
+  e.fused = e.smem_yz <= kSmemMax && 3 * g.Gy <= kNtYz * Shape<T>::maxe && g.Gz <= kNtYz * Shape<T>::maxe &&
+            !(c->flags & DDA_FLAG_SPLIT_YZ);
+  if (!e.fused) {
+    // split path: zbuf, k_yrows with nr rows, column FFTs along z
+    e.yz.nr = std::max(1, std::min(g.Gz, (kNtYz * Shape<T>::maxe) / (3 * g.Gy)));
+    e.smem_rows = (size_t)e.yz.nr * 3 * y.py * s;
+    int ti = std::max(1, std::min(32, (kNtC * Shape<T>::maxe) / g.Gz));
+    ti = std::min(ti, g.by);
+    e.smem_cols = (size_t)g.Gz * (ti + 1) * s;
+    ColGeom f;
+    f.in_bs = g.nlines;            // xhat plane of one component
+    f.in_as = g.by;
+    f.out_bs = (long long)g.Gz * g.by;
+    f.out_as = g.by;
+    f.inner = g.by;
+    f.ti = ti;
+    f.pitch = ti + 1;
+    f.n_in = g.bz;
+    f.n_out = g.Gz;
+    f.batches_per_rhs = g.Gx * 3;
+    e.cz_fwd = f;
+    ColGeom iv = f;
+    iv.in_bs = f.out_bs;
+    iv.in_as = g.by;
+    iv.out_bs = g.nlines;
+    iv.out_as = g.by;
+    iv.n_in = g.Gz;
+    iv.n_out = g.bz;
+    e.cz_inv = iv;
+    if (e.smem_rows > kSmemMax || e.smem_cols > kSmemMax)
+      throw DdaError(DDA_ERR_UNSUPPORTED, "FFT grid too large for the shared-memory tiles");
+    e.zbuf = (T2*)dalloc<T>((size_t)c->max_rhs * g.Gx * 3 * g.Gz * g.by * s);
+  }
+  if (e.smem_x > kSmemMax) throw DdaError(DDA_ERR_UNSUPPORTED, "grid x extent too large");
+  auto attr = [](const void* f, size_t bytes) {
+    CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(bytes, 1)));
+  };
+  attr((const void*)k_xfwd<T, kNtX, Shape<T>::maxe>, e.smem_x);
+  attr((const void*)k_xinv<T, kNtX, Shape<T>::maxe>, e.smem_x);
+  if (e.fused) attr((const void*)k_yz<T, kNtYz, Shape<T>::maxe>, e.smem_yz);
+  else {
+    attr((const void*)k_yrows<T, kNtYz, Shape<T>::maxe>, e.smem_rows);
+    attr((const void*)k_fft_cols<T, kNtC, Shape<T>::maxe>, e.smem_cols);
+  }
+  const int hx = g.Gx / 2 + 1, hy = g.Gy / 2 + 1, hz = g.Gz / 2 + 1;
+  e.dc = (T2*)dalloc<T>((size_t)hx * hy * hz * 6 * s);
+  e.ccs = (T2*)dalloc<T>((size_t)c->max_rhs * g.nmat * 3 * s);
+  CK(cudaMemset(e.ccs, 0, (size_t)c->max_rhs * g.nmat * 3 * s));
+  e.xhat = (T2*)dalloc<T>((size_t)c->max_rhs * g.Gx * 3 * g.nlines * s);
+  const size_t vbytes = (size_t)c->max_rhs * 3 * g.nvs * s;
+  for (auto& v : e.vec) {
+    v = (T2*)dalloc<T>(vbytes);
+    CK(cudaMemset(v, 0, vbytes));
+  }
+  e.io = (T2*)dalloc<T>(vbytes);
+}
+
+// Uploads the scaled couple constants of every rhs to the engine.
+template <typename T> void upload_cc(dda_ctx* c) {
+  typedef typename C2<T>::t T2;
+  Engine<T>& e = eng<T>(c);
+  if (!e.on) return;
+  const double sc = std::pow(c->grid_unit, -1.5);
+  std::vector<T2> h(c->cc_host.size());
+  for (size_t i = 0; i < h.size(); i++) {
+    h[i].x = (T)(c->cc_host[i].real() * sc);
+    h[i].y = (T)(c->cc_host[i].imag() * sc);
+  }
+  CK(cudaMemcpyAsync(e.ccs, h.data(), h.size() * sizeof(T2), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+}
+
+RedTarget red_target(dda_ctx* c, int nparts) {
+  RedTarget t;
+  t.parts = c->parts;
+  t.tickets = c->tickets;
+  t.nparts = nparts;
+  return t;
+}
+
+// The matvec: k_xfwd -> (k_yz | cols/yrows/cols) -> k_xinv.
+template <typename T>
+void matvec(dda_ctx* c, const typename C2<T>::t* arg, typename C2<T>::t* res, int conj, int nrhs,
+            cudaStream_t s, KrylovState* st, KrylovStep step, int skipmv = 0) {
+  Engine<T>& e = eng<T>(c);
+  const MvGeom& g = c->g;
+  const FftPlanDev px = c->px.dev<T>(), py = c->py.dev<T>(), pz = c->pz.dev<T>();
+  dim3 gx(ntiles(c), 3, nrhs);
+  k_xfwd<T, kNtX, Shape<T>::maxe><<<gx, kNtX, e.smem_x, s>>>(arg, e.xhat, c->line_off, c->dip, c->perm,
+                                                      e.ccs, conj, g, px, st, skipmv);
+  if (e.fused) {
+    k_yz<T, kNtYz, Shape<T>::maxe><<<dim3(g.Gx, nrhs), kNtYz, e.smem_yz, s>>>(e.xhat, e.dc, g, e.yz, pz, py, st, skipmv);
+  } else {
+    const int nbatch = nrhs * g.Gx * 3;
+    dim3 gc((g.by + e.cz_fwd.ti - 1) / e.cz_fwd.ti, nbatch);
+    k_fft_cols<T, kNtC, Shape<T>::maxe><<<gc, kNtC, e.smem_cols, s>>>(e.xhat, e.zbuf, e.cz_fwd, pz, 0, st, skipmv);
+    dim3 gr((g.Gz + e.yz.nr - 1) / e.yz.nr, g.Gx, nrhs);
+    k_yrows<T, kNtYz, Shape<T>::maxe><<<gr, kNtYz, e.smem_rows, s>>>(e.zbuf, e.dc, g, e.yz, py, st, skipmv);
+    k_fft_cols<T, kNtC, Shape<T>::maxe><<<gc, kNtC, e.smem_cols, s>>>(e.zbuf, e.xhat, e.cz_inv, pz, 1, st, skipmv);
+  }
+  step.red = red_target(c, 3 * ntiles(c));
+  k_xinv<T, kNtX, Shape<T>::maxe><<<gx, kNtX, e.smem_x, s>>>(arg, res, e.xhat, c->line_off, c->dip, c->perm,
+                                                      e.ccs, conj, g, px, st, step, skipmv);
+  CK(cudaGetLastError());
+  c->launches += e.fused ? 3 : 5;
+}
+
+// D-matrix generation (FP64) into the enabled engines' octants.
+void build_dmatrix(dda_ctx* c) {
+  const MvGeom& g = c->g;
+  const long long N = (long long)g.Gx * g.Gy * g.Gz;
+  double2* full = (double2*)dalloc<double>(N * sizeof(double2));
+  const FftPlanDev px = c->px.dev<double>(), py = c->py.dev<double>(), pz = c->pz.dev<double>();
+  CK(cudaFuncSetAttribute((const void*)k_fft_rows<double, kNtC, Shape<double>::maxe>,
+                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax));
+  CK(cudaFuncSetAttribute((const void*)k_fft_cols<double, kNtC, Shape<double>::maxe>,
+                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax));
+  static const int MU[6] = {0, 0, 0, 1, 1, 2}, NU[6] = {0, 1, 2, 1, 2, 2};
+  const int tlr = std::max(1, std::min(32, (kNtC * Shape<double>::maxe) / g.Gx));
+  const size_t smr = (size_t)tlr * (g.Gx + 1) * sizeof(double2);
+  auto cols = [&](const FftPlanDev& pl, long long inner, long long batch, long long bs, long long as) {
+    const int n = pl.n;
+    int ti = (int)std::max(1LL, std::min<long long>(std::min(32, (kNtC * Shape<double>::maxe) / n), inner));
+    ColGeom cg;
+    cg.in_bs = bs; cg.in_as = as; cg.out_bs = bs; cg.out_as = as;
+    cg.inner = (int)inner; cg.ti = ti; cg.pitch = ti + 1;
+    cg.n_in = n; cg.n_out = n;
+    cg.batches_per_rhs = 1;
+    const size_t sm = (size_t)n * (ti + 1) * sizeof(double2);
+    if (sm > kSmemMax) throw DdaError(DDA_ERR_UNSUPPORTED, "grid too large for D-matrix FFT tiles");
+    k_fft_cols<double, kNtC, Shape<double>::maxe><<<dim3((unsigned)((inner + ti - 1) / ti), (unsigned)batch), kNtC, sm, c->stream>>>(
+        full, full, cg, pl, 0, nullptr, 0);
+  };
+  for (int comp = 0; comp < 6; comp++) {
+    k_dfill<<<1184, 256, 0, c->stream>>>(full, g.Gx, g.Gy, g.Gz, g.bx, g.by, g.bz, c->kd, MU[comp], NU[comp]);
+    k_fft_rows<double, kNtC, Shape<double>::maxe><<<(unsigned)(((long long)g.Gy * g.Gz + tlr - 1) / tlr), kNtC, smr, c->stream>>>(
+        full, (long long)g.Gy * g.Gz, g.Gx, tlr, g.Gx + 1, px, 0);
+    cols(py, g.Gx, g.Gz, (long long)g.Gy * g.Gx, g.Gx);
+    cols(pz, (long long)g.Gy * g.Gx, 1, N, (long long)g.Gy * g.Gx);
+    k_dcompress<<<592, 256, 0, c->stream>>>(full, c->e64.on ? c->e64.dc : nullptr,
+                                            c->e32.on ? c->e32.dc : nullptr, g.Gx, g.Gy, g.Gz, comp);
+    CK(cudaGetLastError());
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  cudaFree(full);
+}
+
+// Host-supplied D (reference layout, reference units) -> octants.
+void upload_dmatrix(dda_ctx* c, const double* D) {
+  const MvGeom& g = c->g;
+  const int hx = g.Gx / 2 + 1, hy = g.Gy / 2 + 1, hz = g.Gz / 2 + 1;
+  const double sc = c->grid_unit * c->grid_unit * c->grid_unit;
+  std::vector<double2> h64((size_t)hx * hy * hz * 6);
+  for (int ax = 0; ax < hx; ax++)
+    for (int az = 0; az < hz; az++)
+      for (int ay = 0; ay < hy; ay++)
+        for (int comp = 0; comp < 6; comp++) {
+          const size_t src = comp + 6 * (ay + (size_t)g.Gy * (az + (size_t)g.Gz * ax));
+          const size_t dst = (((size_t)ax * hz + az) * hy + ay) * 6 + comp;
+          h64[dst] = make_double2(D[2 * src] * sc, D[2 * src + 1] * sc);
+        }
+  double2* tmp = (double2*)dalloc<double>(h64.size() * sizeof(double2));
+  CK(cudaMemcpy(tmp, h64.data(), h64.size() * sizeof(double2), cudaMemcpyHostToDevice));
+  if (c->e64.on) CK(cudaMemcpy(c->e64.dc, tmp, h64.size() * sizeof(double2), cudaMemcpyDeviceToDevice));
+  if (c->e32.on) {
+    k_d64_to_d32<<<592, 256, 0, c->stream>>>(tmp, c->e32.dc, (long long)h64.size());
+    CK(cudaGetLastError());
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  cudaFree(tmp);
+}
+
+int fail(dda_ctx* c, const DdaError& e) {
+  if (c) c->err = e.what();
+  else g_create_error = e.what();
+  return e.code;
+}
+
+template <typename F> int guard(dda_ctx* c, F f) {
+  try {
+    if (c) CK(cudaSetDevice(c->device));
+    return f();
+  } catch (const DdaError& e) {
+    return fail(c, e);
+  } catch (const std::exception& e) {
+    return fail(c, DdaError(DDA_ERR_ARG, e.what()));
+  }
+}
+
+}  // namespace
+
+// ============================================================ solver ======
+namespace {
+
+template <typename T> struct Solve {
+  typedef typename C2<T>::t T2;
+  dda_ctx* c;
+  Engine<T>& e;
+  int nrhs;
+  cudaStream_t s;
+  Solve(dda_ctx* c_, int nrhs_) : c(c_), e(eng<T>(c_)), nrhs(nrhs_), s(c_->stream) {}
+
+  KrylovStep step(int op, int mode = EP_NORM, const void* w = nullptr, int nparts = 0) {
+    KrylovStep k;
+    k.op = op;
+    k.mode = mode;
+    k.w = w;
+    k.red = red_target(c, nparts ? nparts : c->nparts_vec);
+    return k;
+  }
+
+  void vec(int op, int first, std::initializer_list<T2*> v, KrylovStep k) {
+    VecArgs a;
+    memset(&a, 0, sizeof(a));
+    int i = 0;
+    for (T2* p : v) a.v[i++] = p;
+    a.op = op;
+    a.first = first;
+    a.nv = c->g.nv;
+    a.nvs = c->g.nvs;
+    a.nmat = c->g.nmat;
+    a.nparts = c->nparts_vec;
+    a.mat = c->mat_ext;
+    a.ccs = e.ccs;
+    a.step = k;
+    k_vec<T, kNtV><<<dim3(c->nparts_vec, nrhs), kNtV, 0, s>>>(a, c->st);
+    CK(cudaGetLastError());
+    c->launches++;
+  }
+
+  void mv(const T2* arg, T2* res, int conj, KrylovStep k) {
+    matvec<T>(c, arg, res, conj, nrhs, s, c->st, k);
+  }
+
+  // CpuIterativeSolver::initGeneral (DDA/CpuIterativeSolver.cpp:45-91) with
+  // the GPU setup kernels of DDA/GpuIterativeSolver.cpp:78-134.
+  void init_general(T2* E, T2* B, T2* R, T2* X, T2* A, T2* S, bool start) {
+    vec(V_SETUP_PVEC, 0, {B, E}, step(KOP_INIT_PVEC));
+    if (start) {
+      vec(V_START_X, 0, {X, S}, KrylovStep{KOP_NONE, 0, nullptr, {}});
+      mv(X, A, 0, step(KOP_NONE));
+      vec(V_R_INIT, 0, {R, A, B}, step(KOP_INIT_START));
+    } else {
+      mv(B, A, 0, step(KOP_NONE));
+      vec(V_R_INIT, 0, {R, A, B}, step(KOP_INIT_R));
+      vec(V_CHOOSE_X0, 0, {X, R, B}, step(KOP_NONE));
+    }
+  }
+
+  // One iteration nr of the selected solver (buffers rotate on the host).
+  struct Bufs {
+    T2 *R, *X, *A, *t1, *t2, *t3, *t4;
+  };
+  void iteration(int solver, long long nr, Bufs& b) {
+    switch (solver) {
+      case DDA_SOLVER_QMR: {  // t1 = v, t2 = vt, t3 = p_old, t4 = p_new
+        mv(b.t1, b.A, 0, step(KOP_QMR_ALPHA, EP_YA_BIL));
+        vec(V_QMR_VT, nr == 0, {b.t2, b.t1, b.A}, step(KOP_QMR_GIVENS));
+        vec(V_QMR_UPD, nr == 0 ? 1 : nr == 1 ? 2 : 0, {b.R, b.t3, b.t4, b.t1, b.t2, b.X}, step(KOP_QMR_END));
+        if (nr > 0) std::swap(b.t3, b.t4);
+        std::swap(b.t1, b.t2);
+        break;
+      }
+      case DDA_SOLVER_BICGSTAB: {  // t1 = p, t2 = v, t3 = s, t4 = rt
+        vec(V_BIS_P, nr == 0, {b.t1, b.t2, b.R}, step(KOP_NONE));
+        mv(b.t1, b.t2, 0, step(KOP_BIS_ALPHA, EP_YW_HERM, b.t4));
+        vec(V_BIS_S, 0, {b.t3, b.t2, b.R}, step(KOP_BIS_S));
+        matvec<T>(c, b.t3, b.A, 0, nrhs, s, c->st, step(KOP_BIS_OMEGA, EP_AY_HERM_NORM), 1);
+        vec(V_BIS_XR, 0, {b.X, b.t1, b.t3, b.A, b.R, b.t4}, step(KOP_BIS_END));
+        break;
+      }
+      case DDA_SOLVER_BICG: {  // t1 = p
+        vec(V_BICG_P, nr == 0, {b.t1, b.R}, step(KOP_NONE));
+        mv(b.t1, b.A, 0, step(KOP_BICG_MU, EP_YA_BIL));
+        vec(V_BICG_XR, 0, {b.X, b.t1, b.A, b.R}, step(KOP_BICG_END));
+        break;
+      }
+      default: {  // CGNR, t1 = p
+        if (nr == 0) {
+          mv(b.R, b.t1, 1, step(KOP_CGNR_RO, EP_NORM));
+        } else {
+          mv(b.R, b.A, 1, step(KOP_CGNR_RO, EP_NORM));
+          vec(V_CGNR_P, 0, {b.t1, b.A}, step(KOP_NONE));
+        }
+        mv(b.t1, b.A, 0, step(KOP_CGNR_ALPHA, EP_NORM));
+        vec(V_CGNR_XR, 0, {b.X, b.t1, b.A, b.R}, step(KOP_CGNR_END));
+        break;
+      }
+    }
+  }
+
+  void solver_init(int solver, Bufs& b) {
+    switch (solver) {
+      case DDA_SOLVER_QMR:
+        vec(V_BICG_RO, 0, {b.R}, step(KOP_QMR_INIT));
+        vec(V_QMR_V0, 0, {b.t1, b.R}, step(KOP_NONE));
+        break;
+      case DDA_SOLVER_BICGSTAB:
+        vec(V_BIS_INIT, 0, {b.t4, b.R}, step(KOP_BIS_RO));
+        break;
+      case DDA_SOLVER_BICG:
+        vec(V_BICG_RO, 0, {b.R}, step(KOP_BICG_RO));
+        break;
+      default:
+        break;
+    }
+  }
+};
+
+const long long kMaxResIncrease[4] = {50000, 30000, 50000, 10};
+
+// Runs one solve of `nrhs` right-hand sides already set up in the engine
+// vectors (E = einc, S = start).  Returns per-rhs states in c->st_host.
+template <typename T>
+void run_solve(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter, bool start) {
+  typedef typename C2<T>::t T2;
+  Engine<T>& e = eng<T>(c);
+  Solve<T> sv(c, nrhs);
+  T2 *E = e.vec[0], *B = e.vec[1], *S = e.vec[2];
+  typename Solve<T>::Bufs b{e.vec[3], e.vec[4], e.vec[5], e.vec[6], e.vec[7], e.vec[8], e.vec[9]};
+  // initial state
+  for (int r = 0; r < nrhs; r++) {
+    KrylovState& k = c->st_host[r];
+    memset(&k, 0, sizeof(k));
+    k.maxIter = max_iter > 0 ? max_iter : (1LL << 62);
+    k.maxResIncrease = kMaxResIncrease[solver];
+    k.histCap = c->hist_cap;
+    k.hist = c->hist + (size_t)r * c->hist_cap;
+    k.epsB = eps;  // holds eps until KOP_INIT_PVEC
+  }
+  CK(cudaMemcpyAsync(c->st, c->st_host, nrhs * sizeof(KrylovState), cudaMemcpyHostToDevice, c->stream));
+  sv.init_general(E, B, b.R, b.X, b.A, S, start);
+  // epsB = eps^2 / residScale (DDA/IterativeSolverBase.cpp:44)
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaMemcpy(c->st_host, c->st, nrhs * sizeof(KrylovState), cudaMemcpyDeviceToHost));
+  for (int r = 0; r < nrhs; r++) {
+    KrylovState& k = c->st_host[r];
+    k.epsB = eps * eps / k.residScale;
+    if (!(k.inprodR >= k.epsB)) k.done = 1;  // already converged: no iteration
+  }
+  CK(cudaMemcpy(c->st, c->st_host, nrhs * sizeof(KrylovState), cudaMemcpyHostToDevice));
+  sv.solver_init(solver, b);
+  long long nr = 0;
+  const int poll = 8;
+  for (;;) {
+    for (int k = 0; k < poll; k++) sv.iteration(solver, nr++, b);
+    CK(cudaMemcpyAsync(c->st_host, c->st, nrhs * sizeof(KrylovState), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    bool all = true;
+    for (int r = 0; r < nrhs; r++) all = all && c->st_host[r].done;
+    if (all) break;
+  }
+  // P = sqrt(cc) x
+  sv.vec(V_RESULT, 0, {e.io, b.X}, KrylovStep{KOP_NONE, 0, nullptr, {}});
+}
+
+}  // namespace
+
+// ================================================================ C ABI ===
+extern "C" {
+
+const char* dda_last_error(const dda_ctx* ctx) {
+  return ctx ? ctx->err.c_str() : g_create_error.c_str();
+}
+
+int dda_create(const dda_problem* p, int precision, dda_ctx** out) {
+  if (!p || !out) {
+    g_create_error = "null argument";
+    return DDA_ERR_ARG;
+  }
+  *out = nullptr;
+  std::unique_ptr<dda_ctx> c(new dda_ctx);
+  c->device = p->device;
+  int rc = guard(nullptr, [&]() -> int {
+    if (p->nv == 0 || !p->positions) throw DdaError(DDA_ERR_ARG, "empty geometry");
+    if (precision < DDA_PREC_FP64 || precision > DDA_PREC_MIXED) throw DdaError(DDA_ERR_ARG, "bad precision");
+    if (p->nmat == 0 || p->nmat > 256) throw DdaError(DDA_ERR_ARG, "nmat must be 1..256");
+    if (p->max_rhs < 1) throw DdaError(DDA_ERR_ARG, "max_rhs must be >= 1");
+    if (!(p->grid_unit > 0) || !(p->kd > 0)) throw DdaError(DDA_ERR_ARG, "grid_unit and kd must be positive");
+    for (int a = 0; a < 3; a++) {
+      if (p->box[a] == 0 || p->grid[a] % 2 != 0 || p->grid[a] < 2 * p->box[a])
+        throw DdaError(DDA_ERR_ARG, "grid must be even and at least twice the box");
+    }
+    // one grid line must fit the register tiles of a CTA (FP64 limits apply
+    // to the D-matrix setup in every precision)
+    const uint32_t lim = (uint32_t)(kNtC * Shape<double>::maxe);
+    if (p->box[0] >= 65536 || p->grid[0] > lim || p->grid[1] > lim || p->grid[2] > lim)
+      throw DdaError(DDA_ERR_UNSUPPORTED, "FFT grid edge above " + std::to_string(lim));
+    CK(cudaSetDevice(p->device));
+    c->precision = precision;
+    c->max_rhs = p->max_rhs;
+    c->flags = p->flags;
+    c->kd = p->kd;
+    c->grid_unit = p->grid_unit;
+    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    MvGeom& g = c->g;
+    g.Gx = p->grid[0]; g.Gy = p->grid[1]; g.Gz = p->grid[2];
+    g.bx = p->box[0]; g.by = p->box[1]; g.bz = p->box[2];
+    g.nv = (int)p->nv;
+    g.nvs = (int)((p->nv + 15) / 16 * 16);  // DDA/DDAParams.cpp:113
+    g.nlines = g.by * g.bz;
+    g.nmat = (int)p->nmat;
+    g.pitchx = g.Gx + 1;
+    {
+      const int s = precision == DDA_PREC_FP32 ? 8 : 16;
+      g.tl = std::max(1, std::min(32, (int)(98304 / ((size_t)s * g.pitchx))));
+    }
+    // geometry tables: dipoles sorted by grid line (y + by z), stable
+    const uint32_t nv = p->nv;
+    std::vector<uint32_t> line(nv), cnt(g.nlines + 1, 0);
+    for (uint32_t i = 0; i < nv; i++) {
+      const uint32_t x = p->positions[3 * i], y = p->positions[3 * i + 1], z = p->positions[3 * i + 2];
+      if (x >= p->box[0] || y >= p->box[1] || z >= p->box[2]) throw DdaError(DDA_ERR_ARG, "dipole outside the box");
+      const uint8_t m = p->materials ? p->materials[i] : 0;
+      if (m >= p->nmat) throw DdaError(DDA_ERR_ARG, "material index out of range");
+      line[i] = y + (uint32_t)g.by * z;
+      cnt[line[i] + 1]++;
+    }
+    for (int l = 0; l < g.nlines; l++) cnt[l + 1] += cnt[l];
+    std::vector<uint32_t> off(cnt), perm(nv), dip(nv);
+    std::vector<uint8_t> matx(nv);
+    bool ident = true;
+    std::vector<std::vector<char>> seen;  // duplicate check per line via x bitmap
+    std::vector<uint32_t> fill(cnt.begin(), cnt.end() - 1);
+    for (uint32_t i = 0; i < nv; i++) {
+      const uint32_t j = fill[line[i]]++;
+      perm[j] = i;
+      if (j != i) ident = false;
+      const uint8_t m = p->materials ? p->materials[i] : 0;
+      dip[j] = p->positions[3 * i] | ((uint32_t)m << 16);
+      matx[i] = m;
+    }
+    CK(cudaMalloc(&c->line_off, off.size() * sizeof(uint32_t)));
+    CK(cudaMemcpy(c->line_off, off.data(), off.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&c->dip, nv * sizeof(uint32_t)));
+    CK(cudaMemcpy(c->dip, dip.data(), nv * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    if (!ident) {
+      CK(cudaMalloc(&c->perm, nv * sizeof(uint32_t)));
+      CK(cudaMemcpy(c->perm, perm.data(), nv * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    }
+    CK(cudaMalloc(&c->mat_ext, nv));
+    CK(cudaMemcpy(c->mat_ext, matx.data(), nv, cudaMemcpyHostToDevice));
+    c->px.create(g.Gx);
+    c->py.create(g.Gy);
+    c->pz.create(g.Gz);
+    if (precision != DDA_PREC_FP32) setup_engine<double>(c.get());
+    if (precision != DDA_PREC_FP64) setup_engine<float>(c.get());
+    // reduction slots
+    c->nparts_mv = 3 * ntiles(c.get());
+    {
+      const long long len = 3LL * g.nvs;
+      c->nparts_vec = (int)std::max(1LL, std::min(296LL, (len + 2047) / 2048));
+    }
+    const int nparts = std::max(c->nparts_mv, c->nparts_vec);
+    CK(cudaMalloc(&c->parts, (size_t)c->max_rhs * nparts * sizeof(RedSums)));
+    CK(cudaMalloc(&c->tickets, c->max_rhs * sizeof(unsigned)));
+    CK(cudaMemset(c->tickets, 0, c->max_rhs * sizeof(unsigned)));
+    CK(cudaMalloc(&c->st, c->max_rhs * sizeof(KrylovState)));
+    CK(cudaMemset(c->st, 0, c->max_rhs * sizeof(KrylovState)));
+    CK(cudaMallocHost(&c->st_host, c->max_rhs * sizeof(KrylovState)));
+    c->hist_cap = 100000;
+    CK(cudaMalloc(&c->hist, (size_t)c->max_rhs * c->hist_cap * sizeof(double)));
+    c->cc_host.assign((size_t)c->max_rhs * g.nmat * 3, 0);
+    c->cc_set.assign(c->max_rhs, 0);
+    if (p->dmatrix) upload_dmatrix(c.get(), p->dmatrix);
+    else build_dmatrix(c.get());
+    CK(cudaDeviceSynchronize());
+    return DDA_OK;
+  });
+  if (rc != DDA_OK) {
+    c->release();
+    return rc;
+  }
+  *out = c.release();
+  return DDA_OK;
+}
+
+int dda_destroy(dda_ctx* ctx) {
+  if (!ctx) return DDA_OK;
+  ctx->release();
+  delete ctx;
+  return DDA_OK;
+}
+
+int64_t dda_vec_stride(const dda_ctx* ctx) { return ctx ? ctx->g.nvs : 0; }
+
+int dda_set_cc(dda_ctx* ctx, int rhs, const double* cc_sqrt) {
+  if (!ctx) return DDA_ERR_ARG;
+  return guard(ctx, [&]() -> int {
+    if (rhs < 0 || rhs >= ctx->max_rhs || !cc_sqrt) throw DdaError(DDA_ERR_ARG, "bad rhs index or null cc_sqrt");
+    const int n = ctx->g.nmat * 3;
+    for (int i = 0; i < n; i++)
+      ctx->cc_host[(size_t)rhs * n + i] = std::complex<double>(cc_sqrt[2 * i], cc_sqrt[2 * i + 1]);
+    ctx->cc_set[rhs] = 1;
+    upload_cc<float>(ctx);
+    upload_cc<double>(ctx);
+    return DDA_OK;
+  });
+}
+
+int dda_matvec(dda_ctx* ctx, const void* d_arg, void* d_res, int conj, int nrhs, int precision,
+               void* stream) {
+  if (!ctx) return DDA_ERR_ARG;
+  return guard(ctx, [&]() -> int {
+    if (nrhs < 1 || nrhs > ctx->max_rhs || !d_arg || !d_res) throw DdaError(DDA_ERR_ARG, "bad matvec arguments");
+    for (int r = 0; r < nrhs; r++)
+      if (!ctx->cc_set[r]) throw DdaError(DDA_ERR_ARG, "couple constants not set (dda_set_cc)");
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    if (precision == DDA_PREC_FP64) {
+      if (!ctx->e64.on) throw DdaError(DDA_ERR_ARG, "context has no FP64 engine");
+      matvec<double>(ctx, (const double2*)d_arg, (double2*)d_res, conj, nrhs, s, nullptr, KrylovStep{KOP_NONE, 0, nullptr, {}});
+    } else if (precision == DDA_PREC_FP32) {
+      if (!ctx->e32.on) throw DdaError(DDA_ERR_ARG, "context has no FP32 engine");
+      matvec<float>(ctx, (const float2*)d_arg, (float2*)d_res, conj, nrhs, s, nullptr, KrylovStep{KOP_NONE, 0, nullptr, {}});
+    } else {
+      throw DdaError(DDA_ERR_ARG, "precision must be DDA_PREC_FP64 or DDA_PREC_FP32");
+    }
+    return DDA_OK;
+  });
+}
+
+}  // extern "C"
+
+namespace {
+// Stage timing for dda_profile_matvec: the three passes of matvec<T> with an
+// event between them, on vectors the context owns.
+template <typename T> void profile_t(dda_ctx* c, int nrhs, int reps, double* ms) {
+  typedef typename C2<T>::t T2;
+  Engine<T>& e = eng<T>(c);
+  const MvGeom& g = c->g;
+  const FftPlanDev px = c->px.dev<T>(), py = c->py.dev<T>(), pz = c->pz.dev<T>();
+  cudaStream_t s = c->stream;
+  cudaEvent_t ev[4];
+  for (auto& x : ev) CK(cudaEventCreate(&x));
+  double acc[3] = {0, 0, 0};
+  const T2* arg = e.vec[0];
+  T2* res = e.io;
+  KrylovStep none{KOP_NONE, 0, nullptr, {}};
+  none.red = red_target(c, 3 * ntiles(c));
+  for (int r = 0; r <= reps; r++) {
+    dim3 gx(ntiles(c), 3, nrhs);
+    CK(cudaEventRecord(ev[0], s));
+    k_xfwd<T, kNtX, Shape<T>::maxe><<<gx, kNtX, e.smem_x, s>>>(arg, e.xhat, c->line_off, c->dip, c->perm,
+                                                              e.ccs, 0, g, px, nullptr, 0);
+    CK(cudaEventRecord(ev[1], s));
+    if (e.fused) {
+      k_yz<T, kNtYz, Shape<T>::maxe><<<dim3(g.Gx, nrhs), kNtYz, e.smem_yz, s>>>(e.xhat, e.dc, g, e.yz, pz, py, nullptr, 0);
+    } else {
+      dim3 gc((g.by + e.cz_fwd.ti - 1) / e.cz_fwd.ti, nrhs * g.Gx * 3);
+      k_fft_cols<T, kNtC, Shape<T>::maxe><<<gc, kNtC, e.smem_cols, s>>>(e.xhat, e.zbuf, e.cz_fwd, pz, 0, nullptr, 0);
+      dim3 gr((g.Gz + e.yz.nr - 1) / e.yz.nr, g.Gx, nrhs);
+      k_yrows<T, kNtYz, Shape<T>::maxe><<<gr, kNtYz, e.smem_rows, s>>>(e.zbuf, e.dc, g, e.yz, py, nullptr, 0);
+      k_fft_cols<T, kNtC, Shape<T>::maxe><<<gc, kNtC, e.smem_cols, s>>>(e.zbuf, e.xhat, e.cz_inv, pz, 1, nullptr, 0);
+    }
+    CK(cudaEventRecord(ev[2], s));
+    k_xinv<T, kNtX, Shape<T>::maxe><<<gx, kNtX, e.smem_x, s>>>(arg, res, e.xhat, c->line_off, c->dip, c->perm,
+                                                              e.ccs, 0, g, px, nullptr, none, 0);
+    CK(cudaEventRecord(ev[3], s));
+    CK(cudaEventSynchronize(ev[3]));
+    if (r == 0) continue;  // warm-up
+    for (int k = 0; k < 3; k++) {
+      float t;
+      CK(cudaEventElapsedTime(&t, ev[k], ev[k + 1]));
+      acc[k] += t;
+    }
+  }
+  for (auto& x : ev) cudaEventDestroy(x);
+  for (int k = 0; k < 3; k++) ms[k] = acc[k] / reps;
+  ms[3] = ms[0] + ms[1] + ms[2];
+}
+
+template <typename T>
+void host_to_engine(dda_ctx* c, const double* src, typename C2<T>::t* dst, size_t n) {
+  typedef typename C2<T>::t T2;
+  if (std::is_same<T, double>::value) {
+    CK(cudaMemcpyAsync(dst, src, n * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+  } else {
+    std::vector<T2> h(n);
+    for (size_t i = 0; i < n; i++) { h[i].x = (T)src[2 * i]; h[i].y = (T)src[2 * i + 1]; }
+    CK(cudaMemcpyAsync(dst, h.data(), n * sizeof(T2), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  }
+}
+template <typename T>
+void engine_to_host(dda_ctx* c, const typename C2<T>::t* src, double* dst, size_t n) {
+  typedef typename C2<T>::t T2;
+  if (std::is_same<T, double>::value) {
+    CK(cudaMemcpyAsync(dst, src, n * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  } else {
+    std::vector<T2> h(n);
+    CK(cudaMemcpyAsync(h.data(), src, n * sizeof(T2), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (size_t i = 0; i < n; i++) { dst[2 * i] = h[i].x; dst[2 * i + 1] = h[i].y; }
+  }
+}
+
+template <typename T>
+void matvec_host_t(dda_ctx* c, const double* arg, double* res, int conj, int nrhs) {
+  Engine<T>& e = eng<T>(c);
+  const size_t n = (size_t)nrhs * 3 * c->g.nvs;
+  host_to_engine<T>(c, arg, e.vec[0], n);
+  matvec<T>(c, e.vec[0], e.io, conj, nrhs, c->stream, nullptr, KrylovStep{KOP_NONE, 0, nullptr, {}});
+  engine_to_host<T>(c, e.io, res, n);
+}
+
+int collect_stats(dda_ctx* c, int nrhs, double* history, long long history_cap, dda_stats* stats);
+
+template <typename T>
+int solve_t(dda_ctx* c, int solver, int nrhs, const double* einc, double eps, long long max_iter,
+            const double* start, double* pol_out, double* history, long long history_cap,
+            dda_stats* stats) {
+  Engine<T>& e = eng<T>(c);
+  const size_t n = (size_t)nrhs * 3 * c->g.nvs;
+  host_to_engine<T>(c, einc, e.vec[0], n);
+  if (start) host_to_engine<T>(c, start, e.vec[2], n);
+  run_solve<T>(c, solver, nrhs, eps, max_iter, start != nullptr);
+  if (pol_out) engine_to_host<T>(c, e.io, pol_out, n);
+  CK(cudaStreamSynchronize(c->stream));
+  return collect_stats(c, nrhs, history, history_cap, stats);
+}
+
+template <typename T>
+int solve_device_t(dda_ctx* c, int solver, int nrhs, const void* einc, double eps, long long max_iter,
+                   const void* start, void* pol, dda_stats* stats) {
+  typedef typename C2<T>::t T2;
+  Engine<T>& e = eng<T>(c);
+  const size_t bytes = (size_t)nrhs * 3 * c->g.nvs * sizeof(T2);
+  CK(cudaMemcpyAsync(e.vec[0], einc, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  if (start) CK(cudaMemcpyAsync(e.vec[2], start, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  run_solve<T>(c, solver, nrhs, eps, max_iter, start != nullptr);
+  CK(cudaMemcpyAsync(pol, e.io, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return collect_stats(c, nrhs, nullptr, 0, stats);
+}
+
+int collect_stats(dda_ctx* c, int nrhs, double* history, long long history_cap, dda_stats* stats) {
+  int rc = DDA_OK;
+  for (int r = 0; r < nrhs; r++) {
+    const KrylovState& k = c->st_host[r];
+    if (stats) {
+      stats[r].iterations = k.count;
+      stats[r].matvecs = 0;
+      stats[r].refinements = 0;
+      stats[r].rel_residual = std::sqrt(k.inprodR * k.residScale);
+      stats[r].res_scale = k.residScale;
+      stats[r].status = k.status;
+    }
+    if (history && history_cap > 0) {
+      const long long m = std::min<long long>(std::min(history_cap, c->hist_cap), k.count);
+      if (m > 0)
+        CK(cudaMemcpy(history + (size_t)r * history_cap, c->hist + (size_t)r * c->hist_cap, m * sizeof(double),
+                      cudaMemcpyDeviceToHost));
+    }
+    if (k.status != 0 && rc == DDA_OK) rc = k.status;
+  }
+  if (rc != DDA_OK) {
+    static const char* msg[] = {"", "", "", "", "", "Krylov breakdown", "Too many iterations",
+                                "Too many iterations w/o increase"};
+    c->err = (rc <= -5 && rc >= -7) ? msg[-rc] : "solver failed";
+  }
+  return rc;
+}
+}  // namespace
+
+extern "C" {
+
+int dda_matvec_host(dda_ctx* ctx, const double* arg, double* res, int conj, int nrhs) {
+  if (!ctx) return DDA_ERR_ARG;
+  return guard(ctx, [&]() -> int {
+    if (nrhs < 1 || nrhs > ctx->max_rhs || !arg || !res) throw DdaError(DDA_ERR_ARG, "bad matvec arguments");
+    for (int r = 0; r < nrhs; r++)
+      if (!ctx->cc_set[r]) throw DdaError(DDA_ERR_ARG, "couple constants not set (dda_set_cc)");
+    if (ctx->e64.on) matvec_host_t<double>(ctx, arg, res, conj, nrhs);
+    else matvec_host_t<float>(ctx, arg, res, conj, nrhs);
+    return DDA_OK;
+  });
+}
+
+int dda_solve(dda_ctx* ctx, int solver, int nrhs, const double* einc, double eps, int64_t max_iter,
+              const double* start, double* pol_out, double* history, int64_t history_cap,
+              dda_stats* stats) {
+  if (!ctx) return DDA_ERR_ARG;
+  return guard(ctx, [&]() -> int {
+    if (solver < 0 || solver > 3) throw DdaError(DDA_ERR_ARG, "unknown solver");
+    if (nrhs < 1 || nrhs > ctx->max_rhs || !einc) throw DdaError(DDA_ERR_ARG, "bad solve arguments");
+    if (!(eps > 0)) throw DdaError(DDA_ERR_ARG, "eps must be positive");
+    for (int r = 0; r < nrhs; r++)
+      if (!ctx->cc_set[r]) throw DdaError(DDA_ERR_ARG, "couple constants not set (dda_set_cc)");
+    if (ctx->precision == DDA_PREC_FP32)
+      return solve_t<float>(ctx, solver, nrhs, einc, eps, max_iter, start, pol_out, history, history_cap, stats);
+    return solve_t<double>(ctx, solver, nrhs, einc, eps, max_iter, start, pol_out, history, history_cap, stats);
+  });
+}
+
+int dda_solve_device(dda_ctx* ctx, int solver, int nrhs, const void* d_einc, double eps, int64_t max_iter,
+                     const void* d_start, void* d_pol, dda_stats* stats) {
+  if (!ctx) return DDA_ERR_ARG;
+  return guard(ctx, [&]() -> int {
+    if (solver < 0 || solver > 3) throw DdaError(DDA_ERR_ARG, "unknown solver");
+    if (nrhs < 1 || nrhs > ctx->max_rhs || !d_einc || !d_pol) throw DdaError(DDA_ERR_ARG, "bad solve arguments");
+    if (!(eps > 0)) throw DdaError(DDA_ERR_ARG, "eps must be positive");
+    for (int r = 0; r < nrhs; r++)
+      if (!ctx->cc_set[r]) throw DdaError(DDA_ERR_ARG, "couple constants not set (dda_set_cc)");
+    if (ctx->precision == DDA_PREC_FP64)
+      return solve_device_t<double>(ctx, solver, nrhs, d_einc, eps, max_iter, d_start, d_pol, stats);
+    return solve_device_t<float>(ctx, solver, nrhs, d_einc, eps, max_iter, d_start, d_pol, stats);
+  });
+}
+
+void* dda_stream(dda_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int64_t dda_launch_count(const dda_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int dda_profile_matvec(dda_ctx* ctx, int nrhs, int reps, double* ms) {
+  if (!ctx || !ms || reps < 1) return DDA_ERR_ARG;
+  return guard(ctx, [&]() -> int {
+    if (nrhs < 1 || nrhs > ctx->max_rhs) throw DdaError(DDA_ERR_ARG, "bad nrhs");
+    if (ctx->e32.on) profile_t<float>(ctx, nrhs, reps, ms);
+    else profile_t<double>(ctx, nrhs, reps, ms);
+    return DDA_OK;
+  });
+}
+
+int dda_get_dmatrix(dda_ctx* ctx, double* out) {
+  if (!ctx || !out) return DDA_ERR_ARG;
+  return guard(ctx, [&]() -> int {
+    const MvGeom& g = ctx->g;
+    const int hx = g.Gx / 2 + 1, hy = g.Gy / 2 + 1, hz = g.Gz / 2 + 1;
+    const size_t m = (size_t)hx * hy * hz * 6;
+    std::vector<double2> h(m);
+    if (ctx->e64.on) {
+      CK(cudaMemcpy(h.data(), ctx->e64.dc, m * sizeof(double2), cudaMemcpyDeviceToHost));
+    } else {
+      std::vector<float2> f(m);
+      CK(cudaMemcpy(f.data(), ctx->e32.dc, m * sizeof(float2), cudaMemcpyDeviceToHost));
+      for (size_t i = 0; i < m; i++) h[i] = make_double2(f[i].x, f[i].y);
+    }
+    const double sc = 1.0 / (ctx->grid_unit * ctx->grid_unit * ctx->grid_unit);
+    for (int kx = 0; kx < g.Gx; kx++)
+      for (int kz = 0; kz < g.Gz; kz++)
+        for (int ky = 0; ky < g.Gy; ky++) {
+          const bool fx = kx > g.Gx / 2, fy = ky > g.Gy / 2, fz = kz > g.Gz / 2;
+          const int ax = fx ? g.Gx - kx : kx, ay = fy ? g.Gy - ky : ky, az = fz ? g.Gz - kz : kz;
+          const double2* src = &h[(((size_t)ax * hz + az) * hy + ay) * 6];
+          const double sign[6] = {1, fx != fy ? -1.0 : 1.0, fx != fz ? -1.0 : 1.0, 1, fy != fz ? -1.0 : 1.0, 1};
+          double* dst = out + 2 * 6 * (ky + (size_t)g.Gy * (kz + (size_t)g.Gz * kx));
+          for (int comp = 0; comp < 6; comp++) {
+            dst[2 * comp] = src[comp].x * sign[comp] * sc;
+            dst[2 * comp + 1] = src[comp].y * sign[comp] * sc;
+          }
+        }
+    return DDA_OK;
+  });
+}
+
+int dda_synchronize(dda_ctx* ctx) {
+  if (!ctx) return DDA_ERR_ARG;
+  return guard(ctx, [&]() -> int {
+    CK(cudaStreamSynchronize(ctx->stream));
+    return DDA_OK;
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,224 @@
+// krylov_kernels.cuh -- fused vector steps of the Krylov solvers.
+//
+// One launch per solver step does every linear combination of that step in
+// a single pass over the vectors and the step's dot products in FP64, then
+// the last CTA runs the scalar recurrence (krylov_ops.cuh).  This replaces the
+// per-update linComb kernels, the two-stage reductions and the blocking
+// scalar reads/writes of GpuLinComb / GpuQmrCs / GpuBicgStab
+// (LinAlg/GpuLinCombInst.cl:171-322, DDA/GpuQmrCs.cpp:102-198,
+// DDA/GpuBicgStab.cpp:44-125) and the setup kernels of
+// DDA/GpuIterativeSolverInst.cl:27-108.
+#pragma once
+
+#include "fft_engine.cuh"
+#include "krylov_ops.cuh"
+#include "reduce.cuh"
+
+namespace dda {
+
+enum VecOp {
+  V_SETUP_PVEC = 0,  // v0 = sqrt(cc).v1 (b = sqrt(cc) Einc); n = |v0|^2
+  V_START_X,         // v0 = v1 / sqrt(cc)  (start value, DDA/GpuIterativeSolverInst.cl:52-77)
+  V_R_INIT,          // v0 = -v1 + v2  (r = b - A x); n = |r|^2
+  V_CHOOSE_X0,       // usezero ? (v0 = 0, v1 = v2) : v0 = v2      (x, r, b)
+  V_QMR_V0,          // v0 = v1 . betaInv                          (v = r / beta)
+  V_QMR_VT,          // v0 = [v0 mBeta] + v1 mAlpha + v2; a = v0.v0, n = |v0|^2   (vt, v, A)
+  V_QMR_UPD,         // p/x/v/r update of DDA/QmrCs.cpp:152-167 (first: 1 = iteration 0, 2 = iteration 1)
+  V_BIS_INIT,        // v0 = v1 (rt = r); a = v1.conj(v0)
+  V_BIS_P,           // v0 = first ? v2 : v0 beta + v1 bo + v2     (p, v, r)
+  V_BIS_S,           // v0 = v1 mAlpha + v2; n = |v0|^2            (s, v, r)
+  V_BIS_XR,          // x/r update of DDA/BicgStab.cpp:98-110
+  V_BICG_RO,         // a = v0.v0
+  V_BICG_P,          // v0 = first ? v1 : v0 beta + v1             (p, r)
+  V_BICG_XR,         // x += p alpha; r += A mAlpha; n = |r|^2; a = r.r
+  V_CGNR_P,          // v0 = v0 beta + v1                          (p, Ah)
+  V_CGNR_XR,         // x += p alpha; r += A mAlpha; n = |r|^2
+  V_RESULT,          // v0 = sqrt(cc).v1  (P = sqrt(cc) x)
+  V_NORM,            // n = |v0|^2
+};
+
+struct VecArgs {
+  void* v[6];
+  int op;
+  int first;  // iteration 0 variant
+  int nv, nvs, nmat;
+  int nparts;
+  const uint8_t* mat;  // material per dipole (caller order)
+  const void* ccs;     // [nrhs][nmat][3] complex
+  KrylovStep step;
+};
+
+template <typename T2, typename S2>
+__device__ __forceinline__ T2 cvt(S2 a) {
+  T2 r; r.x = a.x; r.y = a.y; return r;
+}
+
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT) k_vec(VecArgs va, KrylovState* st) {
+  typedef typename C2<T>::t T2;
+  const int b = blockIdx.y;
+  KrylovState& s = st[b];
+  if (s.done) return;
+  const long long len = 3LL * va.nvs;
+  const long long chunk = ((len + va.nparts - 1) / va.nparts + 31) / 32 * 32;
+  const long long i0 = chunk * blockIdx.x;
+  const long long i1 = min(len, i0 + chunk);
+  const size_t off = (size_t)b * len;
+  T2* v0 = va.v[0] ? reinterpret_cast<T2*>(va.v[0]) + off : nullptr;
+  T2* v1 = va.v[1] ? reinterpret_cast<T2*>(va.v[1]) + off : nullptr;
+  T2* v2 = va.v[2] ? reinterpret_cast<T2*>(va.v[2]) + off : nullptr;
+  T2* v3 = va.v[3] ? reinterpret_cast<T2*>(va.v[3]) + off : nullptr;
+  T2* v4 = va.v[4] ? reinterpret_cast<T2*>(va.v[4]) + off : nullptr;
+  T2* v5 = va.v[5] ? reinterpret_cast<T2*>(va.v[5]) + off : nullptr;
+  const T2* ccs = reinterpret_cast<const T2*>(va.ccs) + (size_t)b * va.nmat * 3;
+  // step scalars in working precision
+  const T2 mBeta = cvt<T2>(s.mBeta), mAlpha = cvt<T2>(s.mAlpha), alpha = cvt<T2>(s.alpha);
+  const T2 betaInv = cvt<T2>(s.betaInv), beta = cvt<T2>(s.beta), bo = cvt<T2>(s.bo);
+  const T2 omega = cvt<T2>(s.omega), tau = cvt<T2>(s.tau), cNOT = cvt<T2>(s.cNOT);
+  const T2 zetaInv = cvt<T2>(s.zetaInv), mEtaZeta = cvt<T2>(s.mEtaZeta), mThetaZeta = cvt<T2>(s.mThetaZeta);
+  const T2 mOmega = cvt<T2>(dneg(s.omega));
+  const T normS = (T)s.normSNew;
+  const int skip = s.skipmv, usezero = s.usezero;
+  RedSums acc = red_zero();
+  for (long long i = i0 + threadIdx.x; i < i1; i += NT) {
+    switch (va.op) {
+      case V_SETUP_PVEC:
+      case V_RESULT:
+      case V_START_X: {
+        const int c = (int)(i / va.nvs), j = (int)(i % va.nvs);
+        T2 o = czero<T2>();
+        if (j < va.nv) {
+          const T2 cc = ccs[va.mat[j] * 3 + c];
+          const T2 x = v1[i];
+          if (va.op == V_START_X) {
+            // x / cc (Smith division in working precision)
+            double2 q = ddivc(make_double2(x.x, x.y), make_double2(cc.x, cc.y));
+            o = cvt<T2>(q);
+          } else {
+            o = cmul(cc, x);
+          }
+        }
+        v0[i] = o;
+        acc.n += (double)o.x * o.x + (double)o.y * o.y;
+        break;
+      }
+      case V_R_INIT: {
+        T2 r = csub(v2[i], v1[i]);
+        v0[i] = r;
+        acc.n += (double)r.x * r.x + (double)r.y * r.y;
+        break;
+      }
+      case V_CHOOSE_X0: {
+        const T2 p = v2[i];
+        if (usezero) { v0[i] = czero<T2>(); v1[i] = p; }
+        else v0[i] = p;
+        break;
+      }
+      case V_QMR_V0:
+        v0[i] = cmul(v1[i], betaInv);
+        break;
+      case V_QMR_VT: {
+        T2 t = cadd(cmul(v1[i], mAlpha), v2[i]);
+        if (!va.first) t = cadd(cmul(v0[i], mBeta), t);
+        v0[i] = t;
+        acc.a.x += (double)t.x * t.x - (double)t.y * t.y;
+        acc.a.y += 2.0 * (double)t.x * t.y;
+        acc.n += (double)t.x * t.x + (double)t.y * t.y;
+        break;
+      }
+      case V_QMR_UPD: {
+        // v0 = r, v1 = p_old, v2 = p_new, v3 = v, v4 = vt, v5 = x.  The new
+        // search direction goes to p_new in iteration 0 and to p_old after
+        // that (the caller then swaps p_old and p_new, DDA/QmrCs.cpp:152-160).
+        const T2 v = v3[i];
+        T2 pn;
+        if (va.first == 1) {
+          pn = cmul(v, zetaInv);
+          v2[i] = pn;
+        } else {
+          if (va.first == 2) pn = cadd(cmul(v2[i], mEtaZeta), cmul(v, zetaInv));
+          else pn = cadd(cadd(cmul(v1[i], mThetaZeta), cmul(v2[i], mEtaZeta)), cmul(v, zetaInv));
+          v1[i] = pn;
+        }
+        v5[i] = cadd(cmul(pn, tau), v5[i]);
+        const T2 vn = cmul(v4[i], betaInv);
+        v4[i] = vn;
+        const T2 ro = v0[i];
+        T2 r;
+        r.x = ro.x * normS; r.y = ro.y * normS;
+        r = cadd(r, cmul(vn, cNOT));
+        v0[i] = r;
+        acc.n += (double)r.x * r.x + (double)r.y * r.y;
+        break;
+      }
+      case V_BIS_INIT: {
+        const T2 r = v1[i];
+        v0[i] = r;
+        acc.a.x += (double)r.x * r.x + (double)r.y * r.y;
+        break;
+      }
+      case V_BIS_P:
+        v0[i] = va.first ? v2[i] : cadd(cadd(cmul(v0[i], beta), cmul(v1[i], bo)), v2[i]);
+        break;
+      case V_BIS_S: {
+        const T2 t = cadd(cmul(v1[i], mAlpha), v2[i]);
+        v0[i] = t;
+        acc.n += (double)t.x * t.x + (double)t.y * t.y;
+        break;
+      }
+      case V_BIS_XR: {
+        // v0 = x, v1 = p, v2 = s, v3 = A s, v4 = r, v5 = rt
+        if (skip) {
+          v0[i] = cadd(cmul(v1[i], alpha), v0[i]);
+        } else {
+          const T2 sv = v2[i];
+          v0[i] = cadd(cadd(cmul(v1[i], alpha), cmul(sv, omega)), v0[i]);
+          const T2 r = cadd(cmul(v3[i], mOmega), sv);
+          v4[i] = r;
+          const T2 rt = v5[i];
+          acc.n += (double)r.x * r.x + (double)r.y * r.y;
+          acc.a.x += (double)r.x * rt.x + (double)r.y * rt.y;
+          acc.a.y += (double)r.y * rt.x - (double)r.x * rt.y;
+        }
+        break;
+      }
+      case V_BICG_RO: {
+        const T2 r = v0[i];
+        acc.a.x += (double)r.x * r.x - (double)r.y * r.y;
+        acc.a.y += 2.0 * (double)r.x * r.y;
+        break;
+      }
+      case V_BICG_P:
+        v0[i] = va.first ? v1[i] : cadd(cmul(v0[i], beta), v1[i]);
+        break;
+      case V_BICG_XR:
+      case V_CGNR_XR: {
+        // v0 = x, v1 = p, v2 = A, v3 = r
+        v0[i] = cadd(cmul(v1[i], alpha), v0[i]);
+        const T2 r = cadd(cmul(v2[i], mAlpha), v3[i]);
+        v3[i] = r;
+        acc.n += (double)r.x * r.x + (double)r.y * r.y;
+        acc.a.x += (double)r.x * r.x - (double)r.y * r.y;
+        acc.a.y += 2.0 * (double)r.x * r.y;
+        break;
+      }
+      case V_CGNR_P:
+        v0[i] = cadd(cmul(v0[i], beta), v1[i]);
+        break;
+      case V_NORM: {
+        const T2 r = v0[i];
+        acc.n += (double)r.x * r.x + (double)r.y * r.y;
+        break;
+      }
+      default:
+        break;
+    }
+  }
+  if (va.step.op != KOP_NONE) {
+    RedSums tot;
+    if (block_finish<NT>(acc, va.step.red, b, blockIdx.x, tot) && threadIdx.x == 0)
+      krylov_finalize(s, va.step, tot);
+  }
+}
+
+}  // namespace dda

@@ -1,0 +1,364 @@
+// matvec_kernels.cuh -- the FFT-convolution matvec of the DDA system
+//   y = x + sqrt(cc) . IFFT3( D-hat . FFT3( pad( sqrt(cc) . x ) ) )
+// (GpuMatVec<T>::apply, DDA/GpuMatVec.cpp:144-431; CPU twin
+// DDA/MatVecCpu.cpp:67-150) as three fused passes over HBM:
+//
+//   k_xfwd : scatter sqrt(cc).x into a shared-memory tile of grid lines along
+//            x (initXMatrix, DDA/GpuMatVecInst.cl:31-61), forward FFT along x,
+//            store the x-spectrum plane-major: xhat[b][kx][c][z][y].
+//   k_yz   : one kx plane per CTA, resident in shared memory: forward FFT
+//            along z (zero padded bz -> Gz), then per kz row forward FFT along
+//            y (by -> Gy), the symmetric 3x3 D-hat multiply (innerLoop,
+//            DDA/GpuMatVecInst.cl:104-121), inverse FFT along y, inverse FFT
+//            along z, store back.  Replaces the four GpuTransposePlan calls
+//            and the slab loop of DDA/GpuMatVec.cpp:226-363.
+//   k_xinv : inverse FFT along x, gather, y = sqrt(cc).X + x and the optional
+//            Krylov dot products of the result (createResVec,
+//            DDA/GpuMatVecInst.cl:63-102).
+//
+// When a kx plane does not fit in shared memory, k_yz is replaced by
+// k_fft_cols (z forward) -> k_yrows (y forward, D-hat, y inverse) ->
+// k_fft_cols (z inverse) through a plane buffer zbuf[b][kx][c][kz][y].
+//
+// D-hat is stored as the first octant [kx<=Gx/2][kz<=Gz/2][ky<=Gy/2][6]: the
+// Green's tensor is even in every axis on the diagonal and odd in the two
+// axes of an off-diagonal component, and so is its DFT.
+#pragma once
+
+#include "fft_engine.cuh"
+#include "reduce.cuh"
+#include "krylov_ops.cuh"
+
+namespace dda {
+
+struct MvGeom {
+  int Gx, Gy, Gz;
+  int bx, by, bz;
+  int nv, nvs;
+  int nlines;  // by*bz
+  int nmat;
+  int tl;      // grid lines per k_xfwd / k_xinv tile
+  int pitchx;  // shared row pitch of those tiles (Gx + 1)
+};
+
+// D-hat at (kx, ky, kz) from the octant store.
+template <typename T>
+__device__ __forceinline__ void load_dhat(const typename C2<T>::t* __restrict__ dc, int Gx, int Gy,
+                                          int Gz, int kx, int ky, int kz,
+                                          typename C2<T>::t d[6]) {
+  typedef typename C2<T>::t T2;
+  const int hx = Gx / 2 + 1, hy = Gy / 2 + 1, hz = Gz / 2 + 1;
+  const bool fx = kx > Gx / 2, fy = ky > Gy / 2, fz = kz > Gz / 2;
+  const int ax = fx ? Gx - kx : kx, ay = fy ? Gy - ky : ky, az = fz ? Gz - kz : kz;
+  const T2* p = dc + ((size_t)(ax * hz + az) * hy + ay) * 6;
+#pragma unroll
+  for (int i = 0; i < 6; i++) d[i] = p[i];
+  if (fx != fy) { d[1].x = -d[1].x; d[1].y = -d[1].y; }  // xy: odd in x and y
+  if (fx != fz) { d[2].x = -d[2].x; d[2].y = -d[2].y; }  // xz
+  if (fy != fz) { d[4].x = -d[4].x; d[4].y = -d[4].y; }  // yz
+  (void)hx;
+}
+
+// y = D x for the symmetric 3x3 matrix (xx, xy, xz, yy, yz, zz)
+// (Math/SymMatrix3.hpp:86-92).
+template <typename T2>
+__device__ __forceinline__ void dmul(const T2 d[6], T2& a, T2& b, T2& c) {
+  T2 x = a, y = b, z = c;
+  a = cadd(cadd(cmul(d[0], x), cmul(d[1], y)), cmul(d[2], z));
+  b = cadd(cadd(cmul(d[1], x), cmul(d[3], y)), cmul(d[4], z));
+  c = cadd(cadd(cmul(d[2], x), cmul(d[4], y)), cmul(d[5], z));
+}
+
+// True when right-hand side b needs no work: solved or failed, or (mvskip)
+// the BiCGStab half-step exit made the second matvec unnecessary.
+__device__ __forceinline__ bool rhs_idle(const KrylovState* st, int b, int mvskip) {
+  return st && (st[b].done || (mvskip && st[b].skipmv));
+}
+
+// ------------------------------------------------------------ k_xfwd ----
+// grid (ceil(nlines/tl), 3, nrhs); dynamic smem tl*pitchx*sizeof(T2) + ccs.
+template <typename T, int NT, int MAXE>
+__global__ void __launch_bounds__(NT, 2) k_xfwd(const typename C2<T>::t* __restrict__ arg,
+                                             typename C2<T>::t* __restrict__ xhat,
+                                             const uint32_t* __restrict__ line_off,
+                                             const uint32_t* __restrict__ dip,
+                                             const uint32_t* __restrict__ perm,
+                                             const typename C2<T>::t* __restrict__ ccs, int conj,
+                                             MvGeom g, FftPlanDev px,
+                                             const KrylovState* __restrict__ st, int mvskip) {
+  typedef typename C2<T>::t T2;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T2* sm = reinterpret_cast<T2*>(smraw);
+  T2* scc = sm + (size_t)g.tl * g.pitchx;
+  const int b = blockIdx.z, c = blockIdx.y;
+  if (rhs_idle(st, b, mvskip)) return;
+  const int L0 = blockIdx.x * g.tl;
+  const int nl = min(g.tl, g.nlines - L0);
+  for (int i = threadIdx.x; i < g.nmat; i += NT) scc[i] = ccs[((size_t)b * g.nmat + i) * 3 + c];
+  for (int i = threadIdx.x; i < nl * g.pitchx; i += NT) sm[i] = czero<T2>();
+  __syncthreads();
+  const T2* a = arg + ((size_t)b * 3 + c) * g.nvs;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int l = warp; l < nl; l += NT / 32) {
+    const uint32_t j0 = line_off[L0 + l], j1 = line_off[L0 + l + 1];
+    for (uint32_t j = j0 + lane; j < j1; j += 32) {
+      const uint32_t d = dip[j];
+      const uint32_t jj = perm ? perm[j] : j;
+      T2 v = a[jj];
+      if (conj) v.y = -v.y;
+      sm[l * g.pitchx + (d & 0xffffu)] = cmul(v, scc[d >> 16]);
+    }
+  }
+  __syncthreads();
+  fft_smem<T, NT, MAXE, false>(sm, nl, g.pitchx, 1, false, px);
+  T2* out = xhat + ((size_t)b * g.Gx * 3 + c) * g.nlines + L0;
+  const size_t kstride = (size_t)3 * g.nlines;
+  for (int i = threadIdx.x; i < nl * g.Gx; i += NT) {
+    const int l = i % nl, kx = i / nl;
+    out[kx * kstride + l] = sm[l * g.pitchx + kx];
+  }
+}
+
+// ------------------------------------------------------------ k_xinv ----
+// grid (ceil(nlines/tl), 3, nrhs).  Epilogue: res = conj?(sqrt(cc).X +
+// conj?(arg)), padding nv..nvs zeroed, and optional sums over the result for
+// the solver step `op` (finalised by the last CTA of each right-hand side).
+template <typename T, int NT, int MAXE>
+__global__ void __launch_bounds__(NT, 2) k_xinv(const typename C2<T>::t* __restrict__ arg,
+                                             typename C2<T>::t* __restrict__ res,
+                                             const typename C2<T>::t* __restrict__ xhat,
+                                             const uint32_t* __restrict__ line_off,
+                                             const uint32_t* __restrict__ dip,
+                                             const uint32_t* __restrict__ perm,
+                                             const typename C2<T>::t* __restrict__ ccs, int conj,
+                                             MvGeom g, FftPlanDev px, KrylovState* st,
+                                             KrylovStep step, int mvskip) {
+  typedef typename C2<T>::t T2;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T2* sm = reinterpret_cast<T2*>(smraw);
+  T2* scc = sm + (size_t)g.tl * g.pitchx;
+  const int b = blockIdx.z, c = blockIdx.y;
+  if (rhs_idle(st, b, mvskip)) return;
+  const int L0 = blockIdx.x * g.tl;
+  const int nl = min(g.tl, g.nlines - L0);
+  for (int i = threadIdx.x; i < g.nmat; i += NT) scc[i] = ccs[((size_t)b * g.nmat + i) * 3 + c];
+  const T2* in = xhat + ((size_t)b * g.Gx * 3 + c) * g.nlines + L0;
+  const size_t kstride = (size_t)3 * g.nlines;
+  for (int i = threadIdx.x; i < nl * g.Gx; i += NT) {
+    const int l = i % nl, kx = i / nl;
+    sm[l * g.pitchx + kx] = in[kx * kstride + l];
+  }
+  __syncthreads();
+  fft_smem<T, NT, MAXE, true>(sm, nl, g.pitchx, 1, false, px);
+  const size_t voff = ((size_t)b * 3 + c) * g.nvs;
+  const T2* a = arg + voff;
+  T2* r = res + voff;
+  const T2* w = step.w ? reinterpret_cast<const T2*>(step.w) + voff : nullptr;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  RedSums acc = red_zero();
+  for (int l = warp; l < nl; l += NT / 32) {
+    const uint32_t j0 = line_off[L0 + l], j1 = line_off[L0 + l + 1];
+    for (uint32_t j = j0 + lane; j < j1; j += 32) {
+      const uint32_t d = dip[j];
+      const uint32_t jj = perm ? perm[j] : j;
+      const T2 x = sm[l * g.pitchx + (d & 0xffffu)];
+      const T2 a0 = a[jj];
+      T2 av = a0;
+      if (conj) av.y = -av.y;
+      T2 y = cadd(cmul(x, scc[d >> 16]), av);
+      if (conj) y.y = -y.y;
+      r[jj] = y;
+      if (step.op != KOP_NONE) acc = epilogue_terms<T2>(acc, y, a0, w ? w[jj] : a0, step.mode);
+    }
+  }
+  if (blockIdx.x == 0)
+    for (int i = g.nv + threadIdx.x; i < g.nvs; i += NT) r[i] = czero<T2>();
+  if (step.op != KOP_NONE) {
+    RedSums tot;
+    const int part = blockIdx.y * gridDim.x + blockIdx.x;
+    if (block_finish<NT>(acc, step.red, b, part, tot) && threadIdx.x == 0)
+      krylov_finalize(st[b], step, tot);
+  }
+}
+
+// -------------------------------------------------------------- k_yz ----
+// One (rhs, kx) plane per CTA.  Shared memory: slab S[Gz][q] (q >= 3*by;
+// row kz holds the three components' y values), row scratch R[nr][3][py].
+struct YzGeom {
+  int q;   // slab row pitch
+  int nr;  // kz rows per y pass
+  int py;  // row scratch pitch (Gy + 1)
+};
+
+template <typename T, int NT, int MAXE>
+__device__ __forceinline__ void yz_rows(typename C2<T>::t* S, typename C2<T>::t* R,
+                                        const typename C2<T>::t* __restrict__ dc, const MvGeom& g,
+                                        const YzGeom& y, const FftPlanDev& pyp, int kx,
+                                        int kz0, int nr) {
+  typedef typename C2<T>::t T2;
+  // load rows, zero padding y >= by
+  for (int i = threadIdx.x; i < nr * 3 * g.Gy; i += NT) {
+    const int yy = i % g.Gy, rc = i / g.Gy;  // rc = row*3 + c
+    const int row = rc / 3, c = rc % 3;
+    R[rc * y.py + yy] = yy < g.by ? S[(size_t)(kz0 + row) * y.q + c * g.by + yy] : czero<T2>();
+  }
+  __syncthreads();
+  fft_smem<T, NT, MAXE, false>(R, nr * 3, y.py, 1, false, pyp);
+  for (int i = threadIdx.x; i < nr * g.Gy; i += NT) {
+    const int ky = i % g.Gy, row = i / g.Gy;
+    T2 d[6];
+    load_dhat<T>(dc, g.Gx, g.Gy, g.Gz, kx, ky, kz0 + row, d);
+    T2* p = R + (size_t)row * 3 * y.py + ky;
+    T2 a = p[0], b = p[y.py], c = p[2 * y.py];
+    dmul(d, a, b, c);
+    p[0] = a; p[y.py] = b; p[2 * y.py] = c;
+  }
+  __syncthreads();
+  fft_smem<T, NT, MAXE, true>(R, nr * 3, y.py, 1, false, pyp);
+  for (int i = threadIdx.x; i < nr * 3 * g.by; i += NT) {
+    const int yy = i % g.by, rc = i / g.by;
+    const int row = rc / 3, c = rc % 3;
+    S[(size_t)(kz0 + row) * y.q + c * g.by + yy] = R[rc * y.py + yy];
+  }
+  __syncthreads();
+}
+
+template <typename T, int NT, int MAXE>
+__global__ void __launch_bounds__(NT, 1) k_yz(typename C2<T>::t* __restrict__ xhat,
+                                           const typename C2<T>::t* __restrict__ dc, MvGeom g,
+                                           YzGeom y, FftPlanDev pz, FftPlanDev pyp,
+                                           const KrylovState* __restrict__ st, int mvskip) {
+  typedef typename C2<T>::t T2;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T2* S = reinterpret_cast<T2*>(smraw);
+  T2* R = S + (size_t)g.Gz * y.q;
+  const int kx = blockIdx.x, b = blockIdx.y;
+  if (rhs_idle(st, b, mvskip)) return;
+  T2* plane = xhat + ((size_t)b * g.Gx + kx) * 3 * g.nlines;
+  const int nb = g.by * g.bz;
+  for (int i = threadIdx.x; i < 3 * nb; i += NT) {
+    const int c = i / nb, rem = i % nb;
+    const int z = rem / g.by, yy = rem % g.by;
+    S[(size_t)z * y.q + c * g.by + yy] = plane[i];
+  }
+  for (int i = threadIdx.x; i < (g.Gz - g.bz) * 3 * g.by; i += NT) {
+    const int z = g.bz + i / (3 * g.by), col = i % (3 * g.by);
+    S[(size_t)z * y.q + col] = czero<T2>();
+  }
+  __syncthreads();
+  fft_smem<T, NT, MAXE, false>(S, 3 * g.by, 1, y.q, true, pz);
+  for (int kz0 = 0; kz0 < g.Gz; kz0 += y.nr)
+    yz_rows<T, NT, MAXE>(S, R, dc, g, y, pyp, kx, kz0, min(y.nr, g.Gz - kz0));
+  fft_smem<T, NT, MAXE, true>(S, 3 * g.by, 1, y.q, true, pz);
+  for (int i = threadIdx.x; i < 3 * nb; i += NT) {
+    const int c = i / nb, rem = i % nb;
+    const int z = rem / g.by, yy = rem % g.by;
+    plane[i] = S[(size_t)z * y.q + c * g.by + yy];
+  }
+}
+
+// ----------------------------------------------- split path: k_yrows ----
+// grid (ceil(Gz/nr), Gx, nrhs) over zbuf[b][kx][c][kz][y] (y < by).
+template <typename T, int NT, int MAXE>
+__global__ void __launch_bounds__(NT, 1) k_yrows(typename C2<T>::t* __restrict__ zbuf,
+                                              const typename C2<T>::t* __restrict__ dc,
+                                              MvGeom g, YzGeom y, FftPlanDev pyp,
+                                              const KrylovState* __restrict__ st, int mvskip) {
+  typedef typename C2<T>::t T2;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T2* R = reinterpret_cast<T2*>(smraw);
+  const int kx = blockIdx.y, b = blockIdx.z;
+  if (rhs_idle(st, b, mvskip)) return;
+  const int kz0 = blockIdx.x * y.nr;
+  const int nr = min(y.nr, g.Gz - kz0);
+  T2* base = zbuf + ((size_t)b * g.Gx + kx) * 3 * (size_t)g.Gz * g.by;
+  const size_t cstride = (size_t)g.Gz * g.by;
+  for (int i = threadIdx.x; i < nr * 3 * g.Gy; i += NT) {
+    const int yy = i % g.Gy, rc = i / g.Gy;
+    const int row = rc / 3, c = rc % 3;
+    R[rc * y.py + yy] = yy < g.by ? base[c * cstride + (size_t)(kz0 + row) * g.by + yy] : czero<T2>();
+  }
+  __syncthreads();
+  fft_smem<T, NT, MAXE, false>(R, nr * 3, y.py, 1, false, pyp);
+  for (int i = threadIdx.x; i < nr * g.Gy; i += NT) {
+    const int ky = i % g.Gy, row = i / g.Gy;
+    T2 d[6];
+    load_dhat<T>(dc, g.Gx, g.Gy, g.Gz, kx, ky, kz0 + row, d);
+    T2* p = R + (size_t)row * 3 * y.py + ky;
+    T2 a = p[0], bb = p[y.py], c = p[2 * y.py];
+    dmul(d, a, bb, c);
+    p[0] = a; p[y.py] = bb; p[2 * y.py] = c;
+  }
+  __syncthreads();
+  fft_smem<T, NT, MAXE, true>(R, nr * 3, y.py, 1, false, pyp);
+  for (int i = threadIdx.x; i < nr * 3 * g.by; i += NT) {
+    const int yy = i % g.by, rc = i / g.by;
+    const int row = rc / 3, c = rc % 3;
+    base[c * cstride + (size_t)(kz0 + row) * g.by + yy] = R[rc * y.py + yy];
+  }
+}
+
+// ------------------------------------------- generic strided column FFT ----
+// Transforms along the middle axis of arrays [batch][axis][inner] (inner
+// contiguous).  Input axis length n_in <= n is zero padded, output keeps the
+// first n_out <= n entries.  grid (ceil(inner/ti), nbatch); tile [n][ti+1].
+struct ColGeom {
+  long long in_bs, in_as;    // input batch / axis strides (elements)
+  long long out_bs, out_as;  // output batch / axis strides
+  int inner, ti, pitch;      // inner extent, tile width, smem pitch
+  int n_in, n_out;
+  int batches_per_rhs;       // for skipping converged right-hand sides
+};
+
+template <typename T, int NT, int MAXE>
+__global__ void __launch_bounds__(NT, 2) k_fft_cols(const typename C2<T>::t* in,
+                                                 typename C2<T>::t* out, ColGeom cg,
+                                                 FftPlanDev pl, int inverse,
+                                                 const KrylovState* __restrict__ st, int mvskip) {
+  typedef typename C2<T>::t T2;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T2* sm = reinterpret_cast<T2*>(smraw);
+  const long long batch = blockIdx.y;
+  if (rhs_idle(st, (int)(batch / cg.batches_per_rhs), mvskip)) return;
+  const int i0 = blockIdx.x * cg.ti;
+  const int ti = min(cg.ti, cg.inner - i0);
+  const int n = pl.n;
+  const T2* ib = in + batch * cg.in_bs + i0;
+  for (int i = threadIdx.x; i < n * ti; i += NT) {
+    const int e = i / ti, k = i % ti;
+    sm[e * cg.pitch + k] = e < cg.n_in ? ib[e * cg.in_as + k] : czero<T2>();
+  }
+  __syncthreads();
+  fft_smem_dir<T, NT, MAXE>(sm, ti, 1, cg.pitch, true, pl, inverse != 0);
+  T2* ob = out + batch * cg.out_bs + i0;
+  for (int i = threadIdx.x; i < cg.n_out * ti; i += NT) {
+    const int e = i / ti, k = i % ti;
+    ob[e * cg.out_as + k] = sm[e * cg.pitch + k];
+  }
+}
+
+// -------------------------------------------- generic contiguous row FFT ----
+// grid (ceil(count/tl)); lines of length n at `stride` elements apart.
+template <typename T, int NT, int MAXE>
+__global__ void __launch_bounds__(NT, 2) k_fft_rows(typename C2<T>::t* data, long long count,
+                                                 long long stride, int tl, int pitch,
+                                                 FftPlanDev pl, int inverse) {
+  typedef typename C2<T>::t T2;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T2* sm = reinterpret_cast<T2*>(smraw);
+  const long long l0 = (long long)blockIdx.x * tl;
+  const int nl = (int)min((long long)tl, count - l0);
+  const int n = pl.n;
+  for (int i = threadIdx.x; i < nl * n; i += NT) {
+    const int l = i / n, e = i % n;
+    sm[l * pitch + e] = data[(l0 + l) * stride + e];
+  }
+  __syncthreads();
+  fft_smem_dir<T, NT, MAXE>(sm, nl, pitch, 1, false, pl, inverse != 0);
+  for (int i = threadIdx.x; i < nl * n; i += NT) {
+    const int l = i / n, e = i % n;
+    data[(l0 + l) * stride + e] = sm[l * pitch + e];
+  }
+}
+
+}  // namespace dda

@@ -1,0 +1,174 @@
+/*
+ * dda_cuda.h -- C ABI of the B200 DDA solver (libdda_b200.so).
+ *
+ * The library runs the hot path of steffen-kiess/dda on one NVIDIA B200:
+ * the FFT-convolution matvec of the DDA system A x = x + sqrt(cc) D sqrt(cc) x,
+ * the four Krylov solvers built on it, and the D-matrix setup they need.
+ * Every entry point below names the reference interface it stands in for
+ * (paths relative to the reference tree).
+ *
+ * Conventions
+ *  - Return value 0 on success, a negative DDA_ERR_* code otherwise; the
+ *    message of the last failure is available from dda_last_error().
+ *  - No C++ exception crosses this boundary.
+ *  - Dipole vectors use the reference layout (DDA/DDAParams.hpp:176-186):
+ *    structure of arrays [x: nvs][y: nvs][z: nvs] of complex numbers, with
+ *    nvs = nv rounded up to a multiple of 16 and the padding zero.  Batches of
+ *    right-hand sides are stored one after another: [rhs][3][nvs].
+ *    Complex numbers are (re, im) pairs.
+ *  - Host buffers are owned by the caller; device buffers passed to
+ *    dda_matvec() are owned by the caller; everything else is owned by the
+ *    context.  One context per host thread at a time.
+ */
+#ifndef DDA_CUDA_H
+#define DDA_CUDA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DDA_OK 0
+#define DDA_ERR_ARG (-1)         /* invalid argument */
+#define DDA_ERR_CUDA (-2)        /* CUDA runtime failure */
+#define DDA_ERR_OOM (-3)         /* device allocation failed */
+#define DDA_ERR_UNSUPPORTED (-4) /* grid not 2,3,5,7-smooth, size limits */
+#define DDA_ERR_BREAKDOWN (-5)   /* Krylov breakdown guard fired */
+#define DDA_ERR_MAXITER (-6)     /* "Too many iterations" */
+#define DDA_ERR_NOPROGRESS (-7)  /* "Too many iterations w/o increase" */
+
+/* Arithmetic of the matvec and of the Krylov vectors. */
+#define DDA_PREC_FP64 0  /* everything in FP64 (the reference's --ftype double) */
+#define DDA_PREC_FP32 1  /* complex FP32 vectors/FFTs, FP64 scalars and dot products */
+#define DDA_PREC_MIXED 2 /* FP32 inner solves refined by an outer FP64 residual */
+
+/* Solvers, the reference's --iter names (DDA/DDAMain.cpp:647-656). */
+#define DDA_SOLVER_QMR 0      /* qmr:      DDA/QmrCs.cpp, DDA/GpuQmrCs.cpp */
+#define DDA_SOLVER_BICGSTAB 1 /* bicgstab: DDA/BicgStab.cpp, DDA/GpuBicgStab.cpp */
+#define DDA_SOLVER_BICG 2     /* bicg:     DDA/BicgCs.cpp, DDA/GpuBicgCs.cpp */
+#define DDA_SOLVER_CGNR 3     /* cgnr:     DDA/Cgnr.cpp, DDA/GpuCgnr.cpp */
+
+typedef struct dda_ctx dda_ctx;
+
+/* Problem description: the fields of DDAParams (DDA/DDAParams.hpp:52-217)
+ * the matvec needs. */
+typedef struct dda_problem {
+  uint32_t nv;               /* occupied dipoles */
+  uint32_t box[3];           /* particle box bx, by, bz (dipoles) */
+  uint32_t grid[3];          /* FFT grid Gx, Gy, Gz: even, >= 2*box, 2,3,5,7-smooth */
+  const uint32_t* positions; /* host, nv*3 grid coordinates (x, y, z) per dipole */
+  const uint8_t* materials;  /* host, nv material indices, NULL = all 0 */
+  uint32_t nmat;             /* number of materials (<= 256) */
+  double kd;                 /* wave number times grid unit */
+  double grid_unit;          /* grid unit d in metres */
+  const double* dmatrix;     /* optional host D matrix in the reference layout
+                                ([Gx][Gz][Gy][6] complex FP64, the output of
+                                DMatrixCpu::createDMatrix); NULL = generate it
+                                on the GPU from kd */
+  int32_t max_rhs;           /* right-hand sides per batch (>= 1) */
+  int32_t device;            /* CUDA device ordinal */
+  uint32_t flags;            /* DDA_FLAG_* */
+} dda_problem;
+
+/* dda_problem.flags: run the y/z passes through three kernels and a plane
+ * buffer even when a kx plane fits in shared memory (the path large grids
+ * take); used by tests and tuning. */
+#define DDA_FLAG_SPLIT_YZ 1u
+
+typedef struct dda_stats {
+  int64_t iterations;   /* Krylov iterations (summed over inner solves for MIXED) */
+  int64_t matvecs;      /* matvecs issued for this right-hand side */
+  int64_t refinements;  /* outer FP64 residual steps (MIXED) */
+  double rel_residual;  /* sqrt(best |r|^2 / |b|^2) at exit */
+  double res_scale;     /* 1 / |b|^2 */
+  int32_t status;       /* 0 or a DDA_ERR_* code */
+  int32_t pad;
+} dda_stats;
+
+/* Builds the device-side problem: geometry tables, FFT plans and the D
+ * matrix (generated on the GPU in FP64 when prob->dmatrix is NULL).
+ * Replaces GpuMatVec<T>::create (DDA/GpuMatVec.hpp:85-86),
+ * DMatrixGpu<T>::createDMatrix (DDA/DMatrixGpu.cpp:30-41) and
+ * DMatrixCpu<T>::createDMatrix (DDA/DMatrixCpu.hpp:42). */
+int dda_create(const dda_problem* prob, int precision, dda_ctx** out);
+
+/* Frees every device resource of the context. */
+int dda_destroy(dda_ctx* ctx);
+
+/* Message of the last failure on this context (or of the last failed
+ * dda_create when ctx is NULL). */
+const char* dda_last_error(const dda_ctx* ctx);
+
+/* nvs, the per-component stride of dipole vectors. */
+int64_t dda_vec_stride(const dda_ctx* ctx);
+
+/* Sets the couple-constant square roots sqrt(cc) of right-hand side `rhs`:
+ * nmat*3 complex FP64 (DiagMatrix3 per material), in reference units.
+ * Replaces MatVec<T>::setCoupleConstants (DDA/MatVec.hpp:46) and
+ * GpuMatVec<T>::setCoupleConstants (DDA/GpuMatVec.hpp:89). */
+int dda_set_cc(dda_ctx* ctx, int rhs, const double* cc_sqrt);
+
+/* result = A arg (conj != 0: conj(A conj(arg)), the adjoint product CGNR
+ * uses) for `nrhs` right-hand sides in device memory.  `precision` selects
+ * the buffers' element type: DDA_PREC_FP64 (double pairs) or DDA_PREC_FP32
+ * (float pairs).  `stream` is a cudaStream_t (NULL = the context stream).
+ * Replaces GpuMatVec<T>::apply (DDA/GpuMatVec.hpp:99). */
+int dda_matvec(dda_ctx* ctx, const void* d_arg, void* d_res, int conj, int nrhs,
+               int precision, void* stream);
+
+/* The same product on host FP64 buffers (copies in, matvec, copies out;
+ * FP32 contexts convert on the device).  Replaces MatVec<T>::apply
+ * (DDA/MatVec.hpp:54) as implemented by MatVecGpu<T>::apply
+ * (DDA/MatVecGpu.cpp:51-68). */
+int dda_matvec_host(dda_ctx* ctx, const double* arg, double* res, int conj, int nrhs);
+
+/* Solves A x = sqrt(cc) Einc for `nrhs` right-hand sides (incident fields
+ * einc, host FP64, [nrhs][3][nvs]) to relative residual eps and writes the
+ * dipole polarisations P = sqrt(cc) x to pol_out (host FP64, same layout).
+ * start (may be NULL) holds start polarisations (--load-start-dip-pol).
+ * max_iter <= 0 means unlimited.  history (may be NULL) receives the
+ * per-iteration relative residuals (the RE_ lines), history_cap per rhs.
+ * stats (may be NULL) receives nrhs records.  Returns the first non-zero
+ * per-rhs status.  Replaces IterativeSolverBase<T>::getPolVec
+ * (DDA/IterativeSolverBase.hpp:59) with the GPU solver classes
+ * (DDA/GpuIterativeSolver.hpp, DDA/Gpu{QmrCs,BicgStab,BicgCs,Cgnr}.hpp). */
+int dda_solve(dda_ctx* ctx, int solver, int nrhs, const double* einc, double eps,
+              int64_t max_iter, const double* start, double* pol_out, double* history,
+              int64_t history_cap, dda_stats* stats);
+
+/* dda_solve on device buffers of the context precision (double pairs for
+ * DDA_PREC_FP64, float pairs for DDA_PREC_FP32 and DDA_PREC_MIXED):
+ * d_einc [nrhs][3][nvs] in, d_pol [nrhs][3][nvs] out, d_start may be NULL.
+ * All work is queued on the context stream; the call returns when the solve
+ * has finished.  Replaces GpuIterativeSolver<T>::getPolVec's device part
+ * (DDA/GpuIterativeSolver.cpp:78-144) without the host copies. */
+int dda_solve_device(dda_ctx* ctx, int solver, int nrhs, const void* d_einc, double eps,
+                     int64_t max_iter, const void* d_start, void* d_pol, dda_stats* stats);
+
+/* The context stream (a cudaStream_t) on which the library queues its work. */
+void* dda_stream(dda_ctx* ctx);
+
+/* Number of kernels the context has launched so far (matvec passes,
+ * Krylov steps, setup); a profiling counter. */
+int64_t dda_launch_count(const dda_ctx* ctx);
+
+/* Times the stages of one matvec of nrhs right-hand sides with CUDA events
+ * (`reps` repetitions after one warm-up) and writes the mean milliseconds of
+ * each stage to ms[4]: x forward, y/z passes, x inverse, total.  The
+ * per-phase attribution of the reference's --sync profiling
+ * (DDA/GpuMatVec.cpp:149-153). */
+int dda_profile_matvec(dda_ctx* ctx, int nrhs, int reps, double* ms);
+
+/* Copies the D matrix out in the reference layout ([Gx][Gz][Gy][6] complex
+ * FP64, reference units), expanded from the octant the context stores. */
+int dda_get_dmatrix(dda_ctx* ctx, double* out);
+
+/* Waits for all work queued on the context stream. */
+int dda_synchronize(dda_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DDA_CUDA_H */

@@ -1,0 +1,101 @@
+"""GPU parity of the four Krylov solvers against the oracle's restatement of
+the reference CPU solvers (DDA/QmrCs.cpp, DDA/BicgStab.cpp, DDA/BicgCs.cpp,
+DDA/Cgnr.cpp, loop of DDA/IterativeSolverBase.cpp:40-103)."""
+import numpy as np
+import pytest
+
+import dda_b200
+from tests.pairs import Pair, aniso_arrays, rel
+
+pytestmark = pytest.mark.gpu
+
+SOLVERS = ["qmr", "bicgstab", "bicg", "cgnr"]
+MATS = [1.5 + 0.1j, (1.33 + 0.01j, 1.4 + 0.02j, 1.6 + 0.0j)]
+
+
+@pytest.fixture(scope="module")
+def aniso64():
+    pr = Pair("arrays", aniso_arrays(), MATS, "0.9um", "fp64")
+    pr.set_cc((0.3, 0.4, 0.866), 1, "ldr")
+    return pr
+
+
+@pytest.mark.parametrize("solver", SOLVERS)
+def test_fp64_solver_tracks_oracle(aniso64, solver):
+    pr = aniso64
+    e = pr.p.einc((0.3, 0.4, 0.866), 1)
+    s = dda_b200.CudaSolver(pr.mv, solver)
+    pol = s.get_pol_vec(e, 1e-10)
+    rc, opol, ost, ohist = pr.op.solve(e, solver, 1e-10)
+    assert rc == 0
+    st = s.last_stats[0]
+    assert st.status == 0 and st.rel_residual < 1e-10
+    assert abs(st.iterations - ost.iterations) <= 1
+    h = s.last_history[0]
+    k = min(len(h), len(ohist), 8)
+    assert np.allclose(h[:k], ohist[:k], rtol=1e-8, atol=0)
+    assert rel(pol, opol) < 1e-8
+
+
+@pytest.mark.parametrize("solver", SOLVERS)
+def test_fp32_solver_converges(aniso64, solver):
+    pr = Pair("arrays", aniso_arrays(), MATS, "0.9um", "fp32")
+    pr.set_cc((0.3, 0.4, 0.866), 1, "ldr")
+    e = pr.p.einc((0.3, 0.4, 0.866), 1)
+    s = dda_b200.CudaSolver(pr.mv, solver)
+    pol = s.get_pol_vec(e, 1e-5)
+    assert s.last_stats[0].status == 0
+    rc, opol, _, _ = pr.op.solve(e, solver, 1e-9)
+    assert rel(pol, opol) < 1e-4
+
+
+def test_cfg1_qmr_fp64_iterations():
+    # README workload 1: sphere r = 10 um, d = 0.5 um, m = 1.5+0.1i, 6 um, QMR, 1e-5
+    pr = Pair("sphere", ("10um", "0.5um"), [1.5 + 0.1j], "6um", "fp64")
+    pr.set_cc((0, 0, 1), 1, "ldr")
+    e = pr.p.einc((0, 0, 1), 1)
+    s = dda_b200.CudaSolver(pr.mv, "qmr")
+    pol = s.get_pol_vec(e, 1e-5)
+    rc, opol, ost, ohist = pr.op.solve(e, "qmr", 1e-5)
+    st = s.last_stats[0]
+    assert st.status == 0 and abs(st.iterations - ost.iterations) <= 2
+    assert np.allclose(s.last_history[0][:20], ohist[:20], rtol=1e-7)
+    assert rel(pol, opol) < 1e-5
+
+
+def test_batched_solve_equals_single(aniso64):
+    pr = Pair("arrays", aniso_arrays(), MATS, "0.9um", "fp64", max_rhs=2)
+    cases = [((0.3, 0.4, 0.866), 1), ((0, 1, 0), 2)]
+    es = []
+    for r, (prop, pol) in enumerate(cases):
+        pr.set_cc(prop, pol, "ldr", rhs=r)
+        es.append(pr.p.einc(prop, pol))
+    s = dda_b200.CudaSolver(pr.mv, "bicgstab")
+    both = s.get_pol_vec(np.concatenate(es), 1e-8).reshape(2, -1)
+    it_both = [st.iterations for st in s.last_stats]
+    # rhs 0 alone (same context, cc slot 0) reproduces the batched bits
+    one = s.get_pol_vec(es[0], 1e-8)
+    assert s.last_stats[0].iterations == it_both[0]
+    assert np.array_equal(one, both[0])
+
+
+def test_start_value(aniso64):
+    pr = aniso64
+    e = pr.p.einc((0.3, 0.4, 0.866), 1)
+    s = dda_b200.CudaSolver(pr.mv, "qmr")
+    pol = s.get_pol_vec(e, 1e-6)
+    s2 = dda_b200.CudaSolver(pr.mv, "qmr")
+    pol2 = s2.get_pol_vec(e, 1e-9, start=pol)
+    rc, opol, ost, _ = pr.op.solve(e, "qmr", 1e-9, start=pol)
+    assert rc == 0 and abs(s2.last_stats[0].iterations - ost.iterations) <= 1
+    assert rel(pol2, opol) < 1e-8
+
+
+def test_max_iter_reports_error(aniso64):
+    pr = aniso64
+    e = pr.p.einc((0.3, 0.4, 0.866), 1)
+    s = dda_b200.CudaSolver(pr.mv, "qmr", max_iter=3)
+    with pytest.raises(dda_b200.DDAError) as ei:
+        s.get_pol_vec(e, 1e-10)
+    assert ei.value.code == -6
+    assert s.last_stats[0].iterations == 3

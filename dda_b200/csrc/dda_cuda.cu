@@ -49,11 +49,7 @@ struct DdaError : std::runtime_error {
                      std::string(#call) + ": " + cudaGetErrorString(e_));                 \
   } while (0)
 
-// Kernel shapes.  Register arrays in the FFT stages hold about MAXE complex
-// values per thread.
-template <typename T> struct Shape;
-template <> struct Shape<float> { static constexpr int maxe = 8; };
-template <> struct Shape<double> { static constexpr int maxe = 4; };
+// Kernel shapes (threads per CTA).
 constexpr int kNtX = 256;   // k_xfwd / k_xinv
 constexpr int kNtYz = 512;  // k_yz / k_yrows
 constexpr int kNtC = 256;   // k_fft_cols / k_fft_rows
@@ -64,8 +60,11 @@ constexpr size_t kSmemMax = 227 * 1024;
 struct FftPlan {
   int n = 0;
   std::vector<int> radix;
+  std::vector<int> pos_h;  // frequency -> position after a forward transform
   float2* tw32 = nullptr;
   double2* tw64 = nullptr;
+  int* freq = nullptr;     // device: position -> frequency
+  int* pos = nullptr;      // device: frequency -> position
 
   void create(int n_) {
     n = n_;
@@ -77,7 +76,7 @@ struct FftPlan {
     while (m % 5 == 0) { radix.push_back(5); m /= 5; }
     while (m % 7 == 0) { radix.push_back(7); m /= 7; }
     if (m != 1) throw DdaError(DDA_ERR_UNSUPPORTED, "FFT length " + std::to_string(n) + " is not 2,3,5,7-smooth");
-    if ((int)radix.size() > kMaxStages) throw DdaError(DDA_ERR_UNSUPPORTED, "FFT length too large");
+    if ((int)radix.size() > 8) throw DdaError(DDA_ERR_UNSUPPORTED, "FFT length too large");
     std::vector<double2> h64(n);
     std::vector<float2> h32(n);
     const long double two_pi = 6.2831853071795864769252867665590056L;
@@ -91,21 +90,45 @@ struct FftPlan {
     CK(cudaMalloc(&tw32, n * sizeof(float2)));
     CK(cudaMemcpy(tw64, h64.data(), n * sizeof(double2), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(tw32, h32.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
+    // Mixed-radix digit reversal of the decimation-in-frequency transform:
+    // frequency k = d0 + R0 d1 + R0 R1 d2 + ... sits at position
+    // d0 n/R0 + d1 n/(R0 R1) + ...
+    pos_h.assign(n, 0);
+    std::vector<int> fr(n);
+    for (int k = 0; k < n; k++) {
+      int p = 0, rem = k, unit = n;
+      for (int R : radix) {
+        unit /= R;
+        p += (rem % R) * unit;
+        rem /= R;
+      }
+      pos_h[k] = p;
+      fr[p] = k;
+    }
+    CK(cudaMalloc(&freq, n * sizeof(int)));
+    CK(cudaMalloc(&pos, n * sizeof(int)));
+    CK(cudaMemcpy(freq, fr.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(pos, pos_h.data(), n * sizeof(int), cudaMemcpyHostToDevice));
   }
   template <typename T> FftPlanDev dev() const {
     FftPlanDev d;
     memset(&d, 0, sizeof(d));
     d.n = n;
     d.nst = (int)radix.size();
-    for (size_t i = 0; i < radix.size(); i++) d.radix[i] = radix[i];
+    d.packed = 0;
+    for (size_t i = 0; i < radix.size(); i++) d.packed |= (uint32_t)radix[i] << (4 * i);
     d.tw = std::is_same<T, float>::value ? (const void*)tw32 : (const void*)tw64;
+    d.freq = freq;
     return d;
   }
   void release() {
     if (tw32) cudaFree(tw32);
     if (tw64) cudaFree(tw64);
+    if (freq) cudaFree(freq);
+    if (pos) cudaFree(pos);
     tw32 = nullptr;
     tw64 = nullptr;
+    freq = pos = nullptr;
   }
 };
 
@@ -208,27 +231,28 @@ template <typename T> void setup_engine(dda_ctx* c) {
   const MvGeom& g = c->g;
   const size_t s = sizeof(T2);
   e.on = true;
-  // k_xfwd / k_xinv tiles: shared tile tl x (Gx+1) plus the material table
-  e.smem_x = (size_t)g.tl * g.pitchx * s + (size_t)g.nmat * s;
-  // fused plane kernel: slab Gz x q plus nr rows of 3 x (Gy+1)
+  constexpr int NW = kNtYz / 32;
+  // k_xfwd / k_xinv: twiddles, material table, tile of tl lines x (Gx+1)
+  e.smem_x = ((size_t)g.Gx + g.nmat + (size_t)g.tl * g.pitchx) * s;
+  // fused plane kernel: twiddles, slab Gz x q, row buffers 3 x (Gy+1)
   YzGeom y;
   y.q = 3 * g.by + ((3 * g.by) % 2 == 0 ? 1 : 0);
   y.py = g.Gy + 1;
-  size_t slab = (size_t)g.Gz * y.q * s;
-  int nr = std::max(1, std::min(g.Gz, (kNtYz * Shape<T>::maxe) / (3 * g.Gy)));
-  while (nr > 1 && slab + (size_t)nr * 3 * y.py * s > kSmemMax) nr--;
-  y.nr = nr;
+  const size_t fixed = ((size_t)g.Gz + g.Gy + (size_t)g.Gz * y.q) * s;
+  const size_t row = (size_t)3 * y.py * s;
+  int nrw = NW;
+  while (nrw > 1 && fixed + nrw * row > kSmemMax) nrw--;
+  y.nrw = nrw;
   e.yz = y;
-  e.smem_yz = slab + (size_t)nr * 3 * y.py * s;
-  e.fused = e.smem_yz <= kSmemMax && 3 * g.Gy <= kNtYz * Shape<T>::maxe && g.Gz <= kNtYz * Shape<T>::maxe &&
-            !(c->flags & DDA_FLAG_SPLIT_YZ);
+  e.smem_yz = fixed + nrw * row;
+  e.fused = e.smem_yz <= kSmemMax && !(c->flags & DDA_FLAG_SPLIT_YZ);
   if (!e.fused) {
-    // split path: zbuf, k_yrows with nr rows, column FFTs along z
-    e.yz.nr = std::max(1, std::min(g.Gz, (kNtYz * Shape<T>::maxe) / (3 * g.Gy)));
-    e.smem_rows = (size_t)e.yz.nr * 3 * y.py * s;
-    int ti = std::max(1, std::min(32, (kNtC * Shape<T>::maxe) / g.Gz));
-    ti = std::min(ti, g.by);
-    e.smem_cols = (size_t)g.Gz * (ti + 1) * s;
+    // split path: zbuf, k_yrows over NW rows per CTA, column FFTs along z
+    e.yz.nrw = NW;
+    e.smem_rows = ((size_t)g.Gy + (size_t)NW * 3 * y.py) * s;
+    int ti = std::min(32, g.by);
+    while (ti > 1 && ((size_t)g.Gz + (size_t)g.Gz * (ti + 1)) * s > kSmemMax) ti--;
+    e.smem_cols = ((size_t)g.Gz + (size_t)g.Gz * (ti + 1)) * s;
     ColGeom f;
     f.in_bs = g.nlines;            // xhat plane of one component
     f.in_as = g.by;
@@ -257,12 +281,12 @@ template <typename T> void setup_engine(dda_ctx* c) {
   auto attr = [](const void* f, size_t bytes) {
     CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(bytes, 1)));
   };
-  attr((const void*)k_xfwd<T, kNtX, Shape<T>::maxe>, e.smem_x);
-  attr((const void*)k_xinv<T, kNtX, Shape<T>::maxe>, e.smem_x);
-  if (e.fused) attr((const void*)k_yz<T, kNtYz, Shape<T>::maxe>, e.smem_yz);
+  attr((const void*)k_xfwd<T, kNtX>, e.smem_x);
+  attr((const void*)k_xinv<T, kNtX>, e.smem_x);
+  if (e.fused) attr((const void*)k_yz<T, kNtYz>, e.smem_yz);
   else {
-    attr((const void*)k_yrows<T, kNtYz, Shape<T>::maxe>, e.smem_rows);
-    attr((const void*)k_fft_cols<T, kNtC, Shape<T>::maxe>, e.smem_cols);
+    attr((const void*)k_yrows<T, kNtYz>, e.smem_rows);
+    attr((const void*)k_fft_cols<T, kNtC>, e.smem_cols);
   }
   const int hx = g.Gx / 2 + 1, hy = g.Gy / 2 + 1, hz = g.Gz / 2 + 1;
   e.dc = (T2*)dalloc<T>((size_t)hx * hy * hz * 6 * s);
@@ -308,20 +332,20 @@ void matvec(dda_ctx* c, const typename C2<T>::t* arg, typename C2<T>::t* res, in
   const MvGeom& g = c->g;
   const FftPlanDev px = c->px.dev<T>(), py = c->py.dev<T>(), pz = c->pz.dev<T>();
   dim3 gx(ntiles(c), 3, nrhs);
-  k_xfwd<T, kNtX, Shape<T>::maxe><<<gx, kNtX, e.smem_x, s>>>(arg, e.xhat, c->line_off, c->dip, c->perm,
+  k_xfwd<T, kNtX><<<gx, kNtX, e.smem_x, s>>>(arg, e.xhat, c->line_off, c->dip, c->perm,
                                                       e.ccs, conj, g, px, st, skipmv);
   if (e.fused) {
-    k_yz<T, kNtYz, Shape<T>::maxe><<<dim3(g.Gx, nrhs), kNtYz, e.smem_yz, s>>>(e.xhat, e.dc, g, e.yz, pz, py, st, skipmv);
+    k_yz<T, kNtYz><<<dim3(g.Gx, nrhs), kNtYz, e.smem_yz, s>>>(e.xhat, e.dc, g, e.yz, pz, py, st, skipmv);
   } else {
     const int nbatch = nrhs * g.Gx * 3;
     dim3 gc((g.by + e.cz_fwd.ti - 1) / e.cz_fwd.ti, nbatch);
-    k_fft_cols<T, kNtC, Shape<T>::maxe><<<gc, kNtC, e.smem_cols, s>>>(e.xhat, e.zbuf, e.cz_fwd, pz, 0, st, skipmv);
-    dim3 gr((g.Gz + e.yz.nr - 1) / e.yz.nr, g.Gx, nrhs);
-    k_yrows<T, kNtYz, Shape<T>::maxe><<<gr, kNtYz, e.smem_rows, s>>>(e.zbuf, e.dc, g, e.yz, py, st, skipmv);
-    k_fft_cols<T, kNtC, Shape<T>::maxe><<<gc, kNtC, e.smem_cols, s>>>(e.zbuf, e.xhat, e.cz_inv, pz, 1, st, skipmv);
+    k_fft_cols<T, kNtC><<<gc, kNtC, e.smem_cols, s>>>(e.xhat, e.zbuf, e.cz_fwd, pz, 0, st, skipmv);
+    dim3 gr((g.Gz + e.yz.nrw - 1) / e.yz.nrw, g.Gx, nrhs);
+    k_yrows<T, kNtYz><<<gr, kNtYz, e.smem_rows, s>>>(e.zbuf, e.dc, g, e.yz, py, st, skipmv);
+    k_fft_cols<T, kNtC><<<gc, kNtC, e.smem_cols, s>>>(e.zbuf, e.xhat, e.cz_inv, pz, 1, st, skipmv);
   }
   step.red = red_target(c, 3 * ntiles(c));
-  k_xinv<T, kNtX, Shape<T>::maxe><<<gx, kNtX, e.smem_x, s>>>(arg, res, e.xhat, c->line_off, c->dip, c->perm,
+  k_xinv<T, kNtX><<<gx, kNtX, e.smem_x, s>>>(arg, res, e.xhat, c->line_off, c->dip, c->perm,
                                                       e.ccs, conj, g, px, st, step, skipmv);
   CK(cudaGetLastError());
   c->launches += e.fused ? 3 : 5;
@@ -333,34 +357,37 @@ void build_dmatrix(dda_ctx* c) {
   const long long N = (long long)g.Gx * g.Gy * g.Gz;
   double2* full = (double2*)dalloc<double>(N * sizeof(double2));
   const FftPlanDev px = c->px.dev<double>(), py = c->py.dev<double>(), pz = c->pz.dev<double>();
-  CK(cudaFuncSetAttribute((const void*)k_fft_rows<double, kNtC, Shape<double>::maxe>,
+  CK(cudaFuncSetAttribute((const void*)k_fft_rows<double, kNtC>,
                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax));
-  CK(cudaFuncSetAttribute((const void*)k_fft_cols<double, kNtC, Shape<double>::maxe>,
+  CK(cudaFuncSetAttribute((const void*)k_fft_cols<double, kNtC>,
                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax));
   static const int MU[6] = {0, 0, 0, 1, 1, 2}, NU[6] = {0, 1, 2, 1, 2, 2};
-  const int tlr = std::max(1, std::min(32, (kNtC * Shape<double>::maxe) / g.Gx));
-  const size_t smr = (size_t)tlr * (g.Gx + 1) * sizeof(double2);
+  int tlr = 32;
+  while (tlr > 1 && ((size_t)g.Gx + (size_t)tlr * (g.Gx + 1)) * sizeof(double2) > kSmemMax) tlr--;
+  const size_t smr = ((size_t)g.Gx + (size_t)tlr * (g.Gx + 1)) * sizeof(double2);
   auto cols = [&](const FftPlanDev& pl, long long inner, long long batch, long long bs, long long as) {
     const int n = pl.n;
-    int ti = (int)std::max(1LL, std::min<long long>(std::min(32, (kNtC * Shape<double>::maxe) / n), inner));
+    int ti = (int)std::min<long long>(32, inner);
+    while (ti > 1 && ((size_t)n + (size_t)n * (ti + 1)) * sizeof(double2) > kSmemMax) ti--;
     ColGeom cg;
     cg.in_bs = bs; cg.in_as = as; cg.out_bs = bs; cg.out_as = as;
     cg.inner = (int)inner; cg.ti = ti; cg.pitch = ti + 1;
     cg.n_in = n; cg.n_out = n;
     cg.batches_per_rhs = 1;
-    const size_t sm = (size_t)n * (ti + 1) * sizeof(double2);
+    const size_t sm = ((size_t)n + (size_t)n * (ti + 1)) * sizeof(double2);
     if (sm > kSmemMax) throw DdaError(DDA_ERR_UNSUPPORTED, "grid too large for D-matrix FFT tiles");
-    k_fft_cols<double, kNtC, Shape<double>::maxe><<<dim3((unsigned)((inner + ti - 1) / ti), (unsigned)batch), kNtC, sm, c->stream>>>(
+    k_fft_cols<double, kNtC><<<dim3((unsigned)((inner + ti - 1) / ti), (unsigned)batch), kNtC, sm, c->stream>>>(
         full, full, cg, pl, 0, nullptr, 0);
   };
   for (int comp = 0; comp < 6; comp++) {
     k_dfill<<<1184, 256, 0, c->stream>>>(full, g.Gx, g.Gy, g.Gz, g.bx, g.by, g.bz, c->kd, MU[comp], NU[comp]);
-    k_fft_rows<double, kNtC, Shape<double>::maxe><<<(unsigned)(((long long)g.Gy * g.Gz + tlr - 1) / tlr), kNtC, smr, c->stream>>>(
+    k_fft_rows<double, kNtC><<<(unsigned)(((long long)g.Gy * g.Gz + tlr - 1) / tlr), kNtC, smr, c->stream>>>(
         full, (long long)g.Gy * g.Gz, g.Gx, tlr, g.Gx + 1, px, 0);
     cols(py, g.Gx, g.Gz, (long long)g.Gy * g.Gx, g.Gx);
     cols(pz, (long long)g.Gy * g.Gx, 1, N, (long long)g.Gy * g.Gx);
     k_dcompress<<<592, 256, 0, c->stream>>>(full, c->e64.on ? c->e64.dc : nullptr,
-                                            c->e32.on ? c->e32.dc : nullptr, g.Gx, g.Gy, g.Gz, comp);
+                                            c->e32.on ? c->e32.dc : nullptr, g.Gx, g.Gy, g.Gz, comp,
+                                            c->px.pos, c->py.pos, c->pz.pos);
     CK(cudaGetLastError());
   }
   CK(cudaStreamSynchronize(c->stream));
@@ -605,7 +632,7 @@ int dda_create(const dda_problem* p, int precision, dda_ctx** out) {
     }
     // one grid line must fit the register tiles of a CTA (FP64 limits apply
     // to the D-matrix setup in every precision)
-    const uint32_t lim = (uint32_t)(kNtC * Shape<double>::maxe);
+    const uint32_t lim = 4096;
     if (p->box[0] >= 65536 || p->grid[0] > lim || p->grid[1] > lim || p->grid[2] > lim)
       throw DdaError(DDA_ERR_UNSUPPORTED, "FFT grid edge above " + std::to_string(lim));
     CK(cudaSetDevice(p->device));
@@ -665,6 +692,9 @@ int dda_create(const dda_problem* p, int precision, dda_ctx** out) {
     c->px.create(g.Gx);
     c->py.create(g.Gy);
     c->pz.create(g.Gz);
+    g.fx = c->px.freq;
+    g.fy = c->py.freq;
+    g.fz = c->pz.freq;
     if (precision != DDA_PREC_FP32) setup_engine<double>(c.get());
     if (precision != DDA_PREC_FP64) setup_engine<float>(c.get());
     // reduction slots
@@ -762,20 +792,20 @@ template <typename T> void profile_t(dda_ctx* c, int nrhs, int reps, double* ms)
   for (int r = 0; r <= reps; r++) {
     dim3 gx(ntiles(c), 3, nrhs);
     CK(cudaEventRecord(ev[0], s));
-    k_xfwd<T, kNtX, Shape<T>::maxe><<<gx, kNtX, e.smem_x, s>>>(arg, e.xhat, c->line_off, c->dip, c->perm,
+    k_xfwd<T, kNtX><<<gx, kNtX, e.smem_x, s>>>(arg, e.xhat, c->line_off, c->dip, c->perm,
                                                               e.ccs, 0, g, px, nullptr, 0);
     CK(cudaEventRecord(ev[1], s));
     if (e.fused) {
-      k_yz<T, kNtYz, Shape<T>::maxe><<<dim3(g.Gx, nrhs), kNtYz, e.smem_yz, s>>>(e.xhat, e.dc, g, e.yz, pz, py, nullptr, 0);
+      k_yz<T, kNtYz><<<dim3(g.Gx, nrhs), kNtYz, e.smem_yz, s>>>(e.xhat, e.dc, g, e.yz, pz, py, nullptr, 0);
     } else {
       dim3 gc((g.by + e.cz_fwd.ti - 1) / e.cz_fwd.ti, nrhs * g.Gx * 3);
-      k_fft_cols<T, kNtC, Shape<T>::maxe><<<gc, kNtC, e.smem_cols, s>>>(e.xhat, e.zbuf, e.cz_fwd, pz, 0, nullptr, 0);
-      dim3 gr((g.Gz + e.yz.nr - 1) / e.yz.nr, g.Gx, nrhs);
-      k_yrows<T, kNtYz, Shape<T>::maxe><<<gr, kNtYz, e.smem_rows, s>>>(e.zbuf, e.dc, g, e.yz, py, nullptr, 0);
-      k_fft_cols<T, kNtC, Shape<T>::maxe><<<gc, kNtC, e.smem_cols, s>>>(e.zbuf, e.xhat, e.cz_inv, pz, 1, nullptr, 0);
+      k_fft_cols<T, kNtC><<<gc, kNtC, e.smem_cols, s>>>(e.xhat, e.zbuf, e.cz_fwd, pz, 0, nullptr, 0);
+      dim3 gr((g.Gz + e.yz.nrw - 1) / e.yz.nrw, g.Gx, nrhs);
+      k_yrows<T, kNtYz><<<gr, kNtYz, e.smem_rows, s>>>(e.zbuf, e.dc, g, e.yz, py, nullptr, 0);
+      k_fft_cols<T, kNtC><<<gc, kNtC, e.smem_cols, s>>>(e.zbuf, e.xhat, e.cz_inv, pz, 1, nullptr, 0);
     }
     CK(cudaEventRecord(ev[2], s));
-    k_xinv<T, kNtX, Shape<T>::maxe><<<gx, kNtX, e.smem_x, s>>>(arg, res, e.xhat, c->line_off, c->dip, c->perm,
+    k_xinv<T, kNtX><<<gx, kNtX, e.smem_x, s>>>(arg, res, e.xhat, c->line_off, c->dip, c->perm,
                                                               e.ccs, 0, g, px, nullptr, none, 0);
     CK(cudaEventRecord(ev[3], s));
     CK(cudaEventSynchronize(ev[3]));

@@ -51,9 +51,13 @@ __global__ void k_dfill(double2* __restrict__ full, int Gx, int Gy, int Gz, int 
   }
 }
 
-// full[z][y][x] (x fastest) -> octant [ax][az][ay][comp] scaled by -1/N.
+// full[z][y][x] (x fastest, each axis in the digit-reversed order the
+// forward transforms leave; px/py/pz map a frequency to its position) ->
+// octant [ax][az][ay][comp] scaled by -1/N.
 __global__ void k_dcompress(const double2* __restrict__ full, double2* __restrict__ d64,
-                            float2* __restrict__ d32, int Gx, int Gy, int Gz, int comp) {
+                            float2* __restrict__ d32, int Gx, int Gy, int Gz, int comp,
+                            const int* __restrict__ px, const int* __restrict__ py,
+                            const int* __restrict__ pz) {
   const int hx = Gx / 2 + 1, hy = Gy / 2 + 1, hz = Gz / 2 + 1;
   const long long M = (long long)hx * hy * hz;
   const double scale = -1.0 / ((double)Gx * Gy * Gz);
@@ -62,7 +66,7 @@ __global__ void k_dcompress(const double2* __restrict__ full, double2* __restric
     const int ay = (int)(o % hy);
     const int az = (int)((o / hy) % hz);
     const int ax = (int)(o / ((long long)hy * hz));
-    const double2 v = full[((long long)az * Gy + ay) * Gx + ax];
+    const double2 v = full[((long long)pz[az] * Gy + py[ay]) * Gx + px[ax]];
     const double2 d = make_double2(v.x * scale, v.y * scale);
     if (d64) d64[o * 6 + comp] = d;
     if (d32) d32[o * 6 + comp] = make_float2((float)d.x, (float)d.y);

@@ -1,12 +1,17 @@
 // fft_engine.cuh -- shared-memory mixed-radix FFT for sm_100a.
 //
 // Lines of a batched transform are staged in shared memory by the calling
-// kernel; fft_smem() then runs every radix stage of a Stockham autosort FFT
-// on them with all threads of the CTA.  Each stage reads its butterfly inputs
-// into registers, synchronises, and writes the outputs back in place, so a
-// transform needs no second shared-memory buffer.  Lengths are products of
-// 2, 3, 4, 5, 7 and 8 (every even 2,3,5,7-smooth FFT grid the DDA grid rule
-// produces, DDA/DDAParams.cpp:45-90).
+// kernel; fft_lines() then runs every radix stage on them in place.  Forward
+// transforms are decimation in frequency: natural-order input, output in
+// mixed-radix digit-reversed order.  Inverse transforms are decimation in
+// time: digit-reversed input, natural-order output.  A forward transform, a
+// pointwise product in the permuted order and an inverse transform thus form
+// a convolution with no reordering pass; wherever the actual frequency index
+// is needed (the D-matrix lookup) it comes from the plan's position table.
+// Each butterfly reads and writes the same R shared-memory slots, so threads
+// need only R complex registers and one barrier per stage.  Lengths are
+// products of 2, 3, 4, 5, 7 and 8 (every even 2,3,5,7-smooth FFT grid the
+// DDA grid rule produces, DDA/DDAParams.cpp:45-90).
 //
 // Sign convention: forward = exp(-2 pi i jk/n), inverse = exp(+2 pi i jk/n),
 // both unnormalised (the convention of the FFT plans the reference drives,
@@ -53,8 +58,9 @@ constexpr int kMaxStages = 16;
 struct FftPlanDev {
   int n;
   int nst;
-  int radix[kMaxStages];
-  const void* tw;  // exp(-2 pi i k / n), k = 0..n-1, as float2 or double2
+  const void* tw;    // exp(-2 pi i k / n), k = 0..n-1, as float2 or double2
+  const int* freq;  // frequency index held at each position after a forward transform
+  uint32_t packed;  // radices 4 bits each, stage 0 in the low bits (nst <= 8)
 };
 
 // ------------------------------------------------------------ DFT cores ----
@@ -175,98 +181,150 @@ template <bool INV, typename T2> struct Dft<5, INV, T2> : DftOdd<5, INV, T2> {};
 template <bool INV, typename T2> struct Dft<7, INV, T2> : DftOdd<7, INV, T2> {};
 
 // ------------------------------------------------------------- stages ----
-// One Stockham stage on lines [l0, l0+nl) of the shared-memory tile.  Element
-// e of line l lives at s[l*ls + e*es].  Butterfly b maps to (line, j) with the
-// line index fastest when `line_fast` (column tiles: neighbouring threads touch
-// neighbouring addresses) and j fastest otherwise (row tiles).
-template <typename T, int NT, int MAXE, bool INV, int R>
-__device__ __forceinline__ void fft_stage(typename C2<T>::t* s, int l0, int nl, int ls, int es,
-                                          bool line_fast, int n, int Ns,
-                                          const typename C2<T>::t* __restrict__ tw) {
+// All kernels of the library share one dynamic shared-memory window; the FFT
+// engine addresses it by element offset so every access is a 32-bit shared
+// load/store even though the engine functions are not inlined.
+extern __shared__ __align__(16) unsigned char dda_smem[];
+
+template <typename T>
+__device__ __forceinline__ typename C2<T>::t* smem_at(int off) {
+  return reinterpret_cast<typename C2<T>::t*>(dda_smem) + off;
+}
+
+// floor(a / d) for 0 <= a < 2^20 from an FP32 reciprocal: the fraction of
+// (a + 0.5)/d stays 0.5/d away from an integer, above the rounding error.
+__device__ __forceinline__ int fdiv_i(int a, float rcp) { return (int)(((float)a + 0.5f) * rcp); }
+
+template <int G> __device__ __forceinline__ void group_sync() {
+  if (G == 32) __syncwarp(); else __syncthreads();
+}
+
+// One radix-R stage over nl lines by a group of G threads (one warp, or the
+// whole CTA when G == blockDim.x).  Element e of line l is at shared offset
+// soff + l*ls + e*es; the length-n table exp(-2 pi i k/n) is at shared
+// offset twoff.  L is the stage's block length: butterfly (block, j) works
+// on elements block*L + j + m*L/R, m < R.  Forward (DIF): DFT, then twiddle
+// w_L^(j m).  Inverse (DIT): conjugate twiddle, then inverse DFT.  With `lf`
+// neighbouring threads take neighbouring lines (column tiles), otherwise
+// neighbouring butterflies of one line (row tiles).
+template <typename T, int G, bool INV, int R>
+__device__ __forceinline__ void stage(int soff, int nl, int ls, int es, bool lf, int n, int L,
+                                      int twoff, int tid) {
   typedef typename C2<T>::t T2;
-  constexpr int MB = (MAXE + R - 1) / R;
+  T2* s = smem_at<T>(0);
+  const int S = L / R;
   const int nb = n / R;
   const int total = nl * nb;
-  const int tstride = n / (Ns * R);
-  T2 v[MB][R];
+  const int tstride = n / L;
+  const float rd = 1.0f / (float)(lf ? nl : nb);
+  const float rs = 1.0f / (float)S;
+  const int mstep = S * es;
+#pragma unroll 2
+  for (int b = tid; b < total; b += G) {
+    const int qq = fdiv_i(b, rd);
+    int l, t;
+    if (lf) { t = qq; l = b - qq * nl; } else { l = qq; t = b - qq * nb; }
+    const int blk = fdiv_i(t, rs);
+    const int j = t - blk * S;
+    const int base = soff + l * ls + (blk * L + j) * es;
+    T2 v[R];
 #pragma unroll
-  for (int q = 0; q < MB; q++) {
-    const int b = threadIdx.x + q * NT;
-    if (b < total) {
-      int l, j;
-      if (line_fast) { l = b % nl; j = b / nl; } else { j = b % nb; l = b / nb; }
-      const T2* line = s + (size_t)(l0 + l) * ls;
+    for (int m = 0; m < R; m++) v[m] = s[base + m * mstep];
+    if (INV) {
+      if (j) {
 #pragma unroll
-      for (int r = 0; r < R; r++) v[q][r] = line[(j + r * nb) * es];
-      if (Ns > 1) {
-        const int k = j % Ns;
-#pragma unroll
-        for (int r = 1; r < R; r++) {
-          T2 w = tw[k * r * tstride];
-          if (INV) w.y = -w.y;
-          v[q][r] = cmul(v[q][r], w);
+        for (int m = 1; m < R; m++) {
+          T2 w = s[twoff + j * m * tstride];
+          w.y = -w.y;
+          v[m] = cmul(v[m], w);
         }
       }
-      Dft<R, INV, T2>::run(v[q]);
-    }
-  }
-  __syncthreads();
+      Dft<R, true, T2>::run(v);
+    } else {
+      Dft<R, false, T2>::run(v);
+      if (j) {
 #pragma unroll
-  for (int q = 0; q < MB; q++) {
-    const int b = threadIdx.x + q * NT;
-    if (b < total) {
-      int l, j;
-      if (line_fast) { l = b % nl; j = b / nl; } else { j = b % nb; l = b / nb; }
-      T2* line = s + (size_t)(l0 + l) * ls;
-      const int k = j % Ns;
-      const int base = (j / Ns) * Ns * R + k;
-#pragma unroll
-      for (int r = 0; r < R; r++) line[(base + r * Ns) * es] = v[q][r];
-    }
-  }
-  __syncthreads();
-}
-
-// Transforms `nlines` lines of length pl.n held in shared memory (layout as
-// for fft_stage).  Lines are processed in chunks of at most NT*MAXE elements
-// so every thread holds at most about MAXE elements per stage.  Must be called
-// by all NT threads of the CTA after the tile is complete in shared memory
-// (the caller's __syncthreads); returns after a final __syncthreads.
-template <typename T, int NT, int MAXE, bool INV>
-__device__ __noinline__ void fft_smem(typename C2<T>::t* s, int nlines, int ls, int es,
-                                      bool line_fast, const FftPlanDev& pl) {
-  typedef typename C2<T>::t T2;
-  const T2* tw = reinterpret_cast<const T2*>(pl.tw);
-  const int n = pl.n;
-  int chunk = (NT * MAXE) / n;
-  if (chunk < 1) chunk = 1;
-#pragma unroll 1
-  for (int l0 = 0; l0 < nlines; l0 += chunk) {
-    const int nl = min(chunk, nlines - l0);
-    int Ns = 1;
-#pragma unroll 1
-    for (int st = 0; st < pl.nst; st++) {
-      const int R = pl.radix[st];
-      switch (R) {
-        case 2: fft_stage<T, NT, MAXE, INV, 2>(s, l0, nl, ls, es, line_fast, n, Ns, tw); break;
-        case 3: fft_stage<T, NT, MAXE, INV, 3>(s, l0, nl, ls, es, line_fast, n, Ns, tw); break;
-        case 4: fft_stage<T, NT, MAXE, INV, 4>(s, l0, nl, ls, es, line_fast, n, Ns, tw); break;
-        case 5: fft_stage<T, NT, MAXE, INV, 5>(s, l0, nl, ls, es, line_fast, n, Ns, tw); break;
-        case 7: fft_stage<T, NT, MAXE, INV, 7>(s, l0, nl, ls, es, line_fast, n, Ns, tw); break;
-        default: fft_stage<T, NT, MAXE, INV, 8>(s, l0, nl, ls, es, line_fast, n, Ns, tw); break;
+        for (int m = 1; m < R; m++) v[m] = cmul(v[m], s[twoff + j * m * tstride]);
       }
-      Ns *= R;
+    }
+#pragma unroll
+    for (int m = 0; m < R; m++) s[base + m * mstep] = v[m];
+  }
+  group_sync<G>();
+}
+
+template <typename T, int G, bool INV>
+__device__ __forceinline__ void stage_r(int R, int soff, int nl, int ls, int es, bool lf, int n, int L,
+                                        int twoff, int tid) {
+  switch (R) {
+    case 2: stage<T, G, INV, 2>(soff, nl, ls, es, lf, n, L, twoff, tid); break;
+    case 3: stage<T, G, INV, 3>(soff, nl, ls, es, lf, n, L, twoff, tid); break;
+    case 4: stage<T, G, INV, 4>(soff, nl, ls, es, lf, n, L, twoff, tid); break;
+    case 5: stage<T, G, INV, 5>(soff, nl, ls, es, lf, n, L, twoff, tid); break;
+    case 7: stage<T, G, INV, 7>(soff, nl, ls, es, lf, n, L, twoff, tid); break;
+    default: stage<T, G, INV, 8>(soff, nl, ls, es, lf, n, L, twoff, tid); break;
+  }
+}
+
+// All stages of one transform of lines [0, nlines) by a group of G threads,
+// entered converged; forward stages run first to last, inverse stages last
+// to first.
+template <typename T, int G, bool INV>
+__device__ __noinline__ void fft_group(int soff, int nlines, int ls, int es, bool lf, int n,
+                                       uint32_t packed, int nst, int twoff) {
+  const int tid = G == 32 ? (threadIdx.x & 31) : threadIdx.x;
+  if (!INV) {
+    int L = n;
+#pragma unroll 1
+    for (int st = 0; st < nst; st++) {
+      const int R = (packed >> (4 * st)) & 15;
+      stage_r<T, G, false>(R, soff, nlines, ls, es, lf, n, L, twoff, tid);
+      L /= R;
+    }
+  } else {
+    int L = 1;
+#pragma unroll 1
+    for (int st = nst - 1; st >= 0; st--) {
+      const int R = (packed >> (4 * st)) & 15;
+      L *= R;
+      stage_r<T, G, true>(R, soff, nlines, ls, es, lf, n, L, twoff, tid);
     }
   }
 }
 
-template <typename T, int NT, int MAXE>
-__device__ __forceinline__ void fft_smem_dir(typename C2<T>::t* s, int nlines, int ls, int es,
-                                             bool line_fast, const FftPlanDev& pl, bool inverse) {
-  if (inverse)
-    fft_smem<T, NT, MAXE, true>(s, nlines, ls, es, line_fast, pl);
-  else
-    fft_smem<T, NT, MAXE, false>(s, nlines, ls, es, line_fast, pl);
+// Transforms `nlines` lines (layout as for stage()) with the whole CTA and
+// returns after a CTA barrier.  With at least one line per warp the lines
+// are shared out to warps in contiguous runs and transformed without CTA
+// barriers; otherwise all NT threads work through each stage together.
+template <typename T, int NT, bool INV>
+__device__ __forceinline__ void fft_lines(int soff, int nlines, int ls, int es, bool lf,
+                                          const FftPlanDev& pl, int twoff) {
+  constexpr int NW = NT / 32;
+  if (nlines >= NW) {
+    const int w = threadIdx.x >> 5;
+    const int per = (nlines + NW - 1) / NW;
+    const int l0 = min(nlines, w * per), l1 = min(nlines, l0 + per);
+    if (l1 > l0)
+      fft_group<T, 32, INV>(soff + l0 * ls, l1 - l0, ls, es, lf, pl.n, pl.packed, pl.nst, twoff);
+  } else {
+    fft_group<T, NT, INV>(soff, nlines, ls, es, lf, pl.n, pl.packed, pl.nst, twoff);
+  }
+  __syncthreads();
+}
+
+template <typename T, int NT>
+__device__ __forceinline__ void fft_lines_dir(int soff, int nlines, int ls, int es, bool lf,
+                                              const FftPlanDev& pl, int twoff, bool inverse) {
+  if (inverse) fft_lines<T, NT, true>(soff, nlines, ls, es, lf, pl, twoff);
+  else fft_lines<T, NT, false>(soff, nlines, ls, es, lf, pl, twoff);
+}
+
+// Copies the twiddle table of a plan to shared offset `off` (caller syncs).
+template <typename T, int NT>
+__device__ __forceinline__ void stage_twiddles(int off, const FftPlanDev& pl) {
+  const typename C2<T>::t* src = reinterpret_cast<const typename C2<T>::t*>(pl.tw);
+  typename C2<T>::t* dst = smem_at<T>(off);
+  for (int i = threadIdx.x; i < pl.n; i += NT) dst[i] = src[i];
 }
 
 }  // namespace dda

@@ -58,7 +58,7 @@ __global__ void __launch_bounds__(NT) k_vec(VecArgs va, KrylovState* st) {
   typedef typename C2<T>::t T2;
   const int b = blockIdx.y;
   KrylovState& s = st[b];
-  if (s.done) return;
+  if (s.done && va.op != V_RESULT) return;  // the result copy runs after convergence
   const long long len = 3LL * va.nvs;
   const long long chunk = ((len + va.nparts - 1) / va.nparts + 31) / 32 * 32;
   const long long i0 = chunk * blockIdx.x;

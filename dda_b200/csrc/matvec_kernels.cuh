@@ -39,6 +39,11 @@ struct MvGeom {
   int nmat;
   int tl;      // grid lines per k_xfwd / k_xinv tile
   int pitchx;  // shared row pitch of those tiles (Gx + 1)
+  // frequency held at each position after a forward FFT along x, y, z
+  // (the transforms leave their output in digit-reversed order)
+  const int* fx;
+  const int* fy;
+  const int* fz;
 };
 
 // D-hat at (kx, ky, kz) from the octant store.
@@ -75,9 +80,15 @@ __device__ __forceinline__ bool rhs_idle(const KrylovState* st, int b, int mvski
   return st && (st[b].done || (mvskip && st[b].skipmv));
 }
 
+// Shared-memory layout of k_xfwd / k_xinv (offsets in complex elements):
+//   [0, Gx)            twiddles of the x transform
+//   [Gx, Gx + nmat)    sqrt(cc) of component c per material
+//   [xtile, ...)       tile of tl grid lines, pitch pitchx = Gx + 1
+__host__ __device__ inline int x_tile_off(const MvGeom& g) { return g.Gx + g.nmat; }
+
 // ------------------------------------------------------------ k_xfwd ----
-// grid (ceil(nlines/tl), 3, nrhs); dynamic smem tl*pitchx*sizeof(T2) + ccs.
-template <typename T, int NT, int MAXE>
+// grid (ceil(nlines/tl), 3, nrhs).
+template <typename T, int NT>
 __global__ void __launch_bounds__(NT, 2) k_xfwd(const typename C2<T>::t* __restrict__ arg,
                                              typename C2<T>::t* __restrict__ xhat,
                                              const uint32_t* __restrict__ line_off,
@@ -87,13 +98,14 @@ __global__ void __launch_bounds__(NT, 2) k_xfwd(const typename C2<T>::t* __restr
                                              MvGeom g, FftPlanDev px,
                                              const KrylovState* __restrict__ st, int mvskip) {
   typedef typename C2<T>::t T2;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  T2* sm = reinterpret_cast<T2*>(smraw);
-  T2* scc = sm + (size_t)g.tl * g.pitchx;
   const int b = blockIdx.z, c = blockIdx.y;
   if (rhs_idle(st, b, mvskip)) return;
+  const int toff = x_tile_off(g);
+  T2* scc = smem_at<T>(g.Gx);
+  T2* sm = smem_at<T>(toff);
   const int L0 = blockIdx.x * g.tl;
   const int nl = min(g.tl, g.nlines - L0);
+  stage_twiddles<T, NT>(0, px);
   for (int i = threadIdx.x; i < g.nmat; i += NT) scc[i] = ccs[((size_t)b * g.nmat + i) * 3 + c];
   for (int i = threadIdx.x; i < nl * g.pitchx; i += NT) sm[i] = czero<T2>();
   __syncthreads();
@@ -110,11 +122,11 @@ __global__ void __launch_bounds__(NT, 2) k_xfwd(const typename C2<T>::t* __restr
     }
   }
   __syncthreads();
-  fft_smem<T, NT, MAXE, false>(sm, nl, g.pitchx, 1, false, px);
+  fft_lines<T, NT, false>(toff, nl, g.pitchx, 1, false, px, 0);
   T2* out = xhat + ((size_t)b * g.Gx * 3 + c) * g.nlines + L0;
   const size_t kstride = (size_t)3 * g.nlines;
   for (int i = threadIdx.x; i < nl * g.Gx; i += NT) {
-    const int l = i % nl, kx = i / nl;
+    const int kx = i / nl, l = i - kx * nl;
     out[kx * kstride + l] = sm[l * g.pitchx + kx];
   }
 }
@@ -123,7 +135,7 @@ __global__ void __launch_bounds__(NT, 2) k_xfwd(const typename C2<T>::t* __restr
 // grid (ceil(nlines/tl), 3, nrhs).  Epilogue: res = conj?(sqrt(cc).X +
 // conj?(arg)), padding nv..nvs zeroed, and optional sums over the result for
 // the solver step `op` (finalised by the last CTA of each right-hand side).
-template <typename T, int NT, int MAXE>
+template <typename T, int NT>
 __global__ void __launch_bounds__(NT, 2) k_xinv(const typename C2<T>::t* __restrict__ arg,
                                              typename C2<T>::t* __restrict__ res,
                                              const typename C2<T>::t* __restrict__ xhat,
@@ -134,22 +146,23 @@ __global__ void __launch_bounds__(NT, 2) k_xinv(const typename C2<T>::t* __restr
                                              MvGeom g, FftPlanDev px, KrylovState* st,
                                              KrylovStep step, int mvskip) {
   typedef typename C2<T>::t T2;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  T2* sm = reinterpret_cast<T2*>(smraw);
-  T2* scc = sm + (size_t)g.tl * g.pitchx;
   const int b = blockIdx.z, c = blockIdx.y;
   if (rhs_idle(st, b, mvskip)) return;
+  const int toff = x_tile_off(g);
+  T2* scc = smem_at<T>(g.Gx);
+  T2* sm = smem_at<T>(toff);
   const int L0 = blockIdx.x * g.tl;
   const int nl = min(g.tl, g.nlines - L0);
+  stage_twiddles<T, NT>(0, px);
   for (int i = threadIdx.x; i < g.nmat; i += NT) scc[i] = ccs[((size_t)b * g.nmat + i) * 3 + c];
   const T2* in = xhat + ((size_t)b * g.Gx * 3 + c) * g.nlines + L0;
   const size_t kstride = (size_t)3 * g.nlines;
   for (int i = threadIdx.x; i < nl * g.Gx; i += NT) {
-    const int l = i % nl, kx = i / nl;
+    const int kx = i / nl, l = i - kx * nl;
     sm[l * g.pitchx + kx] = in[kx * kstride + l];
   }
   __syncthreads();
-  fft_smem<T, NT, MAXE, true>(sm, nl, g.pitchx, 1, false, px);
+  fft_lines<T, NT, true>(toff, nl, g.pitchx, 1, false, px, 0);
   const size_t voff = ((size_t)b * 3 + c) * g.nvs;
   const T2* a = arg + voff;
   T2* r = res + voff;
@@ -182,126 +195,138 @@ __global__ void __launch_bounds__(NT, 2) k_xinv(const typename C2<T>::t* __restr
 }
 
 // -------------------------------------------------------------- k_yz ----
-// One (rhs, kx) plane per CTA.  Shared memory: slab S[Gz][q] (q >= 3*by;
-// row kz holds the three components' y values), row scratch R[nr][3][py].
+// One (rhs, kx) plane per CTA.  Shared memory (complex offsets):
+//   [0, Gz) z twiddles, [Gz, Gz+Gy) y twiddles,
+//   slab S[Gz][q] at Gz+Gy (row kz holds the three components' y < by),
+//   row buffers R[nrw][3][py] after the slab.
 struct YzGeom {
-  int q;   // slab row pitch
-  int nr;  // kz rows per y pass
-  int py;  // row scratch pitch (Gy + 1)
+  int q;    // slab row pitch (>= 3 by, odd)
+  int nrw;  // row buffers: warps that run rows (or rows per CTA pass)
+  int py;   // row buffer pitch (Gy + 1)
 };
 
-template <typename T, int NT, int MAXE>
-__device__ __forceinline__ void yz_rows(typename C2<T>::t* S, typename C2<T>::t* R,
-                                        const typename C2<T>::t* __restrict__ dc, const MvGeom& g,
-                                        const YzGeom& y, const FftPlanDev& pyp, int kx,
-                                        int kz0, int nr) {
-  typedef typename C2<T>::t T2;
-  // load rows, zero padding y >= by
-  for (int i = threadIdx.x; i < nr * 3 * g.Gy; i += NT) {
-    const int yy = i % g.Gy, rc = i / g.Gy;  // rc = row*3 + c
-    const int row = rc / 3, c = rc % 3;
-    R[rc * y.py + yy] = yy < g.by ? S[(size_t)(kz0 + row) * y.q + c * g.by + yy] : czero<T2>();
-  }
-  __syncthreads();
-  fft_smem<T, NT, MAXE, false>(R, nr * 3, y.py, 1, false, pyp);
-  for (int i = threadIdx.x; i < nr * g.Gy; i += NT) {
-    const int ky = i % g.Gy, row = i / g.Gy;
-    T2 d[6];
-    load_dhat<T>(dc, g.Gx, g.Gy, g.Gz, kx, ky, kz0 + row, d);
-    T2* p = R + (size_t)row * 3 * y.py + ky;
-    T2 a = p[0], b = p[y.py], c = p[2 * y.py];
-    dmul(d, a, b, c);
-    p[0] = a; p[y.py] = b; p[2 * y.py] = c;
-  }
-  __syncthreads();
-  fft_smem<T, NT, MAXE, true>(R, nr * 3, y.py, 1, false, pyp);
-  for (int i = threadIdx.x; i < nr * 3 * g.by; i += NT) {
-    const int yy = i % g.by, rc = i / g.by;
-    const int row = rc / 3, c = rc % 3;
-    S[(size_t)(kz0 + row) * y.q + c * g.by + yy] = R[rc * y.py + yy];
-  }
-  __syncthreads();
+__host__ __device__ inline int yz_slab_off(const MvGeom& g) { return g.Gz + g.Gy; }
+__host__ __device__ inline int yz_rows_off(const MvGeom& g, const YzGeom& y) {
+  return g.Gz + g.Gy + g.Gz * y.q;
 }
 
-template <typename T, int NT, int MAXE>
+// y forward FFT of the three components of one row (held at shared offset
+// roff, pitch py, zero padded by -> Gy), D-hat multiply and y inverse FFT, by
+// one warp.  kx and kz are frequencies; the y positions are mapped to
+// frequencies through g.fy.
+template <typename T>
+__device__ __forceinline__ void warp_row(int roff, const typename C2<T>::t* __restrict__ dc,
+                                         const MvGeom& g, int py, const FftPlanDev& pyp, int twy,
+                                         int kx, int kz, int lane) {
+  typedef typename C2<T>::t T2;
+  fft_group<T, 32, false>(roff, 3, py, 1, false, g.Gy, pyp.packed, pyp.nst, twy);
+  T2* R = smem_at<T>(roff);
+  for (int p = lane; p < g.Gy; p += 32) {
+    T2 d[6];
+    load_dhat<T>(dc, g.Gx, g.Gy, g.Gz, kx, g.fy[p], kz, d);
+    T2 a = R[p], b = R[py + p], c = R[2 * py + p];
+    dmul(d, a, b, c);
+    R[p] = a; R[py + p] = b; R[2 * py + p] = c;
+  }
+  __syncwarp();
+  fft_group<T, 32, true>(roff, 3, py, 1, false, g.Gy, pyp.packed, pyp.nst, twy);
+}
+
+template <typename T, int NT>
 __global__ void __launch_bounds__(NT, 1) k_yz(typename C2<T>::t* __restrict__ xhat,
                                            const typename C2<T>::t* __restrict__ dc, MvGeom g,
                                            YzGeom y, FftPlanDev pz, FftPlanDev pyp,
                                            const KrylovState* __restrict__ st, int mvskip) {
   typedef typename C2<T>::t T2;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  T2* S = reinterpret_cast<T2*>(smraw);
-  T2* R = S + (size_t)g.Gz * y.q;
-  const int kx = blockIdx.x, b = blockIdx.y;
+  const int kx = blockIdx.x, b = blockIdx.y;  // kx: position after the x transform
   if (rhs_idle(st, b, mvskip)) return;
+  const int soff = yz_slab_off(g), roff = yz_rows_off(g, y);
+  T2* S = smem_at<T>(soff);
   T2* plane = xhat + ((size_t)b * g.Gx + kx) * 3 * g.nlines;
   const int nb = g.by * g.bz;
+  stage_twiddles<T, NT>(0, pz);
+  stage_twiddles<T, NT>(g.Gz, pyp);
   for (int i = threadIdx.x; i < 3 * nb; i += NT) {
-    const int c = i / nb, rem = i % nb;
-    const int z = rem / g.by, yy = rem % g.by;
-    S[(size_t)z * y.q + c * g.by + yy] = plane[i];
+    const int c = i / nb, rem = i - c * nb;
+    const int z = rem / g.by, yy = rem - z * g.by;
+    S[z * y.q + c * g.by + yy] = plane[i];
   }
-  for (int i = threadIdx.x; i < (g.Gz - g.bz) * 3 * g.by; i += NT) {
-    const int z = g.bz + i / (3 * g.by), col = i % (3 * g.by);
-    S[(size_t)z * y.q + col] = czero<T2>();
+  const int w3 = 3 * g.by;
+  for (int i = threadIdx.x; i < (g.Gz - g.bz) * w3; i += NT) {
+    const int zz = i / w3;
+    S[(g.bz + zz) * y.q + (i - zz * w3)] = czero<T2>();
   }
   __syncthreads();
-  fft_smem<T, NT, MAXE, false>(S, 3 * g.by, 1, y.q, true, pz);
-  for (int kz0 = 0; kz0 < g.Gz; kz0 += y.nr)
-    yz_rows<T, NT, MAXE>(S, R, dc, g, y, pyp, kx, kz0, min(y.nr, g.Gz - kz0));
-  fft_smem<T, NT, MAXE, true>(S, 3 * g.by, 1, y.q, true, pz);
+  fft_lines<T, NT, false>(soff, w3, 1, y.q, true, pz, 0);
+  {
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int kxf = g.fx[kx];
+    if (w < y.nrw) {
+      const int ro = roff + w * 3 * y.py;
+      T2* R = smem_at<T>(ro);
+      for (int kz = w; kz < g.Gz; kz += y.nrw) {  // kz: position after the z transform
+        for (int c = 0; c < 3; c++)
+          for (int yy = lane; yy < g.Gy; yy += 32)
+            R[c * y.py + yy] = yy < g.by ? S[kz * y.q + c * g.by + yy] : czero<T2>();
+        __syncwarp();
+        warp_row<T>(ro, dc, g, y.py, pyp, g.Gz, kxf, g.fz[kz], lane);
+        for (int c = 0; c < 3; c++)
+          for (int yy = lane; yy < g.by; yy += 32) S[kz * y.q + c * g.by + yy] = R[c * y.py + yy];
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+  }
+  fft_lines<T, NT, true>(soff, w3, 1, y.q, true, pz, 0);
   for (int i = threadIdx.x; i < 3 * nb; i += NT) {
-    const int c = i / nb, rem = i % nb;
-    const int z = rem / g.by, yy = rem % g.by;
-    plane[i] = S[(size_t)z * y.q + c * g.by + yy];
+    const int c = i / nb, rem = i - c * nb;
+    const int z = rem / g.by, yy = rem - z * g.by;
+    plane[i] = S[z * y.q + c * g.by + yy];
   }
 }
 
 // ----------------------------------------------- split path: k_yrows ----
-// grid (ceil(Gz/nr), Gx, nrhs) over zbuf[b][kx][c][kz][y] (y < by).
-template <typename T, int NT, int MAXE>
+// grid (ceil(Gz/nrw), Gx, nrhs) over zbuf[b][kx][c][kz][y] (y < by), kx and
+// kz positions after the forward x and z transforms; each CTA runs nrw rows,
+// one per warp.  Shared memory: y twiddles at 0, rows R[nrw][3][py] at Gy.
+template <typename T, int NT>
 __global__ void __launch_bounds__(NT, 1) k_yrows(typename C2<T>::t* __restrict__ zbuf,
                                               const typename C2<T>::t* __restrict__ dc,
                                               MvGeom g, YzGeom y, FftPlanDev pyp,
                                               const KrylovState* __restrict__ st, int mvskip) {
   typedef typename C2<T>::t T2;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  T2* R = reinterpret_cast<T2*>(smraw);
   const int kx = blockIdx.y, b = blockIdx.z;
   if (rhs_idle(st, b, mvskip)) return;
-  const int kz0 = blockIdx.x * y.nr;
-  const int nr = min(y.nr, g.Gz - kz0);
+  const int kz0 = blockIdx.x * y.nrw;
+  const int nr = min(y.nrw, g.Gz - kz0);
   T2* base = zbuf + ((size_t)b * g.Gx + kx) * 3 * (size_t)g.Gz * g.by;
-  const size_t cstride = (size_t)g.Gz * g.by;
+  const size_t cs = (size_t)g.Gz * g.by;
+  const int roff = g.Gy;
+  T2* R = smem_at<T>(roff);
+  stage_twiddles<T, NT>(0, pyp);
   for (int i = threadIdx.x; i < nr * 3 * g.Gy; i += NT) {
-    const int yy = i % g.Gy, rc = i / g.Gy;
-    const int row = rc / 3, c = rc % 3;
-    R[rc * y.py + yy] = yy < g.by ? base[c * cstride + (size_t)(kz0 + row) * g.by + yy] : czero<T2>();
+    const int rc = i / g.Gy, yy = i - rc * g.Gy;
+    const int row = rc / 3, c = rc - 3 * row;
+    R[rc * y.py + yy] = yy < g.by ? base[c * cs + (size_t)(kz0 + row) * g.by + yy] : czero<T2>();
   }
   __syncthreads();
-  fft_smem<T, NT, MAXE, false>(R, nr * 3, y.py, 1, false, pyp);
-  for (int i = threadIdx.x; i < nr * g.Gy; i += NT) {
-    const int ky = i % g.Gy, row = i / g.Gy;
-    T2 d[6];
-    load_dhat<T>(dc, g.Gx, g.Gy, g.Gz, kx, ky, kz0 + row, d);
-    T2* p = R + (size_t)row * 3 * y.py + ky;
-    T2 a = p[0], bb = p[y.py], c = p[2 * y.py];
-    dmul(d, a, bb, c);
-    p[0] = a; p[y.py] = bb; p[2 * y.py] = c;
+  {
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (w < nr) warp_row<T>(roff + w * 3 * y.py, dc, g, y.py, pyp, 0, g.fx[kx], g.fz[kz0 + w], lane);
+    __syncthreads();
   }
-  __syncthreads();
-  fft_smem<T, NT, MAXE, true>(R, nr * 3, y.py, 1, false, pyp);
   for (int i = threadIdx.x; i < nr * 3 * g.by; i += NT) {
-    const int yy = i % g.by, rc = i / g.by;
-    const int row = rc / 3, c = rc % 3;
-    base[c * cstride + (size_t)(kz0 + row) * g.by + yy] = R[rc * y.py + yy];
+    const int rc = i / g.by, yy = i - rc * g.by;
+    const int row = rc / 3, c = rc - 3 * row;
+    base[c * cs + (size_t)(kz0 + row) * g.by + yy] = R[rc * y.py + yy];
   }
 }
 
 // ------------------------------------------- generic strided column FFT ----
 // Transforms along the middle axis of arrays [batch][axis][inner] (inner
 // contiguous).  Input axis length n_in <= n is zero padded, output keeps the
-// first n_out <= n entries.  grid (ceil(inner/ti), nbatch); tile [n][ti+1].
+// first n_out <= n entries.  grid (ceil(inner/ti), nbatch).  Shared memory:
+// twiddles at 0, tile [n][pitch] at n.
 struct ColGeom {
   long long in_bs, in_as;    // input batch / axis strides (elements)
   long long out_bs, out_as;  // output batch / axis strides
@@ -310,53 +335,54 @@ struct ColGeom {
   int batches_per_rhs;       // for skipping converged right-hand sides
 };
 
-template <typename T, int NT, int MAXE>
+template <typename T, int NT>
 __global__ void __launch_bounds__(NT, 2) k_fft_cols(const typename C2<T>::t* in,
                                                  typename C2<T>::t* out, ColGeom cg,
                                                  FftPlanDev pl, int inverse,
                                                  const KrylovState* __restrict__ st, int mvskip) {
   typedef typename C2<T>::t T2;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  T2* sm = reinterpret_cast<T2*>(smraw);
   const long long batch = blockIdx.y;
   if (rhs_idle(st, (int)(batch / cg.batches_per_rhs), mvskip)) return;
+  const int n = pl.n;
+  T2* sm = smem_at<T>(n);
   const int i0 = blockIdx.x * cg.ti;
   const int ti = min(cg.ti, cg.inner - i0);
-  const int n = pl.n;
+  stage_twiddles<T, NT>(0, pl);
   const T2* ib = in + batch * cg.in_bs + i0;
   for (int i = threadIdx.x; i < n * ti; i += NT) {
-    const int e = i / ti, k = i % ti;
+    const int e = i / ti, k = i - e * ti;
     sm[e * cg.pitch + k] = e < cg.n_in ? ib[e * cg.in_as + k] : czero<T2>();
   }
   __syncthreads();
-  fft_smem_dir<T, NT, MAXE>(sm, ti, 1, cg.pitch, true, pl, inverse != 0);
+  fft_lines_dir<T, NT>(n, ti, 1, cg.pitch, true, pl, 0, inverse != 0);
   T2* ob = out + batch * cg.out_bs + i0;
   for (int i = threadIdx.x; i < cg.n_out * ti; i += NT) {
-    const int e = i / ti, k = i % ti;
+    const int e = i / ti, k = i - e * ti;
     ob[e * cg.out_as + k] = sm[e * cg.pitch + k];
   }
 }
 
 // -------------------------------------------- generic contiguous row FFT ----
 // grid (ceil(count/tl)); lines of length n at `stride` elements apart.
-template <typename T, int NT, int MAXE>
+// Shared memory: twiddles at 0, tile [tl][pitch] at n.
+template <typename T, int NT>
 __global__ void __launch_bounds__(NT, 2) k_fft_rows(typename C2<T>::t* data, long long count,
                                                  long long stride, int tl, int pitch,
                                                  FftPlanDev pl, int inverse) {
   typedef typename C2<T>::t T2;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  T2* sm = reinterpret_cast<T2*>(smraw);
+  const int n = pl.n;
+  T2* sm = smem_at<T>(n);
   const long long l0 = (long long)blockIdx.x * tl;
   const int nl = (int)min((long long)tl, count - l0);
-  const int n = pl.n;
+  stage_twiddles<T, NT>(0, pl);
   for (int i = threadIdx.x; i < nl * n; i += NT) {
-    const int l = i / n, e = i % n;
+    const int l = i / n, e = i - l * n;
     sm[l * pitch + e] = data[(l0 + l) * stride + e];
   }
   __syncthreads();
-  fft_smem_dir<T, NT, MAXE>(sm, nl, pitch, 1, false, pl, inverse != 0);
+  fft_lines_dir<T, NT>(n, nl, pitch, 1, false, pl, 0, inverse != 0);
   for (int i = threadIdx.x; i < nl * n; i += NT) {
-    const int l = i / n, e = i % n;
+    const int l = i / n, e = i - l * n;
     data[(l0 + l) * stride + e] = sm[l * pitch + e];
   }
 }

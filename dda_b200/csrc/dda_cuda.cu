@@ -471,6 +471,7 @@ template <typename T> struct Solve {
     a.nparts = c->nparts_vec;
     a.mat = c->mat_ext;
     a.ccs = e.ccs;
+    a.pscale = c->grid_unit * c->grid_unit * c->grid_unit;
     a.step = k;
     k_vec<T, kNtV><<<dim3(c->nparts_vec, nrhs), kNtV, 0, s>>>(a, c->st);
     CK(cudaGetLastError());

@@ -44,7 +44,8 @@ struct VecArgs {
   int nv, nvs, nmat;
   int nparts;
   const uint8_t* mat;  // material per dipole (caller order)
-  const void* ccs;     // [nrhs][nmat][3] complex
+  const void* ccs;     // [nrhs][nmat][3] complex, scaled by d^-3/2
+  double pscale;       // d^3: P = pscale * ccs . x (V_RESULT); x = P / (pscale ccs) (V_START_X)
   KrylovStep step;
 };
 
@@ -91,9 +92,11 @@ __global__ void __launch_bounds__(NT) k_vec(VecArgs va, KrylovState* st) {
           const T2 cc = ccs[va.mat[j] * 3 + c];
           const T2 x = v1[i];
           if (va.op == V_START_X) {
-            // x / cc (Smith division in working precision)
+            // x / cc (Smith division in FP64)
             double2 q = ddivc(make_double2(x.x, x.y), make_double2(cc.x, cc.y));
-            o = cvt<T2>(q);
+            o = cvt<T2>(dscale(q, 1.0 / va.pscale));
+          } else if (va.op == V_RESULT) {
+            o = cvt<T2>(dscale(dmulc(make_double2(cc.x, cc.y), make_double2(x.x, x.y)), va.pscale));
           } else {
             o = cmul(cc, x);
           }

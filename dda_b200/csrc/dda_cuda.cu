@@ -186,6 +186,8 @@ struct dda_ctx {
   std::vector<char> cc_set;
   KrylovState* st = nullptr;  // device [max_rhs]
   KrylovState* st_host = nullptr;  // pinned mirror
+  KrylovState* st_outer = nullptr;  // device: FP64 refinement loop (MIXED)
+  KrylovState* sto_host = nullptr;  // pinned mirror
   RedSums* parts = nullptr;
   unsigned* tickets = nullptr;
   int nparts_vec = 0, nparts_mv = 0;
@@ -204,6 +206,10 @@ struct dda_ctx {
                     (void*)parts, (void*)tickets, (void*)hist})
       if (p) cudaFree(p);
     if (st_host) cudaFreeHost(st_host);
+    if (sto_host) cudaFreeHost(sto_host);
+    if (st_outer) cudaFree(st_outer);
+    st_outer = nullptr;
+    sto_host = nullptr;
     if (stream) cudaStreamDestroy(stream);
     line_off = dip = perm = nullptr;
     mat_ext = nullptr;
@@ -447,7 +453,9 @@ template <typename T> struct Solve {
   Engine<T>& e;
   int nrhs;
   cudaStream_t s;
-  Solve(dda_ctx* c_, int nrhs_) : c(c_), e(eng<T>(c_)), nrhs(nrhs_), s(c_->stream) {}
+  KrylovState* st;
+  Solve(dda_ctx* c_, int nrhs_, KrylovState* st_ = nullptr)
+      : c(c_), e(eng<T>(c_)), nrhs(nrhs_), s(c_->stream), st(st_ ? st_ : c_->st) {}
 
   KrylovStep step(int op, int mode = EP_NORM, const void* w = nullptr, int nparts = 0) {
     KrylovStep k;
@@ -473,19 +481,20 @@ template <typename T> struct Solve {
     a.ccs = e.ccs;
     a.pscale = c->grid_unit * c->grid_unit * c->grid_unit;
     a.step = k;
-    k_vec<T, kNtV><<<dim3(c->nparts_vec, nrhs), kNtV, 0, s>>>(a, c->st);
+    k_vec<T, kNtV><<<dim3(c->nparts_vec, nrhs), kNtV, 0, s>>>(a, st);
     CK(cudaGetLastError());
     c->launches++;
   }
 
   void mv(const T2* arg, T2* res, int conj, KrylovStep k) {
-    matvec<T>(c, arg, res, conj, nrhs, s, c->st, k);
+    matvec<T>(c, arg, res, conj, nrhs, s, st, k);
   }
 
   // CpuIterativeSolver::initGeneral (DDA/CpuIterativeSolver.cpp:45-91) with
   // the GPU setup kernels of DDA/GpuIterativeSolver.cpp:78-134.
-  void init_general(T2* E, T2* B, T2* R, T2* X, T2* A, T2* S, bool start) {
-    vec(V_SETUP_PVEC, 0, {B, E}, step(KOP_INIT_PVEC));
+  void init_general(T2* E, T2* B, T2* R, T2* X, T2* A, T2* S, bool start, bool b_given = false) {
+    if (b_given) vec(V_NORM, 0, {B}, step(KOP_INIT_PVEC));
+    else vec(V_SETUP_PVEC, 0, {B, E}, step(KOP_INIT_PVEC));
     if (start) {
       vec(V_START_X, 0, {X, S}, KrylovStep{KOP_NONE, 0, nullptr, {}});
       mv(X, A, 0, step(KOP_NONE));
@@ -515,7 +524,7 @@ template <typename T> struct Solve {
         vec(V_BIS_P, nr == 0, {b.t1, b.t2, b.R}, step(KOP_NONE));
         mv(b.t1, b.t2, 0, step(KOP_BIS_ALPHA, EP_YW_HERM, b.t4));
         vec(V_BIS_S, 0, {b.t3, b.t2, b.R}, step(KOP_BIS_S));
-        matvec<T>(c, b.t3, b.A, 0, nrhs, s, c->st, step(KOP_BIS_OMEGA, EP_AY_HERM_NORM), 1);
+        matvec<T>(c, b.t3, b.A, 0, nrhs, s, st, step(KOP_BIS_OMEGA, EP_AY_HERM_NORM), 1);
         vec(V_BIS_XR, 0, {b.X, b.t1, b.t3, b.A, b.R, b.t4}, step(KOP_BIS_END));
         break;
       }
@@ -559,10 +568,19 @@ template <typename T> struct Solve {
 
 const long long kMaxResIncrease[4] = {50000, 30000, 50000, 10};
 
+struct SolveOpts {
+  bool start = false;              // S holds start polarisations
+  bool b_given = false;            // B already holds b (no sqrt(cc) Einc product)
+  const double* eps_rhs = nullptr; // per-rhs relative residual targets
+  const char* skip = nullptr;      // rhs left untouched (marked done from the start)
+  bool result = true;              // write P = sqrt(cc) x to the engine's io buffer
+};
+
 // Runs one solve of `nrhs` right-hand sides already set up in the engine
-// vectors (E = einc, S = start).  Returns per-rhs states in c->st_host.
+// vectors (E = einc or B = b, S = start).  Per-rhs states end in c->st_host;
+// the solution x is left in engine vector 4.
 template <typename T>
-void run_solve(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter, bool start) {
+void run_solve(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter, const SolveOpts& o) {
   typedef typename C2<T>::t T2;
   Engine<T>& e = eng<T>(c);
   Solve<T> sv(c, nrhs);
@@ -576,16 +594,17 @@ void run_solve(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
     k.maxResIncrease = kMaxResIncrease[solver];
     k.histCap = c->hist_cap;
     k.hist = c->hist + (size_t)r * c->hist_cap;
-    k.epsB = eps;  // holds eps until KOP_INIT_PVEC
+    if (o.skip && o.skip[r]) k.done = 1;
   }
   CK(cudaMemcpyAsync(c->st, c->st_host, nrhs * sizeof(KrylovState), cudaMemcpyHostToDevice, c->stream));
-  sv.init_general(E, B, b.R, b.X, b.A, S, start);
+  sv.init_general(E, B, b.R, b.X, b.A, S, o.start, o.b_given);
   // epsB = eps^2 / residScale (DDA/IterativeSolverBase.cpp:44)
   CK(cudaStreamSynchronize(c->stream));
   CK(cudaMemcpy(c->st_host, c->st, nrhs * sizeof(KrylovState), cudaMemcpyDeviceToHost));
   for (int r = 0; r < nrhs; r++) {
     KrylovState& k = c->st_host[r];
-    k.epsB = eps * eps / k.residScale;
+    const double er = o.eps_rhs ? o.eps_rhs[r] : eps;
+    k.epsB = er * er / k.residScale;
     if (!(k.inprodR >= k.epsB)) k.done = 1;  // already converged: no iteration
   }
   CK(cudaMemcpy(c->st, c->st_host, nrhs * sizeof(KrylovState), cudaMemcpyHostToDevice));
@@ -600,8 +619,84 @@ void run_solve(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
     for (int r = 0; r < nrhs; r++) all = all && c->st_host[r].done;
     if (all) break;
   }
+  if (b.X != e.vec[4])
+    CK(cudaMemcpyAsync(e.vec[4], b.X, (size_t)nrhs * 3 * c->g.nvs * sizeof(T2), cudaMemcpyDeviceToDevice, c->stream));
   // P = sqrt(cc) x
-  sv.vec(V_RESULT, 0, {e.io, b.X}, KrylovStep{KOP_NONE, 0, nullptr, {}});
+  if (o.result) sv.vec(V_RESULT, 0, {e.io, e.vec[4]}, KrylovStep{KOP_NONE, 0, nullptr, {}});
+}
+
+// Mixed precision: FP32 inner solves of A e = r corrected by FP64 residuals
+// r = b - A x until |r| < eps |b| in FP64.  Each inner solve aims at the
+// residual reduction still needed (at least 1e-4 per step, the FP32 floor
+// kept well above single-precision rounding).  Per-rhs totals are returned
+// in out[] (iterations, refinements, status, best relative residual).
+struct MixedOut {
+  long long iterations = 0, refinements = 0;
+  int status = 0;
+  double rel = 0, res_scale = 0;
+};
+
+void run_mixed(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter, bool start,
+               std::vector<MixedOut>& out) {
+  Engine<double>& d = c->e64;
+  Engine<float>& f = c->e32;
+  Solve<double> sd(c, nrhs, c->st_outer);
+  const size_t n = (size_t)nrhs * 3 * c->g.nvs;
+  double2 *E = d.vec[0], *B = d.vec[1], *S = d.vec[2], *X = d.vec[3], *R = d.vec[5], *A = d.vec[6];
+  out.assign(nrhs, MixedOut());
+  for (int r = 0; r < nrhs; r++) memset(&c->sto_host[r], 0, sizeof(KrylovState));
+  CK(cudaMemcpyAsync(c->st_outer, c->sto_host, nrhs * sizeof(KrylovState), cudaMemcpyHostToDevice, c->stream));
+  sd.vec(V_SETUP_PVEC, 0, {B, E}, sd.step(KOP_INIT_PVEC));  // b = sqrt(cc) Einc, |b|^2
+  if (start) sd.vec(V_START_X, 0, {X, S}, KrylovStep{KOP_NONE, 0, nullptr, {}});
+  else CK(cudaMemsetAsync(X, 0, n * sizeof(double2), c->stream));
+  std::vector<char> done(nrhs, 0);
+  std::vector<double> eps_in(nrhs, 1e-4);
+  const int max_outer = 30;
+  for (int outer = 0;; outer++) {
+    // r = b - A x (FP64); reduction n = |r|^2 -> last
+    if (outer == 0 && !start) CK(cudaMemcpyAsync(R, B, n * sizeof(double2), cudaMemcpyDeviceToDevice, c->stream));
+    else sd.mv(X, A, 0, sd.step(KOP_NONE));
+    sd.vec(V_R_INIT, 0, {R, (outer == 0 && !start) ? X : A, B}, sd.step(KOP_NORM));
+    CK(cudaMemcpyAsync(c->sto_host, c->st_outer, nrhs * sizeof(KrylovState), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    bool all = true;
+    long long total_it = 0;
+    for (int r = 0; r < nrhs; r++) {
+      KrylovState& k = c->sto_host[r];
+      const double rel = std::sqrt(k.last * k.residScale);
+      out[r].rel = rel;
+      out[r].res_scale = k.residScale;
+      total_it = std::max(total_it, out[r].iterations);
+      if (!done[r] && (rel < eps || out[r].status != 0)) done[r] = 1;
+      if (!done[r] && outer >= max_outer) { done[r] = 1; out[r].status = DDA_ERR_NOPROGRESS; }
+      if (!done[r] && max_iter > 0 && out[r].iterations >= max_iter) { done[r] = 1; out[r].status = DDA_ERR_MAXITER; }
+      k.done = done[r];
+      eps_in[r] = std::min(0.1, std::max(1e-4, 0.5 * eps / rel));
+      all = all && done[r];
+    }
+    if (all) break;
+    CK(cudaMemcpyAsync(c->st_outer, c->sto_host, nrhs * sizeof(KrylovState), cudaMemcpyHostToDevice, c->stream));
+    // inner FP32 solve of A e = r
+    k_convert<double2, float2><<<592, 256, 0, c->stream>>>(R, f.vec[1], (long long)n);
+    CK(cudaGetLastError());
+    SolveOpts o;
+    o.b_given = true;
+    o.eps_rhs = eps_in.data();
+    o.skip = done.data();
+    o.result = false;
+    run_solve<float>(c, solver, nrhs, 0.0, max_iter > 0 ? max_iter - total_it : 0, o);
+    for (int r = 0; r < nrhs; r++) {
+      if (done[r]) continue;
+      out[r].iterations += c->st_host[r].count;
+      out[r].refinements++;
+      if (c->st_host[r].status != 0 && c->st_host[r].status != DDA_ERR_MAXITER) out[r].status = c->st_host[r].status;
+    }
+    // x += e for the rhs still running
+    k_accum<<<dim3(c->nparts_vec, nrhs), 256, 0, c->stream>>>(X, f.vec[4], c->st_outer, 3LL * c->g.nvs);
+    CK(cudaGetLastError());
+    c->launches += 2;
+  }
+  sd.vec(V_RESULT, 0, {d.io, X}, KrylovStep{KOP_NONE, 0, nullptr, {}});
 }
 
 }  // namespace
@@ -711,6 +806,9 @@ int dda_create(const dda_problem* p, int precision, dda_ctx** out) {
     CK(cudaMalloc(&c->st, c->max_rhs * sizeof(KrylovState)));
     CK(cudaMemset(c->st, 0, c->max_rhs * sizeof(KrylovState)));
     CK(cudaMallocHost(&c->st_host, c->max_rhs * sizeof(KrylovState)));
+    CK(cudaMalloc(&c->st_outer, c->max_rhs * sizeof(KrylovState)));
+    CK(cudaMemset(c->st_outer, 0, c->max_rhs * sizeof(KrylovState)));
+    CK(cudaMallocHost(&c->sto_host, c->max_rhs * sizeof(KrylovState)));
     c->hist_cap = 100000;
     CK(cudaMalloc(&c->hist, (size_t)c->max_rhs * c->hist_cap * sizeof(double)));
     c->cc_host.assign((size_t)c->max_rhs * g.nmat * 3, 0);
@@ -867,7 +965,9 @@ int solve_t(dda_ctx* c, int solver, int nrhs, const double* einc, double eps, lo
   const size_t n = (size_t)nrhs * 3 * c->g.nvs;
   host_to_engine<T>(c, einc, e.vec[0], n);
   if (start) host_to_engine<T>(c, start, e.vec[2], n);
-  run_solve<T>(c, solver, nrhs, eps, max_iter, start != nullptr);
+  SolveOpts o;
+  o.start = start != nullptr;
+  run_solve<T>(c, solver, nrhs, eps, max_iter, o);
   if (pol_out) engine_to_host<T>(c, e.io, pol_out, n);
   CK(cudaStreamSynchronize(c->stream));
   return collect_stats(c, nrhs, history, history_cap, stats);
@@ -881,10 +981,62 @@ int solve_device_t(dda_ctx* c, int solver, int nrhs, const void* einc, double ep
   const size_t bytes = (size_t)nrhs * 3 * c->g.nvs * sizeof(T2);
   CK(cudaMemcpyAsync(e.vec[0], einc, bytes, cudaMemcpyDeviceToDevice, c->stream));
   if (start) CK(cudaMemcpyAsync(e.vec[2], start, bytes, cudaMemcpyDeviceToDevice, c->stream));
-  run_solve<T>(c, solver, nrhs, eps, max_iter, start != nullptr);
+  SolveOpts o;
+  o.start = start != nullptr;
+  run_solve<T>(c, solver, nrhs, eps, max_iter, o);
   CK(cudaMemcpyAsync(pol, e.io, bytes, cudaMemcpyDeviceToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return collect_stats(c, nrhs, nullptr, 0, stats);
+}
+
+int collect_mixed(dda_ctx* c, const std::vector<MixedOut>& mo, double* history, long long history_cap,
+                  dda_stats* stats) {
+  int rc = DDA_OK;
+  const int nrhs = (int)mo.size();
+  for (int r = 0; r < nrhs; r++) {
+    if (stats) {
+      stats[r].iterations = mo[r].iterations;
+      stats[r].matvecs = 0;
+      stats[r].refinements = mo[r].refinements;
+      stats[r].rel_residual = mo[r].rel;
+      stats[r].res_scale = mo[r].res_scale;
+      stats[r].status = mo[r].status;
+    }
+    if (history && history_cap > 0) {  // residual history of the last inner solve
+      const long long m = std::min<long long>(std::min(history_cap, c->hist_cap), c->st_host[r].count);
+      if (m > 0)
+        CK(cudaMemcpy(history + (size_t)r * history_cap, c->hist + (size_t)r * c->hist_cap, m * sizeof(double),
+                      cudaMemcpyDeviceToHost));
+    }
+    if (mo[r].status != 0 && rc == DDA_OK) rc = mo[r].status;
+  }
+  if (rc != DDA_OK) c->err = rc == DDA_ERR_MAXITER ? "Too many iterations" : "refinement did not converge";
+  return rc;
+}
+
+int solve_mixed_host(dda_ctx* c, int solver, int nrhs, const double* einc, double eps, long long max_iter,
+                     const double* start, double* pol_out, double* history, long long history_cap,
+                     dda_stats* stats) {
+  const size_t n = (size_t)nrhs * 3 * c->g.nvs;
+  CK(cudaMemcpyAsync(c->e64.vec[0], einc, n * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+  if (start) CK(cudaMemcpyAsync(c->e64.vec[2], start, n * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+  std::vector<MixedOut> mo;
+  run_mixed(c, solver, nrhs, eps, max_iter, start != nullptr, mo);
+  if (pol_out) CK(cudaMemcpyAsync(pol_out, c->e64.io, n * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return collect_mixed(c, mo, history, history_cap, stats);
+}
+
+int solve_mixed_device(dda_ctx* c, int solver, int nrhs, const void* einc, double eps, long long max_iter,
+                       const void* start, void* pol, dda_stats* stats) {
+  const size_t bytes = (size_t)nrhs * 3 * c->g.nvs * sizeof(double2);
+  CK(cudaMemcpyAsync(c->e64.vec[0], einc, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  if (start) CK(cudaMemcpyAsync(c->e64.vec[2], start, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  std::vector<MixedOut> mo;
+  run_mixed(c, solver, nrhs, eps, max_iter, start != nullptr, mo);
+  CK(cudaMemcpyAsync(pol, c->e64.io, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return collect_mixed(c, mo, nullptr, 0, stats);
 }
 
 int collect_stats(dda_ctx* c, int nrhs, double* history, long long history_cap, dda_stats* stats) {
@@ -942,6 +1094,8 @@ int dda_solve(dda_ctx* ctx, int solver, int nrhs, const double* einc, double eps
       if (!ctx->cc_set[r]) throw DdaError(DDA_ERR_ARG, "couple constants not set (dda_set_cc)");
     if (ctx->precision == DDA_PREC_FP32)
       return solve_t<float>(ctx, solver, nrhs, einc, eps, max_iter, start, pol_out, history, history_cap, stats);
+    if (ctx->precision == DDA_PREC_MIXED)
+      return solve_mixed_host(ctx, solver, nrhs, einc, eps, max_iter, start, pol_out, history, history_cap, stats);
     return solve_t<double>(ctx, solver, nrhs, einc, eps, max_iter, start, pol_out, history, history_cap, stats);
   });
 }
@@ -957,6 +1111,8 @@ int dda_solve_device(dda_ctx* ctx, int solver, int nrhs, const void* d_einc, dou
       if (!ctx->cc_set[r]) throw DdaError(DDA_ERR_ARG, "couple constants not set (dda_set_cc)");
     if (ctx->precision == DDA_PREC_FP64)
       return solve_device_t<double>(ctx, solver, nrhs, d_einc, eps, max_iter, d_start, d_pol, stats);
+    if (ctx->precision == DDA_PREC_MIXED)
+      return solve_mixed_device(ctx, solver, nrhs, d_einc, eps, max_iter, d_start, d_pol, stats);
     return solve_device_t<float>(ctx, solver, nrhs, d_einc, eps, max_iter, d_start, d_pol, stats);
   });
 }

@@ -224,4 +224,20 @@ __global__ void __launch_bounds__(NT) k_vec(VecArgs va, KrylovState* st) {
   }
 }
 
+// x64 += e32 for every right-hand side the refinement loop still runs
+// (grid (parts, nrhs)); the FP64 update of mixed-precision refinement.
+__global__ void __launch_bounds__(256) k_accum(double2* __restrict__ x, const float2* __restrict__ e,
+                                             const KrylovState* __restrict__ st, long long len) {
+  const int b = blockIdx.y;
+  if (st[b].done) return;
+  const size_t off = (size_t)b * len;
+  for (long long i = blockIdx.x * 256LL + threadIdx.x; i < len; i += (long long)gridDim.x * 256) {
+    const float2 d = e[off + i];
+    double2 v = x[off + i];
+    v.x += d.x;
+    v.y += d.y;
+    x[off + i] = v;
+  }
+}
+
 }  // namespace dda

@@ -138,7 +138,8 @@ int dda_solve(dda_ctx* ctx, int solver, int nrhs, const double* einc, double eps
               int64_t history_cap, dda_stats* stats);
 
 /* dda_solve on device buffers of the context precision (double pairs for
- * DDA_PREC_FP64, float pairs for DDA_PREC_FP32 and DDA_PREC_MIXED):
+ * DDA_PREC_FP64 and DDA_PREC_MIXED, whose outer residual is FP64; float
+ * pairs for DDA_PREC_FP32):
  * d_einc [nrhs][3][nvs] in, d_pol [nrhs][3][nvs] out, d_start may be NULL.
  * All work is queued on the context stream; the call returns when the solve
  * has finished.  Replaces GpuIterativeSolver<T>::getPolVec's device part

@@ -99,3 +99,32 @@ def test_max_iter_reports_error(aniso64):
         s.get_pol_vec(e, 1e-10)
     assert ei.value.code == -6
     assert s.last_stats[0].iterations == 3
+
+
+@pytest.mark.parametrize("solver", ["qmr", "bicgstab"])
+def test_mixed_refinement_reaches_fp64_accuracy(solver):
+    # FP32 inner solves refined by FP64 residuals reach residuals FP32 alone cannot
+    pr = Pair("arrays", aniso_arrays(), MATS, "0.9um", "mixed")
+    pr.set_cc((0.3, 0.4, 0.866), 1, "ldr")
+    e = pr.p.einc((0.3, 0.4, 0.866), 1)
+    s = dda_b200.CudaSolver(pr.mv, solver)
+    pol = s.get_pol_vec(e, 1e-9)
+    st = s.last_stats[0]
+    assert st.status == 0 and st.rel_residual < 1e-9 and st.refinements >= 2
+    rc, opol, _, _ = pr.op.solve(e, solver, 1e-11)
+    assert rel(pol, opol) < 1e-7
+
+
+def test_mixed_cfg1_both_pols_batched():
+    pr = Pair("sphere", ("10um", "0.5um"), [1.5 + 0.1j], "6um", "mixed", max_rhs=2)
+    es = []
+    for r, pol in enumerate((1, 2)):
+        pr.set_cc((0, 0, 1), pol, "ldr", rhs=r)
+        es.append(pr.p.einc((0, 0, 1), pol))
+    s = dda_b200.CudaSolver(pr.mv, "qmr")
+    pol = s.get_pol_vec(np.concatenate(es), 1e-5).reshape(2, -1)
+    for r, p in enumerate((1, 2)):
+        assert s.last_stats[r].status == 0 and s.last_stats[r].rel_residual < 1e-5
+        pr.op.set_cc((0, 0, 1), p, "ldr")
+        rc, opol, _, _ = pr.op.solve(es[r], "qmr", 1e-7)
+        assert rel(pol[r], opol) < 2e-5

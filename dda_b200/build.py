@@ -11,8 +11,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libdda_b200.so")
 SOURCES = ["dda_cuda.cu", "frontend.cpp"]
-HEADERS = ["fft_engine.cuh", "reduce.cuh", "krylov_ops.cuh", "krylov_kernels.cuh",
-           "matvec_kernels.cuh", "dmatrix_kernels.cuh"]
+HEADERS = ["fft_engine.cuh", "fft_plan.cuh", "reduce.cuh", "krylov_ops.cuh", "krylov_kernels.cuh",
+           "matvec_kernels.cuh", "matvec_planned.cuh", "matvec_dispatch.cuh", "dmatrix_kernels.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -28,6 +28,8 @@
 #include "krylov_kernels.cuh"
 #include "krylov_ops.cuh"
 #include "matvec_kernels.cuh"
+#include "matvec_dispatch.cuh"
+#include "matvec_planned.cuh"
 #include "reduce.cuh"
 
 using namespace dda;
@@ -51,7 +53,12 @@ struct DdaError : std::runtime_error {
 
 // Kernel shapes (threads per CTA).
 constexpr int kNtX = 256;   // k_xfwd / k_xinv
-constexpr int kNtYz = 512;  // k_yz / k_yrows
+// k_yz / k_yrows: 512 threads in FP32; 256 in FP64, whose FFT stages need
+// more than the 128 registers a 512-thread CTA leaves per thread.
+template <typename T> struct NtYz;
+template <> struct NtYz<float> { static constexpr int v = 512; };
+template <> struct NtYz<double> { static constexpr int v = 256; };
+#define kNtYz NtYz<T>::v
 constexpr int kNtC = 256;   // k_fft_cols / k_fft_rows
 constexpr int kNtV = 256;                 // k_vec
 constexpr size_t kSmemMax = 227 * 1024;
@@ -66,15 +73,22 @@ struct FftPlan {
   int* freq = nullptr;     // device: position -> frequency
   int* pos = nullptr;      // device: frequency -> position
 
-  void create(int n_) {
+  // radices: a compile-time plan's stage radices, or empty for the runtime
+  // engine's factorisation (8s, then 4, 2, 3, 5, 7).
+  void create(int n_, const std::vector<int>& radices = {}) {
     n = n_;
     int m = n;
-    while (m % 8 == 0) { radix.push_back(8); m /= 8; }
-    while (m % 4 == 0) { radix.push_back(4); m /= 4; }
-    while (m % 2 == 0) { radix.push_back(2); m /= 2; }
-    while (m % 3 == 0) { radix.push_back(3); m /= 3; }
-    while (m % 5 == 0) { radix.push_back(5); m /= 5; }
-    while (m % 7 == 0) { radix.push_back(7); m /= 7; }
+    if (!radices.empty()) {
+      radix = radices;
+      for (int r : radix) m /= r;
+    } else {
+      while (m % 8 == 0) { radix.push_back(8); m /= 8; }
+      while (m % 4 == 0) { radix.push_back(4); m /= 4; }
+      while (m % 2 == 0) { radix.push_back(2); m /= 2; }
+      while (m % 3 == 0) { radix.push_back(3); m /= 3; }
+      while (m % 5 == 0) { radix.push_back(5); m /= 5; }
+      while (m % 7 == 0) { radix.push_back(7); m /= 7; }
+    }
     if (m != 1) throw DdaError(DDA_ERR_UNSUPPORTED, "FFT length " + std::to_string(n) + " is not 2,3,5,7-smooth");
     if ((int)radix.size() > 8) throw DdaError(DDA_ERR_UNSUPPORTED, "FFT length too large");
     std::vector<double2> h64(n);
@@ -115,8 +129,8 @@ struct FftPlan {
     memset(&d, 0, sizeof(d));
     d.n = n;
     d.nst = (int)radix.size();
-    d.packed = 0;
-    for (size_t i = 0; i < radix.size(); i++) d.packed |= (uint32_t)radix[i] << (4 * i);
+    d.packed = 0;  // runtime-engine radices (< 16); unused by planned kernels
+    for (size_t i = 0; i < radix.size(); i++) d.packed |= (uint32_t)(radix[i] & 15) << (4 * i);
     d.tw = std::is_same<T, float>::value ? (const void*)tw32 : (const void*)tw64;
     d.freq = freq;
     return d;
@@ -156,6 +170,7 @@ template <typename T> struct Engine {
   YzGeom yz{};
   size_t smem_x = 0, smem_yz = 0, smem_rows = 0, smem_cols = 0;
   ColGeom cz_fwd{}, cz_inv{};
+  MvKernels<T> k;
   void release() {
     for (void* p : {(void*)dc, (void*)ccs, (void*)xhat, (void*)zbuf, (void*)io})
       if (p) cudaFree(p);
@@ -179,7 +194,9 @@ struct dda_ctx {
   uint32_t* dip = nullptr;
   uint32_t* perm = nullptr;
   uint8_t* mat_ext = nullptr;
-  FftPlan px, py, pz;
+  FftPlan px, py, pz;  // runtime-engine plans (D-matrix setup, generic matvec)
+  FftPlan mx, my, mz;  // matvec plans: tuned compile-time plans when `planned`
+  bool planned = false;
   Engine<float> e32;
   Engine<double> e64;
   std::vector<std::complex<double>> cc_host;  // [max_rhs][nmat][3], reference units
@@ -202,6 +219,9 @@ struct dda_ctx {
     px.release();
     py.release();
     pz.release();
+    mx.release();
+    my.release();
+    mz.release();
     for (void* p : {(void*)line_off, (void*)dip, (void*)perm, (void*)mat_ext, (void*)st,
                     (void*)parts, (void*)tickets, (void*)hist})
       if (p) cudaFree(p);
@@ -251,7 +271,9 @@ template <typename T> void setup_engine(dda_ctx* c) {
   y.nrw = nrw;
   e.yz = y;
   e.smem_yz = fixed + nrw * row;
-  e.fused = e.smem_yz <= kSmemMax && !(c->flags & DDA_FLAG_SPLIT_YZ);
+  e.k = c->planned ? planned_kernels<T, kNtX, kNtYz, kNtC>(g.Gx, g.Gy, g.Gz)
+                   : generic_kernels<T, kNtX, kNtYz, kNtC>();
+  e.fused = e.k.yz && e.smem_yz <= kSmemMax && !(c->flags & DDA_FLAG_SPLIT_YZ);
   if (!e.fused) {
     // split path: zbuf, k_yrows over NW rows per CTA, column FFTs along z
     e.yz.nrw = NW;
@@ -287,12 +309,12 @@ template <typename T> void setup_engine(dda_ctx* c) {
   auto attr = [](const void* f, size_t bytes) {
     CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(bytes, 1)));
   };
-  attr((const void*)k_xfwd<T, kNtX>, e.smem_x);
-  attr((const void*)k_xinv<T, kNtX>, e.smem_x);
-  if (e.fused) attr((const void*)k_yz<T, kNtYz>, e.smem_yz);
+  attr((const void*)e.k.xfwd, e.smem_x);
+  attr((const void*)e.k.xinv, e.smem_x);
+  if (e.fused) attr((const void*)e.k.yz, e.smem_yz);
   else {
-    attr((const void*)k_yrows<T, kNtYz>, e.smem_rows);
-    attr((const void*)k_fft_cols<T, kNtC>, e.smem_cols);
+    attr((const void*)e.k.yrows, e.smem_rows);
+    attr((const void*)e.k.cols, e.smem_cols);
   }
   const int hx = g.Gx / 2 + 1, hy = g.Gy / 2 + 1, hz = g.Gz / 2 + 1;
   e.dc = (T2*)dalloc<T>((size_t)hx * hy * hz * 6 * s);
@@ -336,23 +358,22 @@ void matvec(dda_ctx* c, const typename C2<T>::t* arg, typename C2<T>::t* res, in
             cudaStream_t s, KrylovState* st, KrylovStep step, int skipmv = 0) {
   Engine<T>& e = eng<T>(c);
   const MvGeom& g = c->g;
-  const FftPlanDev px = c->px.dev<T>(), py = c->py.dev<T>(), pz = c->pz.dev<T>();
+  const FftPlanDev px = c->mx.dev<T>(), py = c->my.dev<T>(), pz = c->mz.dev<T>();
   dim3 gx(ntiles(c), 3, nrhs);
-  k_xfwd<T, kNtX><<<gx, kNtX, e.smem_x, s>>>(arg, e.xhat, c->line_off, c->dip, c->perm,
-                                                      e.ccs, conj, g, px, st, skipmv);
+  e.k.xfwd<<<gx, kNtX, e.smem_x, s>>>(arg, e.xhat, c->line_off, c->dip, c->perm, e.ccs, conj, g, px, st, skipmv);
   if (e.fused) {
-    k_yz<T, kNtYz><<<dim3(g.Gx, nrhs), kNtYz, e.smem_yz, s>>>(e.xhat, e.dc, g, e.yz, pz, py, st, skipmv);
+    e.k.yz<<<dim3(g.Gx, nrhs), kNtYz, e.smem_yz, s>>>(e.xhat, e.dc, g, e.yz, pz, py, st, skipmv);
   } else {
     const int nbatch = nrhs * g.Gx * 3;
     dim3 gc((g.by + e.cz_fwd.ti - 1) / e.cz_fwd.ti, nbatch);
-    k_fft_cols<T, kNtC><<<gc, kNtC, e.smem_cols, s>>>(e.xhat, e.zbuf, e.cz_fwd, pz, 0, st, skipmv);
+    e.k.cols<<<gc, kNtC, e.smem_cols, s>>>(e.xhat, e.zbuf, e.cz_fwd, pz, 0, st, skipmv);
     dim3 gr((g.Gz + e.yz.nrw - 1) / e.yz.nrw, g.Gx, nrhs);
-    k_yrows<T, kNtYz><<<gr, kNtYz, e.smem_rows, s>>>(e.zbuf, e.dc, g, e.yz, py, st, skipmv);
-    k_fft_cols<T, kNtC><<<gc, kNtC, e.smem_cols, s>>>(e.zbuf, e.xhat, e.cz_inv, pz, 1, st, skipmv);
+    e.k.yrows<<<gr, kNtYz, e.smem_rows, s>>>(e.zbuf, e.dc, g, e.yz, py, st, skipmv);
+    e.k.cols<<<gc, kNtC, e.smem_cols, s>>>(e.zbuf, e.xhat, e.cz_inv, pz, 1, st, skipmv);
   }
   step.red = red_target(c, 3 * ntiles(c));
-  k_xinv<T, kNtX><<<gx, kNtX, e.smem_x, s>>>(arg, res, e.xhat, c->line_off, c->dip, c->perm,
-                                                      e.ccs, conj, g, px, st, step, skipmv);
+  e.k.xinv<<<gx, kNtX, e.smem_x, s>>>(arg, res, e.xhat, c->line_off, c->dip, c->perm, e.ccs, conj, g, px, st, step,
+                                      skipmv);
   CK(cudaGetLastError());
   c->launches += e.fused ? 3 : 5;
 }
@@ -788,9 +809,14 @@ int dda_create(const dda_problem* p, int precision, dda_ctx** out) {
     c->px.create(g.Gx);
     c->py.create(g.Gy);
     c->pz.create(g.Gz);
-    g.fx = c->px.freq;
-    g.fy = c->py.freq;
-    g.fz = c->pz.freq;
+    c->planned = has_tuned_plan(g.Gx) && has_tuned_plan(g.Gy) && has_tuned_plan(g.Gz) &&
+                 !(c->flags & DDA_FLAG_RUNTIME_PLANS);
+    c->mx.create(g.Gx, c->planned ? tuned_radices(g.Gx) : std::vector<int>());
+    c->my.create(g.Gy, c->planned ? tuned_radices(g.Gy) : std::vector<int>());
+    c->mz.create(g.Gz, c->planned ? tuned_radices(g.Gz) : std::vector<int>());
+    g.fx = c->mx.freq;
+    g.fy = c->my.freq;
+    g.fz = c->mz.freq;
     if (precision != DDA_PREC_FP32) setup_engine<double>(c.get());
     if (precision != DDA_PREC_FP64) setup_engine<float>(c.get());
     // reduction slots
@@ -879,7 +905,7 @@ template <typename T> void profile_t(dda_ctx* c, int nrhs, int reps, double* ms)
   typedef typename C2<T>::t T2;
   Engine<T>& e = eng<T>(c);
   const MvGeom& g = c->g;
-  const FftPlanDev px = c->px.dev<T>(), py = c->py.dev<T>(), pz = c->pz.dev<T>();
+  const FftPlanDev px = c->mx.dev<T>(), py = c->my.dev<T>(), pz = c->mz.dev<T>();
   cudaStream_t s = c->stream;
   cudaEvent_t ev[4];
   for (auto& x : ev) CK(cudaEventCreate(&x));
@@ -891,21 +917,20 @@ template <typename T> void profile_t(dda_ctx* c, int nrhs, int reps, double* ms)
   for (int r = 0; r <= reps; r++) {
     dim3 gx(ntiles(c), 3, nrhs);
     CK(cudaEventRecord(ev[0], s));
-    k_xfwd<T, kNtX><<<gx, kNtX, e.smem_x, s>>>(arg, e.xhat, c->line_off, c->dip, c->perm,
-                                                              e.ccs, 0, g, px, nullptr, 0);
+    e.k.xfwd<<<gx, kNtX, e.smem_x, s>>>(arg, e.xhat, c->line_off, c->dip, c->perm, e.ccs, 0, g, px, nullptr, 0);
     CK(cudaEventRecord(ev[1], s));
     if (e.fused) {
-      k_yz<T, kNtYz><<<dim3(g.Gx, nrhs), kNtYz, e.smem_yz, s>>>(e.xhat, e.dc, g, e.yz, pz, py, nullptr, 0);
+      e.k.yz<<<dim3(g.Gx, nrhs), kNtYz, e.smem_yz, s>>>(e.xhat, e.dc, g, e.yz, pz, py, nullptr, 0);
     } else {
       dim3 gc((g.by + e.cz_fwd.ti - 1) / e.cz_fwd.ti, nrhs * g.Gx * 3);
-      k_fft_cols<T, kNtC><<<gc, kNtC, e.smem_cols, s>>>(e.xhat, e.zbuf, e.cz_fwd, pz, 0, nullptr, 0);
+      e.k.cols<<<gc, kNtC, e.smem_cols, s>>>(e.xhat, e.zbuf, e.cz_fwd, pz, 0, nullptr, 0);
       dim3 gr((g.Gz + e.yz.nrw - 1) / e.yz.nrw, g.Gx, nrhs);
-      k_yrows<T, kNtYz><<<gr, kNtYz, e.smem_rows, s>>>(e.zbuf, e.dc, g, e.yz, py, nullptr, 0);
-      k_fft_cols<T, kNtC><<<gc, kNtC, e.smem_cols, s>>>(e.zbuf, e.xhat, e.cz_inv, pz, 1, nullptr, 0);
+      e.k.yrows<<<gr, kNtYz, e.smem_rows, s>>>(e.zbuf, e.dc, g, e.yz, py, nullptr, 0);
+      e.k.cols<<<gc, kNtC, e.smem_cols, s>>>(e.zbuf, e.xhat, e.cz_inv, pz, 1, nullptr, 0);
     }
     CK(cudaEventRecord(ev[2], s));
-    k_xinv<T, kNtX><<<gx, kNtX, e.smem_x, s>>>(arg, res, e.xhat, c->line_off, c->dip, c->perm,
-                                                              e.ccs, 0, g, px, nullptr, none, 0);
+    e.k.xinv<<<gx, kNtX, e.smem_x, s>>>(arg, res, e.xhat, c->line_off, c->dip, c->perm, e.ccs, 0, g, px, nullptr, none,
+                                        0);
     CK(cudaEventRecord(ev[3], s));
     CK(cudaEventSynchronize(ev[3]));
     if (r == 0) continue;  // warm-up

@@ -27,26 +27,26 @@ template <typename T> struct C2;
 template <> struct C2<float> { typedef float2 t; };
 template <> struct C2<double> { typedef double2 t; };
 
-template <typename T2> __device__ __forceinline__ T2 czero() {
+template <typename T2> __host__ __device__ __forceinline__ T2 czero() {
   T2 r; r.x = 0; r.y = 0; return r;
 }
-template <typename T2> __device__ __forceinline__ T2 cmul(T2 a, T2 b) {
+template <typename T2> __host__ __device__ __forceinline__ T2 cmul(T2 a, T2 b) {
   T2 r;
   r.x = a.x * b.x - a.y * b.y;
   r.y = a.x * b.y + a.y * b.x;
   return r;
 }
-template <typename T2> __device__ __forceinline__ T2 cadd(T2 a, T2 b) {
+template <typename T2> __host__ __device__ __forceinline__ T2 cadd(T2 a, T2 b) {
   T2 r; r.x = a.x + b.x; r.y = a.y + b.y; return r;
 }
-template <typename T2> __device__ __forceinline__ T2 csub(T2 a, T2 b) {
+template <typename T2> __host__ __device__ __forceinline__ T2 csub(T2 a, T2 b) {
   T2 r; r.x = a.x - b.x; r.y = a.y - b.y; return r;
 }
-template <typename T2> __device__ __forceinline__ T2 cconj(T2 a) {
+template <typename T2> __host__ __device__ __forceinline__ T2 cconj(T2 a) {
   a.y = -a.y; return a;
 }
 // multiply by -i (forward) or +i (inverse)
-template <bool INV, typename T2> __device__ __forceinline__ T2 mul_mi(T2 a) {
+template <bool INV, typename T2> __host__ __device__ __forceinline__ T2 mul_mi(T2 a) {
   T2 r;
   if (INV) { r.x = -a.y; r.y = a.x; } else { r.x = a.y; r.y = -a.x; }
   return r;
@@ -67,7 +67,7 @@ struct FftPlanDev {
 template <int R, bool INV, typename T2> struct Dft;
 
 template <bool INV, typename T2> struct Dft<2, INV, T2> {
-  static __device__ __forceinline__ void run(T2* v) {
+  static __host__ __device__ __forceinline__ void run(T2* v) {
     T2 a = v[0], b = v[1];
     v[0] = cadd(a, b);
     v[1] = csub(a, b);
@@ -75,7 +75,7 @@ template <bool INV, typename T2> struct Dft<2, INV, T2> {
 };
 
 template <bool INV, typename T2> struct Dft<4, INV, T2> {
-  static __device__ __forceinline__ void run(T2* v) {
+  static __host__ __device__ __forceinline__ void run(T2* v) {
     T2 t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
     T2 t2 = cadd(v[1], v[3]), t3 = mul_mi<INV>(csub(v[1], v[3]));
     v[0] = cadd(t0, t2);
@@ -86,7 +86,7 @@ template <bool INV, typename T2> struct Dft<4, INV, T2> {
 };
 
 template <bool INV, typename T2> struct Dft<8, INV, T2> {
-  static __device__ __forceinline__ void run(T2* v) {
+  static __host__ __device__ __forceinline__ void run(T2* v) {
     typedef decltype(v[0].x) T;
     const T h = (T)0.7071067811865475244008444;
     T2 e[4] = {v[0], v[2], v[4], v[6]};
@@ -111,16 +111,16 @@ template <bool INV, typename T2> struct Dft<8, INV, T2> {
 // Odd prime radix via symmetric pairs: y_k = a0 + sum_m C(mk) t_m -/+ i sum_m S(mk) u_m.
 template <int R> struct OddConst;
 template <> struct OddConst<3> {
-  static __device__ __forceinline__ double c(int j) { return -0.5; }
-  static __device__ __forceinline__ double s(int j) {
+  static __host__ __device__ __forceinline__ double c(int j) { return -0.5; }
+  static __host__ __device__ __forceinline__ double s(int j) {
     return j == 1 ? 0.8660254037844386467637232 : -0.8660254037844386467637232;
   }
 };
 template <> struct OddConst<5> {
-  static __device__ __forceinline__ double c(int j) {
+  static __host__ __device__ __forceinline__ double c(int j) {
     return (j == 1 || j == 4) ? 0.3090169943749474241022934 : -0.8090169943749474241022934;
   }
-  static __device__ __forceinline__ double s(int j) {
+  static __host__ __device__ __forceinline__ double s(int j) {
     return j == 1 ? 0.9510565162951535721164393
          : j == 2 ? 0.587785252292473129168706
          : j == 3 ? -0.587785252292473129168706
@@ -128,12 +128,12 @@ template <> struct OddConst<5> {
   }
 };
 template <> struct OddConst<7> {
-  static __device__ __forceinline__ double c(int j) {
+  static __host__ __device__ __forceinline__ double c(int j) {
     return (j == 1 || j == 6) ? 0.6234898018587335305250049
          : (j == 2 || j == 5) ? -0.2225209339563144042889026
                               : -0.9009688679024191262361023;
   }
-  static __device__ __forceinline__ double s(int j) {
+  static __host__ __device__ __forceinline__ double s(int j) {
     return j == 1 ? 0.7818314824680298087084445
          : j == 2 ? 0.9749279121818236070181317
          : j == 3 ? 0.4338837391175581204757683
@@ -146,7 +146,7 @@ template <> struct OddConst<7> {
 template <int R, bool INV, typename T2> struct DftOdd {
   // In place: the pair sums/differences replace v[1..R-1] before the outputs
   // are written back, so no second output array is live.
-  static __device__ __forceinline__ void run(T2* v) {
+  static __host__ __device__ __forceinline__ void run(T2* v) {
     typedef decltype(v[0].x) T;
     constexpr int H = (R - 1) / 2;
     T2 t[H], u[H];

@@ -1,0 +1,93 @@
+// matvec_dispatch.cuh -- selection of the matvec kernels for a context: the
+// compile-time-planned kernels of matvec_planned.cuh when every grid edge has
+// a tuned plan, the runtime-planned kernels of matvec_kernels.cuh otherwise.
+#pragma once
+
+#include "matvec_kernels.cuh"
+#include "matvec_planned.cuh"
+
+namespace dda {
+
+template <typename T> struct MvKernels {
+  typedef typename C2<T>::t T2;
+  typedef void (*XfwdFn)(const T2*, T2*, const uint32_t*, const uint32_t*, const uint32_t*, const T2*, int,
+                         MvGeom, FftPlanDev, const KrylovState*, int);
+  typedef void (*XinvFn)(const T2*, T2*, const T2*, const uint32_t*, const uint32_t*, const uint32_t*,
+                         const T2*, int, MvGeom, FftPlanDev, KrylovState*, KrylovStep, int);
+  typedef void (*YzFn)(T2*, const T2*, MvGeom, YzGeom, FftPlanDev, FftPlanDev, const KrylovState*, int);
+  typedef void (*YrowsFn)(T2*, const T2*, MvGeom, YzGeom, FftPlanDev, const KrylovState*, int);
+  typedef void (*ColsFn)(const T2*, T2*, ColGeom, FftPlanDev, int, const KrylovState*, int);
+  XfwdFn xfwd = nullptr;
+  XinvFn xinv = nullptr;
+  YzFn yz = nullptr;        // fused plane kernel (nullptr: none for this shape)
+  YrowsFn yrows = nullptr;  // split path
+  ColsFn cols = nullptr;
+  bool planned = false;
+};
+
+#define DDA_TUNED_LENGTHS(X) X(64) X(80) X(96) X(100) X(128) X(160) X(192) X(200) X(256) X(512)
+#define DDA_FUSED_LENGTHS(X) X(64) X(80) X(96) X(100) X(128)
+
+inline bool has_tuned_plan(int n) {
+  switch (n) {
+#define C(N) case N:
+    DDA_TUNED_LENGTHS(C)
+#undef C
+    return true;
+    default: return false;
+  }
+}
+
+// Planned kernels for grid (gx, gy, gz), all edges tuned.
+template <typename T, int NTX, int NTYZ, int NTC>
+MvKernels<T> planned_kernels(int gx, int gy, int gz) {
+  MvKernels<T> k;
+  k.planned = true;
+  switch (gx) {
+#define C(N)                                                           \
+  case N:                                                              \
+    k.xfwd = k_xfwd<T, NTX, typename PlanFor<N>::type>;                \
+    k.xinv = k_xinv<T, NTX, typename PlanFor<N>::type>;                \
+    break;
+    DDA_TUNED_LENGTHS(C)
+#undef C
+    default: break;
+  }
+  switch (gy) {
+#define C(N)                                                           \
+  case N: k.yrows = k_yrows_p<T, NTYZ, typename PlanFor<N>::type>; break;
+    DDA_TUNED_LENGTHS(C)
+#undef C
+    default: break;
+  }
+  switch (gz) {
+#define C(N)                                                           \
+  case N: k.cols = k_fft_cols<T, NTC, typename PlanFor<N>::type>; break;
+    DDA_TUNED_LENGTHS(C)
+#undef C
+    default: break;
+  }
+  if (gy == gz) {
+    switch (gy) {
+#define C(N)                                                                                     \
+  case N: k.yz = k_yz_p<T, NTYZ, typename PlanFor<N>::type, typename PlanFor<N>::type>; break;
+      DDA_FUSED_LENGTHS(C)
+#undef C
+      default: break;
+    }
+  }
+  return k;
+}
+
+template <typename T, int NTX, int NTYZ, int NTC>
+MvKernels<T> generic_kernels() {
+  MvKernels<T> k;
+  k.xfwd = k_xfwd<T, NTX>;
+  k.xinv = k_xinv<T, NTX>;
+  k.yz = k_yz<T, NTYZ>;
+  k.yrows = k_yrows<T, NTYZ>;
+  k.cols = k_fft_cols<T, NTC>;
+  return k;
+}
+
+}  // namespace dda

@@ -26,6 +26,7 @@
 #pragma once
 
 #include "fft_engine.cuh"
+#include "fft_plan.cuh"
 #include "reduce.cuh"
 #include "krylov_ops.cuh"
 
@@ -87,9 +88,10 @@ __device__ __forceinline__ bool rhs_idle(const KrylovState* st, int b, int mvski
 __host__ __device__ inline int x_tile_off(const MvGeom& g) { return g.Gx + g.nmat; }
 
 // ------------------------------------------------------------ k_xfwd ----
-// grid (ceil(nlines/tl), 3, nrhs).
-template <typename T, int NT>
-__global__ void __launch_bounds__(NT, 2) k_xfwd(const typename C2<T>::t* __restrict__ arg,
+// grid (ceil(nlines/tl), 3, nrhs).  PX: compile-time plan of the x
+// transform, or void for the runtime-planned engine.
+template <typename T, int NT, typename PX = void>
+__global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 1 : 2) k_xfwd(const typename C2<T>::t* __restrict__ arg,
                                              typename C2<T>::t* __restrict__ xhat,
                                              const uint32_t* __restrict__ line_off,
                                              const uint32_t* __restrict__ dip,
@@ -122,7 +124,8 @@ __global__ void __launch_bounds__(NT, 2) k_xfwd(const typename C2<T>::t* __restr
     }
   }
   __syncthreads();
-  fft_lines<T, NT, false>(toff, nl, g.pitchx, 1, false, px, 0);
+  if constexpr (std::is_void<PX>::value) fft_lines<T, NT, false>(toff, nl, g.pitchx, 1, false, px, 0);
+  else plines<T, PX, NT, false>(toff, nl, g.pitchx, 1, 0);
   T2* out = xhat + ((size_t)b * g.Gx * 3 + c) * g.nlines + L0;
   const size_t kstride = (size_t)3 * g.nlines;
   for (int i = threadIdx.x; i < nl * g.Gx; i += NT) {
@@ -135,8 +138,8 @@ __global__ void __launch_bounds__(NT, 2) k_xfwd(const typename C2<T>::t* __restr
 // grid (ceil(nlines/tl), 3, nrhs).  Epilogue: res = conj?(sqrt(cc).X +
 // conj?(arg)), padding nv..nvs zeroed, and optional sums over the result for
 // the solver step `op` (finalised by the last CTA of each right-hand side).
-template <typename T, int NT>
-__global__ void __launch_bounds__(NT, 2) k_xinv(const typename C2<T>::t* __restrict__ arg,
+template <typename T, int NT, typename PX = void>
+__global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 1 : 2) k_xinv(const typename C2<T>::t* __restrict__ arg,
                                              typename C2<T>::t* __restrict__ res,
                                              const typename C2<T>::t* __restrict__ xhat,
                                              const uint32_t* __restrict__ line_off,
@@ -162,7 +165,8 @@ __global__ void __launch_bounds__(NT, 2) k_xinv(const typename C2<T>::t* __restr
     sm[l * g.pitchx + kx] = in[kx * kstride + l];
   }
   __syncthreads();
-  fft_lines<T, NT, true>(toff, nl, g.pitchx, 1, false, px, 0);
+  if constexpr (std::is_void<PX>::value) fft_lines<T, NT, true>(toff, nl, g.pitchx, 1, false, px, 0);
+  else plines<T, PX, NT, true>(toff, nl, g.pitchx, 1, 0);
   const size_t voff = ((size_t)b * 3 + c) * g.nvs;
   const T2* a = arg + voff;
   T2* r = res + voff;
@@ -335,8 +339,8 @@ struct ColGeom {
   int batches_per_rhs;       // for skipping converged right-hand sides
 };
 
-template <typename T, int NT>
-__global__ void __launch_bounds__(NT, 2) k_fft_cols(const typename C2<T>::t* in,
+template <typename T, int NT, typename PL = void>
+__global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 1 : 2) k_fft_cols(const typename C2<T>::t* in,
                                                  typename C2<T>::t* out, ColGeom cg,
                                                  FftPlanDev pl, int inverse,
                                                  const KrylovState* __restrict__ st, int mvskip) {
@@ -354,7 +358,9 @@ __global__ void __launch_bounds__(NT, 2) k_fft_cols(const typename C2<T>::t* in,
     sm[e * cg.pitch + k] = e < cg.n_in ? ib[e * cg.in_as + k] : czero<T2>();
   }
   __syncthreads();
-  fft_lines_dir<T, NT>(n, ti, 1, cg.pitch, true, pl, 0, inverse != 0);
+  if constexpr (std::is_void<PL>::value) fft_lines_dir<T, NT>(n, ti, 1, cg.pitch, true, pl, 0, inverse != 0);
+  else if (inverse) plines<T, PL, NT, true>(n, ti, 1, cg.pitch, 0);
+  else plines<T, PL, NT, false>(n, ti, 1, cg.pitch, 0);
   T2* ob = out + batch * cg.out_bs + i0;
   for (int i = threadIdx.x; i < cg.n_out * ti; i += NT) {
     const int e = i / ti, k = i - e * ti;

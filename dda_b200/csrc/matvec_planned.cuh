@@ -1,0 +1,252 @@
+// matvec_planned.cuh -- the y/z passes of the matvec with compile-time FFT
+// plans (fft_plan.cuh) for the tuned grid lengths.
+//
+// Per kx plane (k_yz_p), shared memory as for k_yz:
+//   z stage 0 runs on the fly while the plane is read from HBM (zero rows
+//   z >= bz are never stored), the remaining z stages run on the slab;
+//   each warp then takes kz rows: y stage 0 reads the row straight from the
+//   slab (zero padded), middle stages run on the warp's row buffer, and the
+//   last forward stage, the D-hat multiply and the first inverse stage are
+//   done in registers by one thread for all three components (the blocks of
+//   the last stage are contiguous, so no shared-memory pass separates them);
+//   the inverse y stage 0 writes the kept y < by entries back to the slab;
+//   the inverse z stages end with stage 0 writing z < bz to HBM.
+#pragma once
+
+#include "fft_plan.cuh"
+#include "matvec_kernels.cuh"
+
+namespace dda {
+
+// Tuned plans: a large first radix and a last radix of at most 8, so the
+// fused last stage holds 3 x R_last complex values per thread.
+template <int N> struct PlanFor { typedef void type; };
+template <> struct PlanFor<64> { typedef Plan<8, 8> type; };
+template <> struct PlanFor<80> { typedef Plan<10, 8> type; };
+template <> struct PlanFor<96> { typedef Plan<12, 8> type; };
+template <> struct PlanFor<100> { typedef Plan<20, 5> type; };
+template <> struct PlanFor<128> { typedef Plan<16, 8> type; };
+template <> struct PlanFor<160> { typedef Plan<20, 8> type; };
+template <> struct PlanFor<192> { typedef Plan<24, 8> type; };
+template <> struct PlanFor<200> { typedef Plan<25, 8> type; };
+template <> struct PlanFor<256> { typedef Plan<8, 4, 8> type; };
+template <> struct PlanFor<512> { typedef Plan<8, 8, 8> type; };
+
+// Radices of the tuned plan for n (host side), empty when there is none.
+inline std::vector<int> tuned_radices(int n) {
+  auto get = [](auto p) { return std::vector<int>(std::begin(decltype(p)::r), std::end(decltype(p)::r)); };
+  switch (n) {
+    case 64: return get(PlanFor<64>::type());
+    case 80: return get(PlanFor<80>::type());
+    case 96: return get(PlanFor<96>::type());
+    case 100: return get(PlanFor<100>::type());
+    case 128: return get(PlanFor<128>::type());
+    case 160: return get(PlanFor<160>::type());
+    case 192: return get(PlanFor<192>::type());
+    case 200: return get(PlanFor<200>::type());
+    case 256: return get(PlanFor<256>::type());
+    case 512: return get(PlanFor<512>::type());
+    default: return {};
+  }
+}
+
+// ---- z stage 0 fused with the plane read / write (whole CTA) -------------
+template <typename T, int NT, typename PZ>
+__device__ __forceinline__ void zp_first(const typename C2<T>::t* __restrict__ plane, int soff, int q,
+                                         int by, int bz, int twz) {
+  typedef typename C2<T>::t T2;
+  constexpr int R = PZ::r[0], S0 = PZ::N / R;
+  T2* sm = smem_at<T>(0);
+  const int W = 3 * by, nb = by * bz;
+  for (int b = threadIdx.x; b < W * S0; b += NT) {
+    const int j = b / W, l = b - j * W;
+    const int c = l / by, y = l - c * by;
+    T2 v[R];
+#pragma unroll
+    for (int m = 0; m < R; m++) {
+      const int z = j + m * S0;
+      v[m] = z < bz ? plane[c * nb + z * by + y] : czero<T2>();
+    }
+    butterfly<PZ, 0, false>(v, j, sm + twz);
+#pragma unroll
+    for (int m = 0; m < R; m++) sm[soff + (j + m * S0) * q + l] = v[m];
+  }
+  __syncthreads();
+}
+
+template <typename T, int NT, typename PZ>
+__device__ __forceinline__ void zp_last(typename C2<T>::t* __restrict__ plane, int soff, int q, int by,
+                                        int bz, int twz) {
+  typedef typename C2<T>::t T2;
+  constexpr int R = PZ::r[0], S0 = PZ::N / R;
+  T2* sm = smem_at<T>(0);
+  const int W = 3 * by, nb = by * bz;
+  for (int b = threadIdx.x; b < W * S0; b += NT) {
+    const int j = b / W, l = b - j * W;
+    const int c = l / by, y = l - c * by;
+    T2 v[R];
+#pragma unroll
+    for (int m = 0; m < R; m++) v[m] = sm[soff + (j + m * S0) * q + l];
+    butterfly<PZ, 0, true>(v, j, sm + twz);
+#pragma unroll
+    for (int m = 0; m < R; m++) {
+      const int z = j + m * S0;
+      if (z < bz) plane[c * nb + z * by + y] = v[m];
+    }
+  }
+}
+
+// ---- fused last y stage: forward, D-hat, inverse in registers -------------
+// Row buffer at shared offset ro (three lines, pitch py); kx, kz are
+// frequencies.  One warp.
+template <typename T, typename PY>
+__device__ __forceinline__ void row_dmul_stage(int ro, int py, const typename C2<T>::t* __restrict__ dc,
+                                               const MvGeom& g, int kx, int kz, int lane) {
+  typedef typename C2<T>::t T2;
+  constexpr int K = PY::K;
+  constexpr int R = PY::r[K - 1];
+  constexpr int NB = PY::N / R;
+  T2* sm = smem_at<T>(0);
+  for (int t = lane; t < NB; t += 32) {
+    T2 v0[R], v1[R], v2[R];
+    const int base = ro + t * R;
+#pragma unroll
+    for (int m = 0; m < R; m++) {
+      v0[m] = sm[base + m];
+      v1[m] = sm[base + py + m];
+      v2[m] = sm[base + 2 * py + m];
+    }
+    DftN<R, false, T2>::run(v0);
+    DftN<R, false, T2>::run(v1);
+    DftN<R, false, T2>::run(v2);
+#pragma unroll
+    for (int m = 0; m < R; m++) {
+      T2 d[6];
+      load_dhat<T>(dc, g.Gx, g.Gy, g.Gz, kx, PY::freq_of(t * R + m), kz, d);
+      dmul(d, v0[m], v1[m], v2[m]);
+    }
+    DftN<R, true, T2>::run(v0);
+    DftN<R, true, T2>::run(v1);
+    DftN<R, true, T2>::run(v2);
+#pragma unroll
+    for (int m = 0; m < R; m++) {
+      sm[base + m] = v0[m];
+      sm[base + py + m] = v1[m];
+      sm[base + 2 * py + m] = v2[m];
+    }
+  }
+  __syncwarp();
+}
+
+// y stage 0 fused with the row read from the slab (row kz, y < by) or the
+// write back; items (component, butterfly) over the warp's lanes.
+template <typename T, typename PY, bool INV>
+__device__ __forceinline__ void row_stage0(typename C2<T>::t* S, int kz, int q, int by, int ro, int py,
+                                           int twy, int lane) {
+  typedef typename C2<T>::t T2;
+  constexpr int R = PY::r[0], S0 = PY::N / R;
+  T2* sm = smem_at<T>(0);
+  for (int it = lane; it < 3 * S0; it += 32) {
+    const int c = it / S0, j = it - c * S0;
+    T2 v[R];
+    if (!INV) {
+#pragma unroll
+      for (int m = 0; m < R; m++) {
+        const int y = j + m * S0;
+        v[m] = y < by ? S[kz * q + c * by + y] : czero<T2>();
+      }
+      butterfly<PY, 0, false>(v, j, sm + twy);
+#pragma unroll
+      for (int m = 0; m < R; m++) sm[ro + c * py + j + m * S0] = v[m];
+    } else {
+#pragma unroll
+      for (int m = 0; m < R; m++) v[m] = sm[ro + c * py + j + m * S0];
+      butterfly<PY, 0, true>(v, j, sm + twy);
+#pragma unroll
+      for (int m = 0; m < R; m++) {
+        const int y = j + m * S0;
+        if (y < by) S[kz * q + c * by + y] = v[m];
+      }
+    }
+  }
+  __syncwarp();
+}
+
+template <typename T, int NT, typename PZ, typename PY>
+__global__ void __launch_bounds__(NT, 1) k_yz_p(typename C2<T>::t* __restrict__ xhat,
+                                             const typename C2<T>::t* __restrict__ dc, MvGeom g,
+                                             YzGeom y, FftPlanDev pz, FftPlanDev pyp,
+                                             const KrylovState* __restrict__ st, int mvskip) {
+  static_assert(PY::K >= 2 && PZ::K >= 2, "tuned plans have at least two stages");
+  typedef typename C2<T>::t T2;
+  const int kx = blockIdx.x, b = blockIdx.y;  // kx: position after the x transform
+  if (rhs_idle(st, b, mvskip)) return;
+  const int soff = yz_slab_off(g), roff = yz_rows_off(g, y);
+  T2* S = smem_at<T>(soff);
+  T2* plane = xhat + ((size_t)b * g.Gx + kx) * 3 * g.nlines;
+  stage_twiddles<T, NT>(0, pz);
+  stage_twiddles<T, NT>(g.Gz, pyp);
+  __syncthreads();
+  zp_first<T, NT, PZ>(plane, soff, y.q, g.by, g.bz, 0);
+  const int w3 = 3 * g.by;
+  plines<T, PZ, NT, false, 1, PZ::K>(soff, w3, 1, y.q, 0);
+  {
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int kxf = g.fx[kx];
+    if (w < y.nrw) {
+      const int ro = roff + w * 3 * y.py;
+      for (int kz = w; kz < g.Gz; kz += y.nrw) {  // kz: position after the z transform
+        row_stage0<T, PY, false>(S, kz, y.q, g.by, ro, y.py, g.Gz, lane);
+        pstages<T, PY, false, 32, 1, PY::K - 1>(ro, 3, y.py, 1, g.Gz, lane);
+        row_dmul_stage<T, PY>(ro, y.py, dc, g, kxf, PZ::freq_of(kz), lane);
+        pstages<T, PY, true, 32, 1, PY::K - 1>(ro, 3, y.py, 1, g.Gz, lane);
+        row_stage0<T, PY, true>(S, kz, y.q, g.by, ro, y.py, g.Gz, lane);
+      }
+    }
+    __syncthreads();
+  }
+  plines<T, PZ, NT, true, 1, PZ::K>(soff, w3, 1, y.q, 0);
+  zp_last<T, NT, PZ>(plane, soff, y.q, g.by, g.bz, 0);
+}
+
+// Split path rows with a compile-time y plan: each warp one kz row, copied
+// into its row buffer (zero padded), then the fused pipeline, then back.
+template <typename T, int NT, typename PY>
+__global__ void __launch_bounds__(NT, 1) k_yrows_p(typename C2<T>::t* __restrict__ zbuf,
+                                                const typename C2<T>::t* __restrict__ dc, MvGeom g,
+                                                YzGeom y, FftPlanDev pyp,
+                                                const KrylovState* __restrict__ st, int mvskip) {
+  typedef typename C2<T>::t T2;
+  const int kx = blockIdx.y, b = blockIdx.z;
+  if (rhs_idle(st, b, mvskip)) return;
+  const int kz0 = blockIdx.x * y.nrw;
+  const int nr = min(y.nrw, g.Gz - kz0);
+  T2* base = zbuf + ((size_t)b * g.Gx + kx) * 3 * (size_t)g.Gz * g.by;
+  const size_t cs = (size_t)g.Gz * g.by;
+  const int roff = g.Gy;
+  T2* R = smem_at<T>(roff);
+  stage_twiddles<T, NT>(0, pyp);
+  for (int i = threadIdx.x; i < nr * 3 * g.Gy; i += NT) {
+    const int rc = i / g.Gy, yy = i - rc * g.Gy;
+    const int row = rc / 3, c = rc - 3 * row;
+    R[rc * y.py + yy] = yy < g.by ? base[c * cs + (size_t)(kz0 + row) * g.by + yy] : czero<T2>();
+  }
+  __syncthreads();
+  {
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (w < nr) {
+      const int ro = roff + w * 3 * y.py;
+      pstages<T, PY, false, 32, 0, PY::K - 1>(ro, 3, y.py, 1, 0, lane);
+      row_dmul_stage<T, PY>(ro, y.py, dc, g, g.fx[kx], g.fz[kz0 + w], lane);
+      pstages<T, PY, true, 32, 0, PY::K - 1>(ro, 3, y.py, 1, 0, lane);
+    }
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < nr * 3 * g.by; i += NT) {
+    const int rc = i / g.by, yy = i - rc * g.by;
+    const int row = rc / 3, c = rc - 3 * row;
+    base[c * cs + (size_t)(kz0 + row) * g.by + yy] = R[rc * y.py + yy];
+  }
+}
+
+}  // namespace dda

@@ -75,6 +75,9 @@ typedef struct dda_problem {
  * buffer even when a kx plane fits in shared memory (the path large grids
  * take); used by tests and tuning. */
 #define DDA_FLAG_SPLIT_YZ 1u
+/* dda_problem.flags: use the runtime-planned FFT kernels even when every grid
+ * edge has a compile-time plan; used by tests and tuning. */
+#define DDA_FLAG_RUNTIME_PLANS 2u
 
 typedef struct dda_stats {
   int64_t iterations;   /* Krylov iterations (summed over inner solves for MIXED) */

@@ -55,6 +55,19 @@ def test_matvec_split_yz_path(prec, tol):
     assert rel(pr.mv.apply(x), pr.op.matvec(x)) < tol
 
 
+@pytest.mark.parametrize("flags", [0, 1, 2, 3])
+@pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("fp32", FP32_TOL)])
+def test_matvec_kernel_paths(flags, prec, tol):
+    # README workload 1 (grid 80^3) has compile-time FFT plans; flags select
+    # the split y/z path (1) and the runtime-planned kernels (2).
+    kind, args, mats, lam = CASES["cfg1"]
+    pr = Pair(kind, args, mats, lam, prec, flags=flags)
+    pr.set_cc((0, 0, 1), 2, "ldr")
+    x = pr.rand_vec(17)
+    assert rel(pr.mv.apply(x), pr.op.matvec(x)) < tol
+    assert rel(pr.mv.apply(x, conj=True), pr.op.matvec(x, conj=True)) < tol
+
+
 def test_matvec_host_dmatrix():
     kind, args, mats, lam = CASES["aniso"]
     pr = Pair(kind, args, mats, lam, "fp64", host_d=True)

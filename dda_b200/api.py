@@ -71,6 +71,7 @@ def lib():
         "dda_launch_count": ([vp], ctypes.c_int64),
         "dda_profile_matvec": ([vp, ctypes.c_int, ctypes.c_int, dp], ctypes.c_int),
         "dda_synchronize": ([vp], ctypes.c_int),
+        "dda_far_field": ([vp, ctypes.c_int, dp, ctypes.c_int64, dp, dp], ctypes.c_int),
         "dda_frontend_error": ([], cp),
         "dda_fft_fit": ([ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int], ctypes.c_uint32),
         "dda_parse_length_m": ([cp, dp], ctypes.c_int),
@@ -317,6 +318,17 @@ class CudaMatVec:
 
     def synchronize(self):
         self._check(lib().dda_synchronize(self.h))
+
+    def far_field(self, dirs, nrhs=1, pol=None):
+        """Scattered far field E(n) for directions dirs [ndir][3] (particle
+        frame) of `pol` ([nrhs][3 nvs]) or of the last solve: [ndir][nrhs][3]."""
+        d = np.ascontiguousarray(dirs, dtype=np.float64).reshape(-1, 3)
+        out = np.zeros((len(d), nrhs, 3), dtype=np.complex128)
+        pp = None
+        if pol is not None:
+            pa, pp = _cbuf(pol)
+        self._check(lib().dda_far_field(self.h, nrhs, pp, len(d), _dp(d), _dp(out.view(np.float64))))
+        return out
 
     @property
     def stream(self):

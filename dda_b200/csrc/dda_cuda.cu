@@ -24,6 +24,7 @@
 
 #include "../../include/dda_cuda.h"
 #include "dmatrix_kernels.cuh"
+#include "farfield_kernels.cuh"
 #include "fft_engine.cuh"
 #include "krylov_kernels.cuh"
 #include "krylov_ops.cuh"
@@ -266,13 +267,15 @@ template <typename T> void setup_engine(dda_ctx* c) {
   y.py = g.Gy + 1;
   const size_t fixed = ((size_t)g.Gz + g.Gy + (size_t)g.Gz * y.q) * s;
   const size_t row = (size_t)3 * y.py * s;
-  int nrw = NW;
+  e.k = c->planned ? planned_kernels<T, kNtX, kNtYz, kNtC>(g.Gx, g.Gy, g.Gz)
+                   : generic_kernels<T, kNtX, kNtYz, kNtC>();
+  // row buffers: one per warp in the runtime-planned kernel, batches of up
+  // to 32 rows in the planned one
+  int nrw = c->planned ? 32 : NW;
   while (nrw > 1 && fixed + nrw * row > kSmemMax) nrw--;
   y.nrw = nrw;
   e.yz = y;
   e.smem_yz = fixed + nrw * row;
-  e.k = c->planned ? planned_kernels<T, kNtX, kNtYz, kNtC>(g.Gx, g.Gy, g.Gz)
-                   : generic_kernels<T, kNtX, kNtYz, kNtC>();
   e.fused = e.k.yz && e.smem_yz <= kSmemMax && !(c->flags & DDA_FLAG_SPLIT_YZ);
   if (!e.fused) {
     // split path: zbuf, k_yrows over NW rows per CTA, column FFTs along z
@@ -1152,6 +1155,61 @@ int dda_profile_matvec(dda_ctx* ctx, int nrhs, int reps, double* ms) {
     if (nrhs < 1 || nrhs > ctx->max_rhs) throw DdaError(DDA_ERR_ARG, "bad nrhs");
     if (ctx->e32.on) profile_t<float>(ctx, nrhs, reps, ms);
     else profile_t<double>(ctx, nrhs, reps, ms);
+    return DDA_OK;
+  });
+}
+
+}  // extern "C"
+
+namespace {
+template <typename T>
+void far_field_t(dda_ctx* c, int nrhs, const double* pol, long long ndir, const double* dirs, double* out) {
+  typedef typename C2<T>::t T2;
+  Engine<T>& e = eng<T>(c);
+  const size_t n = (size_t)nrhs * 3 * c->g.nvs;
+  if (pol) host_to_engine<T>(c, pol, e.io, n);
+  double* ddirs = nullptr;
+  double2* dout = nullptr;
+  CK(cudaMalloc(&ddirs, ndir * 3 * sizeof(double)));
+  CK(cudaMalloc(&dout, (size_t)ndir * nrhs * 3 * sizeof(double2)));
+  CK(cudaMemcpyAsync(ddirs, dirs, ndir * 3 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  FfGeom g;
+  g.nv = c->g.nv;
+  g.nvs = c->g.nvs;
+  g.by = c->g.by;
+  g.nlines = c->g.nlines;
+  g.bx = c->g.bx;
+  g.kd = c->kd;
+  g.k = c->kd / c->grid_unit;
+  // DipoleGeometry::moveToCenter (DDA/DipoleGeometry.cpp:75-80)
+  g.ox = -((double)c->g.bx - 1) / 2 * c->grid_unit;
+  g.oy = -((double)c->g.by - 1) / 2 * c->grid_unit;
+  g.oz = -((double)c->g.bz - 1) / 2 * c->grid_unit;
+  constexpr int DB = 4, NT = 256;
+  const size_t smem = (size_t)DB * g.bx * sizeof(double2);
+  if (smem > kSmemMax) throw DdaError(DDA_ERR_UNSUPPORTED, "box too long for the far-field tables");
+  CK(cudaFuncSetAttribute((const void*)k_farfield<T, NT, DB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)std::max<size_t>(smem, 1)));
+  k_farfield<T, NT, DB><<<dim3((unsigned)((ndir + DB - 1) / DB), nrhs), NT, smem, c->stream>>>(
+      e.io, c->line_off, c->dip, c->perm, ddirs, (int)ndir, g, dout);
+  CK(cudaGetLastError());
+  c->launches++;
+  CK(cudaMemcpyAsync(out, dout, (size_t)ndir * nrhs * 3 * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  cudaFree(ddirs);
+  cudaFree(dout);
+}
+}  // namespace
+
+extern "C" {
+
+int dda_far_field(dda_ctx* ctx, int nrhs, const double* pol, int64_t ndir, const double* dirs, double* out) {
+  if (!ctx) return DDA_ERR_ARG;
+  return guard(ctx, [&]() -> int {
+    if (nrhs < 1 || nrhs > ctx->max_rhs || ndir < 1 || !dirs || !out) throw DdaError(DDA_ERR_ARG, "bad far-field arguments");
+    if (ndir > (1LL << 31) / 4) throw DdaError(DDA_ERR_ARG, "too many directions");
+    if (ctx->precision == DDA_PREC_FP32) far_field_t<float>(ctx, nrhs, pol, ndir, dirs, out);
+    else far_field_t<double>(ctx, nrhs, pol, ndir, dirs, out);
     return DDA_OK;
   });
 }

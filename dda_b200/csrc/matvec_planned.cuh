@@ -172,6 +172,90 @@ __device__ __forceinline__ void row_stage0(typename C2<T>::t* S, int kz, int q, 
   __syncwarp();
 }
 
+// ---- CTA-wide batches of kz rows ------------------------------------------
+// Rows [kz0, kz0+nr) of the slab are transformed together by the whole CTA:
+// row r, component c lives in the row buffers at ro + (3 r + c) py.
+
+// y stage 0 fused with the read from (INV: write to) the slab, zero padded.
+template <typename T, int NT, typename PY, bool INV>
+__device__ __forceinline__ void rows_stage0(typename C2<T>::t* S, int kz0, int nr, int q, int by, int ro,
+                                            int py, int twy) {
+  typedef typename C2<T>::t T2;
+  constexpr int R = PY::r[0], S0 = PY::N / R;
+  T2* sm = smem_at<T>(0);
+  const int total = nr * 3 * S0;
+  for (int it = threadIdx.x; it < total; it += NT) {
+    const int j = it % S0, rc = it / S0;
+    const int row = rc / 3, c = rc - 3 * row;
+    const int srow = (kz0 + row) * q + c * by;
+    const int rb = ro + rc * py;
+    T2 v[R];
+    if (!INV) {
+#pragma unroll
+      for (int m = 0; m < R; m++) {
+        const int yy = j + m * S0;
+        v[m] = yy < by ? S[srow + yy] : czero<T2>();
+      }
+      butterfly<PY, 0, false>(v, j, sm + twy);
+#pragma unroll
+      for (int m = 0; m < R; m++) sm[rb + j + m * S0] = v[m];
+    } else {
+#pragma unroll
+      for (int m = 0; m < R; m++) v[m] = sm[rb + j + m * S0];
+      butterfly<PY, 0, true>(v, j, sm + twy);
+#pragma unroll
+      for (int m = 0; m < R; m++) {
+        const int yy = j + m * S0;
+        if (yy < by) S[srow + yy] = v[m];
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// last forward y stage, D-hat multiply, first inverse y stage, in registers
+// (kz positions kz0.. map to frequencies through PZ).
+template <typename T, int NT, typename PY, typename PZ>
+__device__ __forceinline__ void rows_dmul(int kz0, int nr, int ro, int py,
+                                          const typename C2<T>::t* __restrict__ dc, const MvGeom& g, int kx) {
+  typedef typename C2<T>::t T2;
+  constexpr int K = PY::K;
+  constexpr int R = PY::r[K - 1];
+  constexpr int NB = PY::N / R;
+  T2* sm = smem_at<T>(0);
+  for (int it = threadIdx.x; it < nr * NB; it += NT) {
+    const int t = it % NB, row = it / NB;
+    const int kz = PZ::freq_of(kz0 + row);
+    const int base = ro + 3 * row * py + t * R;
+    T2 v0[R], v1[R], v2[R];
+#pragma unroll
+    for (int m = 0; m < R; m++) {
+      v0[m] = sm[base + m];
+      v1[m] = sm[base + py + m];
+      v2[m] = sm[base + 2 * py + m];
+    }
+    DftN<R, false, T2>::run(v0);
+    DftN<R, false, T2>::run(v1);
+    DftN<R, false, T2>::run(v2);
+#pragma unroll
+    for (int m = 0; m < R; m++) {
+      T2 d[6];
+      load_dhat<T>(dc, g.Gx, g.Gy, g.Gz, kx, PY::freq_of(t * R + m), kz, d);
+      dmul(d, v0[m], v1[m], v2[m]);
+    }
+    DftN<R, true, T2>::run(v0);
+    DftN<R, true, T2>::run(v1);
+    DftN<R, true, T2>::run(v2);
+#pragma unroll
+    for (int m = 0; m < R; m++) {
+      sm[base + m] = v0[m];
+      sm[base + py + m] = v1[m];
+      sm[base + 2 * py + m] = v2[m];
+    }
+  }
+  __syncthreads();
+}
+
 template <typename T, int NT, typename PZ, typename PY>
 __global__ void __launch_bounds__(NT, 1) k_yz_p(typename C2<T>::t* __restrict__ xhat,
                                              const typename C2<T>::t* __restrict__ dc, MvGeom g,
@@ -191,19 +275,15 @@ __global__ void __launch_bounds__(NT, 1) k_yz_p(typename C2<T>::t* __restrict__ 
   const int w3 = 3 * g.by;
   plines<T, PZ, NT, false, 1, PZ::K>(soff, w3, 1, y.q, 0);
   {
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int kxf = g.fx[kx];
-    if (w < y.nrw) {
-      const int ro = roff + w * 3 * y.py;
-      for (int kz = w; kz < g.Gz; kz += y.nrw) {  // kz: position after the z transform
-        row_stage0<T, PY, false>(S, kz, y.q, g.by, ro, y.py, g.Gz, lane);
-        pstages<T, PY, false, 32, 1, PY::K - 1>(ro, 3, y.py, 1, g.Gz, lane);
-        row_dmul_stage<T, PY>(ro, y.py, dc, g, kxf, PZ::freq_of(kz), lane);
-        pstages<T, PY, true, 32, 1, PY::K - 1>(ro, 3, y.py, 1, g.Gz, lane);
-        row_stage0<T, PY, true>(S, kz, y.q, g.by, ro, y.py, g.Gz, lane);
-      }
+    for (int kz0 = 0; kz0 < g.Gz; kz0 += y.nrw) {  // kz: positions after the z transform
+      const int nr = min(y.nrw, g.Gz - kz0);
+      rows_stage0<T, NT, PY, false>(S, kz0, nr, y.q, g.by, roff, y.py, g.Gz);
+      pstages<T, PY, false, NT, 1, PY::K - 1>(roff, 3 * nr, y.py, 1, g.Gz, threadIdx.x);
+      rows_dmul<T, NT, PY, PZ>(kz0, nr, roff, y.py, dc, g, kxf);
+      pstages<T, PY, true, NT, 1, PY::K - 1>(roff, 3 * nr, y.py, 1, g.Gz, threadIdx.x);
+      rows_stage0<T, NT, PY, true>(S, kz0, nr, y.q, g.by, roff, y.py, g.Gz);
     }
-    __syncthreads();
   }
   plines<T, PZ, NT, true, 1, PZ::K>(soff, w3, 1, y.q, 0);
   zp_last<T, NT, PZ>(plane, soff, y.q, g.by, g.bz, 0);

@@ -1,0 +1,93 @@
+"""Far-field and cross-section post-processing of the dipole polarisations.
+
+The per-direction sums run on the GPU (dda_far_field); this module restates
+the reference's host-side assembly around them:
+
+  grid_angles        GridAngleList (EMSim/AngleList.cpp:71-106): theta-major
+                     grid from "start..end/count" specifications in degrees
+  scattering_frame   FarFieldCalc::calcEField (DDA/FarFieldCalc.cpp:119-160):
+                     direction, perpendicular and parallel vectors per angle
+  jones              JonesCalculus::getJonesMatrix (EMSim/JonesCalculus.cpp:74-86)
+  cross_sections     PlaneWave::extCross (DDA/Beam.cpp:126-133),
+                     AbsCross::absCross (DDA/AbsCross.cpp:28-48) and the
+                     efficiencies of outputCrossSections (DDA/DDAMain.cpp:284-304)
+"""
+import math
+
+import numpy as np
+
+from . import api
+
+
+def parse_angles(spec):
+    """'a' or 'start..end/count' in degrees -> (start_rad, step_rad, count)."""
+    if ".." not in spec:
+        return math.radians(float(spec)), 0.0, 1
+    start, rest = spec.split("..")
+    end, n = rest.split("/")
+    start, end, n = math.radians(float(start)), math.radians(float(end)), int(n)
+    step = 0.0 if n <= 1 else (end - start) / (n - 1)
+    return start, step, n
+
+
+def grid_angles(theta_spec="0..180/91", phi_spec="0..360/61"):
+    """Theta-major angle grid: angle i has theta index i // nPhi."""
+    t0, dt, nt = parse_angles(theta_spec)
+    p0, dp, npf = parse_angles(phi_spec)
+    i = np.arange(nt * npf)
+    return t0 + (i // npf) * dt, p0 + (i % npf) * dp
+
+
+def scattering_frame(prop, theta, phi):
+    """Directions n, perpendicular and parallel vectors for each angle, in
+    the frame (prop, incPolX = polarisation 2, incPolY = polarisation 1)."""
+    px, pn = api.beam_pol(prop, 2)
+    py, _ = api.beam_pol(prop, 1)
+    st, ct = np.sin(theta)[:, None], np.cos(theta)[:, None]
+    sp, cp = np.sin(phi)[:, None], np.cos(phi)[:, None]
+    n = ct * pn + st * (cp * px + sp * py)
+    perp = sp * px - cp * py
+    par = -st * pn + ct * (cp * px + sp * py)
+    return n, perp, par
+
+
+def jones(e1, e2, theta, phi, perp, par):
+    """Jones matrices [count][2][2] from the far fields e1 (polarisation 1)
+    and e2 (polarisation 2), each [count][3] complex."""
+    f1par, f1perp = np.einsum("ij,ij->i", e1, par), np.einsum("ij,ij->i", e1, perp)
+    f2par, f2perp = np.einsum("ij,ij->i", e2, par), np.einsum("ij,ij->i", e2, perp)
+    sp, cp = np.sin(phi), np.cos(phi)
+    out = np.empty((len(theta), 2, 2), dtype=np.complex128)
+    out[:, 0, 0] = cp * f2par + sp * f1par
+    out[:, 0, 1] = sp * f2par - cp * f1par
+    out[:, 1, 0] = cp * f2perp + sp * f1perp
+    out[:, 1, 1] = sp * f2perp - cp * f1perp
+    return out
+
+
+def jones_far_field(mv, prop, theta, phi, pol=None):
+    """Jones matrices on an angle grid from the two polarisations of the last
+    solve (right-hand sides 0 and 1 of `mv`) or of `pol` ([2][3 nvs])."""
+    n, perp, par = scattering_frame(prop, theta, phi)
+    e = mv.far_field(n, nrhs=2, pol=pol)  # [count][2][3]
+    return jones(e[:, 0, :], e[:, 1, :], theta, phi, perp, par)
+
+
+def cross_sections(params, cc, pol_vec, e_forward, prop, pol):
+    """(Cext, Cabs, Qext, Qabs) of one solution: e_forward = far field in the
+    propagation direction, cc the CoupleConstants of that right-hand side."""
+    inc, _ = api.beam_pol(prop, pol)
+    k = params.wave_num
+    cext = -np.dot(np.real(e_forward), inc) * 4 * np.pi / k
+    temp1 = k ** 3 * 2 / 3
+    multdr = -np.imag(1.0 / cc.cc) - temp1  # [nmat*3]
+    nvs, nv = params.nvs, params.nv
+    mat = params.geometry.materials.astype(np.int64)
+    p = np.asarray(pol_vec).reshape(3, nvs)[:, :nv]
+    cabs = 0.0
+    for c in range(3):
+        cabs += np.sum(multdr[mat * 3 + c] * np.abs(p[c]) ** 2)
+    cabs *= 4 * np.pi * k
+    a_eq = (3.0 / (4 * np.pi) * nv) ** (1.0 / 3) * params.grid_unit
+    norm = 1.0 / (np.pi * a_eq * a_eq)
+    return cext, cabs, cext * norm, cabs * norm

@@ -164,6 +164,16 @@ int64_t dda_launch_count(const dda_ctx* ctx);
  * (DDA/GpuMatVec.cpp:149-153). */
 int dda_profile_matvec(dda_ctx* ctx, int nrhs, int reps, double* ms);
 
+/* Scattered far field E(n) = i k^2 exp(-i k origin.n) (S - n (n.S)),
+ * S = sum_j P_j exp(-i kd n.r_j), for ndir unit directions `dirs` (host,
+ * ndir*3, particle frame) and nrhs right-hand sides: out[ndir][nrhs][3]
+ * complex (host).  P is `pol` (host, [nrhs][3][nvs]) or, when pol is NULL,
+ * the polarisations of the last dda_solve / dda_solve_device on the context.
+ * Replaces FieldCalculator<T>::calcField (DDA/FieldCalculator.hpp:57-58,
+ * DDA/CpuFieldCalculator.cpp:48-98, DDA/GpuFieldCalculatorInst.cl:27-70) and
+ * its per-direction host loop (DDA/FarFieldCalc.cpp:131-155). */
+int dda_far_field(dda_ctx* ctx, int nrhs, const double* pol, int64_t ndir, const double* dirs, double* out);
+
 /* Copies the D matrix out in the reference layout ([Gx][Gz][Gy][6] complex
  * FP64, reference units), expanded from the octant the context stores. */
 int dda_get_dmatrix(dda_ctx* ctx, double* out);

@@ -1093,3 +1093,128 @@ int orc_solve(orc_problem* p, int solver, const double* eincD, double eps,
 }
 
 }  // extern "C"
+
+// ========================================================= post-process ===
+extern "C" {
+
+// CpuFieldCalculator::calcField (DDA/CpuFieldCalculator.cpp:48-98): scattered
+// far field in direction n (particle frame) of polarisations pvec:
+// E = i k^2 exp(-i k origin.n) (S - n (n.S)), S = sum_j P_j exp(-i kd n.r_j).
+void orc_calc_field(const orc_problem* p, const double* pvecD, const double* n, double* out6) {
+  const cd* pv = reinterpret_cast<const cd*>(pvecD);
+  cd sum[3] = {0, 0, 0};
+  for (uint32_t j = 0; j < p->nv; j++) {
+    const double ph = -p->kd * (n[0] * p->pos[3 * j] + n[1] * p->pos[3 * j + 1] + n[2] * p->pos[3 * j + 2]);
+    const cd a = std::polar(1.0, ph);
+    for (int c = 0; c < 3; c++) sum[c] += pv[j + c * p->nvs] * a;
+  }
+  const cd ndots = n[0] * sum[0] + n[1] * sum[1] + n[2] * sum[2];
+  double on = 0;
+  for (int c = 0; c < 3; c++) on += (double)p->origin[c] * n[c];
+  const cd f = cd(0, p->waveNum * p->waveNum) * std::polar(1.0, -p->waveNum * on);
+  for (int c = 0; c < 3; c++) {
+    const cd e = f * (sum[c] - n[c] * ndots);
+    out6[2 * c] = e.real();
+    out6[2 * c + 1] = e.imag();
+  }
+}
+
+// PlaneWave::extCross (DDA/Beam.cpp:126-133) and AbsCross::absCross
+// (DDA/AbsCross.cpp:28-48) for the couple constants currently set.
+void orc_cross_sections(const orc_problem* p, const double* pvecD, const double* propIn, int pol,
+                        double* cext, double* cabs) {
+  double incPol[3], prop[3];
+  orc_beam_pol(propIn, pol, incPol, prop);
+  double e[6];
+  orc_calc_field(p, pvecD, prop, e);
+  double s = -(e[0] * incPol[0] + e[2] * incPol[1] + e[4] * incPol[2]);
+  *cext = s * (double)kFourPi / p->waveNum;
+  const cd* pv = reinterpret_cast<const cd*>(pvecD);
+  const double temp1 = std::pow(p->waveNum, 3.0) * 2 / 3;
+  double sum = 0;
+  for (uint32_t i = 0; i < p->nv; i++)
+    for (int c = 0; c < 3; c++) {
+      const double mdr = -std::imag(1.0 / p->cc[p->mat[i] * 3 + c]) - temp1;
+      sum += mdr * std::norm(pv[i + c * p->nvs]);
+    }
+  *cabs = (double)kFourPi * p->waveNum * sum;
+}
+
+// Jones far field (DDA/FarFieldCalc.cpp:119-160, EMSim/JonesCalculus.cpp:74-86)
+// from the polarisations of the two incident polarisations (no symmetry
+// shortcut): jones[i] = {S11, S12, S21, S22} complex for angle i.
+void orc_jones(const orc_problem* p, const double* pol1, const double* pol2, const double* propIn,
+               const double* theta, const double* phi, int64_t count, double* jones) {
+  double px[3], py[3], prop[3];
+  orc_beam_pol(propIn, 2, px, prop);  // incPolX = polarisation 2
+  orc_beam_pol(propIn, 1, py, nullptr);  // incPolY = polarisation 1
+#pragma omp parallel for schedule(dynamic)
+  for (long long i = 0; i < count; i++) {
+    const double st = std::sin(theta[i]), ct = std::cos(theta[i]);
+    const double sp = std::sin(phi[i]), cp = std::cos(phi[i]);
+    double n[3], perp[3], par[3];
+    for (int a = 0; a < 3; a++) {
+      n[a] = ct * prop[a] + st * (cp * px[a] + sp * py[a]);
+      perp[a] = sp * px[a] - cp * py[a];
+      par[a] = -st * prop[a] + ct * (cp * px[a] + sp * py[a]);
+    }
+    cd fpar[2], fperp[2];
+    const double* pols[2] = {pol1, pol2};
+    for (int k = 0; k < 2; k++) {
+      double e[6];
+      orc_calc_field(p, pols[k], n, e);
+      cd ev[3] = {cd(e[0], e[1]), cd(e[2], e[3]), cd(e[4], e[5])};
+      fpar[k] = ev[0] * par[0] + ev[1] * par[1] + ev[2] * par[2];
+      fperp[k] = ev[0] * perp[0] + ev[1] * perp[1] + ev[2] * perp[2];
+    }
+    cd out[4] = {cp * fpar[1] + sp * fpar[0], sp * fpar[1] - cp * fpar[0],
+                 cp * fperp[1] + sp * fperp[0], sp * fperp[1] - cp * fperp[0]};
+    for (int k = 0; k < 4; k++) {
+      jones[8 * i + 2 * k] = out[k].real();
+      jones[8 * i + 2 * k + 1] = out[k].imag();
+    }
+  }
+}
+
+// Bohren & Huffman BHMIE efficiencies as restated in EMSim/Mie.cpp:41-174
+// (long double): size parameter x, relative index m.
+void orc_mie(double xD, double mre, double mim, double* qext, double* qsca, double* qabs) {
+  typedef long double f;
+  typedef std::complex<f> c;
+  const f x = xD;
+  const c refrel(mre, mim);
+  const c cxy = x * refrel;
+  const f xstop = x + 4 * std::pow(x, (f)1 / 3) + 2;
+  const size_t nstop = (size_t)xstop;
+  const f ymod = std::abs(cxy);
+  const size_t nmx = (size_t)(std::max(xstop, ymod) + 15);
+  std::vector<c> cxd(nmx);
+  cxd[nmx - 1] = 0;
+  for (size_t i = nmx - 1; i > 0; i--) cxd[i - 1] = f(i + 1) / cxy - c(1) / (cxd[i] + f(i + 1) / cxy);
+  f psi0 = std::cos(x), psi1 = std::sin(x), chi0 = -std::sin(x), chi1 = std::cos(x);
+  f apsi1 = psi1;
+  c cxxi1 = c(apsi1, -chi1);
+  f qs = 0;
+  c s1fwd = 0;
+  for (size_t n = 0; n < nstop; n++) {
+    const f rn = n + 1;
+    const f fn = (2 * rn + 1) / (rn * (rn + 1));
+    const f psi = (2 * rn - 1) * psi1 / x - psi0;
+    const f chi = (2 * rn - 1) * chi1 / x - chi0;
+    const c cxxi = c(psi, -chi);
+    const c an = ((cxd[n] / refrel + rn / x) * psi - apsi1) / ((cxd[n] / refrel + rn / x) * cxxi - cxxi1);
+    const c bn = ((refrel * cxd[n] + rn / x) * psi - apsi1) / ((refrel * cxd[n] + rn / x) * cxxi - cxxi1);
+    qs += (2 * rn + 1) * (std::norm(an) + std::norm(bn));
+    // forward direction (mu = 1): pi_n = tau_n = n (n+1) / 2
+    const f pin = rn * (rn + 1) / 2;
+    s1fwd += fn * (an * pin + bn * pin);
+    psi0 = psi1; psi1 = psi; apsi1 = psi1;
+    chi0 = chi1; chi1 = chi;
+    cxxi1 = c(apsi1, -chi1);
+  }
+  *qsca = (double)((2 / (x * x)) * qs);
+  *qext = (double)((4 / (x * x)) * std::real(s1fwd));
+  *qabs = *qext - *qsca;
+}
+
+}  // extern "C"

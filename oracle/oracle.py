@@ -83,6 +83,10 @@ def lib():
                                 dp, dp, ctypes.POINTER(OrcStats), ctypes.c_int64, dp,
                                 ctypes.c_int64]
         L.orc_solve.restype = ctypes.c_int
+        L.orc_calc_field.argtypes = [vp, dp, dp, dp]
+        L.orc_cross_sections.argtypes = [vp, dp, dp, ctypes.c_int, dp, dp]
+        L.orc_jones.argtypes = [vp, dp, dp, dp, dp, dp, ctypes.c_int64, dp]
+        L.orc_mie.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double, dp, dp, dp]
         _lib = L
     return _lib
 
@@ -273,6 +277,31 @@ class Problem:
         lib().orc_einc(self.h, _dp(np.asarray(prop, dtype=np.float64)), pol, _dp(out))
         return out
 
+    def calc_field(self, pvec, n):
+        p = np.ascontiguousarray(pvec, dtype=np.complex128)
+        out = np.zeros(3, dtype=np.complex128)
+        lib().orc_calc_field(self.h, _dp(p), _dp(np.asarray(n, dtype=np.float64)), _dp(out))
+        return out
+
+    def cross_sections(self, pvec, prop, pol):
+        """(Cext, Cabs) for the couple constants currently set."""
+        p = np.ascontiguousarray(pvec, dtype=np.complex128)
+        a, b = ctypes.c_double(), ctypes.c_double()
+        lib().orc_cross_sections(self.h, _dp(p), _dp(np.asarray(prop, dtype=np.float64)), pol,
+                                 ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
+
+    def jones(self, pol1, pol2, prop, theta, phi):
+        """Jones matrices [count][2][2] for polarisation-1/2 solutions."""
+        p1 = np.ascontiguousarray(pol1, dtype=np.complex128)
+        p2 = np.ascontiguousarray(pol2, dtype=np.complex128)
+        th = np.ascontiguousarray(theta, dtype=np.float64)
+        ph = np.ascontiguousarray(phi, dtype=np.float64)
+        out = np.zeros((len(th), 2, 2), dtype=np.complex128)
+        lib().orc_jones(self.h, _dp(p1), _dp(p2), _dp(np.asarray(prop, dtype=np.float64)), _dp(th),
+                        _dp(ph), len(th), _dp(out))
+        return out
+
     def solve(self, einc, solver="qmr", eps=1e-5, max_iter=0, start=None, stop_after=0,
               history_cap=100000):
         e = np.ascontiguousarray(einc, dtype=np.complex128)
@@ -284,6 +313,13 @@ class Problem:
                              None if s is None else _dp(s), _dp(pol), ctypes.byref(st),
                              stop_after, _dp(hist), history_cap)
         return rc, pol, st, hist[:min(st.iterations, history_cap)].copy()
+
+
+def mie(x, m):
+    """Bohren-Huffman efficiencies (Qext, Qsca, Qabs) of a sphere."""
+    a, b, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    lib().orc_mie(x, complex(m).real, complex(m).imag, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+    return a.value, b.value, c.value
 
 
 def set_threads(n):

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 import dda_b200
-from dda_b200 import api
+from dda_b200 import api, postprocess
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 FIXTURE = os.path.join(ROOT, "tests", "golden", "box_10_8_6.geom")
@@ -116,3 +116,12 @@ def test_beam_pol_convention():
     assert np.allclose(p1, (0, 1, 0)) and np.allclose(p2, (1, 0, 0))
     q1, pn = dda_b200.beam_pol((0, 1, 0), 1)
     assert abs(np.dot(q1, pn)) < 1e-15
+
+
+def test_grid_angles_follow_angle_list():
+    t, p = postprocess.grid_angles("0..180/3", "0..360/4")
+    assert len(t) == 12
+    assert np.allclose(np.degrees(t[::4]), [0, 90, 180])
+    assert np.allclose(np.degrees(p[:4]), [0, 120, 240, 360])
+    t1, p1 = postprocess.grid_angles("30", "45")
+    assert np.allclose(np.degrees([t1[0], p1[0]]), [30, 45])

@@ -166,3 +166,36 @@ def test_couple_constants_cm_ldr(oracle):
     t1 = 1j * 2 / 3 * kd ** 3 + (1.8915316 + (-0.1648469) * m2) * kd ** 2
     want = cm / (1 - cm / vol * t1)
     assert abs(ldr[0] - want) < 1e-13 * abs(want)
+
+
+def test_mie_pins_oracle_cross_sections(oracle):
+    # Physics pin: the oracle's DDA (LDR, FFT matvec, QMR-CS, Cext/Cabs of
+    # DDA/Beam.cpp:126-133 and DDA/AbsCross.cpp:28-48) converges to the
+    # Bohren-Huffman Mie series (EMSim/Mie.cpp) as the grid is refined.
+    a = 1e-6
+    x = 2 * np.pi * a / 4e-6
+    qe, qs, qa = oracle.mie(x, 1.5 + 0.1j)
+    errs = []
+    for d in ("0.1um", "0.05um"):
+        g = oracle.Geometry.sphere("1um", d)
+        p = oracle.Problem(g, [1.5 + 0.1j], "4um")
+        p.build_dmatrix()
+        p.set_cc((0, 0, 1), 1, "ldr")
+        e = p.einc((0, 0, 1), 1)
+        rc, pol, st, _ = p.solve(e, "qmr", 1e-8)
+        assert rc == 0
+        cext, cabs = p.cross_sections(pol, (0, 0, 1), 1)
+        errs.append((abs(cext / (np.pi * a * a) - qe) / qe, abs(cabs / (np.pi * a * a) - qa) / qa))
+    assert errs[1][0] < 1e-3 and errs[1][1] < 3e-3
+    assert errs[1][0] < errs[0][0]
+
+
+def test_mie_known_values(oracle):
+    # small-particle limit: Qext ~ Qabs ~ 4x Im((m^2-1)/(m^2+2)) for x -> 0
+    x = 1e-3
+    m = 1.5 + 0.1j
+    qe, qs, qa = oracle.mie(x, m)
+    ray = 4 * x * ((m * m - 1) / (m * m + 2)).imag
+    assert abs(qa - ray) < 1e-3 * ray
+    qe2, qs2, qa2 = oracle.mie(5.0, 1.33)
+    assert abs(qa2) < 1e-9 and 2.0 < qe2 < 4.5

@@ -72,6 +72,7 @@ def lib():
         "dda_profile_matvec": ([vp, ctypes.c_int, ctypes.c_int, dp], ctypes.c_int),
         "dda_synchronize": ([vp], ctypes.c_int),
         "dda_far_field": ([vp, ctypes.c_int, dp, ctypes.c_int64, dp, dp], ctypes.c_int),
+        "dda_far_field_noalloc": ([vp, ctypes.c_int, ctypes.c_int64, dp, dp], ctypes.c_int),
         "dda_frontend_error": ([], cp),
         "dda_fft_fit": ([ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int], ctypes.c_uint32),
         "dda_parse_length_m": ([cp, dp], ctypes.c_int),
@@ -328,6 +329,14 @@ class CudaMatVec:
         if pol is not None:
             pa, pp = _cbuf(pol)
         self._check(lib().dda_far_field(self.h, nrhs, pp, len(d), _dp(d), _dp(out.view(np.float64))))
+        return out
+
+    def far_field_noalloc(self, dirs, nrhs=1):
+        """far_field() of the last solve through dda_far_field_noalloc: no
+        allocation, at most 1 MiB of directions and fields per call."""
+        d = np.ascontiguousarray(dirs, dtype=np.float64).reshape(-1, 3)
+        out = np.zeros((len(d), nrhs, 3), dtype=np.complex128)
+        self._check(lib().dda_far_field_noalloc(self.h, nrhs, len(d), _dp(d), _dp(out.view(np.float64))))
         return out
 
     @property

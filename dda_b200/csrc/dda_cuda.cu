@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <numeric>
 #include <stdexcept>
 #include <string>
@@ -1199,6 +1200,74 @@ void far_field_t(dda_ctx* c, int nrhs, const double* pol, long long ndir, const 
   cudaFree(ddirs);
   cudaFree(dout);
 }
+
+// Far field without any allocation (dda_far_field_noalloc).  The device
+// copies of the directions and of the fields live in one file-scope device
+// array that is part of the module image, so it exists once the module is
+// loaded and no call allocates it.  Layout: directions at offset 0
+// (24*ndir bytes, rounded up to 256), fields after them (48*ndir*nrhs
+// bytes).  Nothing in it needs to start at zero: each call writes every
+// byte it later reads.  One array per device, shared by every context on
+// that device, so calls that overlap in time race on it.
+constexpr size_t kFfScratchBytes = size_t(1) << 20;
+static __device__ __align__(256) unsigned char g_ff_scratch[kFfScratchBytes];
+
+constexpr int kFfMaxDevices = 64;
+std::mutex g_ff_scratch_mu;
+unsigned char* g_ff_scratch_ptr[kFfMaxDevices];
+
+size_t ff_noalloc_bytes(long long ndir, int nrhs) {
+  return (((size_t)ndir * 3 * sizeof(double) + 255) & ~(size_t)255) + (size_t)ndir * nrhs * 3 * sizeof(double2);
+}
+
+// Address of the scratch on `device`, which must be the current device.
+// Looked up once per device, on the first call there.
+unsigned char* ff_scratch(int device) {
+  if (device < 0 || device >= kFfMaxDevices)
+    throw DdaError(DDA_ERR_UNSUPPORTED, "device ordinal beyond the no-allocation far-field table");
+  std::lock_guard<std::mutex> lock(g_ff_scratch_mu);
+  if (!g_ff_scratch_ptr[device]) {
+    void* ptr = nullptr;
+    const cudaError_t rc = cudaGetSymbolAddress((void**)&ptr, g_ff_scratch);
+    if (rc != cudaSuccess || !ptr)
+      throw DdaError(DDA_ERR_CUDA, std::string("cudaGetSymbolAddress of the far-field scratch: ") +
+                                       cudaGetErrorString(rc));
+    g_ff_scratch_ptr[device] = static_cast<unsigned char*>(ptr);
+  }
+  return g_ff_scratch_ptr[device];
+}
+
+template <typename T>
+void far_field_noalloc_t(dda_ctx* c, int nrhs, long long ndir, const double* dirs, double* out) {
+  Engine<T>& e = eng<T>(c);
+  unsigned char* scratch = ff_scratch(c->device);
+  double* ddirs = reinterpret_cast<double*>(scratch);
+  double2* dout = reinterpret_cast<double2*>(scratch + ((ndir * 3 * sizeof(double) + 255) & ~(size_t)255));
+  CK(cudaMemcpyAsync(ddirs, dirs, ndir * 3 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  FfGeom g;
+  g.nv = c->g.nv;
+  g.nvs = c->g.nvs;
+  g.by = c->g.by;
+  g.nlines = c->g.nlines;
+  g.bx = c->g.bx;
+  g.kd = c->kd;
+  g.k = c->kd / c->grid_unit;
+  // DipoleGeometry::moveToCenter (DDA/DipoleGeometry.cpp:75-80)
+  g.ox = -((double)c->g.bx - 1) / 2 * c->grid_unit;
+  g.oy = -((double)c->g.by - 1) / 2 * c->grid_unit;
+  g.oz = -((double)c->g.bz - 1) / 2 * c->grid_unit;
+  constexpr int DB = 4, NT = 256;
+  const size_t smem = (size_t)DB * g.bx * sizeof(double2);
+  if (smem > kSmemMax) throw DdaError(DDA_ERR_UNSUPPORTED, "box too long for the far-field tables");
+  CK(cudaFuncSetAttribute((const void*)k_farfield<T, NT, DB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)std::max<size_t>(smem, 1)));
+  k_farfield<T, NT, DB><<<dim3((unsigned)((ndir + DB - 1) / DB), nrhs), NT, smem, c->stream>>>(
+      e.io, c->line_off, c->dip, c->perm, ddirs, (int)ndir, g, dout);
+  CK(cudaGetLastError());
+  c->launches++;
+  CK(cudaMemcpyAsync(out, dout, (size_t)ndir * nrhs * 3 * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+}
 }  // namespace
 
 extern "C" {
@@ -1210,6 +1279,21 @@ int dda_far_field(dda_ctx* ctx, int nrhs, const double* pol, int64_t ndir, const
     if (ndir > (1LL << 31) / 4) throw DdaError(DDA_ERR_ARG, "too many directions");
     if (ctx->precision == DDA_PREC_FP32) far_field_t<float>(ctx, nrhs, pol, ndir, dirs, out);
     else far_field_t<double>(ctx, nrhs, pol, ndir, dirs, out);
+    return DDA_OK;
+  });
+}
+
+int dda_far_field_noalloc(dda_ctx* ctx, int nrhs, int64_t ndir, const double* dirs, double* out) {
+  if (!ctx) return DDA_ERR_ARG;
+  return guard(ctx, [&]() -> int {
+    if (nrhs < 1 || nrhs > ctx->max_rhs || ndir < 1 || !dirs || !out) throw DdaError(DDA_ERR_ARG, "bad far-field arguments");
+    if (ndir > (long long)(kFfScratchBytes / 72) || ff_noalloc_bytes(ndir, nrhs) > kFfScratchBytes)
+      throw DdaError(DDA_ERR_ARG, "dda_far_field_noalloc: " + std::to_string(ndir) + " directions x " +
+                                      std::to_string(nrhs) + " right-hand sides exceed its fixed scratch of " +
+                                      std::to_string(kFfScratchBytes) +
+                                      " bytes (24 bytes per direction, rounded up to 256, + 48 per direction and right-hand side)");
+    if (ctx->precision == DDA_PREC_FP32) far_field_noalloc_t<float>(ctx, nrhs, ndir, dirs, out);
+    else far_field_noalloc_t<double>(ctx, nrhs, ndir, dirs, out);
     return DDA_OK;
   });
 }

@@ -174,6 +174,32 @@ int dda_profile_matvec(dda_ctx* ctx, int nrhs, int reps, double* ms);
  * its per-direction host loop (DDA/FarFieldCalc.cpp:131-155). */
 int dda_far_field(dda_ctx* ctx, int nrhs, const double* pol, int64_t ndir, const double* dirs, double* out);
 
+/* dda_far_field(ctx, nrhs, NULL, ndir, dirs, out) without any allocation:
+ * the far field of the polarisations of the last solve on the context, with
+ * the device copies of `dirs` and `out` kept in one fixed scratch array of
+ * 1 MiB per device that is part of the library's device image.  No
+ * counterpart in the reference (its far field, DDA/FarFieldCalc.cpp:131-155,
+ * allocates its device buffers per call).
+ *
+ * For callers that must not allocate device memory while they evaluate far
+ * fields: a serving loop that keeps solves of other contexts in flight on
+ * other streams of the same device (cudaFree waits for the whole device,
+ * which would stall those solves), or a process that has handed the free
+ * device memory to its solver contexts (dda_far_field's per-call cudaMalloc
+ * then fails with DDA_ERR_OOM).
+ *
+ * Limit: 24*ndir bytes rounded up to 256, plus 48*ndir*nrhs bytes, at most
+ * 1 MiB (14,560 directions for one right-hand side, 8,736 for two); larger
+ * requests return DDA_ERR_ARG with the sizes in dda_last_error and touch
+ * nothing.  Nothing in the scratch needs to start at zero: each call writes
+ * every byte it reads.  The first call on each device looks up the scratch
+ * address (cudaGetSymbolAddress with that device current) and keeps it, so
+ * make that first call before any stream capture begins.  Every context on
+ * a device shares the one scratch array: calls that overlap in time (from
+ * two host threads, on any contexts of the same device) race on it and must
+ * be serialised by the caller.  Each call returns after `out` is written. */
+int dda_far_field_noalloc(dda_ctx* ctx, int nrhs, int64_t ndir, const double* dirs, double* out);
+
 /* Copies the D matrix out in the reference layout ([Gx][Gz][Gy][6] complex
  * FP64, reference units), expanded from the octant the context stores. */
 int dda_get_dmatrix(dda_ctx* ctx, double* out);

@@ -69,6 +69,7 @@ def lib():
                               ctypes.POINTER(Stats)], ctypes.c_int),
         "dda_stream": ([vp], vp),
         "dda_launch_count": ([vp], ctypes.c_int64),
+        "dda_matvec_layout": ([vp, ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
         "dda_profile_matvec": ([vp, ctypes.c_int, ctypes.c_int, dp], ctypes.c_int),
         "dda_synchronize": ([vp], ctypes.c_int),
         "dda_far_field": ([vp, ctypes.c_int, dp, ctypes.c_int64, dp, dp], ctypes.c_int),
@@ -348,6 +349,17 @@ class CudaMatVec:
     def launches(self):
         """Kernels launched by this context so far."""
         return int(lib().dda_launch_count(self.h))
+
+    @property
+    def layout(self):
+        """dda_matvec_layout as a dict."""
+        v = (ctypes.c_int64 * 8)()
+        self._check(lib().dda_matvec_layout(self.h, v))
+        keys = ("yz_path", "clusters", "cluster_size", "rows_per_batch", "smem_yz", "lines_per_x_tile",
+                "compile_time_plans", "device_bytes")
+        d = dict(zip(keys, (int(x) for x in v)))
+        d["yz_path"] = ("fused", "cluster", "split")[d["yz_path"]]
+        return d
 
     def profile(self, nrhs=1, reps=10):
         """Mean ms of the matvec stages: x forward, y/z, x inverse, total."""

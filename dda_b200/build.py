@@ -13,7 +13,7 @@ LIB = os.path.join(HERE, "libdda_b200.so")
 SOURCES = ["dda_cuda.cu", "frontend.cpp"]
 HEADERS = ["fft_engine.cuh", "fft_plan.cuh", "reduce.cuh", "krylov_ops.cuh", "krylov_kernels.cuh",
            "matvec_kernels.cuh", "matvec_planned.cuh", "matvec_dispatch.cuh", "dmatrix_kernels.cuh",
-           "farfield_kernels.cuh"]
+           "farfield_kernels.cuh", "matvec_slot.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

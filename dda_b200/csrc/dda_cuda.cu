@@ -65,6 +65,16 @@ constexpr int kNtC = 256;   // k_fft_cols / k_fft_rows
 constexpr int kNtV = 256;                 // k_vec
 constexpr size_t kSmemMax = 227 * 1024;
 
+// Device allocations that a context keeps go through dmalloc, which counts
+// them for the thread building the context (dda_matvec_layout reports the
+// total of dda_create); temporaries use cudaMalloc directly.
+thread_local size_t g_dalloc_bytes = 0;
+
+void dmalloc(void** p, size_t bytes) {
+  CK(cudaMalloc(p, bytes));
+  g_dalloc_bytes += bytes;
+}
+
 // ----------------------------------------------------------- FFT plans ----
 struct FftPlan {
   int n = 0;
@@ -102,8 +112,8 @@ struct FftPlan {
       h64[k] = make_double2((double)c, (double)s);
       h32[k] = make_float2((float)c, (float)s);
     }
-    CK(cudaMalloc(&tw64, n * sizeof(double2)));
-    CK(cudaMalloc(&tw32, n * sizeof(float2)));
+    dmalloc((void**)&tw64, n * sizeof(double2));
+    dmalloc((void**)&tw32, n * sizeof(float2));
     CK(cudaMemcpy(tw64, h64.data(), n * sizeof(double2), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(tw32, h32.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
     // Mixed-radix digit reversal of the decimation-in-frequency transform:
@@ -121,8 +131,8 @@ struct FftPlan {
       pos_h[k] = p;
       fr[p] = k;
     }
-    CK(cudaMalloc(&freq, n * sizeof(int)));
-    CK(cudaMalloc(&pos, n * sizeof(int)));
+    dmalloc((void**)&freq, n * sizeof(int));
+    dmalloc((void**)&pos, n * sizeof(int));
     CK(cudaMemcpy(freq, fr.data(), n * sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(pos, pos_h.data(), n * sizeof(int), cudaMemcpyHostToDevice));
   }
@@ -151,7 +161,7 @@ struct FftPlan {
 template <typename T> void* dalloc(size_t bytes) {
   void* p = nullptr;
   if (bytes == 0) return nullptr;
-  CK(cudaMalloc(&p, bytes));
+  dmalloc(&p, bytes);
   return p;
 }
 
@@ -169,16 +179,22 @@ template <typename T> struct Engine {
   T2* vec[10] = {};    // Krylov vectors [max_rhs][3 nvs]
   T2* io = nullptr;    // host-API staging [max_rhs][3 nvs]
   bool fused = false;
+  bool slot_path = false;     // k_yz_slot: cluster per plane through L2 slots
+  T2* slots = nullptr;        // [ncl][Gz][wp]
+  uint32_t* order = nullptr;  // kx positions, mirrored frequencies adjacent
+  SlotGeom sg{};
+  int ncl = 0, cl = 0;
   YzGeom yz{};
-  size_t smem_x = 0, smem_yz = 0, smem_rows = 0, smem_cols = 0;
+  size_t smem_x = 0, smem_yz = 0, smem_rows = 0, smem_cols = 0, smem_slot = 0;
   ColGeom cz_fwd{}, cz_inv{};
   MvKernels<T> k;
   void release() {
-    for (void* p : {(void*)dc, (void*)ccs, (void*)xhat, (void*)zbuf, (void*)io})
+    for (void* p : {(void*)dc, (void*)ccs, (void*)xhat, (void*)zbuf, (void*)io, (void*)slots, (void*)order})
       if (p) cudaFree(p);
     for (auto& v : vec)
       if (v) cudaFree(v);
-    dc = ccs = xhat = zbuf = io = nullptr;
+    dc = ccs = xhat = zbuf = io = slots = nullptr;
+    order = nullptr;
     for (auto& v : vec) v = nullptr;
   }
 };
@@ -213,6 +229,7 @@ struct dda_ctx {
   double* hist = nullptr;
   long long hist_cap = 0;
   long long launches = 0;  // kernels this context has launched
+  size_t dev_bytes = 0;    // device memory held after dda_create
 
   void release() {
     if (device >= 0) cudaSetDevice(device);
@@ -252,6 +269,55 @@ template <typename T> Engine<T>& eng(dda_ctx* c);
 template <> Engine<float>& eng<float>(dda_ctx* c) { return c->e32; }
 template <> Engine<double>& eng<double>(dda_ctx* c) { return c->e64; }
 
+// k_yz_slot set-up: row batch, cluster size, resident clusters, one slot per
+// cluster, and the kx order that puts the planes kx and -kx (one D-hat
+// octant plane) next to each other.  Leaves e.slot_path false when the
+// cluster shape cannot be scheduled (the split path then runs).
+template <typename T> void setup_slot(dda_ctx* c, Engine<T>& e) {
+  typedef typename C2<T>::t T2;
+  const MvGeom& g = c->g;
+  SlotGeom sg;
+  sg.wp = (3 * g.by + 31) / 32 * 32;
+  sg.py = g.Gy + 1;
+  const int cl = 8;
+  int nrw = std::min(16, (g.Gz + cl - 1) / cl);
+  while (nrw > 1 && slot_smem_bytes<T>(g, nrw) > kSmemMax) nrw--;
+  sg.nrw = nrw;
+  const size_t smem = slot_smem_bytes<T>(g, nrw);
+  if (smem > kSmemMax) return;
+  CK(cudaFuncSetAttribute((const void*)e.k.slot, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = cl;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3(cl);
+  cfg.blockDim = dim3(kNtYz);
+  cfg.dynamicSmemBytes = smem;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  int ncl = 0;
+  if (cudaOccupancyMaxActiveClusters(&ncl, (const void*)e.k.slot, &cfg) != cudaSuccess || ncl < 1) {
+    cudaGetLastError();
+    return;
+  }
+  ncl = std::min(ncl, g.Gx * c->max_rhs);
+  std::vector<uint32_t> order;
+  for (int f = 0; f <= g.Gx / 2; f++) {
+    order.push_back((uint32_t)c->mx.pos_h[f]);
+    if (f != 0 && f != g.Gx / 2) order.push_back((uint32_t)c->mx.pos_h[g.Gx - f]);
+  }
+  e.order = (uint32_t*)dalloc<float>(order.size() * sizeof(uint32_t));
+  CK(cudaMemcpy(e.order, order.data(), order.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+  e.slots = (T2*)dalloc<T>((size_t)ncl * g.Gz * sg.wp * sizeof(T2));
+  e.sg = sg;
+  e.cl = cl;
+  e.ncl = ncl;
+  e.smem_slot = smem;
+  e.slot_path = true;
+}
+
 // Chooses tile shapes and allocates the matvec buffers of one precision.
 template <typename T> void setup_engine(dda_ctx* c) {
   typedef typename C2<T>::t T2;
@@ -277,8 +343,9 @@ template <typename T> void setup_engine(dda_ctx* c) {
   y.nrw = nrw;
   e.yz = y;
   e.smem_yz = fixed + nrw * row;
-  e.fused = e.k.yz && e.smem_yz <= kSmemMax && !(c->flags & DDA_FLAG_SPLIT_YZ);
-  if (!e.fused) {
+  e.fused = e.k.yz && e.smem_yz <= kSmemMax && !(c->flags & (DDA_FLAG_SPLIT_YZ | DDA_FLAG_SLOT_YZ));
+  if (!e.fused && e.k.slot && !(c->flags & DDA_FLAG_SPLIT_YZ)) setup_slot<T>(c, e);
+  if (!e.fused && !e.slot_path) {
     // split path: zbuf, k_yrows over NW rows per CTA, column FFTs along z
     e.yz.nrw = NW;
     e.smem_rows = ((size_t)g.Gy + (size_t)NW * 3 * y.py) * s;
@@ -316,7 +383,7 @@ template <typename T> void setup_engine(dda_ctx* c) {
   attr((const void*)e.k.xfwd, e.smem_x);
   attr((const void*)e.k.xinv, e.smem_x);
   if (e.fused) attr((const void*)e.k.yz, e.smem_yz);
-  else {
+  else if (!e.slot_path) {
     attr((const void*)e.k.yrows, e.smem_rows);
     attr((const void*)e.k.cols, e.smem_cols);
   }
@@ -356,17 +423,30 @@ RedTarget red_target(dda_ctx* c, int nparts) {
   return t;
 }
 
-// The matvec: k_xfwd -> (k_yz | cols/yrows/cols) -> k_xinv.
+// The y/z passes: the fused plane kernel, the cluster kernel, or the split
+// path (column FFTs along z around the row kernel).
 template <typename T>
-void matvec(dda_ctx* c, const typename C2<T>::t* arg, typename C2<T>::t* res, int conj, int nrhs,
-            cudaStream_t s, KrylovState* st, KrylovStep step, int skipmv = 0) {
+void launch_yz(dda_ctx* c, int nrhs, cudaStream_t s, KrylovState* st, int skipmv) {
   Engine<T>& e = eng<T>(c);
   const MvGeom& g = c->g;
-  const FftPlanDev px = c->mx.dev<T>(), py = c->my.dev<T>(), pz = c->mz.dev<T>();
-  dim3 gx(ntiles(c), 3, nrhs);
-  e.k.xfwd<<<gx, kNtX, e.smem_x, s>>>(arg, e.xhat, c->line_off, c->dip, c->perm, e.ccs, conj, g, px, st, skipmv);
+  const FftPlanDev py = c->my.dev<T>(), pz = c->mz.dev<T>();
   if (e.fused) {
     e.k.yz<<<dim3(g.Gx, nrhs), kNtYz, e.smem_yz, s>>>(e.xhat, e.dc, g, e.yz, pz, py, st, skipmv);
+  } else if (e.slot_path) {
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = e.cl;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(std::min(e.ncl, g.Gx * nrhs) * e.cl);
+    cfg.blockDim = dim3(kNtYz);
+    cfg.dynamicSmemBytes = e.smem_slot;
+    cfg.stream = s;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    CK(cudaLaunchKernelEx(&cfg, e.k.slot, e.xhat, (const typename C2<T>::t*)e.dc, g, e.sg,
+                          (const uint32_t*)e.order, nrhs, e.slots, pz, py, (const KrylovState*)st, skipmv));
   } else {
     const int nbatch = nrhs * g.Gx * 3;
     dim3 gc((g.by + e.cz_fwd.ti - 1) / e.cz_fwd.ti, nbatch);
@@ -375,18 +455,31 @@ void matvec(dda_ctx* c, const typename C2<T>::t* arg, typename C2<T>::t* res, in
     e.k.yrows<<<gr, kNtYz, e.smem_rows, s>>>(e.zbuf, e.dc, g, e.yz, py, st, skipmv);
     e.k.cols<<<gc, kNtC, e.smem_cols, s>>>(e.zbuf, e.xhat, e.cz_inv, pz, 1, st, skipmv);
   }
+}
+
+// The matvec: k_xfwd -> (k_yz | k_yz_slot | cols/yrows/cols) -> k_xinv.
+template <typename T>
+void matvec(dda_ctx* c, const typename C2<T>::t* arg, typename C2<T>::t* res, int conj, int nrhs,
+            cudaStream_t s, KrylovState* st, KrylovStep step, int skipmv = 0) {
+  Engine<T>& e = eng<T>(c);
+  const MvGeom& g = c->g;
+  const FftPlanDev px = c->mx.dev<T>();
+  dim3 gx(ntiles(c), 3, nrhs);
+  e.k.xfwd<<<gx, kNtX, e.smem_x, s>>>(arg, e.xhat, c->line_off, c->dip, c->perm, e.ccs, conj, g, px, st, skipmv);
+  launch_yz<T>(c, nrhs, s, st, skipmv);
   step.red = red_target(c, 3 * ntiles(c));
   e.k.xinv<<<gx, kNtX, e.smem_x, s>>>(arg, res, e.xhat, c->line_off, c->dip, c->perm, e.ccs, conj, g, px, st, step,
                                       skipmv);
   CK(cudaGetLastError());
-  c->launches += e.fused ? 3 : 5;
+  c->launches += (e.fused || e.slot_path) ? 3 : 5;
 }
 
 // D-matrix generation (FP64) into the enabled engines' octants.
 void build_dmatrix(dda_ctx* c) {
   const MvGeom& g = c->g;
   const long long N = (long long)g.Gx * g.Gy * g.Gz;
-  double2* full = (double2*)dalloc<double>(N * sizeof(double2));
+  double2* full = nullptr;
+  CK(cudaMalloc(&full, N * sizeof(double2)));
   const FftPlanDev px = c->px.dev<double>(), py = c->py.dev<double>(), pz = c->pz.dev<double>();
   CK(cudaFuncSetAttribute((const void*)k_fft_rows<double, kNtC>,
                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax));
@@ -439,7 +532,8 @@ void upload_dmatrix(dda_ctx* c, const double* D) {
           const size_t dst = (((size_t)ax * hz + az) * hy + ay) * 6 + comp;
           h64[dst] = make_double2(D[2 * src] * sc, D[2 * src + 1] * sc);
         }
-  double2* tmp = (double2*)dalloc<double>(h64.size() * sizeof(double2));
+  double2* tmp = nullptr;
+  CK(cudaMalloc(&tmp, h64.size() * sizeof(double2)));
   CK(cudaMemcpy(tmp, h64.data(), h64.size() * sizeof(double2), cudaMemcpyHostToDevice));
   if (c->e64.on) CK(cudaMemcpy(c->e64.dc, tmp, h64.size() * sizeof(double2), cudaMemcpyDeviceToDevice));
   if (c->e32.on) {
@@ -757,6 +851,7 @@ int dda_create(const dda_problem* p, int precision, dda_ctx** out) {
     if (p->box[0] >= 65536 || p->grid[0] > lim || p->grid[1] > lim || p->grid[2] > lim)
       throw DdaError(DDA_ERR_UNSUPPORTED, "FFT grid edge above " + std::to_string(lim));
     CK(cudaSetDevice(p->device));
+    g_dalloc_bytes = 0;
     c->precision = precision;
     c->max_rhs = p->max_rhs;
     c->flags = p->flags;
@@ -800,15 +895,15 @@ int dda_create(const dda_problem* p, int precision, dda_ctx** out) {
       dip[j] = p->positions[3 * i] | ((uint32_t)m << 16);
       matx[i] = m;
     }
-    CK(cudaMalloc(&c->line_off, off.size() * sizeof(uint32_t)));
+    dmalloc((void**)&c->line_off, off.size() * sizeof(uint32_t));
     CK(cudaMemcpy(c->line_off, off.data(), off.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
-    CK(cudaMalloc(&c->dip, nv * sizeof(uint32_t)));
+    dmalloc((void**)&c->dip, nv * sizeof(uint32_t));
     CK(cudaMemcpy(c->dip, dip.data(), nv * sizeof(uint32_t), cudaMemcpyHostToDevice));
     if (!ident) {
-      CK(cudaMalloc(&c->perm, nv * sizeof(uint32_t)));
+      dmalloc((void**)&c->perm, nv * sizeof(uint32_t));
       CK(cudaMemcpy(c->perm, perm.data(), nv * sizeof(uint32_t), cudaMemcpyHostToDevice));
     }
-    CK(cudaMalloc(&c->mat_ext, nv));
+    dmalloc((void**)&c->mat_ext, nv);
     CK(cudaMemcpy(c->mat_ext, matx.data(), nv, cudaMemcpyHostToDevice));
     c->px.create(g.Gx);
     c->py.create(g.Gy);
@@ -830,22 +925,23 @@ int dda_create(const dda_problem* p, int precision, dda_ctx** out) {
       c->nparts_vec = (int)std::max(1LL, std::min(296LL, (len + 2047) / 2048));
     }
     const int nparts = std::max(c->nparts_mv, c->nparts_vec);
-    CK(cudaMalloc(&c->parts, (size_t)c->max_rhs * nparts * sizeof(RedSums)));
-    CK(cudaMalloc(&c->tickets, c->max_rhs * sizeof(unsigned)));
+    dmalloc((void**)&c->parts, (size_t)c->max_rhs * nparts * sizeof(RedSums));
+    dmalloc((void**)&c->tickets, c->max_rhs * sizeof(unsigned));
     CK(cudaMemset(c->tickets, 0, c->max_rhs * sizeof(unsigned)));
-    CK(cudaMalloc(&c->st, c->max_rhs * sizeof(KrylovState)));
+    dmalloc((void**)&c->st, c->max_rhs * sizeof(KrylovState));
     CK(cudaMemset(c->st, 0, c->max_rhs * sizeof(KrylovState)));
     CK(cudaMallocHost(&c->st_host, c->max_rhs * sizeof(KrylovState)));
-    CK(cudaMalloc(&c->st_outer, c->max_rhs * sizeof(KrylovState)));
+    dmalloc((void**)&c->st_outer, c->max_rhs * sizeof(KrylovState));
     CK(cudaMemset(c->st_outer, 0, c->max_rhs * sizeof(KrylovState)));
     CK(cudaMallocHost(&c->sto_host, c->max_rhs * sizeof(KrylovState)));
     c->hist_cap = 100000;
-    CK(cudaMalloc(&c->hist, (size_t)c->max_rhs * c->hist_cap * sizeof(double)));
+    dmalloc((void**)&c->hist, (size_t)c->max_rhs * c->hist_cap * sizeof(double));
     c->cc_host.assign((size_t)c->max_rhs * g.nmat * 3, 0);
     c->cc_set.assign(c->max_rhs, 0);
     if (p->dmatrix) upload_dmatrix(c.get(), p->dmatrix);
     else build_dmatrix(c.get());
     CK(cudaDeviceSynchronize());
+    c->dev_bytes = g_dalloc_bytes;
     return DDA_OK;
   });
   if (rc != DDA_OK) {
@@ -909,7 +1005,7 @@ template <typename T> void profile_t(dda_ctx* c, int nrhs, int reps, double* ms)
   typedef typename C2<T>::t T2;
   Engine<T>& e = eng<T>(c);
   const MvGeom& g = c->g;
-  const FftPlanDev px = c->mx.dev<T>(), py = c->my.dev<T>(), pz = c->mz.dev<T>();
+  const FftPlanDev px = c->mx.dev<T>();
   cudaStream_t s = c->stream;
   cudaEvent_t ev[4];
   for (auto& x : ev) CK(cudaEventCreate(&x));
@@ -923,15 +1019,7 @@ template <typename T> void profile_t(dda_ctx* c, int nrhs, int reps, double* ms)
     CK(cudaEventRecord(ev[0], s));
     e.k.xfwd<<<gx, kNtX, e.smem_x, s>>>(arg, e.xhat, c->line_off, c->dip, c->perm, e.ccs, 0, g, px, nullptr, 0);
     CK(cudaEventRecord(ev[1], s));
-    if (e.fused) {
-      e.k.yz<<<dim3(g.Gx, nrhs), kNtYz, e.smem_yz, s>>>(e.xhat, e.dc, g, e.yz, pz, py, nullptr, 0);
-    } else {
-      dim3 gc((g.by + e.cz_fwd.ti - 1) / e.cz_fwd.ti, nrhs * g.Gx * 3);
-      e.k.cols<<<gc, kNtC, e.smem_cols, s>>>(e.xhat, e.zbuf, e.cz_fwd, pz, 0, nullptr, 0);
-      dim3 gr((g.Gz + e.yz.nrw - 1) / e.yz.nrw, g.Gx, nrhs);
-      e.k.yrows<<<gr, kNtYz, e.smem_rows, s>>>(e.zbuf, e.dc, g, e.yz, py, nullptr, 0);
-      e.k.cols<<<gc, kNtC, e.smem_cols, s>>>(e.zbuf, e.xhat, e.cz_inv, pz, 1, nullptr, 0);
-    }
+    launch_yz<T>(c, nrhs, s, nullptr, 0);
     CK(cudaEventRecord(ev[2], s));
     e.k.xinv<<<gx, kNtX, e.smem_x, s>>>(arg, res, e.xhat, c->line_off, c->dip, c->perm, e.ccs, 0, g, px, nullptr, none,
                                         0);
@@ -1149,6 +1237,23 @@ int dda_solve_device(dda_ctx* ctx, int solver, int nrhs, const void* d_einc, dou
 void* dda_stream(dda_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
 int64_t dda_launch_count(const dda_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int dda_matvec_layout(const dda_ctx* ctx, int64_t* out) {
+  if (!ctx || !out) return DDA_ERR_ARG;
+  auto fill = [&](const auto& e) {
+    out[0] = e.fused ? 0 : e.slot_path ? 1 : 2;
+    out[1] = e.ncl;
+    out[2] = e.cl;
+    out[3] = e.slot_path ? e.sg.nrw : e.yz.nrw;
+    out[4] = (int64_t)(e.fused ? e.smem_yz : e.slot_path ? e.smem_slot : e.smem_rows);
+  };
+  if (ctx->e32.on) fill(ctx->e32);
+  else fill(ctx->e64);
+  out[5] = ctx->g.tl;
+  out[6] = ctx->planned ? 1 : 0;
+  out[7] = (int64_t)ctx->dev_bytes;
+  return DDA_OK;
+}
 
 int dda_profile_matvec(dda_ctx* ctx, int nrhs, int reps, double* ms) {
   if (!ctx || !ms || reps < 1) return DDA_ERR_ARG;

@@ -5,6 +5,7 @@
 
 #include "matvec_kernels.cuh"
 #include "matvec_planned.cuh"
+#include "matvec_slot.cuh"
 
 namespace dda {
 
@@ -17,11 +18,14 @@ template <typename T> struct MvKernels {
   typedef void (*YzFn)(T2*, const T2*, MvGeom, YzGeom, FftPlanDev, FftPlanDev, const KrylovState*, int);
   typedef void (*YrowsFn)(T2*, const T2*, MvGeom, YzGeom, FftPlanDev, const KrylovState*, int);
   typedef void (*ColsFn)(const T2*, T2*, ColGeom, FftPlanDev, int, const KrylovState*, int);
+  typedef void (*SlotFn)(T2*, const T2*, MvGeom, SlotGeom, const uint32_t*, int, T2*, FftPlanDev, FftPlanDev,
+                         const KrylovState*, int);
   XfwdFn xfwd = nullptr;
   XinvFn xinv = nullptr;
   YzFn yz = nullptr;        // fused plane kernel (nullptr: none for this shape)
   YrowsFn yrows = nullptr;  // split path
   ColsFn cols = nullptr;
+  SlotFn slot = nullptr;    // cluster plane kernel for planes beyond shared memory
   bool planned = false;
 };
 
@@ -75,6 +79,13 @@ MvKernels<T> planned_kernels(int gx, int gy, int gz) {
 #undef C
       default: break;
     }
+    switch (gy) {
+#define C(N)                                                                                        \
+  case N: k.slot = k_yz_slot<T, NTYZ, typename PlanFor<N>::type, typename PlanFor<N>::type>; break;
+      DDA_TUNED_LENGTHS(C)
+#undef C
+      default: break;
+    }
   }
   return k;
 }
@@ -87,6 +98,7 @@ MvKernels<T> generic_kernels() {
   k.yz = k_yz<T, NTYZ>;
   k.yrows = k_yrows<T, NTYZ>;
   k.cols = k_fft_cols<T, NTC>;
+  k.slot = k_yz_slot<T, NTYZ, void, void>;
   return k;
 }
 

@@ -223,8 +223,14 @@ __device__ __forceinline__ void rows_dmul(int kz0, int nr, int ro, int py,
   constexpr int R = PY::r[K - 1];
   constexpr int NB = PY::N / R;
   T2* sm = smem_at<T>(0);
+  // A thread reads R contiguous elements of each component.  With even R,
+  // neighbouring butterflies of one row are 2R words apart and share banks
+  // (16-way for R = 8), so neighbouring threads take neighbouring rows
+  // instead (3 py complex apart); with odd R they take neighbouring
+  // butterflies.
+  constexpr bool ROW_FAST = R % 2 == 0;
   for (int it = threadIdx.x; it < nr * NB; it += NT) {
-    const int t = it % NB, row = it / NB;
+    const int t = ROW_FAST ? it / nr : it % NB, row = ROW_FAST ? it - t * nr : it / NB;
     const int kz = PZ::freq_of(kz0 + row);
     const int base = ro + 3 * row * py + t * R;
     T2 v0[R], v1[R], v2[R];

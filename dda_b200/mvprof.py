@@ -35,7 +35,7 @@ def main():
         mv.set_couple_constants(D.CoupleConstants(p, (0, 0, 1), 1 + r % 2, "ldr"), rhs=r)
     ms = mv.profile(nrhs=a.nrhs, reps=a.reps)
     print(json.dumps({"shape": a.shape, "grid": list(p.grid), "nv": p.nv, "precision": a.precision,
-                      "nrhs": a.nrhs, "flags": a.flags,
+                      "nrhs": a.nrhs, "flags": a.flags, "layout": mv.layout,
                       "ms": {"x_forward": ms[0], "yz": ms[1], "x_inverse": ms[2], "total": ms[3]}}))
 
 

@@ -78,6 +78,11 @@ typedef struct dda_problem {
 /* dda_problem.flags: use the runtime-planned FFT kernels even when every grid
  * edge has a compile-time plan; used by tests and tuning. */
 #define DDA_FLAG_RUNTIME_PLANS 2u
+/* dda_problem.flags: run the y/z passes through the cluster kernel (a
+ * thread-block cluster per kx plane exchanging through an L2-resident plane
+ * buffer, the path for planes beyond one CTA's shared memory) even when a
+ * plane fits; used by tests and tuning.  DDA_FLAG_SPLIT_YZ takes precedence. */
+#define DDA_FLAG_SLOT_YZ 4u
 
 typedef struct dda_stats {
   int64_t iterations;   /* Krylov iterations (summed over inner solves for MIXED) */
@@ -156,6 +161,16 @@ void* dda_stream(dda_ctx* ctx);
 /* Number of kernels the context has launched so far (matvec passes,
  * Krylov steps, setup); a profiling counter. */
 int64_t dda_launch_count(const dda_ctx* ctx);
+
+/* Layout the context chose for its matvec (working precision: FP32 for
+ * DDA_PREC_FP32 and DDA_PREC_MIXED, FP64 otherwise), 8 values:
+ * [0] y/z path (0 fused plane kernel, 1 cluster kernel, 2 split path),
+ * [1] resident clusters, [2] CTAs per cluster, [3] rows per y batch,
+ * [4] dynamic shared memory of the y/z kernel (bytes), [5] grid lines per
+ * x tile, [6] compile-time FFT plans (1) or runtime plans (0),
+ * [7] device bytes the context holds.  A diagnostic for tuning and
+ * benchmark reports; no counterpart in the reference. */
+int dda_matvec_layout(const dda_ctx* ctx, int64_t* out);
 
 /* Times the stages of one matvec of nrhs right-hand sides with CUDA events
  * (`reps` repetitions after one warm-up) and writes the mean milliseconds of

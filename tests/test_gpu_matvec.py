@@ -55,17 +55,52 @@ def test_matvec_split_yz_path(prec, tol):
     assert rel(pr.mv.apply(x), pr.op.matvec(x)) < tol
 
 
-@pytest.mark.parametrize("flags", [0, 1, 2, 3])
+@pytest.mark.parametrize("flags", [0, 1, 2, 3, 4, 6])
 @pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("fp32", FP32_TOL)])
 def test_matvec_kernel_paths(flags, prec, tol):
     # README workload 1 (grid 80^3) has compile-time FFT plans; flags select
-    # the split y/z path (1) and the runtime-planned kernels (2).
+    # the split y/z path (1), the runtime-planned kernels (2) and the cluster
+    # plane kernel (4).
     kind, args, mats, lam = CASES["cfg1"]
     pr = Pair(kind, args, mats, lam, prec, flags=flags)
     pr.set_cc((0, 0, 1), 2, "ldr")
     x = pr.rand_vec(17)
     assert rel(pr.mv.apply(x), pr.op.matvec(x)) < tol
     assert rel(pr.mv.apply(x, conj=True), pr.op.matvec(x, conj=True)) < tol
+
+
+@pytest.mark.parametrize("case", ["aniso", "scrambled", "cylinder"])
+@pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("fp32", FP32_TOL)])
+def test_matvec_cluster_path_small_grids(case, prec, tol):
+    # runtime-planned grids (odd sizes) through the cluster plane kernel
+    kind, args, mats, lam = CASES[case]
+    pr = Pair(kind, args, mats, lam, prec, flags=4)
+    assert pr.mv.layout["yz_path"] == "cluster"
+    pr.set_cc((0.6, 0.0, 0.8), 1, "ldr")
+    x = pr.rand_vec(23)
+    assert rel(pr.mv.apply(x), pr.op.matvec(x)) < tol
+    assert rel(pr.mv.apply(x, conj=True), pr.op.matvec(x, conj=True)) < tol
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("fp32", FP32_TOL)])
+def test_matvec_plane_beyond_shared_memory(prec, tol):
+    # sphere of radius 40 dipoles: grid 160^3, a kx plane (160 x 3 x 80
+    # complex) does not fit one CTA, so the default path is the cluster
+    # kernel; two right-hand sides with different couple constants
+    pr = Pair("sphere", ("2um", "0.05um"), [1.5 + 0.1j], "1.2um", prec, max_rhs=2)
+    assert pr.p.grid == (160, 160, 160)
+    assert pr.mv.layout["yz_path"] == "cluster"
+    xs = [pr.rand_vec(31), pr.rand_vec(32)]
+    want = []
+    for r, pol in enumerate((1, 2)):
+        pr.set_cc((0, 0, 1), pol, "ldr", rhs=r)
+        want.append(pr.op.matvec(xs[r]))
+    y = pr.mv.apply(np.concatenate(xs))
+    n = pr.p.vec_size
+    for r in range(2):
+        assert rel(y[r * n:(r + 1) * n], want[r]) < tol
+    # one right-hand side of a two-rhs context
+    assert rel(pr.mv.apply(xs[0]), want[0]) < tol
 
 
 def test_matvec_host_dmatrix():

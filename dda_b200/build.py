@@ -10,7 +10,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libdda_b200.so")
-SOURCES = ["dda_cuda.cu", "frontend.cpp"]
+SOURCES = ["dda_cuda.cu", "frontend.cpp", "serve.cpp"]
 HEADERS = ["fft_engine.cuh", "fft_plan.cuh", "reduce.cuh", "krylov_ops.cuh", "krylov_kernels.cuh",
            "matvec_kernels.cuh", "matvec_planned.cuh", "matvec_dispatch.cuh", "dmatrix_kernels.cuh",
            "farfield_kernels.cuh", "matvec_slot.cuh"]
@@ -32,7 +32,7 @@ def _stale():
         return True
     t = os.path.getmtime(LIB)
     deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
-    deps += [os.path.join(HERE, "..", "include", h) for h in ("dda_cuda.h", "dda_frontend.h")]
+    deps += [os.path.join(HERE, "..", "include", h) for h in ("dda_cuda.h", "dda_frontend.h", "dda_serve.h")]
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 

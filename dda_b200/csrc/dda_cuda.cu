@@ -38,7 +38,7 @@ using namespace dda;
 
 namespace {
 
-std::string g_create_error;
+thread_local std::string g_create_error;
 
 struct DdaError : std::runtime_error {
   int code;
@@ -65,13 +65,30 @@ constexpr int kNtC = 256;   // k_fft_cols / k_fft_rows
 constexpr int kNtV = 256;                 // k_vec
 constexpr size_t kSmemMax = 227 * 1024;
 
+// Opts kernel f into the whole shared memory of an SM (less its static
+// shared memory).  The limit is a
+// process-wide attribute of the function, shared by every context (and
+// thread) that launches it, so it is always set to the same maximum; each
+// launch's own size is checked against kSmemMax by its caller.
+inline cudaError_t allow_smem(const void* f) {
+  cudaFuncAttributes a;
+  cudaError_t rc = cudaFuncGetAttributes(&a, f);
+  if (rc != cudaSuccess) return rc;
+  const size_t room = kSmemMax > a.sharedSizeBytes ? kSmemMax - a.sharedSizeBytes : 0;  // minus static
+  return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)room);
+}
+
 // Device allocations that a context keeps go through dmalloc, which counts
 // them for the thread building the context (dda_matvec_layout reports the
 // total of dda_create); temporaries use cudaMalloc directly.
+// Allocations are stream ordered (cudaMallocAsync / cudaFreeAsync on the
+// context stream), so creating or destroying a context never waits for the
+// work of other contexts on the device.
 thread_local size_t g_dalloc_bytes = 0;
+thread_local cudaStream_t g_alloc_stream = nullptr;
 
 void dmalloc(void** p, size_t bytes) {
-  CK(cudaMalloc(p, bytes));
+  CK(cudaMallocAsync(p, bytes, g_alloc_stream));
   g_dalloc_bytes += bytes;
 }
 
@@ -114,8 +131,8 @@ struct FftPlan {
     }
     dmalloc((void**)&tw64, n * sizeof(double2));
     dmalloc((void**)&tw32, n * sizeof(float2));
-    CK(cudaMemcpy(tw64, h64.data(), n * sizeof(double2), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(tw32, h32.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(tw64, h64.data(), n * sizeof(double2), cudaMemcpyHostToDevice, g_alloc_stream));
+    CK(cudaMemcpyAsync(tw32, h32.data(), n * sizeof(float2), cudaMemcpyHostToDevice, g_alloc_stream));
     // Mixed-radix digit reversal of the decimation-in-frequency transform:
     // frequency k = d0 + R0 d1 + R0 R1 d2 + ... sits at position
     // d0 n/R0 + d1 n/(R0 R1) + ...
@@ -133,8 +150,8 @@ struct FftPlan {
     }
     dmalloc((void**)&freq, n * sizeof(int));
     dmalloc((void**)&pos, n * sizeof(int));
-    CK(cudaMemcpy(freq, fr.data(), n * sizeof(int), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(pos, pos_h.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(freq, fr.data(), n * sizeof(int), cudaMemcpyHostToDevice, g_alloc_stream));
+    CK(cudaMemcpyAsync(pos, pos_h.data(), n * sizeof(int), cudaMemcpyHostToDevice, g_alloc_stream));
   }
   template <typename T> FftPlanDev dev() const {
     FftPlanDev d;
@@ -147,11 +164,11 @@ struct FftPlan {
     d.freq = freq;
     return d;
   }
-  void release() {
-    if (tw32) cudaFree(tw32);
-    if (tw64) cudaFree(tw64);
-    if (freq) cudaFree(freq);
-    if (pos) cudaFree(pos);
+  void release(cudaStream_t s) {
+    if (tw32) cudaFreeAsync(tw32, s);
+    if (tw64) cudaFreeAsync(tw64, s);
+    if (freq) cudaFreeAsync(freq, s);
+    if (pos) cudaFreeAsync(pos, s);
     tw32 = nullptr;
     tw64 = nullptr;
     freq = pos = nullptr;
@@ -188,11 +205,11 @@ template <typename T> struct Engine {
   size_t smem_x = 0, smem_yz = 0, smem_rows = 0, smem_cols = 0, smem_slot = 0;
   ColGeom cz_fwd{}, cz_inv{};
   MvKernels<T> k;
-  void release() {
+  void release(cudaStream_t s) {
     for (void* p : {(void*)dc, (void*)ccs, (void*)xhat, (void*)zbuf, (void*)io, (void*)slots, (void*)order})
-      if (p) cudaFree(p);
+      if (p) cudaFreeAsync(p, s);
     for (auto& v : vec)
-      if (v) cudaFree(v);
+      if (v) cudaFreeAsync(v, s);
     dc = ccs = xhat = zbuf = io = slots = nullptr;
     order = nullptr;
     for (auto& v : vec) v = nullptr;
@@ -220,9 +237,9 @@ struct dda_ctx {
   std::vector<std::complex<double>> cc_host;  // [max_rhs][nmat][3], reference units
   std::vector<char> cc_set;
   KrylovState* st = nullptr;  // device [max_rhs]
-  KrylovState* st_host = nullptr;  // pinned mirror
+  KrylovState* st_host = nullptr;  // host mirror (pageable: freeing pinned memory may wait for the device)
   KrylovState* st_outer = nullptr;  // device: FP64 refinement loop (MIXED)
-  KrylovState* sto_host = nullptr;  // pinned mirror
+  KrylovState* sto_host = nullptr;  // host mirror
   RedSums* parts = nullptr;
   unsigned* tickets = nullptr;
   int nparts_vec = 0, nparts_mv = 0;
@@ -231,25 +248,31 @@ struct dda_ctx {
   long long launches = 0;  // kernels this context has launched
   size_t dev_bytes = 0;    // device memory held after dda_create
 
+  // Frees on the context stream once its work is done; other contexts'
+  // work on the device is not waited for.
   void release() {
     if (device >= 0) cudaSetDevice(device);
-    e32.release();
-    e64.release();
-    px.release();
-    py.release();
-    pz.release();
-    mx.release();
-    my.release();
-    mz.release();
+    cudaStream_t s = stream;
+    if (s) cudaStreamSynchronize(s);
+    e32.release(s);
+    e64.release(s);
+    px.release(s);
+    py.release(s);
+    pz.release(s);
+    mx.release(s);
+    my.release(s);
+    mz.release(s);
     for (void* p : {(void*)line_off, (void*)dip, (void*)perm, (void*)mat_ext, (void*)st,
-                    (void*)parts, (void*)tickets, (void*)hist})
-      if (p) cudaFree(p);
-    if (st_host) cudaFreeHost(st_host);
-    if (sto_host) cudaFreeHost(sto_host);
-    if (st_outer) cudaFree(st_outer);
+                    (void*)parts, (void*)tickets, (void*)hist, (void*)st_outer})
+      if (p) cudaFreeAsync(p, s);
+    delete[] st_host;
+    delete[] sto_host;
     st_outer = nullptr;
     sto_host = nullptr;
-    if (stream) cudaStreamDestroy(stream);
+    if (s) {
+      cudaStreamSynchronize(s);
+      cudaStreamDestroy(s);
+    }
     line_off = dip = perm = nullptr;
     mat_ext = nullptr;
     st = nullptr;
@@ -285,7 +308,7 @@ template <typename T> void setup_slot(dda_ctx* c, Engine<T>& e) {
   sg.nrw = nrw;
   const size_t smem = slot_smem_bytes<T>(g, nrw);
   if (smem > kSmemMax) return;
-  CK(cudaFuncSetAttribute((const void*)e.k.slot, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CK(allow_smem((const void*)e.k.slot));
   cudaLaunchConfig_t cfg = {};
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeClusterDimension;
@@ -309,7 +332,7 @@ template <typename T> void setup_slot(dda_ctx* c, Engine<T>& e) {
     if (f != 0 && f != g.Gx / 2) order.push_back((uint32_t)c->mx.pos_h[g.Gx - f]);
   }
   e.order = (uint32_t*)dalloc<float>(order.size() * sizeof(uint32_t));
-  CK(cudaMemcpy(e.order, order.data(), order.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+  CK(cudaMemcpyAsync(e.order, order.data(), order.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream));
   e.slots = (T2*)dalloc<T>((size_t)ncl * g.Gz * sg.wp * sizeof(T2));
   e.sg = sg;
   e.cl = cl;
@@ -378,7 +401,8 @@ template <typename T> void setup_engine(dda_ctx* c) {
   }
   if (e.smem_x > kSmemMax) throw DdaError(DDA_ERR_UNSUPPORTED, "grid x extent too large");
   auto attr = [](const void* f, size_t bytes) {
-    CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(bytes, 1)));
+    if (bytes > kSmemMax) throw DdaError(DDA_ERR_UNSUPPORTED, "shared-memory tile above the SM limit");
+    CK(allow_smem(f));
   };
   attr((const void*)e.k.xfwd, e.smem_x);
   attr((const void*)e.k.xinv, e.smem_x);
@@ -390,12 +414,12 @@ template <typename T> void setup_engine(dda_ctx* c) {
   const int hx = g.Gx / 2 + 1, hy = g.Gy / 2 + 1, hz = g.Gz / 2 + 1;
   e.dc = (T2*)dalloc<T>((size_t)hx * hy * hz * 6 * s);
   e.ccs = (T2*)dalloc<T>((size_t)c->max_rhs * g.nmat * 3 * s);
-  CK(cudaMemset(e.ccs, 0, (size_t)c->max_rhs * g.nmat * 3 * s));
+  CK(cudaMemsetAsync(e.ccs, 0, (size_t)c->max_rhs * g.nmat * 3 * s, c->stream));
   e.xhat = (T2*)dalloc<T>((size_t)c->max_rhs * g.Gx * 3 * g.nlines * s);
   const size_t vbytes = (size_t)c->max_rhs * 3 * g.nvs * s;
   for (auto& v : e.vec) {
     v = (T2*)dalloc<T>(vbytes);
-    CK(cudaMemset(v, 0, vbytes));
+    CK(cudaMemsetAsync(v, 0, vbytes, c->stream));
   }
   e.io = (T2*)dalloc<T>(vbytes);
 }
@@ -479,12 +503,10 @@ void build_dmatrix(dda_ctx* c) {
   const MvGeom& g = c->g;
   const long long N = (long long)g.Gx * g.Gy * g.Gz;
   double2* full = nullptr;
-  CK(cudaMalloc(&full, N * sizeof(double2)));
+  CK(cudaMallocAsync(&full, N * sizeof(double2), c->stream));
   const FftPlanDev px = c->px.dev<double>(), py = c->py.dev<double>(), pz = c->pz.dev<double>();
-  CK(cudaFuncSetAttribute((const void*)k_fft_rows<double, kNtC>,
-                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax));
-  CK(cudaFuncSetAttribute((const void*)k_fft_cols<double, kNtC>,
-                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax));
+  CK(allow_smem((const void*)k_fft_rows<double, kNtC>));
+  CK(allow_smem((const void*)k_fft_cols<double, kNtC>));
   static const int MU[6] = {0, 0, 0, 1, 1, 2}, NU[6] = {0, 1, 2, 1, 2, 2};
   int tlr = 32;
   while (tlr > 1 && ((size_t)g.Gx + (size_t)tlr * (g.Gx + 1)) * sizeof(double2) > kSmemMax) tlr--;
@@ -514,8 +536,8 @@ void build_dmatrix(dda_ctx* c) {
                                             c->px.pos, c->py.pos, c->pz.pos);
     CK(cudaGetLastError());
   }
+  CK(cudaFreeAsync(full, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  cudaFree(full);
 }
 
 // Host-supplied D (reference layout, reference units) -> octants.
@@ -533,15 +555,16 @@ void upload_dmatrix(dda_ctx* c, const double* D) {
           h64[dst] = make_double2(D[2 * src] * sc, D[2 * src + 1] * sc);
         }
   double2* tmp = nullptr;
-  CK(cudaMalloc(&tmp, h64.size() * sizeof(double2)));
-  CK(cudaMemcpy(tmp, h64.data(), h64.size() * sizeof(double2), cudaMemcpyHostToDevice));
-  if (c->e64.on) CK(cudaMemcpy(c->e64.dc, tmp, h64.size() * sizeof(double2), cudaMemcpyDeviceToDevice));
+  CK(cudaMallocAsync(&tmp, h64.size() * sizeof(double2), c->stream));
+  CK(cudaMemcpyAsync(tmp, h64.data(), h64.size() * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+  if (c->e64.on)
+    CK(cudaMemcpyAsync(c->e64.dc, tmp, h64.size() * sizeof(double2), cudaMemcpyDeviceToDevice, c->stream));
   if (c->e32.on) {
     k_d64_to_d32<<<592, 256, 0, c->stream>>>(tmp, c->e32.dc, (long long)h64.size());
     CK(cudaGetLastError());
   }
+  CK(cudaFreeAsync(tmp, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  cudaFree(tmp);
 }
 
 int fail(dda_ctx* c, const DdaError& e) {
@@ -718,15 +741,15 @@ void run_solve(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
   CK(cudaMemcpyAsync(c->st, c->st_host, nrhs * sizeof(KrylovState), cudaMemcpyHostToDevice, c->stream));
   sv.init_general(E, B, b.R, b.X, b.A, S, o.start, o.b_given);
   // epsB = eps^2 / residScale (DDA/IterativeSolverBase.cpp:44)
+  CK(cudaMemcpyAsync(c->st_host, c->st, nrhs * sizeof(KrylovState), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  CK(cudaMemcpy(c->st_host, c->st, nrhs * sizeof(KrylovState), cudaMemcpyDeviceToHost));
   for (int r = 0; r < nrhs; r++) {
     KrylovState& k = c->st_host[r];
     const double er = o.eps_rhs ? o.eps_rhs[r] : eps;
     k.epsB = er * er / k.residScale;
     if (!(k.inprodR >= k.epsB)) k.done = 1;  // already converged: no iteration
   }
-  CK(cudaMemcpy(c->st, c->st_host, nrhs * sizeof(KrylovState), cudaMemcpyHostToDevice));
+  CK(cudaMemcpyAsync(c->st, c->st_host, nrhs * sizeof(KrylovState), cudaMemcpyHostToDevice, c->stream));
   sv.solver_init(solver, b);
   long long nr = 0;
   const int poll = 8;
@@ -858,6 +881,7 @@ int dda_create(const dda_problem* p, int precision, dda_ctx** out) {
     c->kd = p->kd;
     c->grid_unit = p->grid_unit;
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    g_alloc_stream = c->stream;
     MvGeom& g = c->g;
     g.Gx = p->grid[0]; g.Gy = p->grid[1]; g.Gz = p->grid[2];
     g.bx = p->box[0]; g.by = p->box[1]; g.bz = p->box[2];
@@ -896,15 +920,15 @@ int dda_create(const dda_problem* p, int precision, dda_ctx** out) {
       matx[i] = m;
     }
     dmalloc((void**)&c->line_off, off.size() * sizeof(uint32_t));
-    CK(cudaMemcpy(c->line_off, off.data(), off.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(c->line_off, off.data(), off.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream));
     dmalloc((void**)&c->dip, nv * sizeof(uint32_t));
-    CK(cudaMemcpy(c->dip, dip.data(), nv * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(c->dip, dip.data(), nv * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream));
     if (!ident) {
       dmalloc((void**)&c->perm, nv * sizeof(uint32_t));
-      CK(cudaMemcpy(c->perm, perm.data(), nv * sizeof(uint32_t), cudaMemcpyHostToDevice));
+      CK(cudaMemcpyAsync(c->perm, perm.data(), nv * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream));
     }
     dmalloc((void**)&c->mat_ext, nv);
-    CK(cudaMemcpy(c->mat_ext, matx.data(), nv, cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(c->mat_ext, matx.data(), nv, cudaMemcpyHostToDevice, c->stream));
     c->px.create(g.Gx);
     c->py.create(g.Gy);
     c->pz.create(g.Gz);
@@ -927,20 +951,20 @@ int dda_create(const dda_problem* p, int precision, dda_ctx** out) {
     const int nparts = std::max(c->nparts_mv, c->nparts_vec);
     dmalloc((void**)&c->parts, (size_t)c->max_rhs * nparts * sizeof(RedSums));
     dmalloc((void**)&c->tickets, c->max_rhs * sizeof(unsigned));
-    CK(cudaMemset(c->tickets, 0, c->max_rhs * sizeof(unsigned)));
+    CK(cudaMemsetAsync(c->tickets, 0, c->max_rhs * sizeof(unsigned), c->stream));
     dmalloc((void**)&c->st, c->max_rhs * sizeof(KrylovState));
-    CK(cudaMemset(c->st, 0, c->max_rhs * sizeof(KrylovState)));
-    CK(cudaMallocHost(&c->st_host, c->max_rhs * sizeof(KrylovState)));
+    CK(cudaMemsetAsync(c->st, 0, c->max_rhs * sizeof(KrylovState), c->stream));
+    c->st_host = new KrylovState[c->max_rhs];
     dmalloc((void**)&c->st_outer, c->max_rhs * sizeof(KrylovState));
-    CK(cudaMemset(c->st_outer, 0, c->max_rhs * sizeof(KrylovState)));
-    CK(cudaMallocHost(&c->sto_host, c->max_rhs * sizeof(KrylovState)));
+    CK(cudaMemsetAsync(c->st_outer, 0, c->max_rhs * sizeof(KrylovState), c->stream));
+    c->sto_host = new KrylovState[c->max_rhs];
     c->hist_cap = 100000;
     dmalloc((void**)&c->hist, (size_t)c->max_rhs * c->hist_cap * sizeof(double));
     c->cc_host.assign((size_t)c->max_rhs * g.nmat * 3, 0);
     c->cc_set.assign(c->max_rhs, 0);
     if (p->dmatrix) upload_dmatrix(c.get(), p->dmatrix);
     else build_dmatrix(c.get());
-    CK(cudaDeviceSynchronize());
+    CK(cudaStreamSynchronize(c->stream));
     c->dev_bytes = g_dalloc_bytes;
     return DDA_OK;
   });
@@ -1122,11 +1146,12 @@ int collect_mixed(dda_ctx* c, const std::vector<MixedOut>& mo, double* history, 
     if (history && history_cap > 0) {  // residual history of the last inner solve
       const long long m = std::min<long long>(std::min(history_cap, c->hist_cap), c->st_host[r].count);
       if (m > 0)
-        CK(cudaMemcpy(history + (size_t)r * history_cap, c->hist + (size_t)r * c->hist_cap, m * sizeof(double),
-                      cudaMemcpyDeviceToHost));
+        CK(cudaMemcpyAsync(history + (size_t)r * history_cap, c->hist + (size_t)r * c->hist_cap,
+                           m * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     }
     if (mo[r].status != 0 && rc == DDA_OK) rc = mo[r].status;
   }
+  CK(cudaStreamSynchronize(c->stream));  // history copies done
   if (rc != DDA_OK) c->err = rc == DDA_ERR_MAXITER ? "Too many iterations" : "refinement did not converge";
   return rc;
 }
@@ -1171,11 +1196,12 @@ int collect_stats(dda_ctx* c, int nrhs, double* history, long long history_cap, 
     if (history && history_cap > 0) {
       const long long m = std::min<long long>(std::min(history_cap, c->hist_cap), k.count);
       if (m > 0)
-        CK(cudaMemcpy(history + (size_t)r * history_cap, c->hist + (size_t)r * c->hist_cap, m * sizeof(double),
-                      cudaMemcpyDeviceToHost));
+        CK(cudaMemcpyAsync(history + (size_t)r * history_cap, c->hist + (size_t)r * c->hist_cap,
+                           m * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     }
     if (k.status != 0 && rc == DDA_OK) rc = k.status;
   }
+  CK(cudaStreamSynchronize(c->stream));  // history copies done
   if (rc != DDA_OK) {
     static const char* msg[] = {"", "", "", "", "", "Krylov breakdown", "Too many iterations",
                                 "Too many iterations w/o increase"};
@@ -1238,6 +1264,45 @@ void* dda_stream(dda_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
 int64_t dda_launch_count(const dda_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
+// Upper bound of the device memory dda_create takes for `p`: the buffers the
+// context keeps (resident) and, in addition while it is built, the FP64 grid
+// of the D-matrix generation (peak).  Mirrors setup_engine: a y/z plane that
+// does not fit one CTA is costed as the split path's plane buffer, which is
+// larger than the cluster path's slots.
+int dda_footprint(const dda_problem* p, int precision, int64_t* resident, int64_t* peak) {
+  if (!p || precision < DDA_PREC_FP64 || precision > DDA_PREC_MIXED || p->max_rhs < 1) return DDA_ERR_ARG;
+  const long long Gx = p->grid[0], Gy = p->grid[1], Gz = p->grid[2];
+  const long long bx = p->box[0], by = p->box[1], bz = p->box[2];
+  (void)bx;
+  const long long nv = p->nv, nvs = (nv + 15) / 16 * 16, nl = by * bz, R = p->max_rhs;
+  const long long nmat = std::max<uint32_t>(1, p->nmat);
+  const bool planned = has_tuned_plan((int)Gx) && has_tuned_plan((int)Gy) && has_tuned_plan((int)Gz) &&
+                       !(p->flags & DDA_FLAG_RUNTIME_PLANS);
+  long long bytes = 4 * (nl + 1) + 9 * nv;                    // line offsets, dipoles, permutation, materials
+  bytes += 6 * (Gx + Gy + Gz) * (8 + 16 + 4 + 4);              // plans
+  auto engine = [&](long long s) {
+    long long e = (Gx / 2 + 1) * (Gy / 2 + 1) * (Gz / 2 + 1) * 6 * s;  // D-hat octant
+    e += R * nmat * 3 * s + R * Gx * 3 * nl * s + 11 * R * 3 * nvs * s;
+    const long long q = 3 * by + ((3 * by) % 2 == 0 ? 1 : 0);
+    const long long smem_yz = (Gz + Gy + Gz * q + 3 * (Gy + 1)) * s;
+    const bool has_yz = !planned || (Gy == Gz && (Gy == 64 || Gy == 80 || Gy == 96 || Gy == 100 || Gy == 128));
+    if (!(has_yz && smem_yz <= (long long)kSmemMax) || (p->flags & (DDA_FLAG_SPLIT_YZ | DDA_FLAG_SLOT_YZ)))
+      e += R * Gx * 3 * Gz * by * s;
+    return e;
+  };
+  if (precision != DDA_PREC_FP32) bytes += engine(16);
+  if (precision != DDA_PREC_FP64) bytes += engine(8);
+  const long long sx = precision == DDA_PREC_FP32 ? 8 : 16;
+  const long long tl = std::max(1LL, std::min(32LL, 98304 / (sx * (Gx + 1))));
+  const long long tiles = (nl + tl - 1) / tl;
+  bytes += R * std::max(3 * tiles, 296LL) * (long long)sizeof(RedSums) + R * 4;
+  bytes += 2 * R * (long long)sizeof(KrylovState) + R * 100000LL * 8;
+  if (resident) *resident = bytes;
+  const long long tmp = p->dmatrix ? (Gx / 2 + 1) * (Gy / 2 + 1) * (Gz / 2 + 1) * 6 * 16 : Gx * Gy * Gz * 16;
+  if (peak) *peak = bytes + tmp;
+  return DDA_OK;
+}
+
 int dda_matvec_layout(const dda_ctx* ctx, int64_t* out) {
   if (!ctx || !out) return DDA_ERR_ARG;
   auto fill = [&](const auto& e) {
@@ -1276,8 +1341,8 @@ void far_field_t(dda_ctx* c, int nrhs, const double* pol, long long ndir, const 
   if (pol) host_to_engine<T>(c, pol, e.io, n);
   double* ddirs = nullptr;
   double2* dout = nullptr;
-  CK(cudaMalloc(&ddirs, ndir * 3 * sizeof(double)));
-  CK(cudaMalloc(&dout, (size_t)ndir * nrhs * 3 * sizeof(double2)));
+  CK(cudaMallocAsync(&ddirs, ndir * 3 * sizeof(double), c->stream));
+  CK(cudaMallocAsync(&dout, (size_t)ndir * nrhs * 3 * sizeof(double2), c->stream));
   CK(cudaMemcpyAsync(ddirs, dirs, ndir * 3 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   FfGeom g;
   g.nv = c->g.nv;
@@ -1294,16 +1359,15 @@ void far_field_t(dda_ctx* c, int nrhs, const double* pol, long long ndir, const 
   constexpr int DB = 4, NT = 256;
   const size_t smem = (size_t)DB * g.bx * sizeof(double2);
   if (smem > kSmemMax) throw DdaError(DDA_ERR_UNSUPPORTED, "box too long for the far-field tables");
-  CK(cudaFuncSetAttribute((const void*)k_farfield<T, NT, DB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)std::max<size_t>(smem, 1)));
+  CK(allow_smem((const void*)k_farfield<T, NT, DB>));
   k_farfield<T, NT, DB><<<dim3((unsigned)((ndir + DB - 1) / DB), nrhs), NT, smem, c->stream>>>(
       e.io, c->line_off, c->dip, c->perm, ddirs, (int)ndir, g, dout);
   CK(cudaGetLastError());
   c->launches++;
   CK(cudaMemcpyAsync(out, dout, (size_t)ndir * nrhs * 3 * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaFreeAsync(ddirs, c->stream));
+  CK(cudaFreeAsync(dout, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  cudaFree(ddirs);
-  cudaFree(dout);
 }
 
 // Far field without any allocation (dda_far_field_noalloc).  The device
@@ -1364,8 +1428,7 @@ void far_field_noalloc_t(dda_ctx* c, int nrhs, long long ndir, const double* dir
   constexpr int DB = 4, NT = 256;
   const size_t smem = (size_t)DB * g.bx * sizeof(double2);
   if (smem > kSmemMax) throw DdaError(DDA_ERR_UNSUPPORTED, "box too long for the far-field tables");
-  CK(cudaFuncSetAttribute((const void*)k_farfield<T, NT, DB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)std::max<size_t>(smem, 1)));
+  CK(allow_smem((const void*)k_farfield<T, NT, DB>));
   k_farfield<T, NT, DB><<<dim3((unsigned)((ndir + DB - 1) / DB), nrhs), NT, smem, c->stream>>>(
       e.io, c->line_off, c->dip, c->perm, ddirs, (int)ndir, g, dout);
   CK(cudaGetLastError());
@@ -1411,10 +1474,12 @@ int dda_get_dmatrix(dda_ctx* ctx, double* out) {
     const size_t m = (size_t)hx * hy * hz * 6;
     std::vector<double2> h(m);
     if (ctx->e64.on) {
-      CK(cudaMemcpy(h.data(), ctx->e64.dc, m * sizeof(double2), cudaMemcpyDeviceToHost));
+      CK(cudaMemcpyAsync(h.data(), ctx->e64.dc, m * sizeof(double2), cudaMemcpyDeviceToHost, ctx->stream));
+      CK(cudaStreamSynchronize(ctx->stream));
     } else {
       std::vector<float2> f(m);
-      CK(cudaMemcpy(f.data(), ctx->e32.dc, m * sizeof(float2), cudaMemcpyDeviceToHost));
+      CK(cudaMemcpyAsync(f.data(), ctx->e32.dc, m * sizeof(float2), cudaMemcpyDeviceToHost, ctx->stream));
+      CK(cudaStreamSynchronize(ctx->stream));
       for (size_t i = 0; i < m; i++) h[i] = make_double2(f[i].x, f[i].y);
     }
     const double sc = 1.0 / (ctx->grid_unit * ctx->grid_unit * ctx->grid_unit);

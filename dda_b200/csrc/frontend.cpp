@@ -17,7 +17,7 @@
 namespace {
 
 typedef long double ld;
-std::string g_err;
+thread_local std::string g_err;
 
 const ld kTwoPi = 6.2831853071795864769252867665590056L;
 const ld kFourPi = 12.5663706143591729538505735331180112L;

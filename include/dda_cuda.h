@@ -162,6 +162,12 @@ void* dda_stream(dda_ctx* ctx);
  * Krylov steps, setup); a profiling counter. */
 int64_t dda_launch_count(const dda_ctx* ctx);
 
+/* Upper bound of the device memory dda_create(prob, precision) takes:
+ * `resident` = what the context keeps, `peak` = resident plus the temporary
+ * FP64 grid of the D-matrix generation.  Used to admit requests by HBM
+ * footprint; no counterpart in the reference. */
+int dda_footprint(const dda_problem* prob, int precision, int64_t* resident, int64_t* peak);
+
 /* Layout the context chose for its matvec (working precision: FP32 for
  * DDA_PREC_FP32 and DDA_PREC_MIXED, FP64 otherwise), 8 values:
  * [0] y/z path (0 fused plane kernel, 1 cluster kernel, 2 split path),

@@ -16,7 +16,7 @@ FIXTURE = os.path.join(ROOT, "tests", "golden", "box_10_8_6.geom")
 
 def _declared_symbols():
     names = set()
-    for h in ("dda_cuda.h", "dda_frontend.h"):
+    for h in ("dda_cuda.h", "dda_frontend.h", "dda_serve.h"):
         text = open(os.path.join(ROOT, "include", h)).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
         for m in re.finditer(r"\b(dda_[a-z0-9_]+)\s*\(", text):

@@ -45,6 +45,13 @@ def parse():
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64", "mixed"])
     ap.add_argument("--solver", default="bicgstab")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--workload", default="box", choices=["box", "batched", "mixed512", "serve"],
+                    help="box: the default line; batched: 128-rhs spheroid; mixed512: 512^3 sphere "
+                         "with FP64 refinement; serve: Poisson request stream")
+    ap.add_argument("--requests", type=int, default=120, help="serve: requests in the stream")
+    ap.add_argument("--rate", type=float, default=50.0, help="serve: mean arrivals per second")
+    ap.add_argument("--slots", type=int, default=8, help="serve: concurrent requests")
+    ap.add_argument("--max-iter", type=int, default=4000, help="mixed512: iteration cap of each solve")
     return ap.parse_args()
 
 
@@ -330,5 +337,8 @@ if __name__ == "__main__":
     a = parse()
     if a.impl == "reference":
         run_reference(a)
-    else:
+    elif a.workload == "box":
         run_ours(a)
+    else:
+        import bench_workloads
+        getattr(bench_workloads, "run_" + a.workload)(a)

@@ -10,6 +10,7 @@ lib_path = os.path.join(_HERE, "libdda_b200.so")
 SOLVERS = {"qmr": 0, "bicgstab": 1, "bicg": 2, "cgnr": 3}
 PRECISIONS = {"fp64": 0, "fp32": 1, "mixed": 2}
 POLARIZABILITIES = {"cm": 0, "ldr": 1, "ldr-avgpol": 2}
+GRID_POLICIES = {"reference": 0, "tuned": 1}
 ERRORS = {-1: "invalid argument", -2: "CUDA failure", -3: "out of device memory",
           -4: "unsupported size", -5: "Krylov breakdown", -6: "Too many iterations",
           -7: "Too many iterations w/o increase"}
@@ -193,7 +194,7 @@ class Geometry:
 class DDAParams:
     """Grid and vector layout of one target (DDA/DDAParams.cpp:93-214)."""
 
-    def __init__(self, geometry, materials, wavelength, grid=None, support_nonpot=True):
+    def __init__(self, geometry, materials, wavelength, grid=None, support_nonpot=True, grid_policy="reference"):
         self.geometry = geometry
         self.materials = [m if isinstance(m, (list, tuple)) else (m, m, m) for m in materials]
         if len(self.materials) < geometry.nmat:
@@ -204,6 +205,17 @@ class DDAParams:
         self.box = geometry.box
         g = grid or (0, 0, 0)
         self.grid = tuple(fft_fit(2 * b, o, support_nonpot) for b, o in zip(self.box, g))
+        if grid is None and grid_policy != "reference":
+            # dda_choose_grid: lengths with compile-time FFT plans (same
+            # matvec up to rounding, the zero padding being exact)
+            box = (ctypes.c_uint32 * 3)(*self.box)
+            out = (ctypes.c_uint32 * 3)()
+            L = lib()
+            L.dda_choose_grid.argtypes = [ctypes.POINTER(ctypes.c_uint32), ctypes.c_int,
+                                          ctypes.POINTER(ctypes.c_uint32)]
+            if L.dda_choose_grid(box, GRID_POLICIES[grid_policy], out) != 0:
+                raise DDAError(-1, "bad grid policy")
+            self.grid = tuple(out)
         self.grid_unit = geometry.grid_unit
         self.wave_num = 2 * np.pi / self.wavelength
         self.kd = self.wave_num * self.grid_unit

@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "../../include/dda_cuda.h"
+#include "../../include/dda_frontend.h"
 #include "dmatrix_kernels.cuh"
 #include "farfield_kernels.cuh"
 #include "fft_engine.cuh"
@@ -716,6 +717,7 @@ struct SolveOpts {
   const double* eps_rhs = nullptr; // per-rhs relative residual targets
   const char* skip = nullptr;      // rhs left untouched (marked done from the start)
   bool result = true;              // write P = sqrt(cc) x to the engine's io buffer
+  long long max_res_increase = 0;  // > 0: stagnation limit instead of the solver's
 };
 
 // Runs one solve of `nrhs` right-hand sides already set up in the engine
@@ -733,7 +735,7 @@ void run_solve(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
     KrylovState& k = c->st_host[r];
     memset(&k, 0, sizeof(k));
     k.maxIter = max_iter > 0 ? max_iter : (1LL << 62);
-    k.maxResIncrease = kMaxResIncrease[solver];
+    k.maxResIncrease = o.max_res_increase > 0 ? o.max_res_increase : kMaxResIncrease[solver];
     k.histCap = c->hist_cap;
     k.hist = c->hist + (size_t)r * c->hist_cap;
     if (o.skip && o.skip[r]) k.done = 1;
@@ -793,7 +795,16 @@ void run_mixed(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
   else CK(cudaMemsetAsync(X, 0, n * sizeof(double2), c->stream));
   std::vector<char> done(nrhs, 0);
   std::vector<double> eps_in(nrhs, 1e-4);
-  const int max_outer = 30;
+  // An inner FP32 solve ends at its target or when its residual has not
+  // reached a new minimum for kInnerStall iterations (FP32 Krylov
+  // recurrences stagnate on hard problems); the outer FP64 residual then
+  // restarts it.  The refinement fails once kOuterStall outer steps in a row
+  // reduce the FP64 residual by less than 2x.
+  const int max_outer = 60;
+  const long long kInnerStall = 200;
+  const int kOuterStall = 3;
+  std::vector<double> prev_rel(nrhs, 0.0);
+  std::vector<int> stalls(nrhs, 0);
   for (int outer = 0;; outer++) {
     // r = b - A x (FP64); reduction n = |r|^2 -> last
     if (outer == 0 && !start) CK(cudaMemcpyAsync(R, B, n * sizeof(double2), cudaMemcpyDeviceToDevice, c->stream));
@@ -809,7 +820,13 @@ void run_mixed(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
       out[r].rel = rel;
       out[r].res_scale = k.residScale;
       total_it = std::max(total_it, out[r].iterations);
+      if (!done[r] && !(rel == rel)) { done[r] = 1; out[r].status = DDA_ERR_BREAKDOWN; }
       if (!done[r] && (rel < eps || out[r].status != 0)) done[r] = 1;
+      if (!done[r] && outer > 0) {
+        stalls[r] = rel > 0.5 * prev_rel[r] ? stalls[r] + 1 : 0;
+        if (stalls[r] >= kOuterStall) { done[r] = 1; out[r].status = DDA_ERR_NOPROGRESS; }
+      }
+      prev_rel[r] = rel;
       if (!done[r] && outer >= max_outer) { done[r] = 1; out[r].status = DDA_ERR_NOPROGRESS; }
       if (!done[r] && max_iter > 0 && out[r].iterations >= max_iter) { done[r] = 1; out[r].status = DDA_ERR_MAXITER; }
       k.done = done[r];
@@ -826,12 +843,16 @@ void run_mixed(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
     o.eps_rhs = eps_in.data();
     o.skip = done.data();
     o.result = false;
+    o.max_res_increase = kInnerStall;
     run_solve<float>(c, solver, nrhs, 0.0, max_iter > 0 ? max_iter - total_it : 0, o);
     for (int r = 0; r < nrhs; r++) {
       if (done[r]) continue;
       out[r].iterations += c->st_host[r].count;
       out[r].refinements++;
-      if (c->st_host[r].status != 0 && c->st_host[r].status != DDA_ERR_MAXITER) out[r].status = c->st_host[r].status;
+      // an inner solve that stopped early (stagnation, breakdown, its share
+      // of max_iter) still contributes its correction; the outer FP64
+      // residual decides
+      (void)c->st_host[r].status;
     }
     // x += e for the rhs still running
     k_accum<<<dim3(c->nparts_vec, nrhs), 256, 0, c->stream>>>(X, f.vec[4], c->st_outer, 3LL * c->g.nvs);
@@ -1264,6 +1285,26 @@ void* dda_stream(dda_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
 int64_t dda_launch_count(const dda_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
+int dda_choose_grid(const uint32_t* box, int policy, uint32_t* grid) {
+  if (!box || !grid || policy < DDA_GRID_REFERENCE || policy > DDA_GRID_TUNED) return DDA_ERR_ARG;
+  for (int a = 0; a < 3; a++) grid[a] = dda_fft_fit(2 * box[a], 0, 1);  // DDA/DDAParams.cpp:290-335
+  if (policy == DDA_GRID_REFERENCE) return DDA_OK;
+  auto tuned_ceil = [](uint32_t x) -> uint32_t {
+    uint32_t best = 0;
+#define C(N) if ((uint32_t)N >= x && (best == 0 || (uint32_t)N < best)) best = N;
+    DDA_TUNED_LENGTHS(C)
+#undef C
+    return best;
+  };
+  const uint32_t gx = tuned_ceil(2 * box[0]), gyz = tuned_ceil(2 * std::max(box[1], box[2]));
+  if (!gx || !gyz) return DDA_OK;
+  const double ref = (double)grid[0] * grid[1] * grid[2], tun = (double)gx * gyz * gyz;
+  if (tun > 2.0 * ref) return DDA_OK;  // padding would cost more than the plans gain
+  grid[0] = gx;
+  grid[1] = grid[2] = gyz;
+  return DDA_OK;
+}
+
 // Upper bound of the device memory dda_create takes for `p`: the buffers the
 // context keeps (resident) and, in addition while it is built, the FP64 grid
 // of the D-matrix generation (peak).  Mirrors setup_engine: a y/z plane that
@@ -1285,7 +1326,11 @@ int dda_footprint(const dda_problem* p, int precision, int64_t* resident, int64_
     e += R * nmat * 3 * s + R * Gx * 3 * nl * s + 11 * R * 3 * nvs * s;
     const long long q = 3 * by + ((3 * by) % 2 == 0 ? 1 : 0);
     const long long smem_yz = (Gz + Gy + Gz * q + 3 * (Gy + 1)) * s;
-    const bool has_yz = !planned || (Gy == Gz && (Gy == 64 || Gy == 80 || Gy == 96 || Gy == 100 || Gy == 128));
+    bool fused_len = false;
+#define C(N) fused_len = fused_len || Gy == N;
+    DDA_FUSED_LENGTHS(C)
+#undef C
+    const bool has_yz = !planned || (Gy == Gz && fused_len);
     if (!(has_yz && smem_yz <= (long long)kSmemMax) || (p->flags & (DDA_FLAG_SPLIT_YZ | DDA_FLAG_SLOT_YZ)))
       e += R * Gx * 3 * Gz * by * s;
     return e;

@@ -29,8 +29,6 @@ template <typename T> struct MvKernels {
   bool planned = false;
 };
 
-#define DDA_TUNED_LENGTHS(X) X(64) X(80) X(96) X(100) X(128) X(160) X(192) X(200) X(256) X(512)
-#define DDA_FUSED_LENGTHS(X) X(64) X(80) X(96) X(100) X(128)
 
 inline bool has_tuned_plan(int n) {
   switch (n) {

@@ -18,37 +18,51 @@
 
 namespace dda {
 
+// Grid lengths with compile-time plans, and those whose kx plane the fused
+// plane kernel k_yz_p handles (y and z both of that length).
+#define DDA_TUNED_LENGTHS(X)                                                                               \
+  X(32) X(48) X(56) X(64) X(80) X(96) X(100) X(112) X(120) X(128) X(144) X(160) X(168) X(192) X(200) X(224) \
+  X(240) X(256) X(288) X(320) X(384) X(512)
+#define DDA_FUSED_LENGTHS(X) X(32) X(48) X(56) X(64) X(80) X(96) X(100) X(112) X(120) X(128)
+
 // Tuned plans: a large first radix and a last radix of at most 8, so the
 // fused last stage holds 3 x R_last complex values per thread.
 template <int N> struct PlanFor { typedef void type; };
+template <> struct PlanFor<32> { typedef Plan<4, 8> type; };
+template <> struct PlanFor<48> { typedef Plan<6, 8> type; };
+template <> struct PlanFor<56> { typedef Plan<7, 8> type; };
 template <> struct PlanFor<64> { typedef Plan<8, 8> type; };
 template <> struct PlanFor<80> { typedef Plan<10, 8> type; };
 template <> struct PlanFor<96> { typedef Plan<12, 8> type; };
 template <> struct PlanFor<100> { typedef Plan<20, 5> type; };
+template <> struct PlanFor<112> { typedef Plan<14, 8> type; };
+template <> struct PlanFor<120> { typedef Plan<15, 8> type; };
 template <> struct PlanFor<128> { typedef Plan<16, 8> type; };
+template <> struct PlanFor<144> { typedef Plan<18, 8> type; };
 template <> struct PlanFor<160> { typedef Plan<20, 8> type; };
+template <> struct PlanFor<168> { typedef Plan<21, 8> type; };
 template <> struct PlanFor<192> { typedef Plan<24, 8> type; };
 template <> struct PlanFor<200> { typedef Plan<25, 8> type; };
+template <> struct PlanFor<224> { typedef Plan<28, 8> type; };
+template <> struct PlanFor<240> { typedef Plan<30, 8> type; };
 template <> struct PlanFor<256> { typedef Plan<8, 4, 8> type; };
+template <> struct PlanFor<288> { typedef Plan<6, 6, 8> type; };
+template <> struct PlanFor<320> { typedef Plan<5, 8, 8> type; };
+template <> struct PlanFor<384> { typedef Plan<6, 8, 8> type; };
 template <> struct PlanFor<512> { typedef Plan<8, 8, 8> type; };
 
 // Radices of the tuned plan for n (host side), empty when there is none.
 inline std::vector<int> tuned_radices(int n) {
   auto get = [](auto p) { return std::vector<int>(std::begin(decltype(p)::r), std::end(decltype(p)::r)); };
   switch (n) {
-    case 64: return get(PlanFor<64>::type());
-    case 80: return get(PlanFor<80>::type());
-    case 96: return get(PlanFor<96>::type());
-    case 100: return get(PlanFor<100>::type());
-    case 128: return get(PlanFor<128>::type());
-    case 160: return get(PlanFor<160>::type());
-    case 192: return get(PlanFor<192>::type());
-    case 200: return get(PlanFor<200>::type());
-    case 256: return get(PlanFor<256>::type());
-    case 512: return get(PlanFor<512>::type());
+#define C(N) \
+  case N: return get(typename PlanFor<N>::type());
+    DDA_TUNED_LENGTHS(C)
+#undef C
     default: return {};
   }
 }
+
 
 // ---- z stage 0 fused with the plane read / write (whole CTA) -------------
 template <typename T, int NT, typename PZ>

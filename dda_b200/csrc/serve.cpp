@@ -107,25 +107,29 @@ void dda_server::run(Job& j, Done& d) {
   int rc = dda_create(&P, q.precision, &ctx);
   if (rc != DDA_OK) return set_error(d, dda_last_error(nullptr), rc);
   std::unique_ptr<dda_ctx, int (*)(dda_ctx*)> cc(ctx, dda_destroy);
+  d.res.t_setup = now();
   int64_t layout[8] = {};
   dda_matvec_layout(ctx, layout);
   d.res.device_bytes = layout[7];
   const int64_t nvs = dda_vec_stride(ctx);
   d.res.nvs = nvs;
   const size_t vlen = (size_t)3 * nvs * 2;  // doubles per right-hand side
+  const int pol0 = (q.npol == 1 && q.first_pol == 2) ? 2 : 1;  // polarisation of right-hand side 0
   std::vector<double> einc(vlen * q.npol), cc_all(q.nmat * 6 * q.npol);
   for (int r = 0; r < q.npol; r++) {
     std::vector<double> ccv(q.nmat * 6), ccs(q.nmat * 6), chi(q.nmat * 6);
-    if (dda_couple_constants(q.polarizability, q.nmat, j.refr.data(), d_m, k, q.prop, r + 1, ccv.data(), ccs.data(),
-                             chi.data()))
+    if (dda_couple_constants(q.polarizability, q.nmat, j.refr.data(), d_m, k, q.prop, pol0 + r, ccv.data(),
+                             ccs.data(), chi.data()))
       return set_error(d, dda_frontend_error(), DDA_ERR_ARG);
     std::copy(ccv.begin(), ccv.end(), cc_all.begin() + (size_t)r * q.nmat * 6);
     if ((rc = dda_set_cc(ctx, r, ccs.data())) != DDA_OK) return set_error(d, dda_last_error(ctx), rc);
-    if (dda_einc_plane(g, k, q.prop, r + 1, einc.data() + r * vlen)) return set_error(d, dda_frontend_error(), DDA_ERR_ARG);
+    if (dda_einc_plane(g, k, q.prop, pol0 + r, einc.data() + r * vlen))
+      return set_error(d, dda_frontend_error(), DDA_ERR_ARG);
   }
   d.pol.assign(vlen * q.npol, 0.0);
   rc = dda_solve(ctx, q.solver, q.npol, einc.data(), q.eps, q.max_iter, nullptr, d.pol.data(), nullptr, 0,
                  d.res.stats);
+  d.res.t_solved = now();
   if (rc != DDA_OK) {
     set_error(d, dda_last_error(ctx), rc);
     if (!q.keep_pol) d.pol.clear();
@@ -141,7 +145,7 @@ void dda_server::run(Job& j, Done& d) {
     return set_error(d, dda_last_error(ctx), rc);
   const double four_pi = 4 * M_PI, temp1 = k * k * k * 2 / 3;
   for (int r = 0; r < q.npol; r++) {
-    dda_beam_pol(q.prop, r + 1, inc, pn);
+    dda_beam_pol(q.prop, pol0 + r, inc, pn);
     const double* e = ef.data() + (size_t)r * 6;
     d.res.cext[r] = -(e[0] * inc[0] + e[2] * inc[1] + e[4] * inc[2]) * four_pi / k;
     const std::complex<double>* ccr = reinterpret_cast<const std::complex<double>*>(cc_all.data()) + (size_t)r * q.nmat * 3;
@@ -239,6 +243,16 @@ int dda_serve_create(int device, int64_t hbm_budget, int max_active, dda_server*
     }
     hbm_budget = (int64_t)(0.9 * (double)fr);
   }
+  // Contexts allocate from the device's default memory pool on their
+  // streams.  Let the pool keep up to the budget mapped between requests
+  // instead of returning memory to the driver at every synchronisation
+  // (a process-local pool attribute).
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t keep = (uint64_t)hbm_budget;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  cudaGetLastError();
   dda_server* s = new dda_server;
   s->device = device;
   s->budget = hbm_budget;
@@ -275,9 +289,10 @@ int dda_serve_submit(dda_server* s, const dda_serve_request* q, int64_t* id) {
   P.nmat = q->nmat;
   P.max_rhs = q->npol;
   P.device = s->device;
-  for (int a = 0; a < 3; a++) {
-    P.box[a] = box[a];
-    P.grid[a] = dda_fft_fit(2 * box[a], 0, 1);
+  for (int a = 0; a < 3; a++) P.box[a] = box[a];
+  if (dda_choose_grid(box, q->grid_policy, P.grid) != DDA_OK) {
+    g_serve_err = "bad grid policy";
+    return DDA_ERR_ARG;
   }
   int64_t resident = 0;
   if (dda_footprint(&P, q->precision, &resident, &j->peak) != DDA_OK) {

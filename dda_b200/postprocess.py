@@ -91,3 +91,40 @@ def cross_sections(params, cc, pol_vec, e_forward, prop, pol):
     a_eq = (3.0 / (4 * np.pi) * nv) ** (1.0 / 3) * params.grid_unit
     norm = 1.0 / (np.pi * a_eq * a_eq)
     return cext, cabs, cext * norm, cabs * norm
+
+
+def mie(x, m):
+    """Mie efficiencies (Qext, Qsca, Qabs) of a homogeneous sphere of size
+    parameter x and relative refractive index m: the Bohren-Huffman series
+    the reference prints beside the DDA cross sections (EMSim/Mie.cpp:41-174,
+    DDA/DDAMain.cpp:431-460).  Downward recurrence for the logarithmic
+    derivative, upward for the Riccati-Bessel functions; forward-scattering
+    amplitude for Qext."""
+    m = complex(m)
+    mx = x * m
+    xstop = x + 4 * x ** (1.0 / 3) + 2
+    nstop = int(xstop)
+    nmx = int(max(xstop, abs(mx)) + 15)
+    d = np.zeros(nmx, dtype=np.complex128)
+    for i in range(nmx - 1, 0, -1):
+        d[i - 1] = (i + 1) / mx - 1.0 / (d[i] + (i + 1) / mx)
+    psi0, psi1 = math.cos(x), math.sin(x)
+    chi0, chi1 = -math.sin(x), math.cos(x)
+    xi1 = complex(psi1, -chi1)
+    qs = 0.0
+    s1 = 0j
+    for n in range(nstop):
+        rn = n + 1.0
+        psi = (2 * rn - 1) * psi1 / x - psi0
+        chi = (2 * rn - 1) * chi1 / x - chi0
+        xi = complex(psi, -chi)
+        a = ((d[n] / m + rn / x) * psi - psi1) / ((d[n] / m + rn / x) * xi - xi1)
+        b = ((m * d[n] + rn / x) * psi - psi1) / ((m * d[n] + rn / x) * xi - xi1)
+        qs += (2 * rn + 1) * (abs(a) ** 2 + abs(b) ** 2)
+        s1 += (2 * rn + 1) / (rn * (rn + 1)) * (a + b) * rn * (rn + 1) / 2
+        psi0, psi1 = psi1, psi
+        chi0, chi1 = chi1, chi
+        xi1 = complex(psi1, -chi1)
+    qsca = 2 / (x * x) * qs
+    qext = 4 / (x * x) * s1.real
+    return qext, qsca, qext - qsca

@@ -17,6 +17,7 @@ import numpy as np
 from .api import DDAError, POLARIZABILITIES, PRECISIONS, SOLVERS, Stats, lib
 
 vp = ctypes.c_void_p
+GRID_POLICIES = {"reference": 0, "tuned": 1}
 
 
 class Request(ctypes.Structure):
@@ -25,14 +26,16 @@ class Request(ctypes.Structure):
                 ("grid_unit", ctypes.c_char_p), ("wavelength", ctypes.c_char_p), ("prop", ctypes.c_double * 3),
                 ("npol", ctypes.c_int32), ("polarizability", ctypes.c_int32), ("solver", ctypes.c_int32),
                 ("precision", ctypes.c_int32), ("eps", ctypes.c_double), ("max_iter", ctypes.c_int64),
-                ("keep_pol", ctypes.c_int32), ("pad", ctypes.c_int32), ("tag", ctypes.c_uint64)]
+                ("keep_pol", ctypes.c_int32), ("first_pol", ctypes.c_int32), ("grid_policy", ctypes.c_int32),
+                ("pad", ctypes.c_int32), ("tag", ctypes.c_uint64)]
 
 
 class Result(ctypes.Structure):
     _fields_ = [("id", ctypes.c_int64), ("tag", ctypes.c_uint64), ("status", ctypes.c_int32),
                 ("npol", ctypes.c_int32), ("stats", Stats * 2), ("cext", ctypes.c_double * 2),
                 ("cabs", ctypes.c_double * 2), ("t_submit", ctypes.c_double), ("t_admit", ctypes.c_double),
-                ("t_done", ctypes.c_double), ("footprint", ctypes.c_int64), ("device_bytes", ctypes.c_int64),
+                ("t_done", ctypes.c_double), ("t_setup", ctypes.c_double), ("t_solved", ctypes.c_double),
+                ("footprint", ctypes.c_int64), ("device_bytes", ctypes.c_int64),
                 ("grid", ctypes.c_uint32 * 3), ("nv", ctypes.c_uint32), ("nvs", ctypes.c_int64),
                 ("pol", ctypes.POINTER(ctypes.c_double)), ("error", ctypes.c_char * 160)]
 
@@ -80,7 +83,7 @@ class Server:
 
     def submit(self, positions, materials, refr, grid_unit, wavelength, prop=(0, 0, 1), npol=2,
                polarizability="ldr", solver="qmr", precision="mixed", eps=1e-5, max_iter=0, keep_pol=False,
-               tag=0):
+               tag=0, first_pol=1, grid_policy="tuned"):
         pos = np.ascontiguousarray(positions, dtype=np.uint32).reshape(-1, 3)
         mat = None if materials is None else np.ascontiguousarray(materials, dtype=np.uint8)
         r = _refr_array(refr)
@@ -100,6 +103,8 @@ class Server:
         q.eps = eps
         q.max_iter = max_iter
         q.keep_pol = 1 if keep_pol else 0
+        q.first_pol = first_pol
+        q.grid_policy = GRID_POLICIES[grid_policy]
         q.tag = tag
         rid = ctypes.c_int64()
         rc = self.L.dda_serve_submit(self.h, ctypes.byref(q), ctypes.byref(rid))
@@ -118,7 +123,8 @@ class Server:
                  "refinements": [r.stats[k].refinements for k in range(r.npol)],
                  "rel_residual": [r.stats[k].rel_residual for k in range(r.npol)],
                  "cext": list(r.cext)[:r.npol], "cabs": list(r.cabs)[:r.npol],
-                 "t_submit": r.t_submit, "t_admit": r.t_admit, "t_done": r.t_done,
+                 "t_submit": r.t_submit, "t_admit": r.t_admit, "t_done": r.t_done, "t_setup": r.t_setup,
+                 "t_solved": r.t_solved,
                  "footprint": r.footprint, "device_bytes": r.device_bytes, "grid": tuple(r.grid),
                  "nv": r.nv, "nvs": r.nvs, "error": r.error.decode(errors="replace")}
             if r.pol:

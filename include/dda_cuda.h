@@ -162,6 +162,17 @@ void* dda_stream(dda_ctx* ctx);
  * Krylov steps, setup); a profiling counter. */
 int64_t dda_launch_count(const dda_ctx* ctx);
 
+/* FFT grid for a particle box.  DDA_GRID_REFERENCE: fftFit(2 box) per axis,
+ * the reference's choice (DDA/DDAParams.cpp:290-335).  DDA_GRID_TUNED: per
+ * axis the smallest length >= 2 box with compile-time FFT plans, y and z
+ * equal so the y/z passes use them, unless that more than doubles the grid.
+ * Any grid >= 2 box gives the same matvec up to rounding (the zero padding
+ * makes the circular convolution the exact linear one); the reference's
+ * --fft-grid sets it the same way. */
+#define DDA_GRID_REFERENCE 0
+#define DDA_GRID_TUNED 1
+int dda_choose_grid(const uint32_t* box, int policy, uint32_t* grid);
+
 /* Upper bound of the device memory dda_create(prob, precision) takes:
  * `resident` = what the context keeps, `peak` = resident plus the temporary
  * FP64 grid of the D-matrix generation.  Used to admit requests by HBM

@@ -48,6 +48,8 @@ typedef struct dda_serve_request {
   double eps;                /* relative residual */
   int64_t max_iter;          /* <= 0: unlimited */
   int32_t keep_pol;          /* 1: keep the polarisations in the result */
+  int32_t first_pol;         /* npol == 1: which polarisation (1 or 2; 0 means 1) */
+  int32_t grid_policy;       /* DDA_GRID_REFERENCE or DDA_GRID_TUNED (dda_choose_grid) */
   int32_t pad;
   uint64_t tag;              /* caller's label, returned in the result */
 } dda_serve_request;
@@ -60,6 +62,7 @@ typedef struct dda_serve_result {
   dda_stats stats[2];
   double cext[2], cabs[2];   /* cross sections, m^2 (DDA/Beam.cpp:126-133, DDA/AbsCross.cpp:28-48) */
   double t_submit, t_admit, t_done;  /* seconds on the server clock */
+  double t_setup, t_solved;  /* context built (D matrix included); solve finished */
   int64_t footprint;         /* bytes reserved at admission (dda_footprint peak) */
   int64_t device_bytes;      /* bytes the request's context held */
   uint32_t grid[3];

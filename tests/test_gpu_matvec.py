@@ -103,6 +103,34 @@ def test_matvec_plane_beyond_shared_memory(prec, tol):
     assert rel(pr.mv.apply(xs[0]), want[0]) < tol
 
 
+@pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("fp32", FP32_TOL)])
+def test_matvec_tuned_grid_matches_reference_grid(prec, tol):
+    # box 35 x 40 x 45 with holes: reference grid 70 x 80 x 90 (runtime
+    # plans), tuned grid 80 x 96 x 96 (compile-time plans, fused y/z); the
+    # matvec restricted to the dipoles is the same linear convolution
+    import dda_b200
+    from oracle import oracle as O
+    pos = np.array([(x, y, z) for z in range(45) for y in range(40) for x in range(35) if (x * 7 + y * 3 + z) % 11],
+                   dtype=np.uint32)
+    mat = np.zeros(len(pos), np.uint8)
+    g = dda_b200.Geometry.from_arrays(pos, mat, "0.05um")
+    p = dda_b200.DDAParams(g, [1.4 + 0.2j], "0.8um", grid_policy="tuned")
+    assert p.grid == (80, 96, 96)
+    mv = dda_b200.CudaMatVec(p, prec)
+    assert mv.layout["compile_time_plans"] == 1
+    og = O.Geometry.from_arrays(pos, mat, "0.05um")
+    op = O.Problem(og, [1.4 + 0.2j], "0.8um")
+    assert op.grid == (70, 80, 90)
+    op.build_dmatrix()
+    mv.set_couple_constants(dda_b200.CoupleConstants(p, (0.6, 0, 0.8), 2, "ldr"))
+    op.set_cc((0.6, 0, 0.8), 2, "ldr")
+    rng = np.random.default_rng(3)
+    x = rng.uniform(-1, 1, p.vec_size) + 1j * rng.uniform(-1, 1, p.vec_size)
+    for c in range(3):
+        x[c * p.nvs + p.nv:(c + 1) * p.nvs] = 0
+    assert rel(mv.apply(x), op.matvec(x)) < tol
+
+
 def test_matvec_host_dmatrix():
     kind, args, mats, lam = CASES["aniso"]
     pr = Pair(kind, args, mats, lam, "fp64", host_d=True)

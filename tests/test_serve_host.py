@@ -51,3 +51,20 @@ def test_served_requests_are_valid_targets():
         m = r["refr"][0]
         assert 1.05 <= m.real <= 2.0 and 0 <= m.imag <= 0.5
         assert abs(np.linalg.norm(r["prop"]) - 1) < 1e-12
+
+
+TUNED = {32, 48, 56, 64, 80, 96, 100, 112, 120, 128, 144, 160, 168, 192, 200, 224, 240, 256, 288, 320, 384, 512}
+
+
+def test_choose_grid_policies():
+    L = api.lib()
+    L.dda_choose_grid.argtypes = [ctypes.POINTER(ctypes.c_uint32), ctypes.c_int, ctypes.POINTER(ctypes.c_uint32)]
+    for box in [(7, 6, 5), (35, 40, 45), (70, 81, 72), (100, 50, 50), (96, 64, 64), (256, 256, 256), (300, 10, 10)]:
+        b = (ctypes.c_uint32 * 3)(*box)
+        ref, tun = (ctypes.c_uint32 * 3)(), (ctypes.c_uint32 * 3)()
+        assert L.dda_choose_grid(b, 0, ref) == 0 and L.dda_choose_grid(b, 1, tun) == 0
+        assert tuple(ref) == tuple(api.fft_fit(2 * x) for x in box)
+        if tuple(tun) != tuple(ref):
+            assert all(g >= 2 * x and g in TUNED for g, x in zip(tun, box))
+            assert tun[1] == tun[2]
+            assert tun[0] * tun[1] * tun[2] <= 2 * ref[0] * ref[1] * ref[2]

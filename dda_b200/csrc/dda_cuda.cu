@@ -16,6 +16,8 @@
 #include <complex>
 #include <cstdio>
 #include <cstring>
+#include <array>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <numeric>
@@ -202,6 +204,8 @@ template <typename T> struct Engine {
   uint32_t* order = nullptr;  // kx positions, mirrored frequencies adjacent
   SlotGeom sg{};
   int ncl = 0, cl = 0;
+  int ncl_by_cl[17] = {};     // resident clusters per cluster size (0: not schedulable)
+  size_t yz_fixed = 0, yz_row = 0;  // fused kernel shared memory: fixed part, per row
   YzGeom yz{};
   size_t smem_x = 0, smem_yz = 0, smem_rows = 0, smem_cols = 0, smem_slot = 0;
   ColGeom cz_fwd{}, cz_inv{};
@@ -293,23 +297,9 @@ template <typename T> Engine<T>& eng(dda_ctx* c);
 template <> Engine<float>& eng<float>(dda_ctx* c) { return c->e32; }
 template <> Engine<double>& eng<double>(dda_ctx* c) { return c->e64; }
 
-// k_yz_slot set-up: row batch, cluster size, resident clusters, one slot per
-// cluster, and the kx order that puts the planes kx and -kx (one D-hat
-// octant plane) next to each other.  Leaves e.slot_path false when the
-// cluster shape cannot be scheduled (the split path then runs).
-template <typename T> void setup_slot(dda_ctx* c, Engine<T>& e) {
-  typedef typename C2<T>::t T2;
-  const MvGeom& g = c->g;
-  SlotGeom sg;
-  sg.wp = (3 * g.by + 31) / 32 * 32;
-  sg.py = g.Gy + 1;
-  const int cl = 8;
-  int nrw = std::min(16, (g.Gz + cl - 1) / cl);
-  while (nrw > 1 && slot_smem_bytes<T>(g, nrw) > kSmemMax) nrw--;
-  sg.nrw = nrw;
-  const size_t smem = slot_smem_bytes<T>(g, nrw);
-  if (smem > kSmemMax) return;
-  CK(allow_smem((const void*)e.k.slot));
+// Clusters of `cl` CTAs of k_yz_slot with `smem` bytes each that fit the
+// device at once (0 when the shape cannot be scheduled).
+template <typename T> int slot_clusters(Engine<T>& e, int cl, size_t smem) {
   cudaLaunchConfig_t cfg = {};
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeClusterDimension;
@@ -321,12 +311,39 @@ template <typename T> void setup_slot(dda_ctx* c, Engine<T>& e) {
   cfg.dynamicSmemBytes = smem;
   cfg.attrs = at;
   cfg.numAttrs = 1;
-  int ncl = 0;
-  if (cudaOccupancyMaxActiveClusters(&ncl, (const void*)e.k.slot, &cfg) != cudaSuccess || ncl < 1) {
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, (const void*)e.k.slot, &cfg) != cudaSuccess) {
     cudaGetLastError();
-    return;
+    return 0;
   }
-  ncl = std::min(ncl, g.Gx * c->max_rhs);
+  return n;
+}
+
+// k_yz_slot set-up: row batch, cluster size, resident clusters, one slot per
+// cluster, and the kx order that puts the planes kx and -kx (one D-hat
+// octant plane) next to each other.  Leaves e.slot_path false when the
+// cluster shape cannot be scheduled (the split path then runs).
+template <typename T> void setup_slot(dda_ctx* c, Engine<T>& e) {
+  typedef typename C2<T>::t T2;
+  const MvGeom& g = c->g;
+  SlotGeom sg;
+  sg.wp = (3 * g.by + 31) / 32 * 32;
+  sg.py = g.Gy + 1;
+  const int cl = 8;  // default shape; autotune may pick 4 or 16
+  int nrw = std::min(16, (g.Gz + cl - 1) / cl);
+  while (nrw > 1 && slot_smem_bytes<T>(g, nrw) > kSmemMax) nrw--;
+  sg.nrw = nrw;
+  const size_t smem = slot_smem_bytes<T>(g, nrw);
+  if (smem > kSmemMax) return;
+  CK(allow_smem((const void*)e.k.slot));
+  CK(cudaFuncSetAttribute((const void*)e.k.slot, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  int ncl_max = 0;
+  for (int cand : {4, 8, 16}) {
+    e.ncl_by_cl[cand] = std::min(slot_clusters<T>(e, cand, slot_smem_bytes<T>(g, 1)), g.Gx * c->max_rhs);
+    ncl_max = std::max(ncl_max, e.ncl_by_cl[cand]);
+  }
+  int ncl = std::min(slot_clusters<T>(e, cl, smem), g.Gx * c->max_rhs);
+  if (ncl < 1) return;
   std::vector<uint32_t> order;
   for (int f = 0; f <= g.Gx / 2; f++) {
     order.push_back((uint32_t)c->mx.pos_h[f]);
@@ -334,7 +351,7 @@ template <typename T> void setup_slot(dda_ctx* c, Engine<T>& e) {
   }
   e.order = (uint32_t*)dalloc<float>(order.size() * sizeof(uint32_t));
   CK(cudaMemcpyAsync(e.order, order.data(), order.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream));
-  e.slots = (T2*)dalloc<T>((size_t)ncl * g.Gz * sg.wp * sizeof(T2));
+  e.slots = (T2*)dalloc<T>((size_t)ncl_max * g.Gz * sg.wp * sizeof(T2));
   e.sg = sg;
   e.cl = cl;
   e.ncl = ncl;
@@ -367,6 +384,8 @@ template <typename T> void setup_engine(dda_ctx* c) {
   y.nrw = nrw;
   e.yz = y;
   e.smem_yz = fixed + nrw * row;
+  e.yz_fixed = fixed;
+  e.yz_row = row;
   e.fused = e.k.yz && e.smem_yz <= kSmemMax && !(c->flags & (DDA_FLAG_SPLIT_YZ | DDA_FLAG_SLOT_YZ));
   if (!e.fused && e.k.slot && !(c->flags & DDA_FLAG_SPLIT_YZ)) setup_slot<T>(c, e);
   if (!e.fused && !e.slot_path) {
@@ -480,6 +499,96 @@ void launch_yz(dda_ctx* c, int nrhs, cudaStream_t s, KrylovState* st, int skipmv
     e.k.yrows<<<gr, kNtYz, e.smem_rows, s>>>(e.zbuf, e.dc, g, e.yz, py, st, skipmv);
     e.k.cols<<<gc, kNtC, e.smem_cols, s>>>(e.zbuf, e.xhat, e.cz_inv, pz, 1, st, skipmv);
   }
+}
+
+// ------------------------------------------------------------ autotune ----
+// Shape parameters of the y/z passes that do not change the arithmetic (each
+// plane and row is transformed the same way whatever the batching), chosen
+// by timing: the fused kernel's rows per batch, the cluster kernel's cluster
+// size and rows per batch.  Timed on the context's own buffers (x spectrum
+// zeroed, one right-hand side) and kept per shape for the process.
+struct TuneChoice {
+  int nrw = 0, cl = 0;
+};
+std::mutex g_tune_mu;
+std::map<std::array<int, 9>, TuneChoice> g_tune_cache;
+
+template <typename T> float time_yz(dda_ctx* c, int reps) {
+  cudaEvent_t a, b;
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  launch_yz<T>(c, 1, c->stream, nullptr, 0);  // warm-up
+  float best = 1e30f;
+  for (int r = 0; r < reps; r++) {
+    CK(cudaEventRecord(a, c->stream));
+    launch_yz<T>(c, 1, c->stream, nullptr, 0);
+    CK(cudaEventRecord(b, c->stream));
+    CK(cudaEventSynchronize(b));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, a, b));
+    best = std::min(best, ms);
+  }
+  CK(cudaGetLastError());
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return best;
+}
+
+template <typename T> void apply_choice(dda_ctx* c, Engine<T>& e, const TuneChoice& t) {
+  const MvGeom& g = c->g;
+  if (e.fused) {
+    e.yz.nrw = t.nrw;
+    e.smem_yz = e.yz_fixed + (size_t)t.nrw * e.yz_row;
+  } else if (e.slot_path) {
+    e.cl = t.cl;
+    e.ncl = e.ncl_by_cl[t.cl];
+    e.sg.nrw = t.nrw;
+    e.smem_slot = slot_smem_bytes<T>(g, t.nrw);
+  }
+}
+
+template <typename T> void autotune(dda_ctx* c) {
+  Engine<T>& e = eng<T>(c);
+  const MvGeom& g = c->g;
+  if (!e.on || !(e.fused || e.slot_path)) return;
+  if ((long long)g.Gx * g.Gy * g.Gz < (1LL << 20)) return;  // small grids keep the defaults
+  const std::array<int, 9> key = {g.Gx, g.Gy, g.Gz, g.bx, g.by, g.bz, (int)sizeof(T), c->planned ? 1 : 0,
+                                  e.fused ? 0 : 1};
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      apply_choice<T>(c, e, it->second);
+      return;
+    }
+  }
+  std::vector<TuneChoice> cands;
+  if (e.fused) {
+    const int max_rows = e.k.planned ? 32 : kNtYz / 32;
+    for (int n : {4, 6, 8, 10, 12, 14, 16, 20, 24, 25, 28, 32})
+      if (n <= max_rows && e.yz_fixed + (size_t)n * e.yz_row <= kSmemMax) cands.push_back({n, 0});
+  } else {
+    for (int cl : {4, 8, 16})
+      for (int n : {4, 8, 16})
+        if (e.ncl_by_cl[cl] > 0 && n <= (g.Gz + cl - 1) / cl && slot_smem_bytes<T>(g, n) <= kSmemMax &&
+            slot_clusters<T>(e, cl, slot_smem_bytes<T>(g, n)) >= e.ncl_by_cl[cl])
+          cands.push_back({n, cl});
+  }
+  if (cands.size() < 2) return;
+  CK(cudaMemsetAsync(e.xhat, 0, (size_t)g.Gx * 3 * g.nlines * sizeof(typename C2<T>::t), c->stream));
+  TuneChoice best = cands[0];
+  float best_ms = 1e30f;
+  for (const TuneChoice& t : cands) {
+    apply_choice<T>(c, e, t);
+    const float ms = time_yz<T>(c, 2);
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = t;
+    }
+  }
+  apply_choice<T>(c, e, best);
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune_cache[key] = best;
 }
 
 // The matvec: k_xfwd -> (k_yz | k_yz_slot | cols/yrows/cols) -> k_xinv.
@@ -985,6 +1094,10 @@ int dda_create(const dda_problem* p, int precision, dda_ctx** out) {
     c->cc_set.assign(c->max_rhs, 0);
     if (p->dmatrix) upload_dmatrix(c.get(), p->dmatrix);
     else build_dmatrix(c.get());
+    if (!(c->flags & DDA_FLAG_NO_AUTOTUNE)) {
+      if (c->e32.on) autotune<float>(c.get());
+      if (c->e64.on) autotune<double>(c.get());
+    }
     CK(cudaStreamSynchronize(c->stream));
     c->dev_bytes = g_dalloc_bytes;
     return DDA_OK;

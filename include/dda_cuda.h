@@ -83,6 +83,11 @@ typedef struct dda_problem {
  * buffer, the path for planes beyond one CTA's shared memory) even when a
  * plane fits; used by tests and tuning.  DDA_FLAG_SPLIT_YZ takes precedence. */
 #define DDA_FLAG_SLOT_YZ 4u
+/* dda_problem.flags: keep the default y/z batching instead of timing the
+ * candidates at dda_create (the autotuner picks, per grid shape, the rows
+ * per batch of the plane kernels and the cluster size of the cluster
+ * kernel; neither changes the results). */
+#define DDA_FLAG_NO_AUTOTUNE 8u
 
 typedef struct dda_stats {
   int64_t iterations;   /* Krylov iterations (summed over inner solves for MIXED) */

@@ -131,6 +131,28 @@ def test_matvec_tuned_grid_matches_reference_grid(prec, tol):
     assert rel(mv.apply(x), op.matvec(x)) < tol
 
 
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+@pytest.mark.parametrize("shape", ["box", "sphere"])
+def test_autotuned_layout_gives_identical_results(prec, shape):
+    # the autotuner changes only the batching of the y/z passes: the
+    # product is bit-for-bit the same as with the default layout
+    import dda_b200
+    if shape == "box":  # grid 200 x 100 x 100, fused plane kernel
+        g = dda_b200.Geometry.box_shape("5um", "2.5um", "2.5um", "0.05um")
+    else:  # grid 160^3, cluster kernel
+        g = dda_b200.Geometry.sphere("2um", "0.05um")
+    p = dda_b200.DDAParams(g, [1.5 + 0.1j], "1.2um")
+    mvs = [dda_b200.CudaMatVec(p, prec, flags=f) for f in (0, 8)]
+    for mv in mvs:
+        mv.set_couple_constants(dda_b200.CoupleConstants(p, (0, 0, 1), 1, "ldr"))
+    rng = np.random.default_rng(9)
+    x = rng.uniform(-1, 1, p.vec_size) + 1j * rng.uniform(-1, 1, p.vec_size)
+    for c in range(3):
+        x[c * p.nvs + p.nv:(c + 1) * p.nvs] = 0
+    assert np.array_equal(mvs[0].apply(x), mvs[1].apply(x))
+    print(mvs[0].layout, mvs[1].layout)
+
+
 def test_matvec_host_dmatrix():
     kind, args, mats, lam = CASES["aniso"]
     pr = Pair(kind, args, mats, lam, "fp64", host_d=True)

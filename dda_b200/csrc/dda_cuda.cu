@@ -511,7 +511,7 @@ struct TuneChoice {
   int nrw = 0, cl = 0;
 };
 std::mutex g_tune_mu;
-std::map<std::array<int, 9>, TuneChoice> g_tune_cache;
+std::map<std::array<int, 6>, TuneChoice> g_tune_cache;
 
 template <typename T> float time_yz(dda_ctx* c, int reps) {
   cudaEvent_t a, b;
@@ -552,8 +552,9 @@ template <typename T> void autotune(dda_ctx* c) {
   const MvGeom& g = c->g;
   if (!e.on || !(e.fused || e.slot_path)) return;
   if ((long long)g.Gx * g.Gy * g.Gz < (1LL << 20)) return;  // small grids keep the defaults
-  const std::array<int, 9> key = {g.Gx, g.Gy, g.Gz, g.bx, g.by, g.bz, (int)sizeof(T), c->planned ? 1 : 0,
-                                  e.fused ? 0 : 1};
+  // the box changes the best batching little next to the grid, so shapes
+  // share a choice per grid (served targets mostly land on tuned grids)
+  const std::array<int, 6> key = {g.Gx, g.Gy, g.Gz, (int)sizeof(T), c->planned ? 1 : 0, e.fused ? 0 : 1};
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune_cache.find(key);
@@ -827,6 +828,7 @@ struct SolveOpts {
   const char* skip = nullptr;      // rhs left untouched (marked done from the start)
   bool result = true;              // write P = sqrt(cc) x to the engine's io buffer
   long long max_res_increase = 0;  // > 0: stagnation limit instead of the solver's
+  long long rate_window = 0;       // > 0: stop when |r| does not halve in this many iterations
 };
 
 // Runs one solve of `nrhs` right-hand sides already set up in the engine
@@ -845,6 +847,7 @@ void run_solve(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
     memset(&k, 0, sizeof(k));
     k.maxIter = max_iter > 0 ? max_iter : (1LL << 62);
     k.maxResIncrease = o.max_res_increase > 0 ? o.max_res_increase : kMaxResIncrease[solver];
+    k.rateWin = o.rate_window;
     k.histCap = c->hist_cap;
     k.hist = c->hist + (size_t)r * c->hist_cap;
     if (o.skip && o.skip[r]) k.done = 1;
@@ -904,14 +907,16 @@ void run_mixed(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
   else CK(cudaMemsetAsync(X, 0, n * sizeof(double2), c->stream));
   std::vector<char> done(nrhs, 0);
   std::vector<double> eps_in(nrhs, 1e-4);
-  // An inner FP32 solve ends at its target or when its residual has not
-  // reached a new minimum for kInnerStall iterations (FP32 Krylov
-  // recurrences stagnate on hard problems); the outer FP64 residual then
-  // restarts it.  The refinement fails once kOuterStall outer steps in a row
-  // reduce the FP64 residual by less than 2x.
+  // An inner FP32 solve ends at its target, when its residual has not
+  // reached a new minimum for kInnerStall iterations, or when it has not
+  // halved over kInnerWindow iterations (FP32 Krylov recurrences lose
+  // accuracy on some problems); the outer FP64 residual then restarts it.
+  // A right-hand side whose FP64 residual does not halve over kOuterStall
+  // outer steps in a row leaves the refinement with DDA_ERR_NOPROGRESS, and
+  // mixed_fallback finishes it with the FP64 solver.
   const int max_outer = 60;
-  const long long kInnerStall = 200;
-  const int kOuterStall = 3;
+  const long long kInnerStall = 200, kInnerWindow = 100;
+  const int kOuterStall = 2;
   std::vector<double> prev_rel(nrhs, 0.0);
   std::vector<int> stalls(nrhs, 0);
   for (int outer = 0;; outer++) {
@@ -953,6 +958,7 @@ void run_mixed(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
     o.skip = done.data();
     o.result = false;
     o.max_res_increase = kInnerStall;
+    o.rate_window = kInnerWindow;
     run_solve<float>(c, solver, nrhs, 0.0, max_iter > 0 ? max_iter - total_it : 0, o);
     for (int r = 0; r < nrhs; r++) {
       if (done[r]) continue;
@@ -1095,8 +1101,9 @@ int dda_create(const dda_problem* p, int precision, dda_ctx** out) {
     if (p->dmatrix) upload_dmatrix(c.get(), p->dmatrix);
     else build_dmatrix(c.get());
     if (!(c->flags & DDA_FLAG_NO_AUTOTUNE)) {
+      // MIXED runs its FP64 engine only for the few outer residuals
       if (c->e32.on) autotune<float>(c.get());
-      if (c->e64.on) autotune<double>(c.get());
+      if (c->e64.on && precision == DDA_PREC_FP64) autotune<double>(c.get());
     }
     CK(cudaStreamSynchronize(c->stream));
     c->dev_bytes = g_dalloc_bytes;
@@ -1264,6 +1271,41 @@ int solve_device_t(dda_ctx* c, int solver, int nrhs, const void* einc, double ep
   return collect_stats(c, nrhs, nullptr, 0, stats);
 }
 
+// Right-hand sides the mixed refinement could not finish (no progress,
+// breakdown) are solved again with the FP64 solver, starting from the
+// refined polarisations (e64.io); the others keep their result.  E (e64
+// vector 0) still holds the incident fields.
+void mixed_fallback(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter, std::vector<MixedOut>& mo) {
+  std::vector<char> skip(nrhs, 1);
+  bool any = false;
+  for (int r = 0; r < nrhs; r++)
+    if (mo[r].status == DDA_ERR_NOPROGRESS || mo[r].status == DDA_ERR_BREAKDOWN) {
+      skip[r] = 0;
+      any = true;
+    }
+  if (!any) return;
+  Engine<double>& d = c->e64;
+  const size_t len = (size_t)3 * c->g.nvs;
+  double2* S = d.vec[2];
+  CK(cudaMemcpyAsync(S, d.io, nrhs * len * sizeof(double2), cudaMemcpyDeviceToDevice, c->stream));
+  SolveOpts o;
+  o.start = true;
+  o.skip = skip.data();
+  long long used = 0;
+  for (int r = 0; r < nrhs; r++) used = std::max(used, mo[r].iterations);
+  run_solve<double>(c, solver, nrhs, eps, max_iter > 0 ? std::max(1LL, max_iter - used) : 0, o);
+  for (int r = 0; r < nrhs; r++) {
+    if (skip[r]) {  // the FP64 pass wrote io for every rhs: put the refined result back
+      CK(cudaMemcpyAsync(d.io + r * len, S + r * len, len * sizeof(double2), cudaMemcpyDeviceToDevice, c->stream));
+      continue;
+    }
+    const KrylovState& k = c->st_host[r];
+    mo[r].iterations += k.count;
+    mo[r].status = k.status;
+    mo[r].rel = std::sqrt(k.inprodR * k.residScale);
+  }
+}
+
 int collect_mixed(dda_ctx* c, const std::vector<MixedOut>& mo, double* history, long long history_cap,
                   dda_stats* stats) {
   int rc = DDA_OK;
@@ -1298,6 +1340,7 @@ int solve_mixed_host(dda_ctx* c, int solver, int nrhs, const double* einc, doubl
   if (start) CK(cudaMemcpyAsync(c->e64.vec[2], start, n * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
   std::vector<MixedOut> mo;
   run_mixed(c, solver, nrhs, eps, max_iter, start != nullptr, mo);
+  mixed_fallback(c, solver, nrhs, eps, max_iter, mo);
   if (pol_out) CK(cudaMemcpyAsync(pol_out, c->e64.io, n * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return collect_mixed(c, mo, history, history_cap, stats);
@@ -1310,6 +1353,7 @@ int solve_mixed_device(dda_ctx* c, int solver, int nrhs, const void* einc, doubl
   if (start) CK(cudaMemcpyAsync(c->e64.vec[2], start, bytes, cudaMemcpyDeviceToDevice, c->stream));
   std::vector<MixedOut> mo;
   run_mixed(c, solver, nrhs, eps, max_iter, start != nullptr, mo);
+  mixed_fallback(c, solver, nrhs, eps, max_iter, mo);
   CK(cudaMemcpyAsync(pol, c->e64.io, bytes, cudaMemcpyDeviceToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return collect_mixed(c, mo, nullptr, 0, stats);

@@ -70,6 +70,11 @@ struct KrylovState {
   double2 zetaInv, mEtaZeta, mThetaZeta, betaInv, cNOT, mAlpha, bo;
   double omega_old, omega_new, c_old, c_new, normSNew, abs_ro_new, sNorm;
   double* hist;
+  // progress-rate stop (inner solves of the mixed refinement): with
+  // rateWin > 0 the solve ends with KS_NOPROGRESS when the best |r| has not
+  // halved over the last rateWin iterations
+  long long rateWin, chkIt;
+  double chkR;
 };
 
 struct KrylovStep {
@@ -152,12 +157,20 @@ __device__ __forceinline__ void loop_update(KrylovState& s, double next) {
   }
   s.last = next;
   if (s.hist && s.count - 1 < s.histCap) s.hist[s.count - 1] = sqrt(s.residScale * next);
+  if (s.rateWin > 0 && s.chkIt == 0 && s.chkR == 0) s.chkR = s.inprodR;
   if (s.inprodR < s.epsB) {
     s.done = 1;
   } else if (s.count >= s.maxIter) {
     kfail(s, KS_MAXITER);
   } else if (s.counter > s.maxResIncrease) {
     kfail(s, KS_NOPROGRESS);
+  } else if (s.rateWin > 0 && s.count - s.chkIt >= s.rateWin) {
+    if (s.inprodR > 0.25 * s.chkR) {
+      kfail(s, KS_NOPROGRESS);
+    } else {
+      s.chkR = s.inprodR;
+      s.chkIt = s.count;
+    }
   }
 }
 

@@ -60,6 +60,22 @@ def dist_env():
         int(os.environ.get("WORLD_SIZE", 1))
 
 
+def max_over_ranks(dist, value, device):
+    """The slowest rank's time (every rank calls it, in the same order)."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(units_per_rank, world, t_max_ms):
+    """Whole-job units per second: every rank does the same work; the job ends
+    with the slowest rank."""
+    return units_per_rank * world / (t_max_ms / 1000.0)
+
+
 # ------------------------------------------------------------ clocks ----
 class ClockSampler:
     """nvidia-smi clock / throttle samples during the timed region."""
@@ -219,12 +235,8 @@ def run_ours(args):
     launches = mv.launches - l0
     torch.cuda.synchronize()
     clocks = sampler.stop()
-    t_max = total_ms
-    if pg:
-        t = torch.tensor([total_ms], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        t_max = float(t.item())
-    value = nrhs * args.steps * world / (t_max / 1000.0)
+    t_max = max_over_ranks(pg, total_ms, "cuda")
+    value = replica_throughput(nrhs * args.steps, world, t_max)
     ms_per_step = t_max / args.steps
 
     # e2e: host FP64 einc in, host FP64 polarisations out, through dda_solve
@@ -240,11 +252,8 @@ def run_ours(args):
         e1.record(stream)
         e1.synchronize()
         e2e_ms += e0.elapsed_time(e1)
-    if pg:
-        t = torch.tensor([e2e_ms], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e = {"value": nrhs * args.steps * world / (e2e_ms / 1000.0), "unit": "solves/s",
+    e2e_ms = max_over_ranks(pg, e2e_ms, "cuda")
+    e2e = {"value": replica_throughput(nrhs * args.steps, world, e2e_ms), "unit": "solves/s",
            "h2d_bytes_per_step": int(einc_host.nbytes), "d2h_bytes_per_step": int(einc_host.nbytes)}
 
     # matvec stage profile and roofline of the dominant pass

@@ -251,12 +251,22 @@ struct dda_ctx {
   double* hist = nullptr;
   long long hist_cap = 0;
   long long launches = 0;  // kernels this context has launched
+  // instantiated graphs of one solver round, per (solver, nrhs, precision):
+  // the round's kernel arguments are the context's fixed buffers
+  struct RoundGraph {
+    int solver, nrhs, tsize;
+    cudaGraphExec_t g;
+    long long launches;
+  };
+  std::vector<RoundGraph> round_graphs;
   size_t dev_bytes = 0;    // device memory held after dda_create
 
   // Frees on the context stream once its work is done; other contexts'
   // work on the device is not waited for.
   void release() {
     if (device >= 0) cudaSetDevice(device);
+    for (auto& rg : round_graphs) cudaGraphExecDestroy(rg.g);
+    round_graphs.clear();
     cudaStream_t s = stream;
     if (s) cudaStreamSynchronize(s);
     e32.release(s);
@@ -866,9 +876,46 @@ void run_solve(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
   CK(cudaMemcpyAsync(c->st, c->st_host, nrhs * sizeof(KrylovState), cudaMemcpyHostToDevice, c->stream));
   sv.solver_init(solver, b);
   long long nr = 0;
+  // The host looks at the convergence flags every `poll` iterations.  The
+  // first round (iterations 0..7 hold the solvers' first-iteration variants)
+  // is launched kernel by kernel; the second round is captured into a CUDA
+  // graph once and every later round replays it.  poll is even, so the
+  // buffers the solvers rotate on the host are back in the captured order
+  // after each round; all other kernel arguments are fixed pointers, and
+  // the kernels read their scalars and done flags from the device state.
   const int poll = 8;
-  for (;;) {
-    for (int k = 0; k < poll; k++) sv.iteration(solver, nr++, b);
+  const bool graphs = !(c->flags & DDA_FLAG_NO_GRAPHS);
+  dda_ctx::RoundGraph* rg = nullptr;
+  for (auto& x : c->round_graphs)
+    if (x.solver == solver && x.nrhs == nrhs && x.tsize == (int)sizeof(T)) rg = &x;
+  for (int round = 0;; round++) {
+    if (!graphs || round == 0) {
+      for (int k = 0; k < poll; k++) sv.iteration(solver, nr++, b);
+    } else {
+      if (!rg) {  // capture once per context, solver, batch and precision
+        const long long l0 = c->launches;
+        cudaGraph_t graph = nullptr;
+        CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        try {
+          for (int k = 0; k < poll; k++) sv.iteration(solver, nr + k, b);
+        } catch (...) {
+          cudaStreamEndCapture(c->stream, &graph);
+          if (graph) cudaGraphDestroy(graph);
+          throw;
+        }
+        CK(cudaStreamEndCapture(c->stream, &graph));
+        cudaGraphExec_t g = nullptr;
+        const cudaError_t rc = cudaGraphInstantiate(&g, graph, 0);
+        cudaGraphDestroy(graph);
+        CK(rc);
+        c->round_graphs.push_back({solver, nrhs, (int)sizeof(T), g, c->launches - l0});
+        rg = &c->round_graphs.back();
+        c->launches = l0;
+      }
+      CK(cudaGraphLaunch(rg->g, c->stream));
+      c->launches += rg->launches;
+      nr += poll;
+    }
     CK(cudaMemcpyAsync(c->st_host, c->st, nrhs * sizeof(KrylovState), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     bool all = true;

@@ -88,6 +88,10 @@ typedef struct dda_problem {
  * per batch of the plane kernels and the cluster size of the cluster
  * kernel; neither changes the results). */
 #define DDA_FLAG_NO_AUTOTUNE 8u
+/* dda_problem.flags: launch every solver iteration kernel by kernel instead of
+ * replaying captured CUDA graphs of eight iterations (the results are the
+ * same; used by tests). */
+#define DDA_FLAG_NO_GRAPHS 16u
 
 typedef struct dda_stats {
   int64_t iterations;   /* Krylov iterations (summed over inner solves for MIXED) */

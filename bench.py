@@ -78,18 +78,31 @@ def replica_throughput(units_per_rank, world, t_max_ms):
 
 # ------------------------------------------------------------ clocks ----
 class ClockSampler:
-    """nvidia-smi clock / throttle samples during the timed region."""
+    """SM clocks and throttle reasons during the timed region: NVML queries
+    taken between timed steps (sample()), plus nvidia-smi polling every
+    200 ms as a second source when the region is long enough."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clocks-event reason bits (nvml.h): sw power cap 0x4, hw slowdown
+    # 0x8, sw thermal 0x20, hw thermal 0x40
+    BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40}
 
     def __init__(self, gpu_index):
         self.idx = gpu_index
         self.proc = None
         self.f = None
+        self.nv = None
+        self.sm, self.mx, self.reasons = [], [], set()
 
     def start(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = (pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.idx))
+        except Exception:
+            self.nv = None
         try:
             self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.proc = subprocess.Popen(
@@ -99,33 +112,50 @@ class ClockSampler:
         except Exception:
             self.proc = None
 
-    def stop(self):
-        if self.proc is None:
-            return None
-        self.proc.terminate()
+    def sample(self):
+        if self.nv is None:
+            return
+        nv, h = self.nv
         try:
-            self.proc.wait(5)
+            self.sm.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+            self.mx.append(float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)))
+            bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+            for name, b in self.BITS.items():
+                if bits & b:
+                    self.reasons.add(name)
         except Exception:
-            self.proc.kill()
-        self.f.flush()
-        self.f.seek(0)
-        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
-        os.unlink(self.f.name)
-        sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in rows:
+            pass
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
             try:
-                sm.append(float(r[1]))
-                mx.append(float(r[2]))
-                for n, v in zip(names, r[5:9]):
-                    if v.strip().lower() == "active":
-                        reasons.add(n)
-            except (ValueError, IndexError):
+                self.proc.wait(5)
+            except Exception:
+                self.proc.kill()
+            self.f.flush()
+            self.f.seek(0)
+            rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+            os.unlink(self.f.name)
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for r in rows:
+                try:
+                    self.sm.append(float(r[1]))
+                    self.mx.append(float(r[2]))
+                    for n, v in zip(names, r[5:9]):
+                        if v.strip().lower() == "active":
+                            self.reasons.add(n)
+                except (ValueError, IndexError):
+                    pass
+        if self.nv is not None:
+            try:
+                self.nv[0].nvmlShutdown()
+            except Exception:
                 pass
-        if not sm:
+        if not self.sm:
             return None
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)),
-                "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": float(np.median(self.sm)), "sm_max_mhz": float(max(self.mx)),
+                "reasons": sorted(self.reasons), "samples": len(self.sm)}
 
 
 # --------------------------------------------------------- CPU sample ----
@@ -232,6 +262,7 @@ def run_ours(args):
         e1.record(stream)
         e1.synchronize()
         total_ms += e0.elapsed_time(e1)
+        sampler.sample()
     launches = mv.launches - l0
     torch.cuda.synchronize()
     clocks = sampler.stop()

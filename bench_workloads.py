@@ -123,6 +123,7 @@ def run_batched(args):
         b.record(stream)
         b.synchronize()
         lat.append(a.elapsed_time(b))
+        sampler.sample()
     total = sum(lat)
     launches = mv.launches - l0
     clocks = sampler.stop()

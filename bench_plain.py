@@ -92,3 +92,66 @@ class PlainSolver:
         P = torch.zeros_like(x).view(3, nvs)
         P[:, :nv] = self.ccs * x.view(3, nvs)[:, :nv]
         return P.view(-1), it
+
+    def solve_qmr(self, einc, eps, max_iter=10000):
+        """QMR-CS as in DDA/QmrCs.cpp:58-168 (bilinear form sum a_i b_i,
+        x0 = 0), host-side scalars; returns (P = sqrt(cc) x, iterations)."""
+        torch = self.torch
+        nv, nvs = self.nv, self.nvs
+        e = torch.from_numpy(np.ascontiguousarray(einc)).to(self.device)
+        b = torch.zeros_like(e).view(3, nvs)
+        b[:, :nv] = self.ccs * e.view(3, nvs)[:, :nv]
+        b = b.view(-1)
+        bil = lambda a, c: torch.sum(a * c).item()  # noqa: E731
+        nrm = lambda a: torch.vdot(a, a).real.item()  # noqa: E731
+        bb = nrm(b)
+        eps2 = eps * eps * bb
+        x = torch.zeros_like(b)
+        r = b.clone()
+        inprod = bb
+        beta = complex(np.sqrt(complex(bil(r, r))))
+        omega_old, omega_new = 0.0, np.sqrt(inprod) / abs(beta)
+        tautilda = omega_new * beta
+        c_old = c_new = 1.0
+        s_old = s_new = 0j
+        v = r / beta
+        vt = torch.zeros_like(b)
+        p_old = torch.zeros_like(b)
+        p_new = torch.zeros_like(b)
+        it = 0
+        while it < max_iter:
+            A = self.matvec(v)
+            alpha = bil(v, A)
+            vt = A - alpha * v if it == 0 else vt * (-beta) - alpha * v + A
+            ctmp3 = bil(vt, vt)
+            rtmp2 = nrm(vt)
+            ctmp1 = omega_old * beta
+            ctmp2 = omega_new * alpha
+            theta = np.conj(s_old) * ctmp1
+            eta = c_old * c_new * ctmp1 + np.conj(s_new) * ctmp2
+            zetatilda = c_new * ctmp2 - c_old * s_new * ctmp1
+            beta = complex(np.sqrt(complex(ctmp3)))
+            omega_old, omega_new = omega_new, np.sqrt(rtmp2) / abs(beta)
+            zetaabs = np.sqrt(abs(zetatilda) ** 2 + rtmp2)
+            rtmp3 = abs(zetatilda)
+            zeta = zetaabs if rtmp3 < 1e-40 else zetaabs / rtmp3 * zetatilda
+            c_old, c_new = c_new, rtmp3 / zetaabs
+            s_old, s_new = s_new, omega_new * (beta / zeta)
+            tau = c_new * tautilda
+            tautilda = -s_new * tautilda
+            if it == 0:
+                p_new = v / zeta
+            else:
+                pn = v / zeta - (eta / zeta) * p_new
+                if it > 1:
+                    pn = pn - (theta / zeta) * p_old
+                p_old, p_new = p_new, pn
+            x = x + tau * p_new
+            v, vt = vt / beta, v  # the new Lanczos vector; vt keeps the previous one
+            r = r * abs(s_new) ** 2 + v * ((c_new / omega_new) * tautilda)
+            it += 1
+            if nrm(r) < eps2:
+                break
+        P = torch.zeros_like(x).view(3, nvs)
+        P[:, :nv] = self.ccs * x.view(3, nvs)[:, :nv]
+        return P.view(-1), it

@@ -30,3 +30,19 @@ def test_plain_baseline_matches_library_solution():
     got = got.cpu().numpy()
     assert its > 5
     assert np.linalg.norm(got - want) / np.linalg.norm(want) < 1e-7
+
+
+def test_plain_qmr_matches_library_solution():
+    import bench_plain
+    g = dda_b200.Geometry.sphere("10um", "0.5um")
+    p = dda_b200.DDAParams(g, [1.5 + 0.1j], "6um")
+    mv = dda_b200.CudaMatVec(p, "fp64")
+    cc = dda_b200.CoupleConstants(p, (0, 0, 1), 2, "ldr")
+    mv.set_couple_constants(cc)
+    e = p.einc((0, 0, 1), 2)
+    s = dda_b200.CudaSolver(mv, "qmr")
+    want = s.get_pol_vec(e, 1e-9)
+    got, its = bench_plain.PlainSolver(mv, p, cc.cc_sqrt).solve_qmr(e, 1e-9)
+    got = got.cpu().numpy()
+    assert abs(its - s.last_stats[0].iterations) <= 2
+    assert np.linalg.norm(got - want) / np.linalg.norm(want) < 1e-7

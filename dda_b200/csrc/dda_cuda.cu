@@ -198,6 +198,8 @@ template <typename T> struct Engine {
   T2* zbuf = nullptr;  // split path [max_rhs][Gx][3][Gz][by]
   T2* vec[10] = {};    // Krylov vectors [max_rhs][3 nvs]
   T2* io = nullptr;    // host-API staging [max_rhs][3 nvs]
+  T2* xo = nullptr;    // MIXED, FP64 engine: refined solution x and b = sqrt(cc) Einc
+  T2* bo = nullptr;
   bool fused = false;
   bool slot_path = false;     // k_yz_slot: cluster per plane through L2 slots
   T2* slots = nullptr;        // [ncl][Gz][wp]
@@ -211,11 +213,12 @@ template <typename T> struct Engine {
   ColGeom cz_fwd{}, cz_inv{};
   MvKernels<T> k;
   void release(cudaStream_t s) {
-    for (void* p : {(void*)dc, (void*)ccs, (void*)xhat, (void*)zbuf, (void*)io, (void*)slots, (void*)order})
+    for (void* p : {(void*)dc, (void*)ccs, (void*)xhat, (void*)zbuf, (void*)io, (void*)slots, (void*)order,
+                    (void*)xo, (void*)bo})
       if (p) cudaFreeAsync(p, s);
     for (auto& v : vec)
       if (v) cudaFreeAsync(v, s);
-    dc = ccs = xhat = zbuf = io = slots = nullptr;
+    dc = ccs = xhat = zbuf = io = slots = xo = bo = nullptr;
     order = nullptr;
     for (auto& v : vec) v = nullptr;
   }
@@ -447,11 +450,19 @@ template <typename T> void setup_engine(dda_ctx* c) {
   CK(cudaMemsetAsync(e.ccs, 0, (size_t)c->max_rhs * g.nmat * 3 * s, c->stream));
   e.xhat = (T2*)dalloc<T>((size_t)c->max_rhs * g.Gx * 3 * g.nlines * s);
   const size_t vbytes = (size_t)c->max_rhs * 3 * g.nvs * s;
-  for (auto& v : e.vec) {
-    v = (T2*)dalloc<T>(vbytes);
-    CK(cudaMemsetAsync(v, 0, vbytes, c->stream));
+  // a MIXED context runs its Krylov vectors in FP64 and only the matvec's
+  // convolution in FP32: the FP32 engine needs one input buffer and io
+  const bool conv_engine = c->precision == DDA_PREC_MIXED && sizeof(T) == 4;
+  for (int i = 0; i < 10; i++) {
+    if (conv_engine && i > 0) break;
+    e.vec[i] = (T2*)dalloc<T>(vbytes);
+    CK(cudaMemsetAsync(e.vec[i], 0, vbytes, c->stream));
   }
   e.io = (T2*)dalloc<T>(vbytes);
+  if (c->precision == DDA_PREC_MIXED && sizeof(T) == 8) {
+    e.xo = (T2*)dalloc<T>(vbytes);
+    e.bo = (T2*)dalloc<T>(vbytes);
+  }
 }
 
 // Uploads the scaled couple constants of every rhs to the engine.
@@ -749,9 +760,44 @@ template <typename T> struct Solve {
     c->launches++;
   }
 
-  void mv(const T2* arg, T2* res, int conj, KrylovStep k) {
-    matvec<T>(c, arg, res, conj, nrhs, s, st, k);
+  // FP64 Krylov vectors with the convolution of the matvec in FP32 (MIXED
+  // inner solves): arg -> FP32, convolution sqrt(cc) IFFT(D FFT(sqrt(cc) .)),
+  // then y = arg + conv and the step's sums in FP64.
+  bool mv32 = false;
+
+  void matvec_any(const T2* arg, T2* res, int conj, KrylovStep k, int skipmv = 0) {
+    if constexpr (std::is_same<T, double>::value) {
+      if (mv32) {
+        Engine<float>& f = c->e32;
+        const long long n = (long long)nrhs * 3 * c->g.nvs;
+        k_convert<double2, float2><<<592, 256, 0, s>>>(arg, f.vec[0], n);
+        CK(cudaGetLastError());
+        c->launches++;
+        KrylovStep conv{KOP_NONE, 0, nullptr, {}};
+        conv.conv_only = 1;
+        matvec<float>(c, f.vec[0], f.io, conj, nrhs, s, st, conv, skipmv);
+        VecArgs a;
+        memset(&a, 0, sizeof(a));
+        a.v[0] = res;
+        a.v[1] = const_cast<T2*>(arg);
+        a.v[2] = f.io;
+        a.op = V_ADD_CONV;
+        a.first = skipmv;
+        a.nv = c->g.nv;
+        a.nvs = c->g.nvs;
+        a.nmat = c->g.nmat;
+        a.nparts = c->nparts_vec;
+        a.step = k;
+        k_vec<T, kNtV><<<dim3(c->nparts_vec, nrhs), kNtV, 0, s>>>(a, st);
+        CK(cudaGetLastError());
+        c->launches++;
+        return;
+      }
+    }
+    matvec<T>(c, arg, res, conj, nrhs, s, st, k, skipmv);
   }
+
+  void mv(const T2* arg, T2* res, int conj, KrylovStep k) { matvec_any(arg, res, conj, k); }
 
   // CpuIterativeSolver::initGeneral (DDA/CpuIterativeSolver.cpp:45-91) with
   // the GPU setup kernels of DDA/GpuIterativeSolver.cpp:78-134.
@@ -787,7 +833,7 @@ template <typename T> struct Solve {
         vec(V_BIS_P, nr == 0, {b.t1, b.t2, b.R}, step(KOP_NONE));
         mv(b.t1, b.t2, 0, step(KOP_BIS_ALPHA, EP_YW_HERM, b.t4));
         vec(V_BIS_S, 0, {b.t3, b.t2, b.R}, step(KOP_BIS_S));
-        matvec<T>(c, b.t3, b.A, 0, nrhs, s, st, step(KOP_BIS_OMEGA, EP_AY_HERM_NORM), 1);
+        matvec_any(b.t3, b.A, 0, step(KOP_BIS_OMEGA, EP_AY_HERM_NORM), 1);
         vec(V_BIS_XR, 0, {b.X, b.t1, b.t3, b.A, b.R, b.t4}, step(KOP_BIS_END));
         break;
       }
@@ -839,6 +885,7 @@ struct SolveOpts {
   bool result = true;              // write P = sqrt(cc) x to the engine's io buffer
   long long max_res_increase = 0;  // > 0: stagnation limit instead of the solver's
   long long rate_window = 0;       // > 0: stop when |r| does not halve in this many iterations
+  bool mv32 = false;               // FP64 solve with the matvec convolution in FP32
 };
 
 // Runs one solve of `nrhs` right-hand sides already set up in the engine
@@ -849,6 +896,7 @@ void run_solve(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
   typedef typename C2<T>::t T2;
   Engine<T>& e = eng<T>(c);
   Solve<T> sv(c, nrhs);
+  sv.mv32 = o.mv32;
   T2 *E = e.vec[0], *B = e.vec[1], *S = e.vec[2];
   typename Solve<T>::Bufs b{e.vec[3], e.vec[4], e.vec[5], e.vec[6], e.vec[7], e.vec[8], e.vec[9]};
   // initial state
@@ -886,8 +934,9 @@ void run_solve(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
   const int poll = 8;
   const bool graphs = !(c->flags & DDA_FLAG_NO_GRAPHS);
   dda_ctx::RoundGraph* rg = nullptr;
+  const int gkey = (int)sizeof(T) + (o.mv32 ? 100 : 0);  // kernel sequences differ per variant
   for (auto& x : c->round_graphs)
-    if (x.solver == solver && x.nrhs == nrhs && x.tsize == (int)sizeof(T)) rg = &x;
+    if (x.solver == solver && x.nrhs == nrhs && x.tsize == gkey) rg = &x;
   for (int round = 0;; round++) {
     if (!graphs || round == 0) {
       for (int k = 0; k < poll; k++) sv.iteration(solver, nr++, b);
@@ -908,7 +957,7 @@ void run_solve(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
         const cudaError_t rc = cudaGraphInstantiate(&g, graph, 0);
         cudaGraphDestroy(graph);
         CK(rc);
-        c->round_graphs.push_back({solver, nrhs, (int)sizeof(T), g, c->launches - l0});
+        c->round_graphs.push_back({solver, nrhs, gkey, g, c->launches - l0});
         rg = &c->round_graphs.back();
         c->launches = l0;
       }
@@ -942,10 +991,12 @@ struct MixedOut {
 void run_mixed(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter, bool start,
                std::vector<MixedOut>& out) {
   Engine<double>& d = c->e64;
-  Engine<float>& f = c->e32;
   Solve<double> sd(c, nrhs, c->st_outer);
   const size_t n = (size_t)nrhs * 3 * c->g.nvs;
-  double2 *E = d.vec[0], *B = d.vec[1], *S = d.vec[2], *X = d.vec[3], *R = d.vec[5], *A = d.vec[6];
+  // E (incident field) and S (start) as for run_solve; the refined solution
+  // and b live in xo, bo; the inner solves take their right-hand side r in
+  // vector 1 and leave their solution in vector 4 (vectors 3..9 are theirs)
+  double2 *E = d.vec[0], *R = d.vec[1], *S = d.vec[2], *A = d.vec[6], *X = d.xo, *B = d.bo;
   out.assign(nrhs, MixedOut());
   for (int r = 0; r < nrhs; r++) memset(&c->sto_host[r], 0, sizeof(KrylovState));
   CK(cudaMemcpyAsync(c->st_outer, c->sto_host, nrhs * sizeof(KrylovState), cudaMemcpyHostToDevice, c->stream));
@@ -954,23 +1005,25 @@ void run_mixed(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
   else CK(cudaMemsetAsync(X, 0, n * sizeof(double2), c->stream));
   std::vector<char> done(nrhs, 0);
   std::vector<double> eps_in(nrhs, 1e-4);
-  // An inner FP32 solve ends at its target, when its residual has not
-  // reached a new minimum for kInnerStall iterations, or when it has not
-  // halved over kInnerWindow iterations (FP32 Krylov recurrences lose
-  // accuracy on some problems); the outer FP64 residual then restarts it.
-  // A right-hand side whose FP64 residual does not halve over kOuterStall
-  // outer steps in a row leaves the refinement with DDA_ERR_NOPROGRESS, and
-  // mixed_fallback finishes it with the FP64 solver.
+  // Each inner solve is an FP64 Krylov solve of A e = r whose matvec runs
+  // the convolution in FP32 (Solve::matvec_any); it aims at half the
+  // remaining reduction and ends early when its residual has not reached a
+  // new minimum for kInnerStall iterations: the FP32 convolution breaks the
+  // complex symmetry of A at the 1e-7 level, which stalls QMR-CS on
+  // ill-conditioned targets, and the restart from the FP64 residual recovers
+  // it.  A right-hand side whose FP64 residual does not
+  // halve over kOuterStall outer steps in a row leaves the refinement with
+  // DDA_ERR_NOPROGRESS, and mixed_fallback finishes it with the FP64 solver.
   const int max_outer = 60;
-  const long long kInnerStall = 200, kInnerWindow = 100;
+  const long long kInnerStall = 200;
   const int kOuterStall = 2;
   std::vector<double> prev_rel(nrhs, 0.0);
   std::vector<int> stalls(nrhs, 0);
   for (int outer = 0;; outer++) {
-    // r = b - A x (FP64); reduction n = |r|^2 -> last
-    if (outer == 0 && !start) CK(cudaMemcpyAsync(R, B, n * sizeof(double2), cudaMemcpyDeviceToDevice, c->stream));
-    else sd.mv(X, A, 0, sd.step(KOP_NONE));
-    sd.vec(V_R_INIT, 0, {R, (outer == 0 && !start) ? X : A, B}, sd.step(KOP_NORM));
+    // r = b - A x (full FP64 matvec); reduction n = |r|^2 -> last
+    if (outer > 0 || start) sd.mv(X, A, 0, sd.step(KOP_NONE));
+    else CK(cudaMemsetAsync(A, 0, n * sizeof(double2), c->stream));
+    sd.vec(V_R_INIT, 0, {R, A, B}, sd.step(KOP_NORM));
     CK(cudaMemcpyAsync(c->sto_host, c->st_outer, nrhs * sizeof(KrylovState), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     bool all = true;
@@ -991,22 +1044,23 @@ void run_mixed(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
       if (!done[r] && outer >= max_outer) { done[r] = 1; out[r].status = DDA_ERR_NOPROGRESS; }
       if (!done[r] && max_iter > 0 && out[r].iterations >= max_iter) { done[r] = 1; out[r].status = DDA_ERR_MAXITER; }
       k.done = done[r];
-      eps_in[r] = std::min(0.1, std::max(1e-4, 0.5 * eps / rel));
+      // the FP64 recurrences can follow the inner system to the final target
+      // in one go; the FP32 convolution then leaves a residual of about its
+      // own rounding times the condition number, which the next outer step
+      // removes
+      eps_in[r] = std::min(0.1, std::max(1e-7, 0.5 * eps / rel));
       all = all && done[r];
     }
     if (all) break;
     CK(cudaMemcpyAsync(c->st_outer, c->sto_host, nrhs * sizeof(KrylovState), cudaMemcpyHostToDevice, c->stream));
-    // inner FP32 solve of A e = r
-    k_convert<double2, float2><<<592, 256, 0, c->stream>>>(R, f.vec[1], (long long)n);
-    CK(cudaGetLastError());
     SolveOpts o;
     o.b_given = true;
     o.eps_rhs = eps_in.data();
     o.skip = done.data();
     o.result = false;
     o.max_res_increase = kInnerStall;
-    o.rate_window = kInnerWindow;
-    run_solve<float>(c, solver, nrhs, 0.0, max_iter > 0 ? max_iter - total_it : 0, o);
+    o.mv32 = true;
+    run_solve<double>(c, solver, nrhs, 0.0, max_iter > 0 ? max_iter - total_it : 0, o);
     for (int r = 0; r < nrhs; r++) {
       if (done[r]) continue;
       out[r].iterations += c->st_host[r].count;
@@ -1014,12 +1068,11 @@ void run_mixed(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
       // an inner solve that stopped early (stagnation, breakdown, its share
       // of max_iter) still contributes its correction; the outer FP64
       // residual decides
-      (void)c->st_host[r].status;
     }
     // x += e for the rhs still running
-    k_accum<<<dim3(c->nparts_vec, nrhs), 256, 0, c->stream>>>(X, f.vec[4], c->st_outer, 3LL * c->g.nvs);
+    k_accum<double2><<<dim3(c->nparts_vec, nrhs), 256, 0, c->stream>>>(X, d.vec[4], c->st_outer, 3LL * c->g.nvs);
     CK(cudaGetLastError());
-    c->launches += 2;
+    c->launches++;
   }
   sd.vec(V_RESULT, 0, {d.io, X}, KrylovStep{KOP_NONE, 0, nullptr, {}});
 }
@@ -1527,7 +1580,10 @@ int dda_footprint(const dda_problem* p, int precision, int64_t* resident, int64_
   bytes += 6 * (Gx + Gy + Gz) * (8 + 16 + 4 + 4);              // plans
   auto engine = [&](long long s) {
     long long e = (Gx / 2 + 1) * (Gy / 2 + 1) * (Gz / 2 + 1) * 6 * s;  // D-hat octant
-    e += R * nmat * 3 * s + R * Gx * 3 * nl * s + 11 * R * 3 * nvs * s;
+    // vectors: 10 Krylov + io; MIXED keeps two more in FP64 (x, b) and only
+    // the matvec input and io in FP32
+    const long long nvec = precision != DDA_PREC_MIXED ? 11 : s == 16 ? 13 : 2;
+    e += R * nmat * 3 * s + R * Gx * 3 * nl * s + nvec * R * 3 * nvs * s;
     const long long q = 3 * by + ((3 * by) % 2 == 0 ? 1 : 0);
     const long long smem_yz = (Gz + Gy + Gz * q + 3 * (Gy + 1)) * s;
     bool fused_len = false;

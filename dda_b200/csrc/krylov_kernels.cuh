@@ -35,6 +35,7 @@ enum VecOp {
   V_CGNR_XR,         // x += p alpha; r += A mAlpha; n = |r|^2
   V_RESULT,          // v0 = sqrt(cc).v1  (P = sqrt(cc) x)
   V_NORM,            // n = |v0|^2
+  V_ADD_CONV,        // v0 = v1 + (FP32) v2; step sums as the matvec epilogue (first: skip on half-step exit)
 };
 
 struct VecArgs {
@@ -60,6 +61,7 @@ __global__ void __launch_bounds__(NT) k_vec(VecArgs va, KrylovState* st) {
   const int b = blockIdx.y;
   KrylovState& s = st[b];
   if (s.done && va.op != V_RESULT) return;  // the result copy runs after convergence
+  if (va.op == V_ADD_CONV && va.first && s.skipmv) return;  // its matvec was skipped too
   const long long len = 3LL * va.nvs;
   const long long chunk = ((len + va.nparts - 1) / va.nparts + 31) / 32 * 32;
   const long long i0 = chunk * blockIdx.x;
@@ -213,6 +215,19 @@ __global__ void __launch_bounds__(NT) k_vec(VecArgs va, KrylovState* st) {
         acc.n += (double)r.x * r.x + (double)r.y * r.y;
         break;
       }
+      case V_ADD_CONV: {
+        // result of a matvec whose convolution ran in FP32: y = x + conv
+        const float2 cv = reinterpret_cast<const float2*>(va.v[2])[off + i];
+        const T2 a = v1[i];
+        T2 y = a;
+        y.x += cv.x;
+        y.y += cv.y;
+        v0[i] = y;
+        if (va.step.op != KOP_NONE)
+          acc = epilogue_terms<T2>(acc, y, a, va.step.w ? reinterpret_cast<const T2*>(va.step.w)[off + i] : a,
+                                   va.step.mode);
+        break;
+      }
       default:
         break;
     }
@@ -224,15 +239,16 @@ __global__ void __launch_bounds__(NT) k_vec(VecArgs va, KrylovState* st) {
   }
 }
 
-// x64 += e32 for every right-hand side the refinement loop still runs
+// x64 += e for every right-hand side the refinement loop still runs
 // (grid (parts, nrhs)); the FP64 update of mixed-precision refinement.
-__global__ void __launch_bounds__(256) k_accum(double2* __restrict__ x, const float2* __restrict__ e,
+template <typename E2>
+__global__ void __launch_bounds__(256) k_accum(double2* __restrict__ x, const E2* __restrict__ e,
                                              const KrylovState* __restrict__ st, long long len) {
   const int b = blockIdx.y;
   if (st[b].done) return;
   const size_t off = (size_t)b * len;
   for (long long i = blockIdx.x * 256LL + threadIdx.x; i < len; i += (long long)gridDim.x * 256) {
-    const float2 d = e[off + i];
+    const E2 d = e[off + i];
     double2 v = x[off + i];
     v.x += d.x;
     v.y += d.y;

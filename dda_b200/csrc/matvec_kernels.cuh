@@ -182,7 +182,7 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 1 : 2) k_xinv(const typen
       const T2 a0 = a[jj];
       T2 av = a0;
       if (conj) av.y = -av.y;
-      T2 y = cadd(cmul(x, scc[d >> 16]), av);
+      T2 y = step.conv_only ? cmul(x, scc[d >> 16]) : cadd(cmul(x, scc[d >> 16]), av);
       if (conj) y.y = -y.y;
       r[jj] = y;
       if (step.op != KOP_NONE) acc = epilogue_terms<T2>(acc, y, a0, w ? w[jj] : a0, step.mode);

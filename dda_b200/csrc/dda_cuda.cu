@@ -1128,7 +1128,7 @@ int dda_create(const dda_problem* p, int precision, dda_ctx** out) {
     g.pitchx = g.Gx + 1;
     {
       const int s = precision == DDA_PREC_FP32 ? 8 : 16;
-      g.tl = std::max(1, std::min(32, (int)(98304 / ((size_t)s * g.pitchx))));
+      g.tl = std::max(1, std::min(32, (int)(73728 / ((size_t)s * g.pitchx))));  // <= 72 KB: three CTAs per SM
     }
     // geometry tables: dipoles sorted by grid line (y + by z), stable
     const uint32_t nv = p->nv;
@@ -1598,7 +1598,7 @@ int dda_footprint(const dda_problem* p, int precision, int64_t* resident, int64_
   if (precision != DDA_PREC_FP32) bytes += engine(16);
   if (precision != DDA_PREC_FP64) bytes += engine(8);
   const long long sx = precision == DDA_PREC_FP32 ? 8 : 16;
-  const long long tl = std::max(1LL, std::min(32LL, 98304 / (sx * (Gx + 1))));
+  const long long tl = std::max(1LL, std::min(32LL, 73728 / (sx * (Gx + 1))));
   const long long tiles = (nl + tl - 1) / tl;
   bytes += R * std::max(3 * tiles, 296LL) * (long long)sizeof(RedSums) + R * 4;
   bytes += 2 * R * (long long)sizeof(KrylovState) + R * 100000LL * 8;

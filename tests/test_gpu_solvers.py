@@ -151,3 +151,33 @@ def test_graph_replay_gives_identical_solutions(solver, prec):
     assert out[0][1] == out[1][1]
     assert max(it for it, _ in out[0][1]) > 16  # replayed rounds were used
     assert np.array_equal(out[0][0], out[1][0])
+
+
+def test_fp32_bench_solution_meets_tolerance_in_fp64():
+    # the default benchmark solves in FP32 (complex64 vectors, FP64 scalars)
+    # and stops on the recurrence residual; the FP64 residual of its answer
+    # must meet the same 1e-5
+    import dda_b200
+    g = dda_b200.Geometry.box_shape("10um", "5um", "5um", "0.1um")
+    p = dda_b200.DDAParams(g, [1.5 + 0.1j], "6um")
+    prop = (0.0, 1.0, 0.0)
+    mv32 = dda_b200.CudaMatVec(p, "fp32", max_rhs=2)
+    mv64 = dda_b200.CudaMatVec(p, "fp64")
+    ccs = []
+    for r, pol in enumerate((1, 2)):
+        ccs.append(dda_b200.CoupleConstants(p, prop, pol, "ldr"))
+        mv32.set_couple_constants(ccs[-1], rhs=r)
+    einc = np.stack([p.einc(prop, 1), p.einc(prop, 2)])
+    P = dda_b200.CudaSolver(mv32, "bicgstab").get_pol_vec(einc, 1e-5)
+    mat = p.geometry.materials.astype(np.int64)
+    for r in range(2):
+        mv64.set_couple_constants(ccs[r])
+        cs = np.zeros(p.vec_size, dtype=np.complex128)
+        for c in range(3):
+            cs[c * p.nvs:c * p.nvs + p.nv] = ccs[r].cc_sqrt[mat * 3 + c]
+        live = cs != 0
+        x = np.zeros_like(P[r])
+        x[live] = P[r][live] / cs[live]
+        b = cs * einc[r]
+        res = np.linalg.norm(b - mv64.apply(x)) / np.linalg.norm(b)
+        assert res < 1e-5, res

@@ -237,6 +237,7 @@ def run_ours(args):
     pol_dev = torch.zeros_like(einc_dev)
     stream = torch.cuda.ExternalStream(mv.stream)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
+    torch.cuda.synchronize()  # the library's stream does not wait for torch's
 
     def step():
         solver.get_pol_vec_device(einc_dev.data_ptr(), pol_dev.data_ptr(), nrhs, EPS)
@@ -270,8 +271,11 @@ def run_ours(args):
     value = replica_throughput(nrhs * args.steps, world, t_max)
     ms_per_step = t_max / args.steps
 
-    # e2e: host FP64 einc in, host FP64 polarisations out, through dda_solve
-    einc_host = np.ascontiguousarray(einc)
+    # e2e: host FP64 einc in, host FP64 polarisations out, through dda_solve,
+    # both from / into pinned host memory
+    einc_host = torch.empty(einc.size, dtype=torch.complex128, pin_memory=True).numpy()
+    einc_host[:] = einc.reshape(-1)
+    pol_host = torch.empty(einc.size, dtype=torch.complex128, pin_memory=True).numpy()
     e2e_ms = 0.0
     for _ in range(args.steps):
         with torch.cuda.stream(stream):
@@ -279,7 +283,7 @@ def run_ours(args):
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-        solver.get_pol_vec(einc_host, EPS, history_cap=1)
+        solver.get_pol_vec(einc_host, EPS, history_cap=1, out=pol_host)
         e1.record(stream)
         e1.synchronize()
         e2e_ms += e0.elapsed_time(e1)

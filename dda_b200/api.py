@@ -391,12 +391,20 @@ class CudaSolver:
         self.last_stats = None
         self.last_history = None
 
-    def get_pol_vec(self, einc, eps, start=None, history_cap=100000, raise_on_error=True):
-        """Solves for one or more right-hand sides; einc is [nrhs][3 nvs]."""
+    def get_pol_vec(self, einc, eps, start=None, history_cap=100000, raise_on_error=True, out=None):
+        """Solves for one or more right-hand sides; einc is [nrhs][3 nvs].
+        `out`, when given, is the complex128 C-contiguous array of einc's size
+        that receives the polarisations (for instance a pinned host buffer,
+        which makes both bus copies asynchronous DMA)."""
         e, ep = _cbuf(einc)
         nvs = self.mv.nvs
         nrhs = e.size // (3 * nvs)
-        pol = np.zeros_like(e)
+        if out is None:
+            pol = np.zeros_like(e)
+        else:
+            if out.dtype != np.complex128 or out.size != e.size or not out.flags["C_CONTIGUOUS"]:
+                raise ValueError("out must be a C-contiguous complex128 array of einc's size")
+            pol = out
         sp = None
         if start is not None:
             s, sp = _cbuf(start)

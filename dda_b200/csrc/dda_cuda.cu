@@ -210,6 +210,7 @@ template <typename T> struct Engine {
   size_t yz_fixed = 0, yz_row = 0;  // fused kernel shared memory: fixed part, per row
   YzGeom yz{};
   size_t smem_x = 0, smem_yz = 0, smem_rows = 0, smem_cols = 0, smem_slot = 0;
+  int tl = 1;                 // grid lines per k_xfwd / k_xinv tile
   ColGeom cz_fwd{}, cz_inv{};
   MvKernels<T> k;
   void release(cudaStream_t s) {
@@ -304,7 +305,13 @@ struct dda_ctx {
 
 namespace {
 
-int ntiles(const dda_ctx* c) { return (c->g.nlines + c->g.tl - 1) / c->g.tl; }
+int ntiles(const dda_ctx* c, int tl) { return (c->g.nlines + tl - 1) / tl; }
+
+// Largest x tile (grid lines) whose shared memory stays within 72 KB, so
+// that three CTAs of k_xfwd / k_xinv share an SM.
+inline int x_tile_max(long long cbytes, long long Gx) {
+  return (int)std::max(1LL, std::min(64LL, 73728 / (cbytes * (Gx + 1))));
+}
 
 template <typename T> Engine<T>& eng(dda_ctx* c);
 template <> Engine<float>& eng<float>(dda_ctx* c) { return c->e32; }
@@ -372,6 +379,40 @@ template <typename T> void setup_slot(dda_ctx* c, Engine<T>& e) {
   e.slot_path = true;
 }
 
+// Lines per k_xfwd / k_xinv tile.  The two x passes launch
+// ntiles x 3 x nrhs CTAs of a few microseconds each, so the count of waves
+// over the SMs decides their time: among tiles from half the 72 KB maximum
+// up to it, the one with the least (waves x (lines + 2)) wins, the 2 lines
+// standing for a CTA's fixed cost (twiddles, material table).  Depends on the
+// grid, the box, max_rhs and the device only, never on timing, so that a
+// problem's arithmetic (the partial sums of the fused dot products follow
+// the tiles) is the same in every context that solves it.
+template <typename T> void pick_x_tile(dda_ctx* c, Engine<T>& e) {
+  const MvGeom& g = c->g;
+  const size_t s = sizeof(typename C2<T>::t);
+  int nsm = 148;
+  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
+  CK(allow_smem((const void*)e.k.xfwd));
+  CK(allow_smem((const void*)e.k.xinv));
+  const int tmax = x_tile_max((long long)s, g.Gx);
+  long long best_cost = -1;
+  for (int tl = std::max(1, tmax / 2); tl <= tmax; tl++) {
+    const size_t smem = ((size_t)g.Gx + g.nmat + (size_t)tl * g.pitchx) * s;
+    int of = 0, oi = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&of, e.k.xfwd, kNtX, smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&oi, e.k.xinv, kNtX, smem));
+    const long long slots = (long long)std::max(1, std::min(of, oi)) * nsm;
+    const long long ctas = (long long)ntiles(c, tl) * 3 * c->max_rhs;
+    const long long cost = (ctas + slots - 1) / slots * (tl + 2);
+    if (best_cost < 0 || cost <= best_cost) {
+      best_cost = cost;
+      e.tl = tl;
+    }
+  }
+  // twiddles, material table, tile of tl lines x (Gx+1)
+  e.smem_x = ((size_t)g.Gx + g.nmat + (size_t)e.tl * g.pitchx) * s;
+}
+
 // Chooses tile shapes and allocates the matvec buffers of one precision.
 template <typename T> void setup_engine(dda_ctx* c) {
   typedef typename C2<T>::t T2;
@@ -380,8 +421,6 @@ template <typename T> void setup_engine(dda_ctx* c) {
   const size_t s = sizeof(T2);
   e.on = true;
   constexpr int NW = kNtYz / 32;
-  // k_xfwd / k_xinv: twiddles, material table, tile of tl lines x (Gx+1)
-  e.smem_x = ((size_t)g.Gx + g.nmat + (size_t)g.tl * g.pitchx) * s;
   // fused plane kernel: twiddles, slab Gz x q, row buffers 3 x (Gy+1)
   YzGeom y;
   y.q = 3 * g.by + ((3 * g.by) % 2 == 0 ? 1 : 0);
@@ -432,6 +471,7 @@ template <typename T> void setup_engine(dda_ctx* c) {
       throw DdaError(DDA_ERR_UNSUPPORTED, "FFT grid too large for the shared-memory tiles");
     e.zbuf = (T2*)dalloc<T>((size_t)c->max_rhs * g.Gx * 3 * g.Gz * g.by * s);
   }
+  pick_x_tile<T>(c, e);
   if (e.smem_x > kSmemMax) throw DdaError(DDA_ERR_UNSUPPORTED, "grid x extent too large");
   auto attr = [](const void* f, size_t bytes) {
     if (bytes > kSmemMax) throw DdaError(DDA_ERR_UNSUPPORTED, "shared-memory tile above the SM limit");
@@ -618,12 +658,13 @@ template <typename T>
 void matvec(dda_ctx* c, const typename C2<T>::t* arg, typename C2<T>::t* res, int conj, int nrhs,
             cudaStream_t s, KrylovState* st, KrylovStep step, int skipmv = 0) {
   Engine<T>& e = eng<T>(c);
-  const MvGeom& g = c->g;
+  MvGeom g = c->g;
+  g.tl = e.tl;
   const FftPlanDev px = c->mx.dev<T>();
-  dim3 gx(ntiles(c), 3, nrhs);
+  dim3 gx(ntiles(c, e.tl), 3, nrhs);
   e.k.xfwd<<<gx, kNtX, e.smem_x, s>>>(arg, e.xhat, c->line_off, c->dip, c->perm, e.ccs, conj, g, px, st, skipmv);
   launch_yz<T>(c, nrhs, s, st, skipmv);
-  step.red = red_target(c, 3 * ntiles(c));
+  step.red = red_target(c, 3 * ntiles(c, e.tl));
   e.k.xinv<<<gx, kNtX, e.smem_x, s>>>(arg, res, e.xhat, c->line_off, c->dip, c->perm, e.ccs, conj, g, px, st, step,
                                       skipmv);
   CK(cudaGetLastError());
@@ -1126,10 +1167,7 @@ int dda_create(const dda_problem* p, int precision, dda_ctx** out) {
     g.nlines = g.by * g.bz;
     g.nmat = (int)p->nmat;
     g.pitchx = g.Gx + 1;
-    {
-      const int s = precision == DDA_PREC_FP32 ? 8 : 16;
-      g.tl = std::max(1, std::min(32, (int)(73728 / ((size_t)s * g.pitchx))));  // <= 72 KB: three CTAs per SM
-    }
+    g.tl = 0;  // per engine (Engine::tl), set in the copy each launch takes
     // geometry tables: dipoles sorted by grid line (y + by z), stable
     const uint32_t nv = p->nv;
     std::vector<uint32_t> line(nv), cnt(g.nlines + 1, 0);
@@ -1179,7 +1217,8 @@ int dda_create(const dda_problem* p, int precision, dda_ctx** out) {
     if (precision != DDA_PREC_FP32) setup_engine<double>(c.get());
     if (precision != DDA_PREC_FP64) setup_engine<float>(c.get());
     // reduction slots
-    c->nparts_mv = 3 * ntiles(c.get());
+    c->nparts_mv = 3 * std::max(c->e32.on ? ntiles(c.get(), c->e32.tl) : 0,
+                                c->e64.on ? ntiles(c.get(), c->e64.tl) : 0);
     {
       const long long len = 3LL * g.nvs;
       c->nparts_vec = (int)std::max(1LL, std::min(296LL, (len + 2047) / 2048));
@@ -1269,7 +1308,8 @@ namespace {
 template <typename T> void profile_t(dda_ctx* c, int nrhs, int reps, double* ms) {
   typedef typename C2<T>::t T2;
   Engine<T>& e = eng<T>(c);
-  const MvGeom& g = c->g;
+  MvGeom g = c->g;
+  g.tl = e.tl;
   const FftPlanDev px = c->mx.dev<T>();
   cudaStream_t s = c->stream;
   cudaEvent_t ev[4];
@@ -1278,9 +1318,9 @@ template <typename T> void profile_t(dda_ctx* c, int nrhs, int reps, double* ms)
   const T2* arg = e.vec[0];
   T2* res = e.io;
   KrylovStep none{KOP_NONE, 0, nullptr, {}};
-  none.red = red_target(c, 3 * ntiles(c));
+  none.red = red_target(c, 3 * ntiles(c, e.tl));
   for (int r = 0; r <= reps; r++) {
-    dim3 gx(ntiles(c), 3, nrhs);
+    dim3 gx(ntiles(c, e.tl), 3, nrhs);
     CK(cudaEventRecord(ev[0], s));
     e.k.xfwd<<<gx, kNtX, e.smem_x, s>>>(arg, e.xhat, c->line_off, c->dip, c->perm, e.ccs, 0, g, px, nullptr, 0);
     CK(cudaEventRecord(ev[1], s));
@@ -1302,30 +1342,76 @@ template <typename T> void profile_t(dda_ctx* c, int nrhs, int reps, double* ms)
   ms[3] = ms[0] + ms[1] + ms[2];
 }
 
+// Host FP64 vectors and the FP32 engine: the FP64 data crosses the bus as it
+// is and is rounded (to nearest, as a host cast would) on the device.  The
+// FP64 copy is staged in two solver workspace vectors, which hold nothing
+// before a solve starts or after it ends and of which each holds half of
+// `n` FP64 complex values (n <= max_rhs 3 nvs, even).  With the input from
+// pinned host memory the copies run at full bus speed and never block the
+// host.
+struct HostStage {
+  double2* part[2];
+  size_t len[2];
+  void* temp = nullptr;
+};
+
+HostStage host_stage(dda_ctx* c, size_t n) {
+  HostStage h;
+  h.len[0] = n / 2;
+  h.len[1] = n - n / 2;
+  Engine<float>& e = c->e32;
+  if (e.vec[8] && e.vec[9]) {
+    h.part[0] = reinterpret_cast<double2*>(e.vec[8]);
+    h.part[1] = reinterpret_cast<double2*>(e.vec[9]);
+  } else {
+    CK(cudaMallocAsync(&h.temp, n * sizeof(double2), c->stream));
+    h.part[0] = static_cast<double2*>(h.temp);
+    h.part[1] = h.part[0] + h.len[0];
+  }
+  return h;
+}
+
+void host_stage_release(dda_ctx* c, HostStage& h) {
+  if (h.temp) CK(cudaFreeAsync(h.temp, c->stream));
+  h.temp = nullptr;
+}
+
 template <typename T>
 void host_to_engine(dda_ctx* c, const double* src, typename C2<T>::t* dst, size_t n) {
-  typedef typename C2<T>::t T2;
-  if (std::is_same<T, double>::value) {
+  if constexpr (std::is_same<T, double>::value) {
     CK(cudaMemcpyAsync(dst, src, n * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
   } else {
-    std::vector<T2> h(n);
-    for (size_t i = 0; i < n; i++) { h[i].x = (T)src[2 * i]; h[i].y = (T)src[2 * i + 1]; }
-    CK(cudaMemcpyAsync(dst, h.data(), n * sizeof(T2), cudaMemcpyHostToDevice, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
+    HostStage h = host_stage(c, n);
+    size_t off = 0;
+    for (int k = 0; k < 2; k++) {
+      CK(cudaMemcpyAsync(h.part[k], src + 2 * off, h.len[k] * sizeof(double2), cudaMemcpyHostToDevice,
+                         c->stream));
+      k_convert<double2, float2><<<592, 256, 0, c->stream>>>(h.part[k], dst + off, (long long)h.len[k]);
+      CK(cudaGetLastError());
+      c->launches++;
+      off += h.len[k];
+    }
+    host_stage_release(c, h);
   }
 }
 template <typename T>
 void engine_to_host(dda_ctx* c, const typename C2<T>::t* src, double* dst, size_t n) {
-  typedef typename C2<T>::t T2;
-  if (std::is_same<T, double>::value) {
+  if constexpr (std::is_same<T, double>::value) {
     CK(cudaMemcpyAsync(dst, src, n * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
   } else {
-    std::vector<T2> h(n);
-    CK(cudaMemcpyAsync(h.data(), src, n * sizeof(T2), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    for (size_t i = 0; i < n; i++) { dst[2 * i] = h[i].x; dst[2 * i + 1] = h[i].y; }
+    HostStage h = host_stage(c, n);
+    size_t off = 0;
+    for (int k = 0; k < 2; k++) {
+      k_convert<float2, double2><<<592, 256, 0, c->stream>>>(src + off, h.part[k], (long long)h.len[k]);
+      CK(cudaGetLastError());
+      c->launches++;
+      CK(cudaMemcpyAsync(dst + 2 * off, h.part[k], h.len[k] * sizeof(double2), cudaMemcpyDeviceToHost,
+                         c->stream));
+      off += h.len[k];
+    }
+    host_stage_release(c, h);
   }
+  CK(cudaStreamSynchronize(c->stream));
 }
 
 template <typename T>
@@ -1597,8 +1683,9 @@ int dda_footprint(const dda_problem* p, int precision, int64_t* resident, int64_
   };
   if (precision != DDA_PREC_FP32) bytes += engine(16);
   if (precision != DDA_PREC_FP64) bytes += engine(8);
+  // the x tiles are at least half their 72 KB maximum (pick_x_tile)
   const long long sx = precision == DDA_PREC_FP32 ? 8 : 16;
-  const long long tl = std::max(1LL, std::min(32LL, 73728 / (sx * (Gx + 1))));
+  const long long tl = std::max(1, x_tile_max(sx, Gx) / 2);
   const long long tiles = (nl + tl - 1) / tl;
   bytes += R * std::max(3 * tiles, 296LL) * (long long)sizeof(RedSums) + R * 4;
   bytes += 2 * R * (long long)sizeof(KrylovState) + R * 100000LL * 8;
@@ -1619,7 +1706,7 @@ int dda_matvec_layout(const dda_ctx* ctx, int64_t* out) {
   };
   if (ctx->e32.on) fill(ctx->e32);
   else fill(ctx->e64);
-  out[5] = ctx->g.tl;
+  out[5] = ctx->e32.on ? ctx->e32.tl : ctx->e64.tl;
   out[6] = ctx->planned ? 1 : 0;
   out[7] = (int64_t)ctx->dev_bytes;
   return DDA_OK;

@@ -153,6 +153,23 @@ def test_autotuned_layout_gives_identical_results(prec, shape):
     print(mvs[0].layout, mvs[1].layout)
 
 
+def test_x_tile_fills_whole_waves():
+    # the x-pass tile is chosen by the count of CTA waves: for the 250 000
+    # dipole box (2 500 grid lines, grid x 200) with two right-hand sides in
+    # FP32 both x passes take one wave of at most three CTAs per SM
+    import torch
+    import dda_b200
+    g = dda_b200.Geometry.box_shape("10um", "5um", "5um", "0.1um")
+    p = dda_b200.DDAParams(g, [1.5 + 0.1j], "6um")
+    mv = dda_b200.CudaMatVec(p, "fp32", max_rhs=2)
+    tl = mv.layout["lines_per_x_tile"]
+    nsm = torch.cuda.get_device_properties(0).multi_processor_count
+    tmax = min(64, 73728 // (8 * 201))
+    assert tmax // 2 <= tl <= tmax
+    assert -(-2500 // tl) * 3 * 2 <= 3 * nsm
+    mv.close()
+
+
 def test_matvec_host_dmatrix():
     kind, args, mats, lam = CASES["aniso"]
     pr = Pair(kind, args, mats, lam, "fp64", host_d=True)

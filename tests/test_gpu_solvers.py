@@ -49,6 +49,29 @@ def test_fp32_solver_converges(aniso64, solver):
     assert rel(pol, opol) < 1e-4
 
 
+def test_fp32_host_path_matches_device_path():
+    # dda_solve converts the host FP64 fields to FP32 on the device (rounding
+    # to nearest, as a host cast does) and the polarisations back: the result
+    # is the device-resident solve's, bit for bit, also into a pinned buffer
+    import torch
+    pr = Pair("arrays", aniso_arrays(), MATS, "0.9um", "fp32")
+    pr.set_cc((0.3, 0.4, 0.866), 1, "ldr")
+    e = np.ascontiguousarray(pr.p.einc((0.3, 0.4, 0.866), 1).reshape(-1))
+    s = dda_b200.CudaSolver(pr.mv, "bicgstab")
+    out = torch.empty(e.size, dtype=torch.complex128, pin_memory=True).numpy()
+    pol = s.get_pol_vec(e, 1e-5, out=out)
+    assert pol is out and s.last_stats[0].status == 0
+    paged = s.get_pol_vec(e, 1e-5)
+    assert np.array_equal(paged, out)
+    ed = torch.from_numpy(e).to(torch.complex64).cuda()
+    pd = torch.zeros_like(ed)
+    torch.cuda.synchronize()
+    s.get_pol_vec_device(ed.data_ptr(), pd.data_ptr(), 1, 1e-5)
+    assert np.array_equal(pd.cpu().numpy().astype(np.complex128), out)
+    with pytest.raises(ValueError):
+        s.get_pol_vec(e, 1e-5, out=np.zeros(e.size, dtype=np.complex64))
+
+
 def test_cfg1_qmr_fp64_iterations():
     # README workload 1: sphere r = 10 um, d = 0.5 um, m = 1.5+0.1i, 6 um, QMR, 1e-5
     pr = Pair("sphere", ("10um", "0.5um"), [1.5 + 0.1j], "6um", "fp64")

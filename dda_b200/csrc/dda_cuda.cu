@@ -66,6 +66,7 @@ template <> struct NtYz<double> { static constexpr int v = 256; };
 #define kNtYz NtYz<T>::v
 constexpr int kNtC = 256;   // k_fft_cols / k_fft_rows
 constexpr int kNtV = 256;                 // k_vec
+constexpr int kVecPartsMax = 8 * 148;     // k_vec CTAs per right-hand side, at most
 constexpr size_t kSmemMax = 227 * 1024;
 
 // Opts kernel f into the whole shared memory of an SM (less its static
@@ -306,6 +307,26 @@ struct dda_ctx {
 namespace {
 
 int ntiles(const dda_ctx* c, int tl) { return (c->g.nlines + tl - 1) / tl; }
+
+// CTAs of the vector steps per right-hand side: every SM filled with as many
+// as it holds of the heaviest step (QMR-CS update: six vector streams), at
+// least 512 elements each.  A fixed function of the problem and the device,
+// as the partial sums of the dot products follow it.
+int vec_parts(dda_ctx* c) {
+  int nsm = 148;
+  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
+  int occ = kVecPartsMax;
+  auto limit = [&](auto fn) {
+    int n = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kNtV, 0));
+    occ = std::min(occ, std::max(1, n));
+  };
+  if (c->e32.on && c->precision == DDA_PREC_FP32) limit(k_vec<float, kNtV, V_QMR_UPD>);
+  if (c->e64.on) limit(k_vec<double, kNtV, V_QMR_UPD>);
+  const long long len = 3LL * c->g.nvs;
+  const long long parts = std::min<long long>((long long)occ * nsm, (len + 511) / 512);
+  return (int)std::max(1LL, std::min<long long>(parts, kVecPartsMax));
+}
 
 // Largest x tile (grid lines) whose shared memory stays within 72 KB, so
 // that three CTAs of k_xfwd / k_xinv share an SM.
@@ -796,7 +817,7 @@ template <typename T> struct Solve {
     a.ccs = e.ccs;
     a.pscale = c->grid_unit * c->grid_unit * c->grid_unit;
     a.step = k;
-    k_vec<T, kNtV><<<dim3(c->nparts_vec, nrhs), kNtV, 0, s>>>(a, st);
+    vec_kernel<T, kNtV>(a.op)<<<dim3(c->nparts_vec, nrhs), kNtV, 0, s>>>(a, st);
     CK(cudaGetLastError());
     c->launches++;
   }
@@ -829,7 +850,7 @@ template <typename T> struct Solve {
         a.nmat = c->g.nmat;
         a.nparts = c->nparts_vec;
         a.step = k;
-        k_vec<T, kNtV><<<dim3(c->nparts_vec, nrhs), kNtV, 0, s>>>(a, st);
+        vec_kernel<T, kNtV>(a.op)<<<dim3(c->nparts_vec, nrhs), kNtV, 0, s>>>(a, st);
         CK(cudaGetLastError());
         c->launches++;
         return;
@@ -1219,10 +1240,7 @@ int dda_create(const dda_problem* p, int precision, dda_ctx** out) {
     // reduction slots
     c->nparts_mv = 3 * std::max(c->e32.on ? ntiles(c.get(), c->e32.tl) : 0,
                                 c->e64.on ? ntiles(c.get(), c->e64.tl) : 0);
-    {
-      const long long len = 3LL * g.nvs;
-      c->nparts_vec = (int)std::max(1LL, std::min(296LL, (len + 2047) / 2048));
-    }
+    c->nparts_vec = vec_parts(c.get());
     const int nparts = std::max(c->nparts_mv, c->nparts_vec);
     dmalloc((void**)&c->parts, (size_t)c->max_rhs * nparts * sizeof(RedSums));
     dmalloc((void**)&c->tickets, c->max_rhs * sizeof(unsigned));
@@ -1687,7 +1705,7 @@ int dda_footprint(const dda_problem* p, int precision, int64_t* resident, int64_
   const long long sx = precision == DDA_PREC_FP32 ? 8 : 16;
   const long long tl = std::max(1, x_tile_max(sx, Gx) / 2);
   const long long tiles = (nl + tl - 1) / tl;
-  bytes += R * std::max(3 * tiles, 296LL) * (long long)sizeof(RedSums) + R * 4;
+  bytes += R * std::max(3 * tiles, (long long)kVecPartsMax) * (long long)sizeof(RedSums) + R * 4;
   bytes += 2 * R * (long long)sizeof(KrylovState) + R * 100000LL * 8;
   if (resident) *resident = bytes;
   const long long tmp = p->dmatrix ? (Gx / 2 + 1) * (Gy / 2 + 1) * (Gz / 2 + 1) * 6 * 16 : Gx * Gy * Gz * 16;

@@ -10,6 +10,9 @@
 // DDA/GpuIterativeSolverInst.cl:27-108.
 #pragma once
 
+#include <array>
+#include <utility>
+
 #include "fft_engine.cuh"
 #include "krylov_ops.cuh"
 #include "reduce.cuh"
@@ -36,6 +39,7 @@ enum VecOp {
   V_RESULT,          // v0 = sqrt(cc).v1  (P = sqrt(cc) x)
   V_NORM,            // n = |v0|^2
   V_ADD_CONV,        // v0 = v1 + (FP32) v2; step sums as the matvec epilogue (first: skip on half-step exit)
+  V_COUNT
 };
 
 struct VecArgs {
@@ -55,13 +59,16 @@ __device__ __forceinline__ T2 cvt(S2 a) {
   T2 r; r.x = a.x; r.y = a.y; return r;
 }
 
-template <typename T, int NT>
-__global__ void __launch_bounds__(NT) k_vec(VecArgs va, KrylovState* st) {
+// One instantiation per operation OP (va.op == OP), so that each keeps only
+// its own registers: the vector steps are streaming kernels, and their speed
+// is the number of loads in flight, i.e. the CTAs an SM holds.
+template <typename T, int NT, int OP>
+__global__ void __launch_bounds__(NT, 4) k_vec(VecArgs va, KrylovState* st) {
   typedef typename C2<T>::t T2;
   const int b = blockIdx.y;
   KrylovState& s = st[b];
-  if (s.done && va.op != V_RESULT) return;  // the result copy runs after convergence
-  if (va.op == V_ADD_CONV && va.first && s.skipmv) return;  // its matvec was skipped too
+  if (s.done && OP != V_RESULT) return;  // the result copy runs after convergence
+  if (OP == V_ADD_CONV && va.first && s.skipmv) return;  // its matvec was skipped too
   const long long len = 3LL * va.nvs;
   const long long chunk = ((len + va.nparts - 1) / va.nparts + 31) / 32 * 32;
   const long long i0 = chunk * blockIdx.x;
@@ -84,7 +91,7 @@ __global__ void __launch_bounds__(NT) k_vec(VecArgs va, KrylovState* st) {
   const int skip = s.skipmv, usezero = s.usezero;
   RedSums acc = red_zero();
   for (long long i = i0 + threadIdx.x; i < i1; i += NT) {
-    switch (va.op) {
+    switch (OP) {
       case V_SETUP_PVEC:
       case V_RESULT:
       case V_START_X: {
@@ -93,11 +100,11 @@ __global__ void __launch_bounds__(NT) k_vec(VecArgs va, KrylovState* st) {
         if (j < va.nv) {
           const T2 cc = ccs[va.mat[j] * 3 + c];
           const T2 x = v1[i];
-          if (va.op == V_START_X) {
+          if (OP == V_START_X) {
             // x / cc (Smith division in FP64)
             double2 q = ddivc(make_double2(x.x, x.y), make_double2(cc.x, cc.y));
             o = cvt<T2>(dscale(q, 1.0 / va.pscale));
-          } else if (va.op == V_RESULT) {
+          } else if (OP == V_RESULT) {
             o = cvt<T2>(dscale(dmulc(make_double2(cc.x, cc.y), make_double2(x.x, x.y)), va.pscale));
           } else {
             o = cmul(cc, x);
@@ -237,6 +244,18 @@ __global__ void __launch_bounds__(NT) k_vec(VecArgs va, KrylovState* st) {
     if (block_finish<NT>(acc, va.step.red, b, blockIdx.x, tot) && threadIdx.x == 0)
       krylov_finalize(s, va.step, tot);
   }
+}
+
+// k_vec<T, NT, op> for a run-time op.
+template <typename T, int NT, int... OPS>
+__host__ inline auto vec_kernel_table(std::integer_sequence<int, OPS...>) {
+  typedef void (*Fn)(VecArgs, KrylovState*);
+  return std::array<Fn, sizeof...(OPS)>{{&k_vec<T, NT, OPS>...}};
+}
+template <typename T, int NT>
+__host__ inline void (*vec_kernel(int op))(VecArgs, KrylovState*) {
+  static const auto tab = vec_kernel_table<T, NT>(std::make_integer_sequence<int, V_COUNT>{});
+  return tab[op];
 }
 
 // x64 += e for every right-hand side the refinement loop still runs

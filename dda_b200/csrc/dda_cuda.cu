@@ -331,7 +331,7 @@ int vec_parts(dda_ctx* c) {
 // Largest x tile (grid lines) whose shared memory stays within 72 KB, so
 // that three CTAs of k_xfwd / k_xinv share an SM.
 inline int x_tile_max(long long cbytes, long long Gx) {
-  return (int)std::max(1LL, std::min(64LL, 73728 / (cbytes * (Gx + 1))));
+  return (int)std::max(1LL, std::min((long long)kXTileMax, 73728 / (cbytes * (Gx + 1))));
 }
 
 template <typename T> Engine<T>& eng(dda_ctx* c);

@@ -87,6 +87,44 @@ __device__ __forceinline__ bool rhs_idle(const KrylovState* st, int b, int mvski
 //   [xtile, ...)       tile of tl grid lines, pitch pitchx = Gx + 1
 __host__ __device__ inline int x_tile_off(const MvGeom& g) { return g.Gx + g.nmat; }
 
+// Grid lines per x tile, at most.
+constexpr int kXTileMax = 64;
+// Global loads a thread of the x passes issues before it waits for the first
+// of them: a tile's loads are independent, and with three CTAs per SM one
+// load per thread at a time leaves HBM latency uncovered.
+constexpr int kXBatch = 8;
+
+// Line within the tile of CSR entry j: the largest l < nl with soff[l] <= j
+// (soff: the tile's nl + 1 line offsets; empty lines are passed over).
+__device__ __forceinline__ int tile_line(const uint32_t* soff, int nl, uint32_t j) {
+  int l = 0;
+#pragma unroll
+  for (int step = kXTileMax / 2; step > 0; step >>= 1)
+    if (l + step <= nl && soff[l + step] <= j) l += step;
+  return l;
+}
+
+// Element i = kx nl + l of a tile's spectrum, walked by one thread in steps
+// of NT without a division per element.
+template <int NT>
+struct TileWalk {
+  int kx, l, dkx, dl;
+  __device__ __forceinline__ TileWalk(int nl) {
+    kx = threadIdx.x / nl;
+    l = threadIdx.x - kx * nl;
+    dkx = NT / nl;
+    dl = NT - dkx * nl;
+  }
+  __device__ __forceinline__ void next(int nl) {
+    l += dl;
+    kx += dkx;
+    if (l >= nl) {
+      l -= nl;
+      kx++;
+    }
+  }
+};
+
 // ------------------------------------------------------------ k_xfwd ----
 // grid (ceil(nlines/tl), 3, nrhs).  PX: compile-time plan of the x
 // transform, or void for the runtime-planned engine.
@@ -107,31 +145,49 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 1 : 3) k_xfwd(const typen
   T2* sm = smem_at<T>(toff);
   const int L0 = blockIdx.x * g.tl;
   const int nl = min(g.tl, g.nlines - L0);
+  __shared__ uint32_t soff[kXTileMax + 1];
   stage_twiddles<T, NT>(0, px);
   for (int i = threadIdx.x; i < g.nmat; i += NT) scc[i] = ccs[((size_t)b * g.nmat + i) * 3 + c];
+  for (int i = threadIdx.x; i <= nl; i += NT) soff[i] = line_off[L0 + i];
   for (int i = threadIdx.x; i < nl * g.pitchx; i += NT) sm[i] = czero<T2>();
   __syncthreads();
+  // the tile's dipoles are one contiguous CSR range: every thread takes
+  // entries of it independently, so many loads are in flight at once
   const T2* a = arg + ((size_t)b * 3 + c) * g.nvs;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int l = warp; l < nl; l += NT / 32) {
-    const uint32_t j0 = line_off[L0 + l], j1 = line_off[L0 + l + 1];
-    for (uint32_t j = j0 + lane; j < j1; j += 32) {
-      const uint32_t d = dip[j];
-      const uint32_t jj = perm ? perm[j] : j;
-      T2 v = a[jj];
-      if (conj) v.y = -v.y;
-      sm[l * g.pitchx + (d & 0xffffu)] = cmul(v, scc[d >> 16]);
+  const uint32_t je = soff[nl];
+  uint32_t j = soff[0] + threadIdx.x;
+  int l = j < je ? tile_line(soff, nl, j) : 0;
+  for (; j < je; j += kXBatch * NT) {
+    int o[kXBatch];  // shared offset of entry j + u NT, -1 past the tile
+    uint32_t d[kXBatch], jj[kXBatch];
+#pragma unroll
+    for (int u = 0; u < kXBatch; u++) {
+      const uint32_t ju = j + u * NT;
+      o[u] = -1;
+      if (ju < je) {
+        while (soff[l + 1] <= ju) l++;  // stops at nl - 1: soff[nl] = je > ju
+        d[u] = dip[ju];
+        jj[u] = perm ? perm[ju] : ju;
+        o[u] = l * g.pitchx;
+      }
     }
+    T2 v[kXBatch];
+#pragma unroll
+    for (int u = 0; u < kXBatch; u++)
+      if (o[u] >= 0) v[u] = a[jj[u]];
+#pragma unroll
+    for (int u = 0; u < kXBatch; u++)
+      if (o[u] >= 0) {
+        if (conj) v[u].y = -v[u].y;
+        sm[o[u] + (d[u] & 0xffffu)] = cmul(v[u], scc[d[u] >> 16]);
+      }
   }
   __syncthreads();
   if constexpr (std::is_void<PX>::value) fft_lines<T, NT, false>(toff, nl, g.pitchx, 1, false, px, 0);
   else plines<T, PX, NT, false>(toff, nl, g.pitchx, 1, 0);
   T2* out = xhat + ((size_t)b * g.Gx * 3 + c) * g.nlines + L0;
   const size_t kstride = (size_t)3 * g.nlines;
-  for (int i = threadIdx.x; i < nl * g.Gx; i += NT) {
-    const int kx = i / nl, l = i - kx * nl;
-    out[kx * kstride + l] = sm[l * g.pitchx + kx];
-  }
+  for (TileWalk<NT> w(nl); w.kx < g.Gx; w.next(nl)) out[w.kx * kstride + w.l] = sm[w.l * g.pitchx + w.kx];
 }
 
 // ------------------------------------------------------------ k_xinv ----
@@ -156,13 +212,27 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 1 : 3) k_xinv(const typen
   T2* sm = smem_at<T>(toff);
   const int L0 = blockIdx.x * g.tl;
   const int nl = min(g.tl, g.nlines - L0);
+  __shared__ uint32_t soff[kXTileMax + 1];
   stage_twiddles<T, NT>(0, px);
   for (int i = threadIdx.x; i < g.nmat; i += NT) scc[i] = ccs[((size_t)b * g.nmat + i) * 3 + c];
+  for (int i = threadIdx.x; i <= nl; i += NT) soff[i] = line_off[L0 + i];
   const T2* in = xhat + ((size_t)b * g.Gx * 3 + c) * g.nlines + L0;
   const size_t kstride = (size_t)3 * g.nlines;
-  for (int i = threadIdx.x; i < nl * g.Gx; i += NT) {
-    const int kx = i / nl, l = i - kx * nl;
-    sm[l * g.pitchx + kx] = in[kx * kstride + l];
+  for (TileWalk<NT> w(nl); w.kx < g.Gx;) {
+    T2 v[kXBatch];
+    int o[kXBatch];  // shared offset, -1 past the tile
+#pragma unroll
+    for (int u = 0; u < kXBatch; u++) {
+      o[u] = -1;
+      if (w.kx < g.Gx) {
+        v[u] = in[w.kx * kstride + w.l];
+        o[u] = w.l * g.pitchx + w.kx;
+      }
+      w.next(nl);
+    }
+#pragma unroll
+    for (int u = 0; u < kXBatch; u++)
+      if (o[u] >= 0) sm[o[u]] = v[u];
   }
   __syncthreads();
   if constexpr (std::is_void<PX>::value) fft_lines<T, NT, true>(toff, nl, g.pitchx, 1, false, px, 0);
@@ -171,22 +241,43 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 1 : 3) k_xinv(const typen
   const T2* a = arg + voff;
   T2* r = res + voff;
   const T2* w = step.w ? reinterpret_cast<const T2*>(step.w) + voff : nullptr;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   RedSums acc = red_zero();
-  for (int l = warp; l < nl; l += NT / 32) {
-    const uint32_t j0 = line_off[L0 + l], j1 = line_off[L0 + l + 1];
-    for (uint32_t j = j0 + lane; j < j1; j += 32) {
-      const uint32_t d = dip[j];
-      const uint32_t jj = perm ? perm[j] : j;
-      const T2 x = sm[l * g.pitchx + (d & 0xffffu)];
-      const T2 a0 = a[jj];
-      T2 av = a0;
-      if (conj) av.y = -av.y;
-      T2 y = step.conv_only ? cmul(x, scc[d >> 16]) : cadd(cmul(x, scc[d >> 16]), av);
-      if (conj) y.y = -y.y;
-      r[jj] = y;
-      if (step.op != KOP_NONE) acc = epilogue_terms<T2>(acc, y, a0, w ? w[jj] : a0, step.mode);
+  const uint32_t je = soff[nl];
+  uint32_t j = soff[0] + threadIdx.x;
+  int l = j < je ? tile_line(soff, nl, j) : 0;
+  constexpr int U = kXBatch / 2;
+  for (; j < je; j += U * NT) {
+    int o[U];  // shared offset of entry j + u NT, -1 past the tile
+    uint32_t d[U], jj[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const uint32_t ju = j + u * NT;
+      o[u] = -1;
+      if (ju < je) {
+        while (soff[l + 1] <= ju) l++;  // stops at nl - 1: soff[nl] = je > ju
+        d[u] = dip[ju];
+        jj[u] = perm ? perm[ju] : ju;
+        o[u] = l * g.pitchx;
+      }
     }
+    T2 a0[U], wv[U];
+#pragma unroll
+    for (int u = 0; u < U; u++)
+      if (o[u] >= 0) {
+        a0[u] = a[jj[u]];
+        if (w) wv[u] = w[jj[u]];
+      }
+#pragma unroll
+    for (int u = 0; u < U; u++)
+      if (o[u] >= 0) {
+        const T2 x = sm[o[u] + (d[u] & 0xffffu)];
+        T2 av = a0[u];
+        if (conj) av.y = -av.y;
+        T2 y = step.conv_only ? cmul(x, scc[d[u] >> 16]) : cadd(cmul(x, scc[d[u] >> 16]), av);
+        if (conj) y.y = -y.y;
+        r[jj[u]] = y;
+        if (step.op != KOP_NONE) acc = epilogue_terms<T2>(acc, y, a0[u], w ? wv[u] : a0[u], step.mode);
+      }
   }
   if (blockIdx.x == 0)
     for (int i = g.nv + threadIdx.x; i < g.nvs; i += NT) r[i] = czero<T2>();

@@ -647,8 +647,8 @@ template <typename T> void autotune(dda_ctx* c) {
   }
   std::vector<TuneChoice> cands;
   if (e.fused) {
-    const int max_rows = e.k.planned ? 32 : kNtYz / 32;
-    for (int n : {4, 6, 8, 10, 12, 14, 16, 20, 24, 25, 28, 32})
+    const int max_rows = e.k.planned ? 48 : kNtYz / 32;
+    for (int n : {4, 6, 8, 10, 12, 14, 16, 20, 24, 25, 28, 32, 34, 36, 40, 43, 48})
       if (n <= max_rows && e.yz_fixed + (size_t)n * e.yz_row <= kSmemMax) cands.push_back({n, 0});
   } else {
     for (int cl : {4, 8, 16})

@@ -129,7 +129,7 @@ struct TileWalk {
 // grid (ceil(nlines/tl), 3, nrhs).  PX: compile-time plan of the x
 // transform, or void for the runtime-planned engine.
 template <typename T, int NT, typename PX = void>
-__global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 1 : 3) k_xfwd(const typename C2<T>::t* __restrict__ arg,
+__global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 3) k_xfwd(const typename C2<T>::t* __restrict__ arg,
                                              typename C2<T>::t* __restrict__ xhat,
                                              const uint32_t* __restrict__ line_off,
                                              const uint32_t* __restrict__ dip,
@@ -195,7 +195,7 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 1 : 3) k_xfwd(const typen
 // conj?(arg)), padding nv..nvs zeroed, and optional sums over the result for
 // the solver step `op` (finalised by the last CTA of each right-hand side).
 template <typename T, int NT, typename PX = void>
-__global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 1 : 3) k_xinv(const typename C2<T>::t* __restrict__ arg,
+__global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 3) k_xinv(const typename C2<T>::t* __restrict__ arg,
                                              typename C2<T>::t* __restrict__ res,
                                              const typename C2<T>::t* __restrict__ xhat,
                                              const uint32_t* __restrict__ line_off,

@@ -59,11 +59,52 @@ __device__ __forceinline__ T2 cvt(S2 a) {
   T2 r; r.x = a.x; r.y = a.y; return r;
 }
 
+// Whether the element loop of step OP reads vector k (first: the
+// iteration-0 variant flag, skip: the BiCGStab half-step exit).
+template <int OP>
+__device__ __forceinline__ bool vec_reads(int k, int first, int skip) {
+  switch (OP) {
+    case V_SETUP_PVEC:
+    case V_RESULT:
+    case V_START_X:
+    case V_QMR_V0:
+    case V_BIS_INIT:
+    case V_ADD_CONV:
+      return k == 1;
+    case V_R_INIT:
+    case V_BIS_S:
+      return k == 1 || k == 2;
+    case V_CHOOSE_X0:
+      return k == 2;
+    case V_QMR_VT:
+      return k == 1 || k == 2 || (k == 0 && !first);
+    case V_QMR_UPD:
+      return k == 0 || k == 3 || k == 4 || k == 5 || (k == 2 && first != 1) || (k == 1 && first == 0);
+    case V_BIS_P:
+      return k == 2 || (!first && (k == 0 || k == 1));
+    case V_BIS_XR:
+      return k == 0 || k == 1 || (!skip && (k == 2 || k == 3 || k == 5));
+    case V_BICG_RO:
+    case V_NORM:
+      return k == 0;
+    case V_BICG_P:
+      return k == 1 || (!first && k == 0);
+    case V_BICG_XR:
+    case V_CGNR_XR:
+      return k <= 3;
+    case V_CGNR_P:
+      return k <= 1;
+    default:
+      return false;
+  }
+}
+
 // One instantiation per operation OP (va.op == OP), so that each keeps only
 // its own registers: the vector steps are streaming kernels, and their speed
-// is the number of loads in flight, i.e. the CTAs an SM holds.
+// is the number of loads in flight, i.e. the CTAs an SM holds times the loads
+// each thread issues before it waits.
 template <typename T, int NT, int OP>
-__global__ void __launch_bounds__(NT, 4) k_vec(VecArgs va, KrylovState* st) {
+__global__ void __launch_bounds__(NT, 3) k_vec(VecArgs va, KrylovState* st) {
   typedef typename C2<T>::t T2;
   const int b = blockIdx.y;
   KrylovState& s = st[b];
@@ -90,153 +131,181 @@ __global__ void __launch_bounds__(NT, 4) k_vec(VecArgs va, KrylovState* st) {
   const T normS = (T)s.normSNew;
   const int skip = s.skipmv, usezero = s.usezero;
   RedSums acc = red_zero();
-  for (long long i = i0 + threadIdx.x; i < i1; i += NT) {
-    switch (OP) {
-      case V_SETUP_PVEC:
-      case V_RESULT:
-      case V_START_X: {
-        const int c = (int)(i / va.nvs), j = (int)(i % va.nvs);
-        T2 o = czero<T2>();
-        if (j < va.nv) {
-          const T2 cc = ccs[va.mat[j] * 3 + c];
-          const T2 x = v1[i];
-          if (OP == V_START_X) {
-            // x / cc (Smith division in FP64)
-            double2 q = ddivc(make_double2(x.x, x.y), make_double2(cc.x, cc.y));
-            o = cvt<T2>(dscale(q, 1.0 / va.pscale));
-          } else if (OP == V_RESULT) {
-            o = cvt<T2>(dscale(dmulc(make_double2(cc.x, cc.y), make_double2(x.x, x.y)), va.pscale));
-          } else {
-            o = cmul(cc, x);
+  // Every element's inputs are loaded for U elements before the first is
+  // used: with one element at a time a thread waits out the memory latency
+  // once per element and the step runs far below the HBM rate.
+  constexpr int U = (sizeof(T) == 4 ? 4 : 2) / (OP == V_QMR_UPD ? 2 : 1);  // six streams: half
+  const int first = va.first;
+  for (long long base = i0 + threadIdx.x; base < i1; base += (long long)U * NT) {
+    T2 in0[U], in1[U], in2[U], in3[U], in4[U], in5[U], wv[U];
+    float2 cvv[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const long long i = base + (long long)u * NT;
+      if (i < i1) {
+        if (vec_reads<OP>(0, first, skip)) in0[u] = v0[i];
+        if (vec_reads<OP>(1, first, skip)) in1[u] = v1[i];
+        if (vec_reads<OP>(2, first, skip)) in2[u] = v2[i];
+        if (vec_reads<OP>(3, first, skip)) in3[u] = v3[i];
+        if (vec_reads<OP>(4, first, skip)) in4[u] = v4[i];
+        if (vec_reads<OP>(5, first, skip)) in5[u] = v5[i];
+        if (OP == V_ADD_CONV) {
+          cvv[u] = reinterpret_cast<const float2*>(va.v[2])[off + i];
+          if (va.step.w) wv[u] = reinterpret_cast<const T2*>(va.step.w)[off + i];
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const long long i = base + (long long)u * NT;
+      if (i >= i1) break;
+      switch (OP) {
+        case V_SETUP_PVEC:
+        case V_RESULT:
+        case V_START_X: {
+          const int c = (int)(i / va.nvs), j = (int)(i % va.nvs);
+          T2 o = czero<T2>();
+          if (j < va.nv) {
+            const T2 cc = ccs[va.mat[j] * 3 + c];
+            const T2 x = in1[u];
+            if (OP == V_START_X) {
+              // x / cc (Smith division in FP64)
+              double2 q = ddivc(make_double2(x.x, x.y), make_double2(cc.x, cc.y));
+              o = cvt<T2>(dscale(q, 1.0 / va.pscale));
+            } else if (OP == V_RESULT) {
+              o = cvt<T2>(dscale(dmulc(make_double2(cc.x, cc.y), make_double2(x.x, x.y)), va.pscale));
+            } else {
+              o = cmul(cc, x);
+            }
           }
+          v0[i] = o;
+          acc.n += (double)o.x * o.x + (double)o.y * o.y;
+          break;
         }
-        v0[i] = o;
-        acc.n += (double)o.x * o.x + (double)o.y * o.y;
-        break;
-      }
-      case V_R_INIT: {
-        T2 r = csub(v2[i], v1[i]);
-        v0[i] = r;
-        acc.n += (double)r.x * r.x + (double)r.y * r.y;
-        break;
-      }
-      case V_CHOOSE_X0: {
-        const T2 p = v2[i];
-        if (usezero) { v0[i] = czero<T2>(); v1[i] = p; }
-        else v0[i] = p;
-        break;
-      }
-      case V_QMR_V0:
-        v0[i] = cmul(v1[i], betaInv);
-        break;
-      case V_QMR_VT: {
-        T2 t = cadd(cmul(v1[i], mAlpha), v2[i]);
-        if (!va.first) t = cadd(cmul(v0[i], mBeta), t);
-        v0[i] = t;
-        acc.a.x += (double)t.x * t.x - (double)t.y * t.y;
-        acc.a.y += 2.0 * (double)t.x * t.y;
-        acc.n += (double)t.x * t.x + (double)t.y * t.y;
-        break;
-      }
-      case V_QMR_UPD: {
-        // v0 = r, v1 = p_old, v2 = p_new, v3 = v, v4 = vt, v5 = x.  The new
-        // search direction goes to p_new in iteration 0 and to p_old after
-        // that (the caller then swaps p_old and p_new, DDA/QmrCs.cpp:152-160).
-        const T2 v = v3[i];
-        T2 pn;
-        if (va.first == 1) {
-          pn = cmul(v, zetaInv);
-          v2[i] = pn;
-        } else {
-          if (va.first == 2) pn = cadd(cmul(v2[i], mEtaZeta), cmul(v, zetaInv));
-          else pn = cadd(cadd(cmul(v1[i], mThetaZeta), cmul(v2[i], mEtaZeta)), cmul(v, zetaInv));
-          v1[i] = pn;
-        }
-        v5[i] = cadd(cmul(pn, tau), v5[i]);
-        const T2 vn = cmul(v4[i], betaInv);
-        v4[i] = vn;
-        const T2 ro = v0[i];
-        T2 r;
-        r.x = ro.x * normS; r.y = ro.y * normS;
-        r = cadd(r, cmul(vn, cNOT));
-        v0[i] = r;
-        acc.n += (double)r.x * r.x + (double)r.y * r.y;
-        break;
-      }
-      case V_BIS_INIT: {
-        const T2 r = v1[i];
-        v0[i] = r;
-        acc.a.x += (double)r.x * r.x + (double)r.y * r.y;
-        break;
-      }
-      case V_BIS_P:
-        v0[i] = va.first ? v2[i] : cadd(cadd(cmul(v0[i], beta), cmul(v1[i], bo)), v2[i]);
-        break;
-      case V_BIS_S: {
-        const T2 t = cadd(cmul(v1[i], mAlpha), v2[i]);
-        v0[i] = t;
-        acc.n += (double)t.x * t.x + (double)t.y * t.y;
-        break;
-      }
-      case V_BIS_XR: {
-        // v0 = x, v1 = p, v2 = s, v3 = A s, v4 = r, v5 = rt
-        if (skip) {
-          v0[i] = cadd(cmul(v1[i], alpha), v0[i]);
-        } else {
-          const T2 sv = v2[i];
-          v0[i] = cadd(cadd(cmul(v1[i], alpha), cmul(sv, omega)), v0[i]);
-          const T2 r = cadd(cmul(v3[i], mOmega), sv);
-          v4[i] = r;
-          const T2 rt = v5[i];
+        case V_R_INIT: {
+          T2 r = csub(in2[u], in1[u]);
+          v0[i] = r;
           acc.n += (double)r.x * r.x + (double)r.y * r.y;
-          acc.a.x += (double)r.x * rt.x + (double)r.y * rt.y;
-          acc.a.y += (double)r.y * rt.x - (double)r.x * rt.y;
+          break;
         }
-        break;
+        case V_CHOOSE_X0: {
+          const T2 p = in2[u];
+          if (usezero) { v0[i] = czero<T2>(); v1[i] = p; }
+          else v0[i] = p;
+          break;
+        }
+        case V_QMR_V0:
+          v0[i] = cmul(in1[u], betaInv);
+          break;
+        case V_QMR_VT: {
+          T2 t = cadd(cmul(in1[u], mAlpha), in2[u]);
+          if (!va.first) t = cadd(cmul(in0[u], mBeta), t);
+          v0[i] = t;
+          acc.a.x += (double)t.x * t.x - (double)t.y * t.y;
+          acc.a.y += 2.0 * (double)t.x * t.y;
+          acc.n += (double)t.x * t.x + (double)t.y * t.y;
+          break;
+        }
+        case V_QMR_UPD: {
+          // v0 = r, v1 = p_old, v2 = p_new, v3 = v, v4 = vt, v5 = x.  The new
+          // search direction goes to p_new in iteration 0 and to p_old after
+          // that (the caller then swaps p_old and p_new, DDA/QmrCs.cpp:152-160).
+          const T2 v = in3[u];
+          T2 pn;
+          if (va.first == 1) {
+            pn = cmul(v, zetaInv);
+            v2[i] = pn;
+          } else {
+            if (va.first == 2) pn = cadd(cmul(in2[u], mEtaZeta), cmul(v, zetaInv));
+            else pn = cadd(cadd(cmul(in1[u], mThetaZeta), cmul(in2[u], mEtaZeta)), cmul(v, zetaInv));
+            v1[i] = pn;
+          }
+          v5[i] = cadd(cmul(pn, tau), in5[u]);
+          const T2 vn = cmul(in4[u], betaInv);
+          v4[i] = vn;
+          const T2 ro = in0[u];
+          T2 r;
+          r.x = ro.x * normS; r.y = ro.y * normS;
+          r = cadd(r, cmul(vn, cNOT));
+          v0[i] = r;
+          acc.n += (double)r.x * r.x + (double)r.y * r.y;
+          break;
+        }
+        case V_BIS_INIT: {
+          const T2 r = in1[u];
+          v0[i] = r;
+          acc.a.x += (double)r.x * r.x + (double)r.y * r.y;
+          break;
+        }
+        case V_BIS_P:
+          v0[i] = va.first ? in2[u] : cadd(cadd(cmul(in0[u], beta), cmul(in1[u], bo)), in2[u]);
+          break;
+        case V_BIS_S: {
+          const T2 t = cadd(cmul(in1[u], mAlpha), in2[u]);
+          v0[i] = t;
+          acc.n += (double)t.x * t.x + (double)t.y * t.y;
+          break;
+        }
+        case V_BIS_XR: {
+          // v0 = x, v1 = p, v2 = s, v3 = A s, v4 = r, v5 = rt
+          if (skip) {
+            v0[i] = cadd(cmul(in1[u], alpha), in0[u]);
+          } else {
+            const T2 sv = in2[u];
+            v0[i] = cadd(cadd(cmul(in1[u], alpha), cmul(sv, omega)), in0[u]);
+            const T2 r = cadd(cmul(in3[u], mOmega), sv);
+            v4[i] = r;
+            const T2 rt = in5[u];
+            acc.n += (double)r.x * r.x + (double)r.y * r.y;
+            acc.a.x += (double)r.x * rt.x + (double)r.y * rt.y;
+            acc.a.y += (double)r.y * rt.x - (double)r.x * rt.y;
+          }
+          break;
+        }
+        case V_BICG_RO: {
+          const T2 r = in0[u];
+          acc.a.x += (double)r.x * r.x - (double)r.y * r.y;
+          acc.a.y += 2.0 * (double)r.x * r.y;
+          break;
+        }
+        case V_BICG_P:
+          v0[i] = va.first ? in1[u] : cadd(cmul(in0[u], beta), in1[u]);
+          break;
+        case V_BICG_XR:
+        case V_CGNR_XR: {
+          // v0 = x, v1 = p, v2 = A, v3 = r
+          v0[i] = cadd(cmul(in1[u], alpha), in0[u]);
+          const T2 r = cadd(cmul(in2[u], mAlpha), in3[u]);
+          v3[i] = r;
+          acc.n += (double)r.x * r.x + (double)r.y * r.y;
+          acc.a.x += (double)r.x * r.x - (double)r.y * r.y;
+          acc.a.y += 2.0 * (double)r.x * r.y;
+          break;
+        }
+        case V_CGNR_P:
+          v0[i] = cadd(cmul(in0[u], beta), in1[u]);
+          break;
+        case V_NORM: {
+          const T2 r = in0[u];
+          acc.n += (double)r.x * r.x + (double)r.y * r.y;
+          break;
+        }
+        case V_ADD_CONV: {
+          // result of a matvec whose convolution ran in FP32: y = x + conv
+          const float2 cv = cvv[u];
+          const T2 a = in1[u];
+          T2 y = a;
+          y.x += cv.x;
+          y.y += cv.y;
+          v0[i] = y;
+          if (va.step.op != KOP_NONE)
+            acc = epilogue_terms<T2>(acc, y, a, va.step.w ? wv[u] : a,
+                                     va.step.mode);
+          break;
+        }
+        default:
+          break;
       }
-      case V_BICG_RO: {
-        const T2 r = v0[i];
-        acc.a.x += (double)r.x * r.x - (double)r.y * r.y;
-        acc.a.y += 2.0 * (double)r.x * r.y;
-        break;
-      }
-      case V_BICG_P:
-        v0[i] = va.first ? v1[i] : cadd(cmul(v0[i], beta), v1[i]);
-        break;
-      case V_BICG_XR:
-      case V_CGNR_XR: {
-        // v0 = x, v1 = p, v2 = A, v3 = r
-        v0[i] = cadd(cmul(v1[i], alpha), v0[i]);
-        const T2 r = cadd(cmul(v2[i], mAlpha), v3[i]);
-        v3[i] = r;
-        acc.n += (double)r.x * r.x + (double)r.y * r.y;
-        acc.a.x += (double)r.x * r.x - (double)r.y * r.y;
-        acc.a.y += 2.0 * (double)r.x * r.y;
-        break;
-      }
-      case V_CGNR_P:
-        v0[i] = cadd(cmul(v0[i], beta), v1[i]);
-        break;
-      case V_NORM: {
-        const T2 r = v0[i];
-        acc.n += (double)r.x * r.x + (double)r.y * r.y;
-        break;
-      }
-      case V_ADD_CONV: {
-        // result of a matvec whose convolution ran in FP32: y = x + conv
-        const float2 cv = reinterpret_cast<const float2*>(va.v[2])[off + i];
-        const T2 a = v1[i];
-        T2 y = a;
-        y.x += cv.x;
-        y.y += cv.y;
-        v0[i] = y;
-        if (va.step.op != KOP_NONE)
-          acc = epilogue_terms<T2>(acc, y, a, va.step.w ? reinterpret_cast<const T2*>(va.step.w)[off + i] : a,
-                                   va.step.mode);
-        break;
-      }
-      default:
-        break;
     }
   }
   if (va.step.op != KOP_NONE) {

@@ -448,7 +448,7 @@ template <typename T> void setup_engine(dda_ctx* c) {
   y.py = g.Gy + 1;
   const size_t fixed = ((size_t)g.Gz + g.Gy + (size_t)g.Gz * y.q) * s;
   const size_t row = (size_t)3 * y.py * s;
-  e.k = c->planned ? planned_kernels<T, kNtX, kNtYz, kNtC>(g.Gx, g.Gy, g.Gz)
+  e.k = c->planned ? planned_kernels<T, kNtX, kNtYz, kNtC>(g.Gx, g.Gy, g.Gz, g.by, g.bz)
                    : generic_kernels<T, kNtX, kNtYz, kNtC>();
   // row buffers: one per warp in the runtime-planned kernel, batches of up
   // to 32 rows in the planned one

@@ -40,9 +40,21 @@ inline bool has_tuned_plan(int n) {
   }
 }
 
-// Planned kernels for grid (gx, gy, gz), all edges tuned.
+// Fused plane kernel for y = z = N; the HALF variant when the box is exactly
+// half the grid in y and z and the first radix is even.
+template <typename T, int NTYZ, int N>
+typename MvKernels<T>::YzFn fused_kernel(bool half) {
+  typedef typename PlanFor<N>::type P;
+  if constexpr (P::r[0] % 2 == 0) {
+    if (half) return k_yz_p<T, NTYZ, P, P, true>;
+  }
+  return k_yz_p<T, NTYZ, P, P, false>;
+}
+
+// Planned kernels for grid (gx, gy, gz) and box extents by, bz, all edges
+// tuned.
 template <typename T, int NTX, int NTYZ, int NTC>
-MvKernels<T> planned_kernels(int gx, int gy, int gz) {
+MvKernels<T> planned_kernels(int gx, int gy, int gz, int by, int bz) {
   MvKernels<T> k;
   k.planned = true;
   switch (gx) {
@@ -72,7 +84,7 @@ MvKernels<T> planned_kernels(int gx, int gy, int gz) {
   if (gy == gz) {
     switch (gy) {
 #define C(N)                                                                                     \
-  case N: k.yz = k_yz_p<T, NTYZ, typename PlanFor<N>::type, typename PlanFor<N>::type>; break;
+  case N: k.yz = fused_kernel<T, NTYZ, N>(2 * by == gy && 2 * bz == gz); break;
       DDA_FUSED_LENGTHS(C)
 #undef C
       default: break;

@@ -65,7 +65,11 @@ inline std::vector<int> tuned_radices(int n) {
 
 
 // ---- z stage 0 fused with the plane read / write (whole CTA) -------------
-template <typename T, int NT, typename PZ>
+// HALF: the box is half the grid along the transformed axis (bz = Gz / 2,
+// first radix even), so inputs z = j + m S0 are zero exactly for m >= R / 2
+// and the inverse keeps exactly the outputs m < R / 2: with that known at
+// compile time the zero operands and the unused outputs fold away.
+template <typename T, int NT, typename PZ, bool HALF = false>
 __device__ __forceinline__ void zp_first(const typename C2<T>::t* __restrict__ plane, int soff, int q,
                                          int by, int bz, int twz) {
   typedef typename C2<T>::t T2;
@@ -79,7 +83,7 @@ __device__ __forceinline__ void zp_first(const typename C2<T>::t* __restrict__ p
 #pragma unroll
     for (int m = 0; m < R; m++) {
       const int z = j + m * S0;
-      v[m] = z < bz ? plane[c * nb + z * by + y] : czero<T2>();
+      v[m] = (HALF ? m < R / 2 : z < bz) ? plane[c * nb + z * by + y] : czero<T2>();
     }
     butterfly<PZ, 0, false>(v, j, sm + twz);
 #pragma unroll
@@ -88,7 +92,7 @@ __device__ __forceinline__ void zp_first(const typename C2<T>::t* __restrict__ p
   __syncthreads();
 }
 
-template <typename T, int NT, typename PZ>
+template <typename T, int NT, typename PZ, bool HALF = false>
 __device__ __forceinline__ void zp_last(typename C2<T>::t* __restrict__ plane, int soff, int q, int by,
                                         int bz, int twz) {
   typedef typename C2<T>::t T2;
@@ -105,7 +109,7 @@ __device__ __forceinline__ void zp_last(typename C2<T>::t* __restrict__ plane, i
 #pragma unroll
     for (int m = 0; m < R; m++) {
       const int z = j + m * S0;
-      if (z < bz) plane[c * nb + z * by + y] = v[m];
+      if (HALF ? m < R / 2 : z < bz) plane[c * nb + z * by + y] = v[m];
     }
   }
 }
@@ -191,7 +195,7 @@ __device__ __forceinline__ void row_stage0(typename C2<T>::t* S, int kz, int q, 
 // row r, component c lives in the row buffers at ro + (3 r + c) py.
 
 // y stage 0 fused with the read from (INV: write to) the slab, zero padded.
-template <typename T, int NT, typename PY, bool INV>
+template <typename T, int NT, typename PY, bool INV, bool HALF = false>
 __device__ __forceinline__ void rows_stage0(typename C2<T>::t* S, int kz0, int nr, int q, int by, int ro,
                                             int py, int twy) {
   typedef typename C2<T>::t T2;
@@ -208,7 +212,7 @@ __device__ __forceinline__ void rows_stage0(typename C2<T>::t* S, int kz0, int n
 #pragma unroll
       for (int m = 0; m < R; m++) {
         const int yy = j + m * S0;
-        v[m] = yy < by ? S[srow + yy] : czero<T2>();
+        v[m] = (HALF ? m < R / 2 : yy < by) ? S[srow + yy] : czero<T2>();
       }
       butterfly<PY, 0, false>(v, j, sm + twy);
 #pragma unroll
@@ -220,7 +224,7 @@ __device__ __forceinline__ void rows_stage0(typename C2<T>::t* S, int kz0, int n
 #pragma unroll
       for (int m = 0; m < R; m++) {
         const int yy = j + m * S0;
-        if (yy < by) S[srow + yy] = v[m];
+        if (HALF ? m < R / 2 : yy < by) S[srow + yy] = v[m];
       }
     }
   }
@@ -276,12 +280,13 @@ __device__ __forceinline__ void rows_dmul(int kz0, int nr, int ro, int py,
   __syncthreads();
 }
 
-template <typename T, int NT, typename PZ, typename PY>
+template <typename T, int NT, typename PZ, typename PY, bool HALF = false>
 __global__ void __launch_bounds__(NT, 1) k_yz_p(typename C2<T>::t* __restrict__ xhat,
                                              const typename C2<T>::t* __restrict__ dc, MvGeom g,
                                              YzGeom y, FftPlanDev pz, FftPlanDev pyp,
                                              const KrylovState* __restrict__ st, int mvskip) {
   static_assert(PY::K >= 2 && PZ::K >= 2, "tuned plans have at least two stages");
+  static_assert(!HALF || (PY::r[0] % 2 == 0 && PZ::r[0] % 2 == 0), "HALF needs an even first radix");
   typedef typename C2<T>::t T2;
   const int kx = blockIdx.x, b = blockIdx.y;  // kx: position after the x transform
   if (rhs_idle(st, b, mvskip)) return;
@@ -291,22 +296,22 @@ __global__ void __launch_bounds__(NT, 1) k_yz_p(typename C2<T>::t* __restrict__ 
   stage_twiddles<T, NT>(0, pz);
   stage_twiddles<T, NT>(g.Gz, pyp);
   __syncthreads();
-  zp_first<T, NT, PZ>(plane, soff, y.q, g.by, g.bz, 0);
+  zp_first<T, NT, PZ, HALF>(plane, soff, y.q, g.by, g.bz, 0);
   const int w3 = 3 * g.by;
   plines<T, PZ, NT, false, 1, PZ::K>(soff, w3, 1, y.q, 0);
   {
     const int kxf = g.fx[kx];
     for (int kz0 = 0; kz0 < g.Gz; kz0 += y.nrw) {  // kz: positions after the z transform
       const int nr = min(y.nrw, g.Gz - kz0);
-      rows_stage0<T, NT, PY, false>(S, kz0, nr, y.q, g.by, roff, y.py, g.Gz);
+      rows_stage0<T, NT, PY, false, HALF>(S, kz0, nr, y.q, g.by, roff, y.py, g.Gz);
       pstages<T, PY, false, NT, 1, PY::K - 1>(roff, 3 * nr, y.py, 1, g.Gz, threadIdx.x);
       rows_dmul<T, NT, PY, PZ>(kz0, nr, roff, y.py, dc, g, kxf);
       pstages<T, PY, true, NT, 1, PY::K - 1>(roff, 3 * nr, y.py, 1, g.Gz, threadIdx.x);
-      rows_stage0<T, NT, PY, true>(S, kz0, nr, y.q, g.by, roff, y.py, g.Gz);
+      rows_stage0<T, NT, PY, true, HALF>(S, kz0, nr, y.q, g.by, roff, y.py, g.Gz);
     }
   }
   plines<T, PZ, NT, true, 1, PZ::K>(soff, w3, 1, y.q, 0);
-  zp_last<T, NT, PZ>(plane, soff, y.q, g.by, g.bz, 0);
+  zp_last<T, NT, PZ, HALF>(plane, soff, y.q, g.by, g.bz, 0);
 }
 
 // Split path rows with a compile-time y plan: each warp one kz row, copied

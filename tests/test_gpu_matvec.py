@@ -153,6 +153,35 @@ def test_autotuned_layout_gives_identical_results(prec, shape):
     print(mvs[0].layout, mvs[1].layout)
 
 
+@pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("fp32", FP32_TOL)])
+def test_matvec_half_padded_box_matches_oracle(prec, tol):
+    # box 40 x 24 x 24 with holes on its own grid 80 x 48 x 48: y and z are
+    # exactly twice the box, so the fused plane kernel takes its variant with
+    # the zero half of the first FFT stage known at compile time
+    import dda_b200
+    from oracle import oracle as O
+    pos = np.array([(x, y, z) for z in range(24) for y in range(24) for x in range(40)
+                    if (x * 5 + y * 3 + z) % 13 or (x, y, z) in ((39, 23, 23), (0, 0, 0))], dtype=np.uint32)
+    mat = (pos[:, 1] % 2).astype(np.uint8)
+    mats = [1.4 + 0.2j, 1.7 + 0.05j]
+    g = dda_b200.Geometry.from_arrays(pos, mat, "0.05um")
+    p = dda_b200.DDAParams(g, mats, "0.8um")
+    assert p.grid == (80, 48, 48) and p.box == (40, 24, 24)
+    mv = dda_b200.CudaMatVec(p, prec)
+    assert mv.layout["yz_path"] == "fused" and mv.layout["compile_time_plans"] == 1
+    og = O.Geometry.from_arrays(pos, mat, "0.05um")
+    op = O.Problem(og, mats, "0.8um")
+    op.build_dmatrix()
+    mv.set_couple_constants(dda_b200.CoupleConstants(p, (0, 0.6, 0.8), 1, "ldr"))
+    op.set_cc((0, 0.6, 0.8), 1, "ldr")
+    rng = np.random.default_rng(11)
+    x = rng.uniform(-1, 1, p.vec_size) + 1j * rng.uniform(-1, 1, p.vec_size)
+    for c in range(3):
+        x[c * p.nvs + p.nv:(c + 1) * p.nvs] = 0
+    assert rel(mv.apply(x), op.matvec(x)) < tol
+    mv.close()
+
+
 def test_x_tile_fills_whole_waves():
     # the x-pass tile is chosen by the count of CTA waves: for the 250 000
     # dipole box (2 500 grid lines, grid x 200) with two right-hand sides in

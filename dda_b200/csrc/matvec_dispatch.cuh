@@ -51,6 +51,16 @@ typename MvKernels<T>::YzFn fused_kernel(bool half) {
   return k_yz_p<T, NTYZ, P, P, false>;
 }
 
+// Cluster plane kernel for y = z = N, likewise.
+template <typename T, int NTYZ, int N>
+typename MvKernels<T>::SlotFn slot_kernel(bool half) {
+  typedef typename PlanFor<N>::type P;
+  if constexpr (P::r[0] % 2 == 0) {
+    if (half) return k_yz_slot<T, NTYZ, P, P, true>;
+  }
+  return k_yz_slot<T, NTYZ, P, P, false>;
+}
+
 // Planned kernels for grid (gx, gy, gz) and box extents by, bz, all edges
 // tuned.
 template <typename T, int NTX, int NTYZ, int NTC>
@@ -91,7 +101,7 @@ MvKernels<T> planned_kernels(int gx, int gy, int gz, int by, int bz) {
     }
     switch (gy) {
 #define C(N)                                                                                        \
-  case N: k.slot = k_yz_slot<T, NTYZ, typename PlanFor<N>::type, typename PlanFor<N>::type>; break;
+  case N: k.slot = slot_kernel<T, NTYZ, N>(2 * by == gy && 2 * bz == gz); break;
       DDA_TUNED_LENGTHS(C)
 #undef C
       default: break;

@@ -57,8 +57,17 @@ __host__ inline size_t slot_smem_bytes(const MvGeom& g, int nrw) {
   return ((size_t)g.Gz + g.Gy + std::max(tile, rows)) * s;
 }
 
+// HALF (planned plans only): the box is half the grid in y and z and the first
+// radices are even, so stage-0 input m is zero padding exactly for m >= R / 2
+// and the inverse keeps exactly the outputs m < R / 2 (as in k_yz_p).
+template <typename P>
+__host__ __device__ constexpr bool even_first_radix() {
+  if constexpr (std::is_void<P>::value) return false;
+  else return P::r[0] % 2 == 0;
+}
+
 // ---- phase Z: column tile [c0, c0+tc) of the plane -------------------------
-template <typename T, int NT, typename PZ>
+template <typename T, int NT, typename PZ, bool HALF = false>
 __device__ __forceinline__ void slot_cols_fwd(const typename C2<T>::t* __restrict__ plane,
                                               typename C2<T>::t* __restrict__ slot, const MvGeom& g,
                                               const SlotGeom& sg, const FftPlanDev& pz, int c0) {
@@ -104,7 +113,7 @@ __device__ __forceinline__ void slot_cols_fwd(const typename C2<T>::t* __restric
 #pragma unroll
         for (int m = 0; m < R; m++) {
           const int z = j + m * S0;
-          v[u][m] = (live && z < g.bz) ? plane[c * nb + z * g.by + y] : czero<T2>();
+          v[u][m] = (live && (HALF ? m < R / 2 : z < g.bz)) ? plane[c * nb + z * g.by + y] : czero<T2>();
         }
       }
 #pragma unroll
@@ -129,7 +138,7 @@ __device__ __forceinline__ void slot_cols_fwd(const typename C2<T>::t* __restric
 }
 
 // ---- phase Z': inverse of the same column tile -----------------------------
-template <typename T, int NT, typename PZ>
+template <typename T, int NT, typename PZ, bool HALF = false>
 __device__ __forceinline__ void slot_cols_inv(typename C2<T>::t* __restrict__ plane,
                                               const typename C2<T>::t* __restrict__ slot, const MvGeom& g,
                                               const SlotGeom& sg, const FftPlanDev& pz, int c0) {
@@ -178,7 +187,7 @@ __device__ __forceinline__ void slot_cols_inv(typename C2<T>::t* __restrict__ pl
 #pragma unroll
         for (int m = 0; m < R; m++) {
           const int z = j + m * S0;
-          if (z < g.bz) plane[c * nb + z * g.by + y] = v[m];
+          if (HALF ? m < R / 2 : z < g.bz) plane[c * nb + z * g.by + y] = v[m];
         }
       }
     }
@@ -189,7 +198,7 @@ __device__ __forceinline__ void slot_cols_inv(typename C2<T>::t* __restrict__ pl
 // ---- phase Y: kz rows [kz0, kz0+nr) -----------------------------------------
 // Planned: y stage 0 fused with the slot read / write, the last forward
 // stage, D-hat and the first inverse stage in registers (rows_dmul).
-template <typename T, int NT, typename PY, bool INV>
+template <typename T, int NT, typename PY, bool INV, bool HALF = false>
 __device__ __forceinline__ void slot_rows_stage0(typename C2<T>::t* __restrict__ slot, const MvGeom& g,
                                                  const SlotGeom& sg, int kz0, int nr, int ro) {
   typedef typename C2<T>::t T2;
@@ -209,7 +218,7 @@ __device__ __forceinline__ void slot_rows_stage0(typename C2<T>::t* __restrict__
 #pragma unroll
         for (int m = 0; m < R; m++) {
           const int yy = j + m * S0;
-          v[u][m] = (it < total && yy < g.by) ? __ldcg(srow + yy) : czero<T2>();
+          v[u][m] = (it < total && (HALF ? m < R / 2 : yy < g.by)) ? __ldcg(srow + yy) : czero<T2>();
         }
       }
 #pragma unroll
@@ -236,14 +245,14 @@ __device__ __forceinline__ void slot_rows_stage0(typename C2<T>::t* __restrict__
 #pragma unroll
       for (int m = 0; m < R; m++) {
         const int yy = j + m * S0;
-        if (yy < g.by) __stcg(srow + yy, v[m]);
+        if (HALF ? m < R / 2 : yy < g.by) __stcg(srow + yy, v[m]);
       }
     }
   }
   __syncthreads();
 }
 
-template <typename T, int NT, typename PY, typename PZ>
+template <typename T, int NT, typename PY, typename PZ, bool HALF = false>
 __device__ __forceinline__ void slot_rows(typename C2<T>::t* __restrict__ slot,
                                           const typename C2<T>::t* __restrict__ dc, const MvGeom& g,
                                           const SlotGeom& sg, const FftPlanDev& pyp, int kxf, int kz0, int nr) {
@@ -282,11 +291,11 @@ __device__ __forceinline__ void slot_rows(typename C2<T>::t* __restrict__ slot,
     }
     __syncthreads();
   } else {
-    slot_rows_stage0<T, NT, PY, false>(slot, g, sg, kz0, nr, ro);
+    slot_rows_stage0<T, NT, PY, false, HALF>(slot, g, sg, kz0, nr, ro);
     pstages<T, PY, false, NT, 1, PY::K - 1>(ro, 3 * nr, sg.py, 1, g.Gz, threadIdx.x);
     rows_dmul<T, NT, PY, PZ>(kz0, nr, ro, sg.py, dc, g, kxf);
     pstages<T, PY, true, NT, 1, PY::K - 1>(ro, 3 * nr, sg.py, 1, g.Gz, threadIdx.x);
-    slot_rows_stage0<T, NT, PY, true>(slot, g, sg, kz0, nr, ro);
+    slot_rows_stage0<T, NT, PY, true, HALF>(slot, g, sg, kz0, nr, ro);
   }
 }
 
@@ -294,7 +303,7 @@ __device__ __forceinline__ void slot_rows(typename C2<T>::t* __restrict__ slot,
 // pairs, item i = (order[i / nrhs], i % nrhs): `order` lists the kx
 // positions so that the two planes sharing a D-hat octant plane (kx and
 // -kx) come together.  slots: one [Gz][wp] buffer per cluster.
-template <typename T, int NT, typename PZ, typename PY>
+template <typename T, int NT, typename PZ, typename PY, bool HALF = false>
 __global__ void __launch_bounds__(NT, 1) k_yz_slot(typename C2<T>::t* __restrict__ xhat,
                                                 const typename C2<T>::t* __restrict__ dc, MvGeom g,
                                                 SlotGeom sg, const uint32_t* __restrict__ order, int nrhs,
@@ -303,6 +312,8 @@ __global__ void __launch_bounds__(NT, 1) k_yz_slot(typename C2<T>::t* __restrict
                                                 int mvskip) {
   typedef typename C2<T>::t T2;
   static_assert(std::is_void<PZ>::value == std::is_void<PY>::value, "both axes planned or neither");
+  static_assert(!HALF || (even_first_radix<PZ>() && even_first_radix<PY>()),
+                "HALF needs planned axes with an even first radix");
   namespace cg = cooperative_groups;
   cg::cluster_group cluster = cg::this_cluster();
   const int cl = (int)cluster.num_blocks();
@@ -321,15 +332,15 @@ __global__ void __launch_bounds__(NT, 1) k_yz_slot(typename C2<T>::t* __restrict
     const int kx = (int)order[it / nrhs], b = it % nrhs;
     if (rhs_idle(st, b, mvskip)) continue;  // the same for every CTA of the cluster
     T2* plane = xhat + ((size_t)b * g.Gx + kx) * 3 * g.nlines;
-    for (int ch = rank; ch < nchunks; ch += cl) slot_cols_fwd<T, NT, PZ>(plane, slot, g, sg, pz, ch * TC);
+    for (int ch = rank; ch < nchunks; ch += cl) slot_cols_fwd<T, NT, PZ, HALF>(plane, slot, g, sg, pz, ch * TC);
     cluster.sync();
     const int kxf = g.fx[kx];
     for (int bt = rank; bt < nbatches; bt += cl) {
       const int kz0 = bt * sg.nrw;
-      slot_rows<T, NT, PY, PZ>(slot, dc, g, sg, pyp, kxf, kz0, min(sg.nrw, g.Gz - kz0));
+      slot_rows<T, NT, PY, PZ, HALF>(slot, dc, g, sg, pyp, kxf, kz0, min(sg.nrw, g.Gz - kz0));
     }
     cluster.sync();
-    for (int ch = rank; ch < nchunks; ch += cl) slot_cols_inv<T, NT, PZ>(plane, slot, g, sg, pz, ch * TC);
+    for (int ch = rank; ch < nchunks; ch += cl) slot_cols_inv<T, NT, PZ, HALF>(plane, slot, g, sg, pz, ch * TC);
   }
 }
 

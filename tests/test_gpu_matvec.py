@@ -154,10 +154,12 @@ def test_autotuned_layout_gives_identical_results(prec, shape):
 
 
 @pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("fp32", FP32_TOL)])
-def test_matvec_half_padded_box_matches_oracle(prec, tol):
+@pytest.mark.parametrize("flags,path", [(0, "fused"), (4, "cluster")])
+def test_matvec_half_padded_box_matches_oracle(prec, tol, flags, path):
     # box 40 x 24 x 24 with holes on its own grid 80 x 48 x 48: y and z are
-    # exactly twice the box, so the fused plane kernel takes its variant with
-    # the zero half of the first FFT stage known at compile time
+    # exactly twice the box, so the fused and the cluster plane kernels take
+    # their variants with the zero half of the first FFT stage known at
+    # compile time
     import dda_b200
     from oracle import oracle as O
     pos = np.array([(x, y, z) for z in range(24) for y in range(24) for x in range(40)
@@ -167,8 +169,8 @@ def test_matvec_half_padded_box_matches_oracle(prec, tol):
     g = dda_b200.Geometry.from_arrays(pos, mat, "0.05um")
     p = dda_b200.DDAParams(g, mats, "0.8um")
     assert p.grid == (80, 48, 48) and p.box == (40, 24, 24)
-    mv = dda_b200.CudaMatVec(p, prec)
-    assert mv.layout["yz_path"] == "fused" and mv.layout["compile_time_plans"] == 1
+    mv = dda_b200.CudaMatVec(p, prec, flags=flags)
+    assert mv.layout["yz_path"] == path and mv.layout["compile_time_plans"] == 1
     og = O.Geometry.from_arrays(pos, mat, "0.05um")
     op = O.Problem(og, mats, "0.8um")
     op.build_dmatrix()

@@ -147,7 +147,9 @@ int dda_matvec_host(dda_ctx* ctx, const double* arg, double* res, int conj, int 
  * max_iter <= 0 means unlimited.  history (may be NULL) receives the
  * per-iteration relative residuals (the RE_ lines), history_cap per rhs.
  * stats (may be NULL) receives nrhs records.  Returns the first non-zero
- * per-rhs status.  Replaces IterativeSolverBase<T>::getPolVec
+ * per-rhs status.  An FP32 context copies the FP64 host vectors as they are
+ * and rounds them on the device; from pinned host memory both copies are
+ * plain DMA.  Replaces IterativeSolverBase<T>::getPolVec
  * (DDA/IterativeSolverBase.hpp:59) with the GPU solver classes
  * (DDA/GpuIterativeSolver.hpp, DDA/Gpu{QmrCs,BicgStab,BicgCs,Cgnr}.hpp). */
 int dda_solve(dda_ctx* ctx, int solver, int nrhs, const double* einc, double eps,

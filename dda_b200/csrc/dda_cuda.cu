@@ -30,6 +30,7 @@
 #include "dmatrix_kernels.cuh"
 #include "farfield_kernels.cuh"
 #include "fft_engine.cuh"
+#include "kernel_shapes.cuh"
 #include "krylov_kernels.cuh"
 #include "krylov_ops.cuh"
 #include "matvec_kernels.cuh"
@@ -56,15 +57,8 @@ struct DdaError : std::runtime_error {
                      std::string(#call) + ": " + cudaGetErrorString(e_));                 \
   } while (0)
 
-// Kernel shapes (threads per CTA).
-constexpr int kNtX = 256;   // k_xfwd / k_xinv
-// k_yz / k_yrows: 512 threads in FP32; 256 in FP64, whose FFT stages need
-// more than the 128 registers a 512-thread CTA leaves per thread.
-template <typename T> struct NtYz;
-template <> struct NtYz<float> { static constexpr int v = 512; };
-template <> struct NtYz<double> { static constexpr int v = 256; };
+// Kernel shapes (threads per CTA): kNtX, NtYz, kNtC in kernel_shapes.cuh.
 #define kNtYz NtYz<T>::v
-constexpr int kNtC = 256;   // k_fft_cols / k_fft_rows
 constexpr int kNtV = 256;                 // k_vec
 constexpr int kVecPartsMax = 8 * 148;     // k_vec CTAs per right-hand side, at most
 constexpr size_t kSmemMax = 227 * 1024;
@@ -448,8 +442,7 @@ template <typename T> void setup_engine(dda_ctx* c) {
   y.py = g.Gy + 1;
   const size_t fixed = ((size_t)g.Gz + g.Gy + (size_t)g.Gz * y.q) * s;
   const size_t row = (size_t)3 * y.py * s;
-  e.k = c->planned ? planned_kernels<T, kNtX, kNtYz, kNtC>(g.Gx, g.Gy, g.Gz, g.by, g.bz)
-                   : generic_kernels<T, kNtX, kNtYz, kNtC>();
+  e.k = select_kernels<T>(c->planned, g.Gx, g.Gy, g.Gz, g.by, g.bz);
   // row buffers: one per warp in the runtime-planned kernel, batches of up
   // to 32 rows in the planned one
   int nrw = c->planned ? 32 : NW;

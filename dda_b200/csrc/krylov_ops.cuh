@@ -208,7 +208,7 @@ __device__ __forceinline__ void bicg_start(KrylovState& s, double2 ro) {
   if (s.count > 0) s.beta = ddivc(s.ro_new, s.ro_old);
 }
 
-__device__ void krylov_finalize(KrylovState& s, const KrylovStep& step, const RedSums& t) {
+static __device__ void krylov_finalize(KrylovState& s, const KrylovStep& step, const RedSums& t) {
   switch (step.op) {
     case KOP_INIT_PVEC:
       s.temp = t.n;

@@ -61,12 +61,13 @@ typename MvKernels<T>::SlotFn slot_kernel(bool half) {
   return k_yz_slot<T, NTYZ, P, P, false>;
 }
 
-// Planned kernels for grid (gx, gy, gz) and box extents by, bz, all edges
-// tuned.
-template <typename T, int NTX, int NTYZ, int NTC>
-MvKernels<T> planned_kernels(int gx, int gy, int gz, int by, int bz) {
-  MvKernels<T> k;
-  k.planned = true;
+// The kernel tables are filled in parts, each compiled in its own
+// translation unit (mv_inst.cu, built once per part and precision) so the
+// several hundred plan instantiations compile in parallel.  Part 0: x passes;
+// 1: split path (y rows, z columns) and the runtime-planned kernels; 2: fused
+// plane kernels; 3: cluster plane kernels.
+template <typename T, int NTX>
+void planned_x(MvKernels<T>& k, int gx) {
   switch (gx) {
 #define C(N)                                                           \
   case N:                                                              \
@@ -77,6 +78,10 @@ MvKernels<T> planned_kernels(int gx, int gy, int gz, int by, int bz) {
 #undef C
     default: break;
   }
+}
+
+template <typename T, int NTYZ, int NTC>
+void planned_split(MvKernels<T>& k, int gy, int gz) {
   switch (gy) {
 #define C(N)                                                           \
   case N: k.yrows = k_yrows_p<T, NTYZ, typename PlanFor<N>::type>; break;
@@ -91,34 +96,67 @@ MvKernels<T> planned_kernels(int gx, int gy, int gz, int by, int bz) {
 #undef C
     default: break;
   }
-  if (gy == gz) {
-    switch (gy) {
+}
+
+template <typename T, int NTYZ>
+void planned_fused(MvKernels<T>& k, int gy, int gz, int by, int bz) {
+  if (gy != gz) return;
+  switch (gy) {
 #define C(N)                                                                                     \
   case N: k.yz = fused_kernel<T, NTYZ, N>(2 * by == gy && 2 * bz == gz); break;
-      DDA_FUSED_LENGTHS(C)
+    DDA_FUSED_LENGTHS(C)
 #undef C
-      default: break;
-    }
-    switch (gy) {
+    default: break;
+  }
+}
+
+template <typename T, int NTYZ>
+void planned_slot(MvKernels<T>& k, int gy, int gz, int by, int bz) {
+  if (gy != gz) return;
+  switch (gy) {
 #define C(N)                                                                                        \
   case N: k.slot = slot_kernel<T, NTYZ, N>(2 * by == gy && 2 * bz == gz); break;
-      DDA_TUNED_LENGTHS(C)
+    DDA_TUNED_LENGTHS(C)
 #undef C
-      default: break;
-    }
+    default: break;
   }
-  return k;
 }
 
 template <typename T, int NTX, int NTYZ, int NTC>
-MvKernels<T> generic_kernels() {
-  MvKernels<T> k;
+void generic_kernels(MvKernels<T>& k) {
   k.xfwd = k_xfwd<T, NTX>;
   k.xinv = k_xinv<T, NTX>;
   k.yz = k_yz<T, NTYZ>;
   k.yrows = k_yrows<T, NTYZ>;
   k.cols = k_fft_cols<T, NTC>;
   k.slot = k_yz_slot<T, NTYZ, void, void>;
+}
+
+// Entry points of the parts (defined in mv_inst.cu).
+void mv_part_x(MvKernels<float>& k, int gx);
+void mv_part_x(MvKernels<double>& k, int gx);
+void mv_part_split(MvKernels<float>& k, int gy, int gz, bool generic);
+void mv_part_split(MvKernels<double>& k, int gy, int gz, bool generic);
+void mv_part_fused(MvKernels<float>& k, int gy, int gz, int by, int bz);
+void mv_part_fused(MvKernels<double>& k, int gy, int gz, int by, int bz);
+void mv_part_slot(MvKernels<float>& k, int gy, int gz, int by, int bz);
+void mv_part_slot(MvKernels<double>& k, int gy, int gz, int by, int bz);
+
+// Kernel table of a context: compile-time-planned kernels for grid
+// (gx, gy, gz) and box extents by, bz when every edge is tuned, the
+// runtime-planned ones otherwise.
+template <typename T>
+MvKernels<T> select_kernels(bool planned, int gx, int gy, int gz, int by, int bz) {
+  MvKernels<T> k;
+  k.planned = planned;
+  if (!planned) {
+    mv_part_split(k, gy, gz, true);
+    return k;
+  }
+  mv_part_x(k, gx);
+  mv_part_split(k, gy, gz, false);
+  mv_part_fused(k, gy, gz, by, bz);
+  mv_part_slot(k, gy, gz, by, bz);
   return k;
 }
 

@@ -13,6 +13,8 @@
 //   the inverse z stages end with stage 0 writing z < bz to HBM.
 #pragma once
 
+#include <vector>
+
 #include "fft_plan.cuh"
 #include "matvec_kernels.cuh"
 

@@ -83,7 +83,7 @@ struct RedTarget {
 // thread of the CTA that completes the set; `total` (thread 0) then holds the
 // fixed-order sum of all slots and the ticket is reset for the next use.
 template <int NT>
-__device__ bool block_finish(RedSums v, const RedTarget& t, int rhs, int part, RedSums& total) {
+static __device__ bool block_finish(RedSums v, const RedTarget& t, int rhs, int part, RedSums& total) {
   __shared__ bool last;
   v = block_reduce<NT>(v);
   if (threadIdx.x == 0) {

@@ -67,8 +67,9 @@ def build(force=False, verbose=False, jobs=None):
     if cxx:
         base += ["-ccbin", cxx]
     cmds = []
+    headers = [d for d in deps if not d.endswith((".cu", ".cpp"))]
     for src, obj, extra in _units():
-        if force or _stale(obj, deps):
+        if force or _stale(obj, headers + [src]):
             cmds.append(base + extra + ["-c", src, "-o", obj + ".tmp"])
     def run(cmd):
         if verbose:

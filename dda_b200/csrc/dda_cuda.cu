@@ -941,7 +941,46 @@ struct SolveOpts {
   long long max_res_increase = 0;  // > 0: stagnation limit instead of the solver's
   long long rate_window = 0;       // > 0: stop when |r| does not halve in this many iterations
   bool mv32 = false;               // FP64 solve with the matvec convolution in FP32
+  // MIXED inner solves (mv32): every check_every iterations the FP64
+  // residual of the current iterate, |B - A x|^2 with the full FP64 matvec,
+  // is compared with the recurrence's |r|^2.  A right-hand side ends when
+  // the FP64 residual is below check_abs[r] (the outer target) or more than
+  // kGapRatio times the recurrence's: the FP32 convolution's rounding has
+  // then become the larger part of the true residual, and only a new
+  // correction from the FP64 residual (the outer step) reduces it further.
+  long long check_every = 0;
+  const double* check_abs = nullptr;
 };
+
+constexpr double kGapRatio = 4.0;  // |r_true|^2 > 4 |r_rec|^2: the gap dominates
+
+// The FP64 check of a MIXED inner solve (SolveOpts::check_every): T = B - A x
+// with the full FP64 matvec into `tmp`, |T|^2 into the outer state's `last`;
+// right-hand sides that met the outer target or whose true residual is
+// dominated by the FP32 rounding gap are marked done.  Returns true when
+// every right-hand side is done.
+bool check_gap(dda_ctx* c, int nrhs, double2* X, double2* B, double2* tmp, const SolveOpts& o) {
+  Solve<double> sc(c, nrhs, c->st_outer);
+  sc.mv(X, tmp, 0, sc.step(KOP_NONE));
+  sc.vec(V_R_INIT, 0, {tmp, tmp, B}, sc.step(KOP_NORM));
+  CK(cudaMemcpyAsync(c->sto_host, c->st_outer, nrhs * sizeof(KrylovState), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  bool changed = false, all = true;
+  for (int r = 0; r < nrhs; r++) {
+    KrylovState& k = c->st_host[r];
+    if (!k.done && !c->sto_host[r].done) {
+      const double t = c->sto_host[r].last;
+      if (t < o.check_abs[r] || t > kGapRatio * k.last || !(t == t)) {
+        k.done = 1;
+        changed = true;
+      }
+    }
+    all = all && k.done;
+  }
+  if (changed)
+    CK(cudaMemcpyAsync(c->st, c->st_host, nrhs * sizeof(KrylovState), cudaMemcpyHostToDevice, c->stream));
+  return all;
+}
 
 // Runs one solve of `nrhs` right-hand sides already set up in the engine
 // vectors (E = einc or B = b, S = start).  Per-rhs states end in c->st_host;
@@ -1025,6 +1064,9 @@ void run_solve(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
     bool all = true;
     for (int r = 0; r < nrhs; r++) all = all && c->st_host[r].done;
     if (all) break;
+    if constexpr (std::is_same<T, double>::value) {
+      if (o.check_every > 0 && nr % o.check_every == 0 && check_gap(c, nrhs, b.X, B, S, o)) break;
+    }
   }
   if (b.X != e.vec[4])
     CK(cudaMemcpyAsync(e.vec[4], b.X, (size_t)nrhs * 3 * c->g.nvs * sizeof(T2), cudaMemcpyDeviceToDevice, c->stream));
@@ -1032,11 +1074,9 @@ void run_solve(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
   if (o.result) sv.vec(V_RESULT, 0, {e.io, e.vec[4]}, KrylovStep{KOP_NONE, 0, nullptr, {}});
 }
 
-// Mixed precision: FP32 inner solves of A e = r corrected by FP64 residuals
-// r = b - A x until |r| < eps |b| in FP64.  Each inner solve aims at the
-// residual reduction still needed (at least 1e-4 per step, the FP32 floor
-// kept well above single-precision rounding).  Per-rhs totals are returned
-// in out[] (iterations, refinements, status, best relative residual).
+// Mixed precision: inner solves of A e = r corrected by FP64 residuals
+// r = b - A x until |r| < eps |b| in FP64.  Per-rhs totals are returned in
+// out[] (iterations, refinements, status, best relative residual).
 struct MixedOut {
   long long iterations = 0, refinements = 0;
   int status = 0;
@@ -1059,18 +1099,23 @@ void run_mixed(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
   if (start) sd.vec(V_START_X, 0, {X, S}, KrylovStep{KOP_NONE, 0, nullptr, {}});
   else CK(cudaMemsetAsync(X, 0, n * sizeof(double2), c->stream));
   std::vector<char> done(nrhs, 0);
-  std::vector<double> eps_in(nrhs, 1e-4);
-  // Each inner solve is an FP64 Krylov solve of A e = r whose matvec runs
-  // the convolution in FP32 (Solve::matvec_any); it aims at half the
-  // remaining reduction and ends early when its residual has not reached a
-  // new minimum for kInnerStall iterations: the FP32 convolution breaks the
-  // complex symmetry of A at the 1e-7 level, which stalls QMR-CS on
-  // ill-conditioned targets, and the restart from the FP64 residual recovers
-  // it.  A right-hand side whose FP64 residual does not
-  // halve over kOuterStall outer steps in a row leaves the refinement with
-  // DDA_ERR_NOPROGRESS, and mixed_fallback finishes it with the FP64 solver.
+  std::vector<double> eps_in(nrhs, 1e-4), thr(nrhs, 0.0);
+  // Each inner solve is an FP64 Krylov solve of A e = r (FP64 vectors,
+  // scalars and dot products) whose matvec runs the convolution in FP32
+  // (Solve::matvec_any).  It keeps one Krylov space for as long as that
+  // helps: it aims at the final target and is checked against the FP64
+  // residual every kCheckEvery iterations (check_gap).  It ends when the
+  // FP64 residual meets the target, or when the residual the recurrences
+  // track has fallen well below the true one: the FP32 convolution's
+  // rounding, carried by every Krylov vector, then dominates, and the next
+  // outer step removes it from a new FP64 residual.  Plateaus of the
+  // recurrence (QMR-CS stagnates for hundreds of iterations on large,
+  // high-index targets) do not end it.  A right-hand side whose FP64
+  // residual does not halve over kOuterStall outer steps in a row leaves the
+  // refinement with DDA_ERR_NOPROGRESS, and mixed_fallback finishes it with
+  // the FP64 solver.
   const int max_outer = 60;
-  const long long kInnerStall = 200;
+  const long long kCheckEvery = 64;
   const int kOuterStall = 2;
   std::vector<double> prev_rel(nrhs, 0.0);
   std::vector<int> stalls(nrhs, 0);
@@ -1104,6 +1149,7 @@ void run_mixed(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
       // own rounding times the condition number, which the next outer step
       // removes
       eps_in[r] = std::min(0.1, std::max(1e-7, 0.5 * eps / rel));
+      thr[r] = 0.81 * eps * eps / k.residScale;  // (0.9 eps |b|)^2
       all = all && done[r];
     }
     if (all) break;
@@ -1113,8 +1159,9 @@ void run_mixed(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
     o.eps_rhs = eps_in.data();
     o.skip = done.data();
     o.result = false;
-    o.max_res_increase = kInnerStall;
     o.mv32 = true;
+    o.check_every = kCheckEvery;
+    o.check_abs = thr.data();
     run_solve<double>(c, solver, nrhs, 0.0, max_iter > 0 ? max_iter - total_it : 0, o);
     for (int r = 0; r < nrhs; r++) {
       if (done[r]) continue;

@@ -1,8 +1,9 @@
 """Runs the oracle's BiCGStab solve of the box workload (10 x 5 x 5 um box,
 d = 0.1 um, m = 1.5+0.1i, lambda = 6 um, propagation (0,1,0), LDR, relative
 residual 1e-5) for both polarisations and records the iteration counts and
-residual histories in cfg2_oracle_bicgstab.json.  bench.py's reference arm
-scales its bounded per-iteration CPU sample by these counts."""
+residual histories in cfg2_oracle_bicgstab.json.  The GPU tests compare the
+library's FP64 solve of the same workload with these counts and histories
+(tests/test_gpu_configs.py)."""
 import json
 import os
 import sys

@@ -13,7 +13,7 @@ POLARIZABILITIES = {"cm": 0, "ldr": 1, "ldr-avgpol": 2}
 GRID_POLICIES = {"reference": 0, "tuned": 1}
 ERRORS = {-1: "invalid argument", -2: "CUDA failure", -3: "out of device memory",
           -4: "unsupported size", -5: "Krylov breakdown", -6: "Too many iterations",
-          -7: "Too many iterations w/o increase"}
+          -7: "Too many iterations w/o increase", -8: "cancelled"}
 
 
 class DDAError(RuntimeError):
@@ -69,6 +69,7 @@ def lib():
         "dda_solve_device": ([vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_double, ctypes.c_int64, vp, vp,
                               ctypes.POINTER(Stats)], ctypes.c_int),
         "dda_stream": ([vp], vp),
+        "dda_cancel": ([vp], ctypes.c_int),
         "dda_launch_count": ([vp], ctypes.c_int64),
         "dda_matvec_layout": ([vp, ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
         "dda_profile_matvec": ([vp, ctypes.c_int, ctypes.c_int, dp], ctypes.c_int),
@@ -351,6 +352,11 @@ class CudaMatVec:
         out = np.zeros((len(d), nrhs, 3), dtype=np.complex128)
         self._check(lib().dda_far_field_noalloc(self.h, nrhs, len(d), _dp(d), _dp(out.view(np.float64))))
         return out
+
+    def cancel(self):
+        """dda_cancel: the solve running on this context (in another thread)
+        stops after its current round and raises DDAError code -8."""
+        self._check(lib().dda_cancel(self.h))
 
     @property
     def stream(self):

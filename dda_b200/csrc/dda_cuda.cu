@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <cstring>
 #include <array>
+#include <atomic>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -221,6 +222,7 @@ template <typename T> struct Engine {
 };
 
 struct dda_ctx {
+  std::atomic<int> cancel{0};  // dda_cancel: the running (or next) solve stops at its next round
   int device = 0;
   int precision = DDA_PREC_FP64;
   int max_rhs = 1;
@@ -950,9 +952,50 @@ struct SolveOpts {
   // correction from the FP64 residual (the outer step) reduces it further.
   long long check_every = 0;
   const double* check_abs = nullptr;
+  bool adapt = false;              // mv32 solve that switches the convolution precision (MixedSwitch)
 };
 
 constexpr double kGapRatio = 4.0;  // |r_true|^2 > 4 |r_rec|^2: the gap dominates
+
+// Precision of the convolution in an adaptive MIXED inner solve
+// (SolveOpts::adapt), decided between rounds from the recurrence residuals.
+struct MixedSwitch {
+  bool start32 = false, mode32 = false;
+  double tau = 1e-3;        // FP64 -> FP32 when every running rhs is below tau
+  long long window = 256;   // FP32 iterations over which the residual must halve
+  long long mark_it = 0;
+  double mark = 0;
+  explicit MixedSwitch(const SolveOpts& o) {
+    if (const char* v = getenv("DDA_MX_TAU")) tau = atof(v);
+    if (const char* v = getenv("DDA_MX_W")) window = atoll(v);
+    if (const char* v = getenv("DDA_MX_START")) start32 = atoi(v) != 0;
+    (void)o;
+    mode32 = start32;
+  }
+  bool update(const KrylovState* st, int nrhs, long long nr) {
+    double worst = 0;
+    for (int r = 0; r < nrhs; r++)
+      if (!st[r].done) worst = std::max(worst, std::sqrt(st[r].inprodR * st[r].residScale));
+    if (!mode32) {
+      if (worst < tau) {
+        mode32 = true;
+        mark_it = nr;
+        mark = worst;
+        if (getenv("DDA_MX_LOG")) fprintf(stderr, "mx: -> fp32 at %lld rel %.3e\n", nr, worst);
+      }
+    } else if (nr - mark_it >= window) {
+      if (worst > 0.5 * mark) {  // stalled: FP64 until one more decade is gained
+        mode32 = false;
+        tau = 0.1 * worst;
+        if (getenv("DDA_MX_LOG")) fprintf(stderr, "mx: -> fp64 at %lld rel %.3e\n", nr, worst);
+      } else {
+        mark_it = nr;
+        mark = worst;
+      }
+    }
+    return mode32;
+  }
+};
 
 // The FP64 check of a MIXED inner solve (SolveOpts::check_every): T = B - A x
 // with the full FP64 matvec into `tmp`, |T|^2 into the outer state's `last`;
@@ -1013,7 +1056,15 @@ void run_solve(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
     KrylovState& k = c->st_host[r];
     const double er = o.eps_rhs ? o.eps_rhs[r] : eps;
     k.epsB = er * er / k.residScale;
-    if (!(k.inprodR >= k.epsB)) k.done = 1;  // already converged: no iteration
+    if (k.done) continue;
+    if (!std::isfinite(k.temp) || !std::isfinite(k.inprodR)) {  // NaN or Inf in Einc, sqrt(cc) or start
+      k.done = 1;
+      k.status = DDA_ERR_ARG;
+    } else if (k.temp == 0) {  // b = 0: x = 0 is the solution
+      k.done = 1;
+    } else if (!(k.inprodR >= k.epsB)) {
+      k.done = 1;  // already converged: no iteration
+    }
   }
   CK(cudaMemcpyAsync(c->st, c->st_host, nrhs * sizeof(KrylovState), cudaMemcpyHostToDevice, c->stream));
   sv.solver_init(solver, b);
@@ -1027,15 +1078,24 @@ void run_solve(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
   // the kernels read their scalars and done flags from the device state.
   const int poll = 8;
   const bool graphs = !(c->flags & DDA_FLAG_NO_GRAPHS);
-  dda_ctx::RoundGraph* rg = nullptr;
-  const int gkey = (int)sizeof(T) + (o.mv32 ? 100 : 0);  // kernel sequences differ per variant
-  for (auto& x : c->round_graphs)
-    if (x.solver == solver && x.nrhs == nrhs && x.tsize == gkey) rg = &x;
+  // graph of the current kernel sequence (index into c->round_graphs, which
+  // may grow while this solve runs: a precision switch captures a second one)
+  auto find_graph = [&](int key) -> int {
+    for (size_t i = 0; i < c->round_graphs.size(); i++) {
+      const auto& x = c->round_graphs[i];
+      if (x.solver == solver && x.nrhs == nrhs && x.tsize == key) return (int)i;
+    }
+    return -1;
+  };
+  MixedSwitch ms(o);
+  if (o.adapt) sv.mv32 = ms.start32;
   for (int round = 0;; round++) {
     if (!graphs || round == 0) {
       for (int k = 0; k < poll; k++) sv.iteration(solver, nr++, b);
     } else {
-      if (!rg) {  // capture once per context, solver, batch and precision
+      const int gkey = (int)sizeof(T) + (sv.mv32 ? 100 : 0);  // kernel sequences differ per variant
+      int gi = find_graph(gkey);
+      if (gi < 0) {  // capture once per context, solver, batch and precision
         const long long l0 = c->launches;
         cudaGraph_t graph = nullptr;
         CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
@@ -1052,11 +1112,11 @@ void run_solve(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
         cudaGraphDestroy(graph);
         CK(rc);
         c->round_graphs.push_back({solver, nrhs, gkey, g, c->launches - l0});
-        rg = &c->round_graphs.back();
+        gi = (int)c->round_graphs.size() - 1;
         c->launches = l0;
       }
-      CK(cudaGraphLaunch(rg->g, c->stream));
-      c->launches += rg->launches;
+      CK(cudaGraphLaunch(c->round_graphs[gi].g, c->stream));
+      c->launches += c->round_graphs[gi].launches;
       nr += poll;
     }
     CK(cudaMemcpyAsync(c->st_host, c->st, nrhs * sizeof(KrylovState), cudaMemcpyDeviceToHost, c->stream));
@@ -1064,8 +1124,18 @@ void run_solve(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
     bool all = true;
     for (int r = 0; r < nrhs; r++) all = all && c->st_host[r].done;
     if (all) break;
+    if (c->cancel.load()) {  // dda_cancel from another thread: stop between rounds
+      for (int r = 0; r < nrhs; r++)
+        if (!c->st_host[r].done) {
+          c->st_host[r].done = 1;
+          c->st_host[r].status = DDA_ERR_CANCELLED;
+        }
+      CK(cudaMemcpyAsync(c->st, c->st_host, nrhs * sizeof(KrylovState), cudaMemcpyHostToDevice, c->stream));
+      break;
+    }
     if constexpr (std::is_same<T, double>::value) {
       if (o.check_every > 0 && nr % o.check_every == 0 && check_gap(c, nrhs, b.X, B, S, o)) break;
+      if (o.adapt) sv.mv32 = ms.update(c->st_host, nrhs, nr);
     }
   }
   if (b.X != e.vec[4])
@@ -1134,6 +1204,8 @@ void run_mixed(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
       out[r].rel = rel;
       out[r].res_scale = k.residScale;
       total_it = std::max(total_it, out[r].iterations);
+      if (!done[r] && outer == 0 && !std::isfinite(k.temp)) { done[r] = 1; out[r].status = DDA_ERR_ARG; }
+      if (!done[r] && outer == 0 && k.temp == 0) done[r] = 1;  // b = 0: x = 0
       if (!done[r] && !(rel == rel)) { done[r] = 1; out[r].status = DDA_ERR_BREAKDOWN; }
       if (!done[r] && (rel < eps || out[r].status != 0)) done[r] = 1;
       if (!done[r] && outer > 0) {
@@ -1143,6 +1215,7 @@ void run_mixed(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
       prev_rel[r] = rel;
       if (!done[r] && outer >= max_outer) { done[r] = 1; out[r].status = DDA_ERR_NOPROGRESS; }
       if (!done[r] && max_iter > 0 && out[r].iterations >= max_iter) { done[r] = 1; out[r].status = DDA_ERR_MAXITER; }
+      if (!done[r] && c->cancel.load()) { done[r] = 1; out[r].status = DDA_ERR_CANCELLED; }
       k.done = done[r];
       // the FP64 recurrences can follow the inner system to the final target
       // in one go; the FP32 convolution then leaves a residual of about its
@@ -1160,6 +1233,7 @@ void run_mixed(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
     o.skip = done.data();
     o.result = false;
     o.mv32 = true;
+    o.adapt = !getenv("DDA_MX_FIXED");
     o.check_every = kCheckEvery;
     o.check_abs = thr.data();
     run_solve<double>(c, solver, nrhs, 0.0, max_iter > 0 ? max_iter - total_it : 0, o);
@@ -1167,6 +1241,7 @@ void run_mixed(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
       if (done[r]) continue;
       out[r].iterations += c->st_host[r].count;
       out[r].refinements++;
+      if (c->st_host[r].status == DDA_ERR_CANCELLED) out[r].status = DDA_ERR_CANCELLED;
       // an inner solve that stopped early (stagnation, breakdown, its share
       // of max_iter) still contributes its correction; the outer FP64
       // residual decides
@@ -1328,6 +1403,8 @@ int dda_set_cc(dda_ctx* ctx, int rhs, const double* cc_sqrt) {
   return guard(ctx, [&]() -> int {
     if (rhs < 0 || rhs >= ctx->max_rhs || !cc_sqrt) throw DdaError(DDA_ERR_ARG, "bad rhs index or null cc_sqrt");
     const int n = ctx->g.nmat * 3;
+    for (int i = 0; i < 2 * n; i++)
+      if (!std::isfinite(cc_sqrt[i])) throw DdaError(DDA_ERR_ARG, "couple constants are not finite");
     for (int i = 0; i < n; i++)
       ctx->cc_host[(size_t)rhs * n + i] = std::complex<double>(cc_sqrt[2 * i], cc_sqrt[2 * i + 1]);
     ctx->cc_set[rhs] = 1;
@@ -1572,7 +1649,11 @@ int collect_mixed(dda_ctx* c, const std::vector<MixedOut>& mo, double* history, 
     if (mo[r].status != 0 && rc == DDA_OK) rc = mo[r].status;
   }
   CK(cudaStreamSynchronize(c->stream));  // history copies done
-  if (rc != DDA_OK) c->err = rc == DDA_ERR_MAXITER ? "Too many iterations" : "refinement did not converge";
+  if (rc != DDA_OK)
+    c->err = rc == DDA_ERR_MAXITER ? "Too many iterations"
+           : rc == DDA_ERR_CANCELLED ? "cancelled"
+           : rc == DDA_ERR_ARG ? "right-hand side or start value is not finite"
+                               : "refinement did not converge";
   return rc;
 }
 
@@ -1625,9 +1706,10 @@ int collect_stats(dda_ctx* c, int nrhs, double* history, long long history_cap, 
   }
   CK(cudaStreamSynchronize(c->stream));  // history copies done
   if (rc != DDA_OK) {
-    static const char* msg[] = {"", "", "", "", "", "Krylov breakdown", "Too many iterations",
-                                "Too many iterations w/o increase"};
-    c->err = (rc <= -5 && rc >= -7) ? msg[-rc] : "solver failed";
+    static const char* msg[] = {"", "right-hand side or start value is not finite", "", "", "",
+                                "Krylov breakdown", "Too many iterations", "Too many iterations w/o increase",
+                                "cancelled"};
+    c->err = (rc <= -5 && rc >= -8) || rc == -1 ? msg[-rc] : "solver failed";
   }
   return rc;
 }
@@ -1651,7 +1733,7 @@ int dda_solve(dda_ctx* ctx, int solver, int nrhs, const double* einc, double eps
               const double* start, double* pol_out, double* history, int64_t history_cap,
               dda_stats* stats) {
   if (!ctx) return DDA_ERR_ARG;
-  return guard(ctx, [&]() -> int {
+  const int rc = guard(ctx, [&]() -> int {
     if (solver < 0 || solver > 3) throw DdaError(DDA_ERR_ARG, "unknown solver");
     if (nrhs < 1 || nrhs > ctx->max_rhs || !einc) throw DdaError(DDA_ERR_ARG, "bad solve arguments");
     if (!(eps > 0)) throw DdaError(DDA_ERR_ARG, "eps must be positive");
@@ -1663,12 +1745,14 @@ int dda_solve(dda_ctx* ctx, int solver, int nrhs, const double* einc, double eps
       return solve_mixed_host(ctx, solver, nrhs, einc, eps, max_iter, start, pol_out, history, history_cap, stats);
     return solve_t<double>(ctx, solver, nrhs, einc, eps, max_iter, start, pol_out, history, history_cap, stats);
   });
+  ctx->cancel.store(0);
+  return rc;
 }
 
 int dda_solve_device(dda_ctx* ctx, int solver, int nrhs, const void* d_einc, double eps, int64_t max_iter,
                      const void* d_start, void* d_pol, dda_stats* stats) {
   if (!ctx) return DDA_ERR_ARG;
-  return guard(ctx, [&]() -> int {
+  const int rc = guard(ctx, [&]() -> int {
     if (solver < 0 || solver > 3) throw DdaError(DDA_ERR_ARG, "unknown solver");
     if (nrhs < 1 || nrhs > ctx->max_rhs || !d_einc || !d_pol) throw DdaError(DDA_ERR_ARG, "bad solve arguments");
     if (!(eps > 0)) throw DdaError(DDA_ERR_ARG, "eps must be positive");
@@ -1680,6 +1764,14 @@ int dda_solve_device(dda_ctx* ctx, int solver, int nrhs, const void* d_einc, dou
       return solve_mixed_device(ctx, solver, nrhs, d_einc, eps, max_iter, d_start, d_pol, stats);
     return solve_device_t<float>(ctx, solver, nrhs, d_einc, eps, max_iter, d_start, d_pol, stats);
   });
+  ctx->cancel.store(0);
+  return rc;
+}
+
+int dda_cancel(dda_ctx* ctx) {
+  if (!ctx) return DDA_ERR_ARG;
+  ctx->cancel.store(1);
+  return DDA_OK;
 }
 
 void* dda_stream(dda_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }

@@ -148,8 +148,16 @@ __device__ __forceinline__ void kfail(KrylovState& s, int code) {
 
 // IterativeSolverBase loop update (DDA/IterativeSolverBase.cpp:56-98) after
 // an iteration returned |r|^2 = next.
+// A residual that is not a number ends the solve with KS_BREAKDOWN (the
+// reference keeps iterating until maxResIncrease, since no NaN compares as an
+// improvement).
 __device__ __forceinline__ void loop_update(KrylovState& s, double next) {
   s.count++;
+  if (!(next == next)) {
+    if (s.hist && s.count - 1 < s.histCap) s.hist[s.count - 1] = next;
+    kfail(s, KS_BREAKDOWN);
+    return;
+  }
   if (next <= s.inprodR) {
     s.inprodR = next;
     s.counter = 0;
@@ -175,12 +183,13 @@ __device__ __forceinline__ void loop_update(KrylovState& s, double next) {
   }
 }
 
-// QMR-CS breakdown guard at the start of iteration nr (DDA/QmrCs.cpp:89-93).
+// QMR-CS breakdown guard at the start of iteration nr (DDA/QmrCs.cpp:89-93),
+// written so that a beta that is not a number fails it as well.
 __device__ __forceinline__ void qmr_check_beta(KrylovState& s) {
   double rtmp1 = dabs2(s.beta) * s.residScale;
   if (s.count == 0) {
-    if (rtmp1 > 1e+38f) kfail(s, KS_BREAKDOWN);
-  } else if (rtmp1 < 1e-10f || rtmp1 > 1e+38f) {
+    if (!(rtmp1 <= 1e+38f)) kfail(s, KS_BREAKDOWN);
+  } else if (!(rtmp1 >= 1e-10f && rtmp1 <= 1e+38f)) {
     kfail(s, KS_BREAKDOWN);
   }
 }

@@ -20,6 +20,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <set>
 #include <string>
 #include <thread>
 #include <vector>
@@ -62,6 +63,9 @@ struct dda_server {
   std::deque<std::unique_ptr<Job>> queue;
   std::deque<std::unique_ptr<Done>> done;
   std::map<int64_t, std::unique_ptr<Done>> held;  // results with kept polarisations
+  std::map<int64_t, dda_ctx*> active;             // running requests' contexts (dda_serve_cancel)
+  std::set<int64_t> running_ids;                  // admitted, not finished
+  std::set<int64_t> cancel_asked;                 // running requests cancelled before their context existed
   int64_t used = 0;
   int64_t running = 0;
   int64_t next_id = 1;
@@ -107,6 +111,18 @@ void dda_server::run(Job& j, Done& d) {
   int rc = dda_create(&P, q.precision, &ctx);
   if (rc != DDA_OK) return set_error(d, dda_last_error(nullptr), rc);
   std::unique_ptr<dda_ctx, int (*)(dda_ctx*)> cc(ctx, dda_destroy);
+  // registered for dda_serve_cancel while it exists (unregistered before
+  // the context is destroyed: `reg` is released before `cc`)
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    active[j.id] = ctx;
+    if (cancel_asked.erase(j.id)) dda_cancel(ctx);
+  }
+  auto unreg = [this, &j](void*) {
+    std::lock_guard<std::mutex> lk(mu);
+    active.erase(j.id);
+  };
+  std::unique_ptr<void, decltype(unreg)> reg(ctx, unreg);
   d.res.t_setup = now();
   int64_t layout[8] = {};
   dda_matvec_layout(ctx, layout);
@@ -193,6 +209,7 @@ void dda_server::worker() {
       }
       used += job->peak;
       running++;
+      running_ids.insert(job->id);
     }
     std::unique_ptr<Done> d(new Done);
     d->res.id = job->id;
@@ -212,6 +229,8 @@ void dda_server::worker() {
       std::lock_guard<std::mutex> lk(mu);
       used -= job->peak;
       running--;
+      running_ids.erase(job->id);
+      cancel_asked.erase(job->id);
       done.push_back(std::move(d));
     }
     cv_done.notify_all();
@@ -338,6 +357,42 @@ int dda_serve_poll(dda_server* s, dda_serve_result* out, int max, int timeout_ms
     n++;
   }
   return n;
+}
+
+int dda_serve_cancel(dda_server* s, int64_t id) {
+  if (!s) return DDA_ERR_ARG;
+  std::unique_ptr<Done> d;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = std::find_if(s->queue.begin(), s->queue.end(),
+                           [&](const std::unique_ptr<Job>& j) { return j->id == id; });
+    if (it != s->queue.end()) {  // still queued: never admitted
+      d.reset(new Done);
+      d->res.id = id;
+      d->res.tag = (*it)->req.tag;
+      d->res.npol = (*it)->req.npol;
+      d->res.nv = (*it)->req.nv;
+      d->res.t_submit = (*it)->t_submit;
+      d->res.t_admit = d->res.t_done = s->now();
+      for (int a = 0; a < 3; a++) d->res.grid[a] = (*it)->prob.grid[a];
+      set_error(*d, "cancelled before admission", DDA_ERR_CANCELLED);
+      s->queue.erase(it);
+      s->done.push_back(std::move(d));
+    } else {
+      auto a = s->active.find(id);
+      if (a != s->active.end()) {
+        dda_cancel(a->second);  // the solve stops after its current round
+      } else if (s->running_ids.count(id)) {
+        s->cancel_asked.insert(id);  // admitted, context not built yet
+      } else {
+        return DDA_ERR_ARG;
+      }
+      return DDA_OK;
+    }
+  }
+  s->cv_done.notify_all();
+  s->cv_work.notify_all();
+  return DDA_OK;
 }
 
 int dda_serve_release(dda_server* s, int64_t id) {

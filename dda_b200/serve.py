@@ -49,6 +49,7 @@ def _bind():
         "dda_serve_submit": ([vp, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
         "dda_serve_poll": ([vp, ctypes.POINTER(Result), ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "dda_serve_release": ([vp, ctypes.c_int64], ctypes.c_int),
+        "dda_serve_cancel": ([vp, ctypes.c_int64], ctypes.c_int),
         "dda_serve_pending": ([vp], ctypes.c_int64),
         "dda_serve_clock": ([vp], ctypes.c_double),
         "dda_serve_destroy": ([vp], ctypes.c_int),
@@ -133,6 +134,13 @@ class Server:
                 self.L.dda_serve_release(self.h, r.id)
             out.append(d)
         return out
+
+    def cancel(self, rid):
+        """dda_serve_cancel: a queued request leaves the queue, a running one
+        stops after its current round; its result has status -8."""
+        rc = self.L.dda_serve_cancel(self.h, rid)
+        if rc != 0:
+            raise DDAError(rc, "request %d is neither queued nor running" % rid)
 
     @property
     def pending(self):

@@ -37,6 +37,7 @@ extern "C" {
 #define DDA_ERR_BREAKDOWN (-5)   /* Krylov breakdown guard fired */
 #define DDA_ERR_MAXITER (-6)     /* "Too many iterations" */
 #define DDA_ERR_NOPROGRESS (-7)  /* "Too many iterations w/o increase" */
+#define DDA_ERR_CANCELLED (-8)   /* stopped by dda_cancel / dda_serve_cancel */
 
 /* Arithmetic of the matvec and of the Krylov vectors. */
 #define DDA_PREC_FP64 0  /* everything in FP64 (the reference's --ftype double) */
@@ -122,6 +123,7 @@ int64_t dda_vec_stride(const dda_ctx* ctx);
 
 /* Sets the couple-constant square roots sqrt(cc) of right-hand side `rhs`:
  * nmat*3 complex FP64 (DiagMatrix3 per material), in reference units.
+ * Values that are not finite are rejected (DDA_ERR_ARG).
  * Replaces MatVec<T>::setCoupleConstants (DDA/MatVec.hpp:46) and
  * GpuMatVec<T>::setCoupleConstants (DDA/GpuMatVec.hpp:89). */
 int dda_set_cc(dda_ctx* ctx, int rhs, const double* cc_sqrt);
@@ -165,6 +167,16 @@ int dda_solve(dda_ctx* ctx, int solver, int nrhs, const double* einc, double eps
  * (DDA/GpuIterativeSolver.cpp:78-144) without the host copies. */
 int dda_solve_device(dda_ctx* ctx, int solver, int nrhs, const void* d_einc, double eps,
                      int64_t max_iter, const void* d_start, void* d_pol, dda_stats* stats);
+
+/* Asks the solve running on `ctx` (dda_solve / dda_solve_device, called
+ * from another thread) to stop: it ends after the round of iterations in
+ * flight (at most eight), with every unfinished right-hand side reported as
+ * DDA_ERR_CANCELLED and the polarisations of the iterate reached.  A cancel
+ * issued while no solve runs stops the next one at its first round; each
+ * solve clears the request when it returns.  Safe to call from any thread.
+ * No counterpart in the reference (its solves run to completion, exit or
+ * abort, DDA/IterativeSolverBase.cpp:56-98). */
+int dda_cancel(dda_ctx* ctx);
 
 /* The context stream (a cudaStream_t) on which the library queues its work. */
 void* dda_stream(dda_ctx* ctx);

@@ -86,6 +86,14 @@ int dda_serve_submit(dda_server* s, const dda_serve_request* req, int64_t* id);
  * (< 0: until at least one is ready) for the first; returns how many. */
 int dda_serve_poll(dda_server* s, dda_serve_result* out, int max, int timeout_ms);
 
+/* Cancels request `id`.  A queued request leaves the queue at once and its
+ * result (status DDA_ERR_CANCELLED) is delivered by dda_serve_poll; a
+ * running request's solve stops after its current round of iterations
+ * (dda_cancel) and its result reports DDA_ERR_CANCELLED with the iterate
+ * reached.  Other requests are not affected.  Returns DDA_ERR_ARG for an id
+ * that is neither queued nor running. */
+int dda_serve_cancel(dda_server* s, int64_t id);
+
 /* Frees the polarisations kept for result `id`. */
 int dda_serve_release(dda_server* s, int64_t id);
 

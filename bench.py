@@ -172,9 +172,12 @@ def cpu_model():
 class CpuArm:
     """The oracle (the C++ restatement of the reference's --cpu path,
     MatVecCpu + BicgStab) on this workload: D matrix built once, then full
-    solves to relative residual 1e-5, timed with the host clock."""
+    solves to relative residual 1e-5, timed with the host clock.  precision
+    "fp32" is the reference's --ftype float path (D, matvec, vectors and
+    scalars in float), "fp64" its --ftype double path."""
 
-    def __init__(self, threads=None):
+    def __init__(self, threads=None, precision="fp32"):
+        self.precision = precision
         from oracle import oracle as O
         self.O = O
         if threads:
@@ -194,30 +197,41 @@ class CpuArm:
         """One full solve of polarisation `pol`: (seconds, iterations)."""
         self.p.set_cc(PROP, pol, "ldr")
         t0 = time.perf_counter()
-        rc, _, st, _ = self.p.solve(self.einc[pol], "bicgstab", EPS)
+        rc, _, st, _ = self.p.solve(self.einc[pol], "bicgstab", EPS, precision=self.precision)
         dt = time.perf_counter() - t0
         if rc != 0:
             raise RuntimeError("oracle solve failed (%d)" % rc)
         return dt, int(st.iterations)
 
 
-def cpu_sample():
+def cpu_sample(precision="fp32"):
     """The default line's CPU baseline: full solves of both polarisations on
-    all host threads, then one full solve of polarisation 1 on one thread
-    (the reference's --cpu path is single-threaded, LinAlg/FFTWPlan.cpp:82)."""
-    arm = CpuArm()
+    all host threads at the line's precision (and, for comparison, at the
+    other one), then one full solve of polarisation 1 on one thread (the
+    reference's --cpu path is single-threaded, LinAlg/FFTWPlan.cpp:82)."""
+    arm = CpuArm(precision=precision)
+    arm.solve(1)  # first use builds the float D matrix
     res = [arm.solve(pol) for pol in (1, 2)]
     secs = [r[0] for r in res]
     threads = arm.threads
+    other = "fp64" if precision == "fp32" else "fp32"
+    arm.precision = other
+    res_o = [arm.solve(pol) for pol in (1, 2)]
+    arm.precision = precision
     arm.O.set_threads(1)
     t1, it1 = arm.solve(1)
     arm.O.set_threads(threads)
     return {"value": 2.0 / sum(secs), "unit": "solves/s", "cores": threads, "kind": "port",
-            "sample": "oracle BiCGStab, full solves of both polarisations to 1e-5 (%.1f s; D matrix built "
-                      "beforehand in %.1f s)" % (sum(secs), arm.setup_s),
+            "precision": precision,
+            "sample": "oracle BiCGStab (%s, the reference's --ftype %s CPU path), full solves of both "
+                      "polarisations to 1e-5 (%.1f s; D matrix built beforehand)"
+                      % (precision, "float" if precision == "fp32" else "double", sum(secs)),
             "seconds": secs, "iterations": [r[1] for r in res],
+            other: {"value": 2.0 / sum(r[0] for r in res_o), "unit": "solves/s", "cores": threads,
+                    "seconds": [r[0] for r in res_o], "iterations": [r[1] for r in res_o]},
             "single_thread": {"value": 1.0 / t1, "unit": "solves/s", "cores": 1, "seconds": t1,
-                              "iterations": it1, "sample": "oracle BiCGStab, full solve of polarisation 1"},
+                              "iterations": it1, "precision": precision,
+                              "sample": "oracle BiCGStab, full solve of polarisation 1"},
             "nproc": os.cpu_count(), "cpu_model": cpu_model()}
 
 
@@ -389,7 +403,7 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
-            cpu = cpu_sample()
+            cpu = cpu_sample("fp64" if prec == "fp64" else "fp32")
         except Exception as ex:  # the CPU baseline is reported, never required
             cpu = {"value": None, "error": str(ex)}
     if rank == 0:
@@ -399,8 +413,8 @@ def run_ours(args):
                 "dtype": "c64+f64" if prec != "fp64" else "c128",
                 "data": "synthetic (the reference README geometry; generated in-process)",
                 "config": dict(WORKLOAD, precision=prec, solver=args.solver,
-                               iterations=iters, l2="flushed between steps (256 MB write)",
                                parallelism="replicas x%d" % world),
+                "iterations": iters, "l2": "flushed between steps (256 MB write)",
                 "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "matvec": matvec,
                 "plain_fp64_single_rhs": plain, "ours_fp64_single_rhs": ours64,
                 "speedup_vs_plain": value / plain["value"] if plain else None,
@@ -412,31 +426,37 @@ def run_ours(args):
 
 
 def run_reference(args):
-    """The reference arm: the oracle on the host cores, one full solve per
-    step (polarisations 1 and 2 alternating), all host threads."""
+    """The reference arm: the oracle on the host cores, all host threads, at
+    the precision of our line; one step is one full solve of both
+    polarisations, like a step of our arm."""
     rank, local, world = dist_env()
     if rank != 0:
         return
-    arm = CpuArm()
-    for i in range(args.warmup):
-        arm.solve(1 + i % 2)
+    prec = args.precision if args.precision in ("fp32", "fp64") else "fp64"
+    arm = CpuArm(precision=prec)
+    for _ in range(args.warmup):
+        arm.solve(1)
+        arm.solve(2)
     secs, its = [], []
-    for i in range(args.steps):
-        dt, it = arm.solve(1 + i % 2)
-        secs.append(dt)
-        its.append(it)
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        its.append([arm.solve(pol)[1] for pol in (1, 2)])
+        secs.append(time.perf_counter() - t0)
     total = sum(secs)
-    v = args.steps / total
+    v = 2 * args.steps / total
     cpu = {"value": v, "unit": "solves/s", "cores": arm.threads, "kind": "port",
-           "sample": "oracle BiCGStab, one full solve to 1e-5 per step (polarisations 1 and 2 alternating), "
-                     "D matrix built once beforehand (%.1f s)" % arm.setup_s,
-           "iterations": sorted(set(its)), "nproc": os.cpu_count(), "cpu_model": cpu_model()}
+           "precision": prec,
+           "sample": "oracle BiCGStab (the reference's --ftype %s CPU path), full solves of both "
+                     "polarisations to 1e-5 per step, D matrix built once beforehand"
+                     % ("float" if prec == "fp32" else "double"),
+           "iterations": its[-1], "nproc": os.cpu_count(), "cpu_model": cpu_model()}
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * total / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
-            "data": "synthetic", "config": dict(WORKLOAD, precision="fp64", solver="bicgstab",
-                                                 rhs_per_step=1),
-            "cpu_baseline": cpu,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "c64" if prec == "fp32" else "c128",
+            "data": "synthetic", "config": dict(WORKLOAD, precision=prec, solver="bicgstab",
+                                                 parallelism="replicas x%d" % world),
+            "iterations": its[-1], "cpu_baseline": cpu,
             "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 

@@ -60,13 +60,16 @@ std::string g_error;
 
 // ---------------------------------------------------------------- FFT ----
 // Restatement of the DFT that FFTW computes (LinAlg/FFTWPlan.cpp:82,113):
-// y_k = sum_j x_j exp(-/+ 2 pi i jk/n), unnormalised both ways.
-struct FftPlan {
+// y_k = sum_j x_j exp(-/+ 2 pi i jk/n), unnormalised both ways, in the
+// precision F of the reference's ftype (fftw_plan / fftwf_plan).
+template <class F>
+struct FftPlanT {
+  typedef std::complex<F> C;
   size_t n;
   std::vector<int> factors;
-  std::vector<cd> tw;  // exp(-2 pi i k / n), k = 0..n-1, from long double
+  std::vector<C> tw;  // exp(-2 pi i k / n), k = 0..n-1, from long double
 
-  explicit FftPlan(size_t n_) : n(n_), tw(n_) {
+  explicit FftPlanT(size_t n_) : n(n_), tw(n_) {
     size_t m = n;
     for (int p : {4, 2, 3, 5, 7}) {
       while (m % p == 0) {
@@ -82,13 +85,13 @@ struct FftPlan {
     }
     for (size_t k = 0; k < n; k++) {
       ldouble a = -kTwoPi * (ldouble)k / (ldouble)n;
-      tw[k] = cd((double)cosl(a), (double)sinl(a));
+      tw[k] = C((F)cosl(a), (F)sinl(a));
     }
   }
 
   // Recursive decimation in time: out[0..len) = DFT of in[0], in[s], ...
-  void rec(const cd* in, size_t stride, cd* out, size_t len, size_t fi,
-           bool inv, std::vector<cd>& t) const {
+  void rec(const C* in, size_t stride, C* out, size_t len, size_t fi,
+           bool inv, std::vector<C>& t) const {
     if (len == 1) {
       out[0] = in[0];
       return;
@@ -100,14 +103,14 @@ struct FftPlan {
     size_t step = n / len;  // table index scale: w_len^j = w_n^(j*step)
     for (size_t k = 0; k < m; k++) {
       for (int q = 0; q < p; q++) {
-        cd w = tw[(q * k * step) % n];
+        C w = tw[(q * k * step) % n];
         if (inv) w = std::conj(w);
         t[q] = out[q * m + k] * w;
       }
       for (int s = 0; s < p; s++) {
-        cd acc = 0;
+        C acc = 0;
         for (int q = 0; q < p; q++) {
-          cd w = tw[((size_t)q * s * m * step) % n];
+          C w = tw[((size_t)q * s * m * step) % n];
           if (inv) w = std::conj(w);
           acc += t[q] * w;
         }
@@ -118,28 +121,30 @@ struct FftPlan {
 
   // In-place transform of `count` lines: line b starts at data + b*dist,
   // elements are `stride` apart.
-  void exec(cd* data, size_t count, size_t stride, size_t dist, bool inv) const {
-    std::vector<cd> a(n), b(n), t(16);
+  void exec(C* data, size_t count, size_t stride, size_t dist, bool inv) const {
+    std::vector<C> a(n), b(n), t(16);
     if (factors.size() && *std::max_element(factors.begin(), factors.end()) > 16)
       t.resize(*std::max_element(factors.begin(), factors.end()));
     for (size_t c = 0; c < count; c++) {
-      cd* d = data + c * dist;
+      C* d = data + c * dist;
       for (size_t i = 0; i < n; i++) a[i] = d[i * stride];
       rec(a.data(), 1, b.data(), n, 0, inv, t);
       for (size_t i = 0; i < n; i++) d[i * stride] = b[i];
     }
   }
 };
+typedef FftPlanT<double> FftPlan;
 
 std::mutex g_plan_mutex;
-std::map<size_t, std::shared_ptr<FftPlan>> g_plans;
 
-std::shared_ptr<FftPlan> plan(size_t n) {
+template <class F>
+std::shared_ptr<FftPlanT<F>> plan(size_t n) {
+  static std::map<size_t, std::shared_ptr<FftPlanT<F>>> plans;
   std::lock_guard<std::mutex> lock(g_plan_mutex);
-  auto it = g_plans.find(n);
-  if (it != g_plans.end()) return it->second;
-  auto p = std::make_shared<FftPlan>(n);
-  g_plans[n] = p;
+  auto it = plans.find(n);
+  if (it != plans.end()) return it->second;
+  auto p = std::make_shared<FftPlanT<F>>(n);
+  plans[n] = p;
   return p;
 }
 
@@ -245,7 +250,7 @@ int orc_parse_length(const char* s, ldouble* out) {
 // Unnormalised in-place DFT of `count` contiguous lines of length n
 // (complex interleaved), the transform the reference gets from FFTW.
 void orc_fft(double* data, uint32_t n, uint32_t count, int inverse) {
-  plan(n)->exec(reinterpret_cast<cd*>(data), count, 1, n, inverse != 0);
+  plan<double>(n)->exec(reinterpret_cast<cd*>(data), count, 1, n, inverse != 0);
 }
 
 uint32_t orc_fft_fit(uint32_t x, uint32_t override, int supportNonPot) {
@@ -387,33 +392,37 @@ struct orc_problem {
   // matvec scratch (DDA/MatVecCpu.cpp:48-50)
   std::vector<cd> X;  // Xmatrix [3][bz][by][Gx] (x fastest)
 
+  // the --ftype float path: D computed in float (DMatrixCpu<float>), its
+  // x-grid scratch, and sqrt(cc) rounded to float
+  std::vector<std::complex<float>> D32, X32;
+
   size_t vecSize() const { return 3 * (size_t)nvs; }
   size_t N() const { return (size_t)grid[0] * grid[1] * grid[2]; }
 };
 
 namespace {
 
-// DDA/DMatrixCpu.cpp:49-63.
-cd singleInteractionTerm(const orc_problem& p, double rx, double ry, double rz,
-                         int mu, int nu) {
-  double r[3] = {rx, ry, rz};
-  double rr = std::sqrt(rx * rx + ry * ry + rz * rz);
-  double q[3] = {rx / rr, ry / rr, rz / rr};
-  double kr = p.waveNum * rr;
-  double kr2 = kr * kr;
-  double qmunu = q[mu] * q[nu];
-  (void)r;
-  cd expval = std::exp(cd(0, kr)) / cd(std::pow(rr, 3.0));
-  cd br = cd(3 - kr2, -3 * kr) * qmunu;
-  if (mu == nu) br += cd(kr2 - 1, kr);
+// DDA/DMatrixCpu.cpp:49-63, in the precision F of the reference's ftype.
+template <class F>
+std::complex<F> singleInteractionTerm(const orc_problem& p, F rx, F ry, F rz, int mu, int nu) {
+  typedef std::complex<F> C;
+  F rr = std::sqrt(rx * rx + ry * ry + rz * rz);
+  F q[3] = {rx / rr, ry / rr, rz / rr};
+  F kr = (F)p.waveNum * rr;
+  F kr2 = kr * kr;
+  F qmunu = q[mu] * q[nu];
+  C expval = std::exp(C(0, kr)) / C(std::pow(rr, F(3)));
+  C br = C(F(3) - kr2, F(-3) * kr) * qmunu;
+  if (mu == nu) br += C(kr2 - F(1), kr);
   return expval * br;
 }
 
 // DDA/DMatrixCpu.cpp:65-74 (periodicity dimension 0).
-cd interactionTerm(const orc_problem& p, int i, int j, int k, int mu, int nu) {
-  if (!i && !j && !k) return cd(0);
-  return singleInteractionTerm(p, (double)i * p.gridUnit, (double)j * p.gridUnit,
-                               (double)k * p.gridUnit, mu, nu);
+template <class F>
+std::complex<F> interactionTerm(const orc_problem& p, int i, int j, int k, int mu, int nu) {
+  if (!i && !j && !k) return std::complex<F>(0);
+  const F d = (F)p.gridUnit;
+  return singleInteractionTerm<F>(p, (F)i * d, (F)j * d, (F)k * d, mu, nu);
 }
 
 uint32_t clip(int32_t n, uint32_t M) {  // DDA/DMatrixCpu.cpp:124-131
@@ -422,7 +431,7 @@ uint32_t clip(int32_t n, uint32_t M) {  // DDA/DMatrixCpu.cpp:124-131
   return n;
 }
 
-inline cd maybeConj(cd f, bool c) { return c ? std::conj(f) : f; }
+template <class C> inline C maybeConj(C f, bool c) { return c ? std::conj(f) : f; }
 
 }  // namespace
 
@@ -574,33 +583,40 @@ void orc_set_cc_sqrt(orc_problem* p, const double* ccSqrt) {
   for (size_t i = 0; i < p->ccSqrt.size(); i++) p->ccSqrt[i] = cd(ccSqrt[2 * i], ccSqrt[2 * i + 1]);
 }
 
-// DMatrixCpu::createDMatrix, DDA/DMatrixCpu.cpp:133-205 (non-periodic).
-void orc_build_dmatrix(orc_problem* p) {
+}  // extern "C"
+
+namespace {
+
+// DMatrixCpu::createDMatrix, DDA/DMatrixCpu.cpp:133-205 (non-periodic), in
+// the precision F of the reference's ftype.
+template <class F>
+void build_dmatrix_t(orc_problem* p, std::vector<std::complex<F>>& D) {
+  typedef std::complex<F> C;
   const uint32_t Gx = p->grid[0], Gy = p->grid[1], Gz = p->grid[2];
   const int bx = p->box[0], by = p->box[1], bz = p->box[2];
   const size_t N = p->N();
-  p->D.assign(6 * N, 0);
-  std::vector<cd> d2(N);  // [Gz][Gy][Gx], x fastest (Fortran [Gx][Gy][Gz])
-  auto px = plan(Gx), py = plan(Gy), pz = plan(Gz);
-  const double scale = -(double)(Gx * (size_t)Gy * Gz);
+  D.assign(6 * N, 0);
+  std::vector<C> d2(N);  // [Gz][Gy][Gx], x fastest (Fortran [Gx][Gy][Gz])
+  auto px = plan<F>(Gx), py = plan<F>(Gy), pz = plan<F>(Gz);
+  const F scale = -(F)(Gx * (size_t)Gy * Gz);
   for (int component = 0; component < 6; component++) {
     static const int MU[6] = {0, 0, 0, 1, 1, 2}, NU[6] = {0, 1, 2, 1, 2, 2};
     int mu = MU[component], nu = NU[component];
-    std::fill(d2.begin(), d2.end(), cd(0));
+    std::fill(d2.begin(), d2.end(), C(0));
 #pragma omp parallel for schedule(dynamic)
     for (int k = 0; k < (int)Gz; k++) {
       int kcor = k > (int)Gz / 2 ? k - (int)Gz : k;
       for (int j = 1 - by; j < by; j++)
         for (int i = 1 - bx; i < bx; i++)
-          d2[clip(i, Gx) + Gx * (clip(j, Gy) + (size_t)Gy * k)] = interactionTerm(*p, i, j, kcor, mu, nu);
+          d2[clip(i, Gx) + Gx * (clip(j, Gy) + (size_t)Gy * k)] = interactionTerm<F>(*p, i, j, kcor, mu, nu);
     }
     // FFT along x over all Gy*Gz lines
 #pragma omp parallel for schedule(dynamic)
     for (long long l = 0; l < (long long)Gy * Gz; l++) px->exec(d2.data() + l * Gx, 1, 1, Gx, false);
 #pragma omp parallel for schedule(dynamic)
     for (int i = 0; i < (int)Gx; i++) {
-      std::vector<cd> slice((size_t)Gz * Gy, 0);   // [Gy][Gz], z fastest
-      std::vector<cd> sliceTr((size_t)Gy * Gz, 0); // [Gz][Gy], y fastest
+      std::vector<C> slice((size_t)Gz * Gy, 0);   // [Gy][Gz], z fastest
+      std::vector<C> sliceTr((size_t)Gy * Gz, 0); // [Gz][Gy], y fastest
       for (int j = 1 - by; j < by; j++)
         for (int k = 1 - bz; k < bz; k++) {
           uint32_t y = clip(j, Gy), z = clip(k, Gz);
@@ -612,45 +628,63 @@ void orc_build_dmatrix(orc_problem* p) {
       py->exec(sliceTr.data(), Gz, 1, Gy, false);
       for (uint32_t k = 0; k < Gz; k++)
         for (uint32_t j = 0; j < Gy; j++)
-          p->D[component + 6 * (j + (size_t)Gy * (k + (size_t)Gz * i))] = sliceTr[j + (size_t)Gy * k] / scale;
+          D[component + 6 * (j + (size_t)Gy * (k + (size_t)Gz * i))] = sliceTr[j + (size_t)Gy * k] / scale;
     }
   }
+}
+
+}  // namespace
+
+extern "C" {
+
+void orc_build_dmatrix(orc_problem* p) {
+  build_dmatrix_t<double>(p, p->D);
+  p->D32.clear();
 }
 
 void orc_get_dmatrix(const orc_problem* p, double* out) {
   std::memcpy(out, p->D.data(), p->D.size() * sizeof(cd));
 }
 void orc_set_dmatrix(orc_problem* p, const double* in) {
+  p->D32.clear();
   p->D.resize(6 * p->N());
   std::memcpy(static_cast<void*>(p->D.data()), in, p->D.size() * sizeof(cd));
 }
 
-// MatVecCpu::apply, DDA/MatVecCpu.cpp:67-150: vectors are SoA
-// [x: nvs][y: nvs][z: nvs] complex (DDA/DDAParams.hpp:176-186).
-void orc_matvec(orc_problem* p, const double* argD, double* resD, int conj) {
-  const cd* arg = reinterpret_cast<const cd*>(argD);
-  cd* res = reinterpret_cast<cd*>(resD);
+}  // extern "C"
+
+namespace {
+
+// MatVecCpu::apply, DDA/MatVecCpu.cpp:67-150, in the precision F of the
+// reference's ftype: vectors are SoA [x: nvs][y: nvs][z: nvs] complex
+// (DDA/DDAParams.hpp:176-186); D, the x-grid scratch X and sqrt(cc) (cs,
+// nmat*3) in F.
+template <class F>
+void matvec_t(orc_problem* p, const std::complex<F>* arg, std::complex<F>* res, int conj,
+              const std::vector<std::complex<F>>& D, std::vector<std::complex<F>>& Xv,
+              const std::vector<std::complex<F>>& cs) {
+  typedef std::complex<F> C;
   const uint32_t Gx = p->grid[0], Gy = p->grid[1], Gz = p->grid[2];
   const uint32_t bx = p->box[0], by = p->box[1], bz = p->box[2];
   (void)bx;
   const size_t nvs = p->nvs;
   const size_t plane = (size_t)Gx * by * bz;
-  p->X.assign(3 * plane, 0);  // Xmatrix[Gx][by][bz][3] Fortran
-  cd* X = p->X.data();
+  Xv.assign(3 * plane, 0);  // Xmatrix[Gx][by][bz][3] Fortran
+  C* X = Xv.data();
   for (uint32_t i = 0; i < p->nv; i++) {
     uint32_t x = p->pos[3 * i], y = p->pos[3 * i + 1], z = p->pos[3 * i + 2];
     for (int c = 0; c < 3; c++) {
-      cd r = p->ccSqrt[p->mat[i] * 3 + c] * maybeConj(arg[i + c * nvs], conj);
+      C r = cs[p->mat[i] * 3 + c] * maybeConj(arg[i + c * nvs], conj != 0);
       X[x + Gx * (y + (size_t)by * (z + (size_t)bz * c))] = r;
     }
   }
-  auto px = plan(Gx), py = plan(Gy), pz = plan(Gz);
+  auto px = plan<F>(Gx), py = plan<F>(Gy), pz = plan<F>(Gz);
 #pragma omp parallel for schedule(static)
   for (long long l = 0; l < (long long)by * bz * 3; l++) px->exec(X + l * Gx, 1, 1, Gx, false);
 #pragma omp parallel for schedule(dynamic)
   for (int i = 0; i < (int)Gx; i++) {
-    std::vector<cd> slices((size_t)Gz * Gy * 3, 0);   // [3][Gy][Gz] z fastest
-    std::vector<cd> slicesTr((size_t)Gy * Gz * 3, 0); // [3][Gz][Gy] y fastest
+    std::vector<C> slices((size_t)Gz * Gy * 3, 0);   // [3][Gy][Gz] z fastest
+    std::vector<C> slicesTr((size_t)Gy * Gz * 3, 0); // [3][Gz][Gy] y fastest
     for (uint32_t j = 0; j < by; j++)
       for (uint32_t k = 0; k < bz; k++)
         for (int c = 0; c < 3; c++)
@@ -663,8 +697,8 @@ void orc_matvec(orc_problem* p, const double* argD, double* resD, int conj) {
     py->exec(slicesTr.data(), (size_t)Gz * 3, 1, Gy, false);
     for (uint32_t k = 0; k < Gz; k++)
       for (uint32_t j = 0; j < Gy; j++) {
-        const cd* d = &p->D[6 * (j + (size_t)Gy * (k + (size_t)Gz * i))];
-        cd xv[3], yv[3];
+        const C* d = &D[6 * (j + (size_t)Gy * (k + (size_t)Gz * i))];
+        C xv[3], yv[3];
         for (int c = 0; c < 3; c++) xv[c] = slicesTr[j + Gy * (k + (size_t)Gz * c)];
         // SymMatrix3 * Vector3, Math/SymMatrix3.hpp:86-92
         yv[0] = d[0] * xv[0] + d[1] * xv[1] + d[2] * xv[2];
@@ -690,11 +724,20 @@ void orc_matvec(orc_problem* p, const double* argD, double* resD, int conj) {
   for (uint32_t i = 0; i < p->nv; i++) {
     uint32_t x = p->pos[3 * i], y = p->pos[3 * i + 1], z = p->pos[3 * i + 2];
     for (int c = 0; c < 3; c++) {
-      cd r = X[x + Gx * (y + (size_t)by * (z + (size_t)bz * c))];
-      cd a = maybeConj(arg[i + c * nvs], conj);
-      res[i + c * nvs] = maybeConj(p->ccSqrt[p->mat[i] * 3 + c] * r + a, conj);
+      C r = X[x + Gx * (y + (size_t)by * (z + (size_t)bz * c))];
+      C a = maybeConj(arg[i + c * nvs], conj != 0);
+      res[i + c * nvs] = maybeConj(cs[p->mat[i] * 3 + c] * r + a, conj != 0);
     }
   }
+}
+
+
+}  // namespace
+
+extern "C" {
+
+void orc_matvec(orc_problem* p, const double* argD, double* resD, int conj) {
+  matvec_t<double>(p, reinterpret_cast<const cd*>(argD), reinterpret_cast<cd*>(resD), conj, p->D, p->X, p->ccSqrt);
 }
 
 // Independent check (not in the reference): the same operator as a direct
@@ -718,7 +761,7 @@ void orc_direct_matvec(const orc_problem* p, const double* argD, double* resD) {
       for (int c = 0; c < 3; c++) xj[c] = p->ccSqrt[p->mat[j] * 3 + c] * arg[j + c * nvs];
       for (int mu = 0; mu < 3; mu++)
         for (int nu = 0; nu < 3; nu++)
-          acc[mu] += interactionTerm(*p, di, dj, dk, std::min(mu, nu), std::max(mu, nu)) * xj[nu];
+          acc[mu] += interactionTerm<double>(*p, di, dj, dk, std::min(mu, nu), std::max(mu, nu)) * xj[nu];
     }
     for (int c = 0; c < 3; c++)
       res[i + c * nvs] = arg[i + c * nvs] - p->ccSqrt[p->mat[i] * 3 + c] * acc[c];
@@ -748,47 +791,59 @@ void orc_einc(const orc_problem* p, const double* propIn, int pol, double* outD)
 }  // extern "C"
 
 // ============================================================ solvers =====
+// The CPU solvers in the precision F of the reference's ftype: vectors,
+// dot products and scalar recurrences in F (std::complex<F>), as
+// QmrCs<F>, BicgStab<F>, BicgCs<F> and Cgnr<F> compute them, with the long
+// double temporaries BicgStab uses.
 namespace {
 
-typedef std::vector<cd> Vec;
+template <class F> using VecT = std::vector<std::complex<F>>;
 
-double vnorm(const Vec& v) {  // LinAlg/LinComb.hpp:67-73
-  double r = 0;
-  for (const cd& x : v) r += std::norm(x);
+template <class F>
+F vnorm(const VecT<F>& v) {  // LinAlg/LinComb.hpp:67-73
+  F r = 0;
+  for (const std::complex<F>& x : v) r += std::norm(x);
   return r;
 }
-cd vecProdConj(const Vec& a, const Vec& b) {  // DDA/QmrCs.cpp:48-55 (bilinear)
-  cd s = 0;
+template <class F>
+std::complex<F> vecProdConj(const VecT<F>& a, const VecT<F>& b) {  // DDA/QmrCs.cpp:48-55 (bilinear)
+  std::complex<F> s = 0;
   for (size_t i = 0; i < a.size(); i++) s += a[i] * b[i];
   return s;
 }
-cd vecProd(const Vec& a, const Vec& b) {  // DDA/BicgStab.cpp:34-41 (Hermitian)
-  cd s = 0;
+template <class F>
+std::complex<F> vecProd(const VecT<F>& a, const VecT<F>& b) {  // DDA/BicgStab.cpp:34-41 (Hermitian)
+  std::complex<F> s = 0;
   for (size_t i = 0; i < a.size(); i++) s += a[i] * std::conj(b[i]);
   return s;
 }
 
+template <class F>
 struct SolveCtx {
+  typedef std::complex<F> C;
+  typedef VecT<F> Vec;
   orc_problem* p;
+  const std::vector<C>& D;
+  std::vector<C>& X;
+  std::vector<C> cs;  // sqrt(cc) per material and axis, in F
   Vec A, r, x, t1, t2, t3, t4;
-  double residScale = 0, epsB = 0, inprodR = 0;
+  F residScale = 0, epsB = 0, inprodR = 0;
   std::vector<double> history;
   int status = 0;
   std::string msg;
 
-  explicit SolveCtx(orc_problem* p_) : p(p_) {
+  SolveCtx(orc_problem* p_, const std::vector<C>& D_, std::vector<C>& X_) : p(p_), D(D_), X(X_) {
     size_t n = p->vecSize();
     A.assign(n, 0); r.assign(n, 0); x.assign(n, 0);
     t1.assign(n, 0); t2.assign(n, 0); t3.assign(n, 0); t4.assign(n, 0);
+    for (const cd& c : p->ccSqrt) cs.push_back(C(c));
   }
-  void matvec(const Vec& a, Vec& out, bool conj) {
-    orc_matvec(p, reinterpret_cast<const double*>(a.data()), reinterpret_cast<double*>(out.data()), conj);
-  }
+  void matvec(const Vec& a, Vec& out, bool conj) { matvec_t<F>(p, a.data(), out.data(), conj, D, X, cs); }
   // multMat / multMatInv, DDA/DDAParams.hpp:188-210
   void multCc(const Vec& in, Vec& out, bool inverse) {
     for (uint32_t i = 0; i < p->nv; i++)
       for (int c = 0; c < 3; c++) {
-        cd s = p->ccSqrt[p->mat[i] * 3 + c];
+        C s = cs[p->mat[i] * 3 + c];
         out[i + c * p->nvs] = inverse ? in[i + c * p->nvs] / s : s * in[i + c * p->nvs];
       }
   }
@@ -800,24 +855,26 @@ struct SolveCtx {
 };
 
 // CpuIterativeSolver::initGeneral, DDA/CpuIterativeSolver.cpp:45-91.
-double initGeneral(SolveCtx& s, const Vec& einc, const Vec& start) {
-  Vec& pvec = s.t1;
-  std::fill(pvec.begin(), pvec.end(), cd(0));
+template <class F>
+F initGeneral(SolveCtx<F>& s, const VecT<F>& einc, const VecT<F>& start) {
+  typedef std::complex<F> C;
+  VecT<F>& pvec = s.t1;
+  std::fill(pvec.begin(), pvec.end(), C(0));
   s.multCc(einc, pvec, false);
-  double temp = vnorm(pvec);
+  F temp = vnorm(pvec);
   s.residScale = 1 / temp;
-  double inprodR;
+  F inprodR;
   if (!start.empty()) {
     s.multCc(start, s.x, true);
     s.matvec(s.x, s.A, false);
-    for (size_t i = 0; i < pvec.size(); i++) s.r[i] = s.A[i] * cd(-1) + pvec[i];
+    for (size_t i = 0; i < pvec.size(); i++) s.r[i] = s.A[i] * C(-1) + pvec[i];
     inprodR = vnorm(s.r);
   } else {
     s.matvec(pvec, s.A, false);
-    for (size_t i = 0; i < pvec.size(); i++) s.r[i] = s.A[i] * cd(-1) + pvec[i];
+    for (size_t i = 0; i < pvec.size(); i++) s.r[i] = s.A[i] * C(-1) + pvec[i];
     inprodR = vnorm(s.r);
     if (temp < inprodR) {
-      std::fill(s.x.begin(), s.x.end(), cd(0));
+      std::fill(s.x.begin(), s.x.end(), C(0));
       std::swap(s.r, pvec);
       inprodR = temp;
     } else {
@@ -828,63 +885,65 @@ double initGeneral(SolveCtx& s, const Vec& einc, const Vec& start) {
 }
 
 // ---- QMR-CS, DDA/QmrCs.cpp:58-168
+template <class F>
 struct Qmr {
-  double omega_old, omega_new, c_old, c_new;
-  cd beta, mBeta, tautilda, s_old, s_new;
-  void init(SolveCtx& s) {
-    Vec& v = s.t1;
-    cd rvec2 = vecProdConj(s.r, s.r);
+  typedef std::complex<F> C;
+  F omega_old, omega_new, c_old, c_new;
+  C beta, mBeta, tautilda, s_old, s_new;
+  void init(SolveCtx<F>& s) {
+    VecT<F>& v = s.t1;
+    C rvec2 = vecProdConj(s.r, s.r);
     omega_old = 0;
     beta = std::sqrt(rvec2);
     mBeta = -beta;
     omega_new = std::sqrt(s.inprodR) / std::abs(beta);
     tautilda = omega_new * beta;
     c_old = 1; c_new = 1; s_old = 0; s_new = 0;
-    cd bi = 1.0 / beta;
+    C bi = F(1) / beta;
     for (size_t i = 0; i < v.size(); i++) v[i] = s.r[i] * bi;
   }
-  bool iteration(SolveCtx& s, size_t nr, double& out) {
-    Vec &r = s.r, &A = s.A, &x = s.x, &v = s.t1, &vt = s.t2, &p_old = s.t3, &p_new = s.t4;
-    double rtmp1 = std::norm(beta) * s.residScale;
+  bool iteration(SolveCtx<F>& s, size_t nr, F& out) {
+    VecT<F> &r = s.r, &A = s.A, &x = s.x, &v = s.t1, &vt = s.t2, &p_old = s.t3, &p_new = s.t4;
+    F rtmp1 = std::norm(beta) * s.residScale;
     if (nr == 0) {
       if (rtmp1 > 1e+38f) return s.fail(-5, "QMR breakdown: beta too large");
     } else if (rtmp1 < 1e-10f || rtmp1 > 1e+38f) {
       return s.fail(-5, "QMR breakdown: beta out of range");
     }
     s.matvec(v, A, false);
-    cd alpha = vecProdConj(v, A);
+    C alpha = vecProdConj(v, A);
     if (nr == 0)
       for (size_t i = 0; i < v.size(); i++) vt[i] = v[i] * (-alpha) + A[i];
     else
       for (size_t i = 0; i < v.size(); i++) vt[i] = vt[i] * mBeta + v[i] * (-alpha) + A[i];
-    cd ctmp3 = vecProdConj(vt, vt);
-    double rtmp2 = vnorm(vt);
-    cd ctmp1 = omega_old * beta;
-    cd ctmp2 = omega_new * alpha;
-    cd theta = std::conj(s_old) * ctmp1;
-    cd eta = c_old * c_new * ctmp1 + std::conj(s_new) * ctmp2;
-    cd zetatilda = c_new * ctmp2 - c_old * s_new * ctmp1;
+    C ctmp3 = vecProdConj(vt, vt);
+    F rtmp2 = vnorm(vt);
+    C ctmp1 = omega_old * beta;
+    C ctmp2 = omega_new * alpha;
+    C theta = std::conj(s_old) * ctmp1;
+    C eta = c_old * c_new * ctmp1 + std::conj(s_new) * ctmp2;
+    C zetatilda = c_new * ctmp2 - c_old * s_new * ctmp1;
     beta = std::sqrt(ctmp3);
     mBeta = -beta;
     omega_old = omega_new;
     omega_new = std::sqrt(rtmp2) / std::abs(beta);
-    double zetaabs = std::sqrt(std::norm(zetatilda) + rtmp2);
-    double rtmp3 = std::sqrt(std::norm(zetatilda));
-    cd zeta;
+    F zetaabs = std::sqrt(std::norm(zetatilda) + rtmp2);
+    F rtmp3 = std::sqrt(std::norm(zetatilda));
+    C zeta;
     if (rtmp3 < 1e-40f) zeta = zetaabs;
     else zeta = zetaabs / rtmp3 * zetatilda;
     c_old = c_new;
     c_new = rtmp3 / zetaabs;
     s_old = s_new;
     s_new = omega_new * (beta / zeta);
-    cd tau = c_new * tautilda;
+    C tau = c_new * tautilda;
     tautilda = -s_new * tautilda;
-    cd zetaInv = 1.0 / zeta;
-    cd mEtaZeta = -eta / zeta;
-    cd mThetaZeta = -theta / zeta;
-    cd betaInv = 1.0 / beta;
-    double normSNew = std::norm(s_new);
-    cd cNewOmegaNewTautilda = (c_new / omega_new) * tautilda;
+    C zetaInv = F(1) / zeta;
+    C mEtaZeta = -eta / zeta;
+    C mThetaZeta = -theta / zeta;
+    C betaInv = F(1) / beta;
+    F normSNew = std::norm(s_new);
+    C cNewOmegaNewTautilda = (c_new / omega_new) * tautilda;
     if (nr == 0) {
       for (size_t i = 0; i < v.size(); i++) p_new[i] = v[i] * zetaInv;
     } else {
@@ -898,21 +957,23 @@ struct Qmr {
     for (size_t i = 0; i < v.size(); i++) x[i] = p_new[i] * tau + x[i];
     for (size_t i = 0; i < v.size(); i++) vt[i] = vt[i] * betaInv;
     std::swap(v, vt);
-    for (size_t i = 0; i < v.size(); i++) r[i] = r[i] * cd(normSNew) + v[i] * cNewOmegaNewTautilda;
+    for (size_t i = 0; i < v.size(); i++) r[i] = r[i] * C(normSNew) + v[i] * cNewOmegaNewTautilda;
     out = vnorm(r);
     return true;
   }
 };
 
 // ---- BiCGStab, DDA/BicgStab.cpp:59-112 (long double for alpha, beta, omega)
+template <class F>
 struct BicgStab {
-  cd beta, ro_new, ro_old, omega, alpha;
-  double denumOmega;
-  void init(SolveCtx& s) { s.t4 = s.r; }
-  bool iteration(SolveCtx& s, size_t nr, double& out) {
-    Vec &r = s.r, &A = s.A, &x = s.x, &pv = s.t1, &v = s.t2, &sv = s.t3, &rt = s.t4;
+  typedef std::complex<F> C;
+  C beta, ro_new, ro_old, omega, alpha;
+  F denumOmega;
+  void init(SolveCtx<F>& s) { s.t4 = s.r; }
+  bool iteration(SolveCtx<F>& s, size_t nr, F& out) {
+    VecT<F> &r = s.r, &A = s.A, &x = s.x, &pv = s.t1, &v = s.t2, &sv = s.t3, &rt = s.t4;
     ro_new = vecProd(r, rt);
-    double dtmp = (double)(std::abs(cld(ro_new)) / (ldouble)s.inprodR);
+    F dtmp = (F)(std::abs(cld(ro_new)) / (ldouble)s.inprodR);
     if (!(dtmp >= 1e-16)) return s.fail(-5, "BiCGStab breakdown: ro_new too small");
     if (nr == 0) {
       pv = r;
@@ -921,21 +982,21 @@ struct BicgStab {
       cld ro_old_omega = cld(ro_old) * cld(omega);
       if (!(std::abs(ro_old_omega) / std::abs(ro_new_alpha) >= 10e-10))
         return s.fail(-5, "BiCGStab breakdown: omega too small");
-      beta = cd(ro_new_alpha / ro_old_omega);
-      cd mbo = -beta * omega;
+      beta = C(ro_new_alpha / ro_old_omega);
+      C mbo = -beta * omega;
       for (size_t i = 0; i < pv.size(); i++) pv[i] = pv[i] * beta + v[i] * mbo + r[i];
     }
     s.matvec(pv, v, false);
     cld vRtilda = cld(vecProd(v, rt));
-    alpha = cd(cld(ro_new) / vRtilda);
+    alpha = C(cld(ro_new) / vRtilda);
     for (size_t i = 0; i < v.size(); i++) sv[i] = v[i] * (-alpha) + r[i];
-    double inprodRplus1 = vnorm(sv);
+    F inprodRplus1 = vnorm(sv);
     if (inprodRplus1 < s.epsB) {
       for (size_t i = 0; i < v.size(); i++) x[i] = pv[i] * alpha + x[i];
     } else {
       s.matvec(sv, A, false);
       denumOmega = vnorm(A);
-      omega = cd(cld(vecProd(sv, A)) / (ldouble)denumOmega);
+      omega = C(cld(vecProd(sv, A)) / (ldouble)denumOmega);
       for (size_t i = 0; i < v.size(); i++) x[i] = pv[i] * alpha + sv[i] * omega + x[i];
       for (size_t i = 0; i < v.size(); i++) r[i] = A[i] * (-omega) + sv[i];
       inprodRplus1 = vnorm(r);
@@ -947,15 +1008,17 @@ struct BicgStab {
 };
 
 // ---- BiCG-CS, DDA/BicgCs.cpp:56-84
+template <class F>
 struct BicgCs {
-  cd alpha, beta, ro_new, ro_old;
-  double abs_ro_new;
-  void init(SolveCtx&) {}
-  bool iteration(SolveCtx& s, size_t nr, double& out) {
-    Vec &r = s.r, &A = s.A, &x = s.x, &pv = s.t1;
+  typedef std::complex<F> C;
+  C alpha, beta, ro_new, ro_old;
+  F abs_ro_new;
+  void init(SolveCtx<F>&) {}
+  bool iteration(SolveCtx<F>& s, size_t nr, F& out) {
+    VecT<F> &r = s.r, &A = s.A, &x = s.x, &pv = s.t1;
     ro_new = vecProdConj(r, r);
     abs_ro_new = std::abs(ro_new);
-    double dtmp = abs_ro_new / s.inprodR;
+    F dtmp = abs_ro_new / s.inprodR;
     if (dtmp < 1e-10 || dtmp > 1e+10) return s.fail(-5, "BiCG-CS breakdown: rho out of range");
     if (nr == 0) {
       pv = r;
@@ -964,8 +1027,8 @@ struct BicgCs {
       for (size_t i = 0; i < pv.size(); i++) pv[i] = pv[i] * beta + r[i];
     }
     s.matvec(pv, A, false);
-    cd mu_k = vecProdConj(pv, A);
-    double dtmp2 = std::abs(mu_k) / abs_ro_new;
+    C mu_k = vecProdConj(pv, A);
+    F dtmp2 = std::abs(mu_k) / abs_ro_new;
     if (dtmp2 < 10e-10) return s.fail(-5, "BiCG-CS breakdown: mu too small");
     alpha = ro_new / mu_k;
     for (size_t i = 0; i < pv.size(); i++) x[i] = pv[i] * alpha + x[i];
@@ -977,12 +1040,14 @@ struct BicgCs {
 };
 
 // ---- CGNR, DDA/Cgnr.cpp:39-73
+template <class F>
 struct Cgnr {
-  cd beta;
-  double ro_new, ro_old;
-  void init(SolveCtx&) { ro_old = 0; }
-  bool iteration(SolveCtx& s, size_t nr, double& out) {
-    Vec &r = s.r, &A = s.A, &x = s.x, &pv = s.t1;
+  typedef std::complex<F> C;
+  C beta;
+  F ro_new, ro_old;
+  void init(SolveCtx<F>&) { ro_old = 0; }
+  bool iteration(SolveCtx<F>& s, size_t nr, F& out) {
+    VecT<F> &r = s.r, &A = s.A, &x = s.x, &pv = s.t1;
     if (nr == 0) {
       s.matvec(r, pv, true);
       ro_new = vnorm(pv);
@@ -993,7 +1058,7 @@ struct Cgnr {
       for (size_t i = 0; i < pv.size(); i++) pv[i] = pv[i] * beta + A[i];
     }
     s.matvec(pv, A, false);
-    cd alpha = ro_new / vnorm(A);
+    C alpha = ro_new / vnorm(A);
     for (size_t i = 0; i < pv.size(); i++) x[i] = pv[i] * alpha + x[i];
     for (size_t i = 0; i < pv.size(); i++) r[i] = A[i] * (-alpha) + r[i];
     ro_old = ro_new;
@@ -1002,8 +1067,8 @@ struct Cgnr {
   }
 };
 
-template <class S>
-int runSolver(SolveCtx& s, S& solver, size_t maxIter, size_t maxResIncrease,
+template <class F, class S>
+int runSolver(SolveCtx<F>& s, S& solver, size_t maxIter, size_t maxResIncrease,
               size_t stopAfter) {
   // IterativeSolverBase::getPolVec loop, DDA/IterativeSolverBase.cpp:53-98
   size_t count = 0, counter = 0;
@@ -1019,7 +1084,7 @@ int runSolver(SolveCtx& s, S& solver, size_t maxIter, size_t maxResIncrease,
       s.msg = "Too many iterations w/o increase";
       return s.status;
     }
-    double next;
+    F next;
     if (!solver.iteration(s, count, next)) return s.status;
     count++;
     if (next <= s.inprodR) {
@@ -1028,7 +1093,7 @@ int runSolver(SolveCtx& s, S& solver, size_t maxIter, size_t maxResIncrease,
     } else {
       counter++;
     }
-    s.history.push_back(std::sqrt(s.residScale * next));
+    s.history.push_back(std::sqrt((double)s.residScale * (double)next));
   }
   return 0;
 }
@@ -1047,22 +1112,30 @@ struct orc_stats {
   int32_t pad;
 };
 
+}  // extern "C"
+
+namespace {
+
 // IterativeSolverBase::getPolVec (DDA/IterativeSolverBase.cpp:40-103)
-// followed by CpuIterativeSolver::getResult (DDA/CpuIterativeSolver.cpp:93-99).
-// solver: 0 = qmr, 1 = bicgstab, 2 = bicg (BiCG-CS), 3 = cgnr.
-// stop_after > 0 stops after that many iterations (a bounded timing sample;
-// status 1).  history (may be NULL) receives up to history_cap RE_ values.
-int orc_solve(orc_problem* p, int solver, const double* eincD, double eps,
-              int64_t maxIter, const double* startD, double* polOut,
-              orc_stats* st, int64_t stopAfter, double* history,
-              int64_t historyCap) {
-  SolveCtx s(p);
+// followed by CpuIterativeSolver::getResult (DDA/CpuIterativeSolver.cpp:93-99),
+// in precision F; host vectors are FP64 complex on both sides.
+template <class F>
+int solve_t(orc_problem* p, const std::vector<std::complex<F>>& D, std::vector<std::complex<F>>& X, int solver,
+            const double* eincD, double eps, int64_t maxIter, const double* startD, double* polOut,
+            orc_stats* st, int64_t stopAfter, double* history, int64_t historyCap) {
+  typedef std::complex<F> C;
+  SolveCtx<F> s(p, D, X);
   size_t n = p->vecSize();
-  Vec einc(reinterpret_cast<const cd*>(eincD), reinterpret_cast<const cd*>(eincD) + n);
-  Vec start;
-  if (startD) start.assign(reinterpret_cast<const cd*>(startD), reinterpret_cast<const cd*>(startD) + n);
+  const cd* ei = reinterpret_cast<const cd*>(eincD);
+  VecT<F> einc(n), start;
+  for (size_t i = 0; i < n; i++) einc[i] = C(ei[i]);
+  if (startD) {
+    const cd* sd = reinterpret_cast<const cd*>(startD);
+    start.resize(n);
+    for (size_t i = 0; i < n; i++) start[i] = C(sd[i]);
+  }
   s.inprodR = initGeneral(s, einc, start);
-  s.epsB = eps * eps / s.residScale;
+  s.epsB = (F)(eps * eps) / s.residScale;
   int rc;
   static const size_t maxInc[4] = {50000, 30000, 50000, 10};
   if (solver < 0 || solver > 3) {
@@ -1070,26 +1143,54 @@ int orc_solve(orc_problem* p, int solver, const double* eincD, double eps,
     return -1;
   }
   size_t mi = maxIter > 0 ? (size_t)maxIter : (size_t)-1;
-  if (solver == 0) { Qmr q; rc = runSolver(s, q, mi, maxInc[0], stopAfter); }
-  else if (solver == 1) { BicgStab q; rc = runSolver(s, q, mi, maxInc[1], stopAfter); }
-  else if (solver == 2) { BicgCs q; rc = runSolver(s, q, mi, maxInc[2], stopAfter); }
-  else { Cgnr q; rc = runSolver(s, q, mi, maxInc[3], stopAfter); }
+  if (solver == 0) { Qmr<F> q; rc = runSolver(s, q, mi, maxInc[0], stopAfter); }
+  else if (solver == 1) { BicgStab<F> q; rc = runSolver(s, q, mi, maxInc[1], stopAfter); }
+  else if (solver == 2) { BicgCs<F> q; rc = runSolver(s, q, mi, maxInc[2], stopAfter); }
+  else { Cgnr<F> q; rc = runSolver(s, q, mi, maxInc[3], stopAfter); }
   if (rc < 0) g_error = s.msg;
   if (polOut) {
-    Vec pv(n, 0);
+    VecT<F> pv(n, 0);
     s.multCc(s.x, pv, false);
-    std::memcpy(polOut, pv.data(), n * sizeof(cd));
+    cd* out = reinterpret_cast<cd*>(polOut);
+    for (size_t i = 0; i < n; i++) out[i] = cd(pv[i]);
   }
   if (st) {
     st->iterations = (int64_t)s.history.size();
     st->residScale = s.residScale;
     st->inprodR = s.inprodR;
-    st->relResidual = std::sqrt(s.inprodR * s.residScale);
+    st->relResidual = std::sqrt((double)s.inprodR * (double)s.residScale);
     st->status = rc;
   }
   if (history)
     for (size_t i = 0; i < s.history.size() && (int64_t)i < historyCap; i++) history[i] = s.history[i];
   return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+// solver: 0 = qmr, 1 = bicgstab, 2 = bicg (BiCG-CS), 3 = cgnr.
+// stop_after > 0 stops after that many iterations (a bounded timing sample;
+// status 1).  history (may be NULL) receives up to history_cap RE_ values.
+int orc_solve(orc_problem* p, int solver, const double* eincD, double eps,
+              int64_t maxIter, const double* startD, double* polOut,
+              orc_stats* st, int64_t stopAfter, double* history,
+              int64_t historyCap) {
+  return solve_t<double>(p, p->D, p->X, solver, eincD, eps, maxIter, startD, polOut, st, stopAfter, history,
+                         historyCap);
+}
+
+// The same solve on the reference's --ftype float CPU path: D (DMatrixCpu<float>,
+// built on first use), the matvec (MatVecCpu<float>) and the solver
+// (QmrCs<float>, ...) in float.
+int orc_solve_f32(orc_problem* p, int solver, const double* eincD, double eps,
+                  int64_t maxIter, const double* startD, double* polOut,
+                  orc_stats* st, int64_t stopAfter, double* history,
+                  int64_t historyCap) {
+  if (p->D32.empty()) build_dmatrix_t<float>(p, p->D32);
+  return solve_t<float>(p, p->D32, p->X32, solver, eincD, eps, maxIter, startD, polOut, st, stopAfter, history,
+                        historyCap);
 }
 
 }  // extern "C"

@@ -83,6 +83,8 @@ def lib():
                                 dp, dp, ctypes.POINTER(OrcStats), ctypes.c_int64, dp,
                                 ctypes.c_int64]
         L.orc_solve.restype = ctypes.c_int
+        L.orc_solve_f32.argtypes = L.orc_solve.argtypes
+        L.orc_solve_f32.restype = ctypes.c_int
         L.orc_calc_field.argtypes = [vp, dp, dp, dp]
         L.orc_cross_sections.argtypes = [vp, dp, dp, ctypes.c_int, dp, dp]
         L.orc_jones.argtypes = [vp, dp, dp, dp, dp, dp, ctypes.c_int64, dp]
@@ -303,13 +305,17 @@ class Problem:
         return out
 
     def solve(self, einc, solver="qmr", eps=1e-5, max_iter=0, start=None, stop_after=0,
-              history_cap=100000):
+              history_cap=100000, precision="fp64"):
+        """getPolVec of the reference's CPU path: precision "fp64" (--ftype
+        double) or "fp32" (--ftype float: D, matvec, vectors and scalars in
+        float).  Returns (status, polarisations, stats, residual history)."""
         e = np.ascontiguousarray(einc, dtype=np.complex128)
         pol = np.zeros(self.vec_size, dtype=np.complex128)
         st = OrcStats()
         hist = np.zeros(history_cap)
         s = None if start is None else np.ascontiguousarray(start, dtype=np.complex128)
-        rc = lib().orc_solve(self.h, SOLVERS[solver], _dp(e), eps, max_iter,
+        fn = lib().orc_solve_f32 if precision == "fp32" else lib().orc_solve
+        rc = fn(self.h, SOLVERS[solver], _dp(e), eps, max_iter,
                              None if s is None else _dp(s), _dp(pol), ctypes.byref(st),
                              stop_after, _dp(hist), history_cap)
         return rc, pol, st, hist[:min(st.iterations, history_cap)].copy()

@@ -51,8 +51,31 @@ def parse():
     ap.add_argument("--requests", type=int, default=120, help="serve: requests in the stream")
     ap.add_argument("--rate", type=float, default=50.0, help="serve: mean arrivals per second")
     ap.add_argument("--slots", type=int, default=8, help="serve: concurrent requests")
-    ap.add_argument("--max-iter", type=int, default=4000, help="mixed512: iteration cap of each solve")
+    ap.add_argument("--max-iter", type=int, default=0, help="mixed512: iteration cap of each solve (0: none)")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="default line without the 128-rhs spheroid block beside it")
+    ap.add_argument("--matvec-only", type=int, default=0,
+                    help="run this many matvecs of the workload and exit (for ncu captures)")
+    ap.add_argument("--rhs", type=int, default=0, help="--matvec-only: right-hand sides (0: the workload's)")
     return ap.parse_args()
+
+
+# DRAM traffic per launch of the y/z plane kernel (dram__bytes_read.sum +
+# dram__bytes_write.sum), from ncu captures of `bench.py --matvec-only`:
+#   box:       the default workload, FP32, 2 rhs (captured at full size)
+#   spheroid:  the 128-rhs block's kernel captured at 8 rhs; the traffic is
+#              a fixed part (D octant, tables) plus a part per rhs, so a full
+#              launch is fixed + 128 * per_rhs
+# Summaries with the commands: profiles/k_yz_p_box10x5x5_fp32.md,
+# profiles/k_yz_p_spheroid_fp32.md.
+TRAFFIC = {"box": None, "spheroid": None}
+
+
+def traffic_per_launch(workload, nrhs):
+    t = TRAFFIC.get(workload)
+    if t is None:
+        return None
+    return int(t["fixed"] + nrhs * t["per_rhs"])
 
 
 def dist_env():
@@ -217,10 +240,11 @@ def cpu_sample(precision="fp32"):
     other = "fp64" if precision == "fp32" else "fp32"
     arm.precision = other
     res_o = [arm.solve(pol) for pol in (1, 2)]
-    arm.precision = precision
+    arm.precision = "fp64"
     arm.O.set_threads(1)
     t1, it1 = arm.solve(1)
     arm.O.set_threads(threads)
+    arm.precision = precision
     return {"value": 2.0 / sum(secs), "unit": "solves/s", "cores": threads, "kind": "port",
             "precision": precision,
             "sample": "oracle BiCGStab (%s, the reference's --ftype %s CPU path), full solves of both "
@@ -230,7 +254,7 @@ def cpu_sample(precision="fp32"):
             other: {"value": 2.0 / sum(r[0] for r in res_o), "unit": "solves/s", "cores": threads,
                     "seconds": [r[0] for r in res_o], "iterations": [r[1] for r in res_o]},
             "single_thread": {"value": 1.0 / t1, "unit": "solves/s", "cores": 1, "seconds": t1,
-                              "iterations": it1, "precision": precision,
+                              "iterations": it1, "precision": "fp64",
                               "sample": "oracle BiCGStab, full solve of polarisation 1"},
             "nproc": os.cpu_count(), "cpu_model": cpu_model()}
 
@@ -299,6 +323,7 @@ def run_ours(args):
     sampler.start()
     l0 = mv.launches
     total_ms = 0.0
+    lat = []
     for _ in range(args.steps):
         with torch.cuda.stream(stream):
             flush.zero_()
@@ -308,7 +333,8 @@ def run_ours(args):
         step()
         e1.record(stream)
         e1.synchronize()
-        total_ms += e0.elapsed_time(e1)
+        lat.append(e0.elapsed_time(e1))
+        total_ms += lat[-1]
         sampler.sample()
     launches = mv.launches - l0
     torch.cuda.synchronize()
@@ -350,7 +376,8 @@ def run_ours(args):
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = sb[names[dom]] / (ms[dom] * 1e-3) / 1e9
     roofline = {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak,
-                "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic_per_launch("box", nrhs) if (prec == "fp32" and names[dom] == "yz_planes") else None,
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                 "algorithmic_bytes_per_launch": sb[names[dom]], "ms_per_launch": float(ms[dom])}
     matvec = {"ms": float(ms[3]), "stages_ms": dict(zip(names, map(float, ms[:3]))),
@@ -400,6 +427,11 @@ def run_ours(args):
         del solvers
         mv64.close()
 
+    # the 128-rhs spheroid block beside the box (rank 0, one GPU)
+    batched = None
+    if rank == 0 and world == 1 and not args.no_batched:
+        import bench_workloads
+        batched = bench_workloads.batched_block(3, 1, local, cpu=not args.no_cpu)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
@@ -418,7 +450,10 @@ def run_ours(args):
                 "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "matvec": matvec,
                 "plain_fp64_single_rhs": plain, "ours_fp64_single_rhs": ours64,
                 "speedup_vs_plain": value / plain["value"] if plain else None,
-                "cpu_baseline": cpu, "clocks": clocks}
+                "cpu_baseline": cpu, "clocks": clocks,
+                "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                               "per": "solve of both polarisations (one step)", "samples": len(lat)},
+                "batched_spheroid_128rhs": batched}
         print(json.dumps(line), flush=True)
     if pg:
         pg.barrier()
@@ -461,9 +496,39 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_matvec_only(args):
+    """Runs args.matvec_only matvecs of the workload's context (FP32 unless
+    --precision says otherwise) and exits: the command ncu captures."""
+    import torch
+    import dda_b200
+    torch.cuda.set_device(0)
+    prec = args.precision if args.precision != "mixed" else "fp32"
+    if args.workload == "batched":
+        import bench_workloads
+        nrhs = args.rhs or 128
+        p, einc, rhs = bench_workloads.spheroid_problem(nrhs)
+        mv = dda_b200.CudaMatVec(p, prec, max_rhs=nrhs)
+        for r, (prop, pol) in enumerate(rhs):
+            mv.set_couple_constants(dda_b200.CoupleConstants(p, prop, pol, "ldr"), rhs=r)
+    else:
+        nrhs = args.rhs or 2
+        p, mv, einc = build_problem(prec, nrhs)
+        einc = einc.reshape(nrhs, -1)
+    cdt = torch.complex128 if prec == "fp64" else torch.complex64
+    x = torch.from_numpy(np.ascontiguousarray(einc[:nrhs])).to(cdt).cuda()
+    y = torch.zeros_like(x)
+    torch.cuda.synchronize()
+    for _ in range(args.matvec_only):
+        mv.apply_device(x.data_ptr(), y.data_ptr(), nrhs=nrhs)
+    mv.synchronize()
+    print("matvecs", args.matvec_only, "nrhs", nrhs, "grid", p.grid, "layout", mv.layout, flush=True)
+
+
 if __name__ == "__main__":
     a = parse()
-    if a.impl == "reference":
+    if a.matvec_only:
+        run_matvec_only(a)
+    elif a.impl == "reference":
         run_reference(a)
     elif a.workload == "box":
         run_ours(a)

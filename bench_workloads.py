@@ -71,12 +71,11 @@ def _line(metric, value, unit, args, ms_per_step, dtype, config, **extra):
 
 
 # ------------------------------------------------------------- batched ----
-def run_batched(args):
-    import torch
+def spheroid_problem(nrhs=128):
+    """The 128-rhs spheroid workload: params, incident fields [nrhs][3 nvs],
+    the (direction, polarisation) of each right-hand side."""
     import dda_b200
     from dda_b200 import targets
-    rank, local, world = dist_env()
-    torch.cuda.set_device(local)
     d_um = 0.05
     kd = 15.0 / (48 * 32 * 32) ** (1.0 / 3)
     lam = "%.17gum" % (2 * math.pi * d_um / kd)
@@ -86,13 +85,52 @@ def run_batched(args):
     rng = np.random.default_rng(SEED)
     dirs = rng.normal(size=(64, 3))
     dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
-    nrhs = 128
-    mv = dda_b200.CudaMatVec(p, "mixed", max_rhs=nrhs)
+    rhs = [(tuple(dirs[r // 2]), 1 + r % 2) for r in range(nrhs)]
     einc = np.empty((nrhs, p.vec_size), dtype=np.complex128)
-    for r in range(nrhs):
-        prop, pol = tuple(dirs[r // 2]), 1 + r % 2
-        mv.set_couple_constants(dda_b200.CoupleConstants(p, prop, pol, "ldr"), rhs=r)
+    for r, (prop, pol) in enumerate(rhs):
         einc[r] = p.einc(prop, pol)
+    return p, einc, rhs
+
+
+def spheroid_cpu_sample(p, rhs0, n_iter, precision="fp32", iters=4):
+    """Bounded CPU sample of one right-hand side of the spheroid block: the
+    oracle's QMR-CS set-up plus `iters` iterations, timed, then scaled to
+    `n_iter` iterations (the mean the GPU block needed).  Extrapolated: a
+    full oracle solve of one right-hand side takes minutes."""
+    from oracle import oracle as O
+    og = O.Geometry.from_arrays(p.geometry.positions, p.geometry.materials, "0.05um")
+    op = O.Problem(og, [1.33 + 0.01j], p.wavelength)
+    t0 = time.perf_counter()
+    op.build_dmatrix()
+    t_d = time.perf_counter() - t0
+    prop, pol = rhs0
+    op.set_cc(prop, pol, "ldr")
+    e = op.einc(prop, pol)
+    t0 = time.perf_counter()
+    op.solve(e, "qmr", 1e-5, stop_after=1, precision=precision)
+    t1 = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    op.solve(e, "qmr", 1e-5, stop_after=1 + iters, precision=precision)
+    tn = time.perf_counter() - t0
+    per_it = (tn - t1) / iters
+    per_solve = (t1 - per_it) + n_iter * per_it
+    return {"value": 1.0 / per_solve, "unit": "solves/s", "cores": O.max_threads(), "kind": "port",
+            "precision": precision, "extrapolated": True, "seconds_per_iteration": per_it,
+            "sample": "oracle QMR-CS (%s), rhs 0: set-up + 1 and %d iterations timed, scaled to %.0f "
+                      "iterations (the GPU block's mean); D matrix %.1f s beforehand"
+                      % (precision, 1 + iters, n_iter, t_d)}
+
+
+def batched_block(steps, warmup, local=0, nrhs=128, cpu=True):
+    """The 128-rhs spheroid block measured on this GPU; returns the line's
+    fields (value, latency, e2e, roofline, matvec, FP64 comparisons, CPU
+    sample)."""
+    import torch
+    import dda_b200
+    p, einc, rhs = spheroid_problem(nrhs)
+    mv = dda_b200.CudaMatVec(p, "mixed", max_rhs=nrhs)
+    for r, (prop, pol) in enumerate(rhs):
+        mv.set_couple_constants(dda_b200.CoupleConstants(p, prop, pol, "ldr"), rhs=r)
     solver = dda_b200.CudaSolver(mv, "qmr")
     e_dev = torch.from_numpy(einc).cuda()  # FP64 pairs: the refinement's outer residual is FP64
     pol_dev = torch.zeros_like(e_dev)
@@ -102,7 +140,7 @@ def run_batched(args):
     def step():
         solver.get_pol_vec_device(e_dev.data_ptr(), pol_dev.data_ptr(), nrhs, 1e-5)
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         step()
     torch.cuda.synchronize()
     iters = [st.iterations for st in solver.last_stats]
@@ -111,9 +149,8 @@ def run_batched(args):
     sampler = ClockSampler(local)
     sampler.start()
     l0 = mv.launches
-    total = 0.0
     lat = []
-    for _ in range(args.steps):
+    for _ in range(steps):
         with torch.cuda.stream(stream):
             flush.zero_()
             a = torch.cuda.Event(enable_timing=True)
@@ -127,13 +164,14 @@ def run_batched(args):
     total = sum(lat)
     launches = mv.launches - l0
     clocks = sampler.stop()
-    value = nrhs * args.steps / (total / 1000.0)
+    value = nrhs * steps / (total / 1000.0)
     # e2e through the host API, from and into pinned host memory
     einc_host = torch.empty(einc.size, dtype=torch.complex128, pin_memory=True).numpy()
     einc_host[:] = einc.reshape(-1)
     pol_host = torch.empty(einc.size, dtype=torch.complex128, pin_memory=True).numpy()
     e2e_ms = 0.0
-    for _ in range(max(1, args.steps // 2)):
+    n_e2e = max(1, steps // 2)
+    for _ in range(n_e2e):
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
         a.record(stream)
@@ -141,10 +179,10 @@ def run_batched(args):
         b.record(stream)
         b.synchronize()
         e2e_ms += a.elapsed_time(b)
-    n_e2e = max(1, args.steps // 2)
     e2e = {"value": nrhs * n_e2e / (e2e_ms / 1000.0), "unit": "solves/s",
            "h2d_bytes_per_step": int(einc.nbytes), "d2h_bytes_per_step": int(einc.nbytes)}
     roof, matvec = _roofline(p, mv, nrhs, 8, reps=3)
+    roof["traffic"] = bench.traffic_per_launch("spheroid", nrhs)
     layout = mv.layout
     mv.close()
     del e_dev, pol_dev, einc_host, pol_host
@@ -161,14 +199,14 @@ def run_batched(args):
     its64 = []
     a.record(st64)
     for r in range(2):
-        mv64.set_couple_constants(dda_b200.CoupleConstants(p, tuple(dirs[0]), 1 + r, "ldr"))
+        mv64.set_couple_constants(dda_b200.CoupleConstants(p, rhs[r][0], rhs[r][1], "ldr"))
         s64.get_pol_vec(einc[r], 1e-5, history_cap=1)
         its64.append(s64.last_stats[0].iterations)
     b.record(st64)
     b.synchronize()
     ours64 = {"value": 2 / (a.elapsed_time(b) / 1000.0), "unit": "solves/s", "iterations": its64,
               "sample": "incidence 0, both polarisations, one FP64 solve each (this library)"}
-    sps = [bench_plain.PlainSolver(mv64, p, dda_b200.CoupleConstants(p, tuple(dirs[0]), 1 + r, "ldr").cc_sqrt)
+    sps = [bench_plain.PlainSolver(mv64, p, dda_b200.CoupleConstants(p, rhs[r][0], rhs[r][1], "ldr").cc_sqrt)
            for r in range(2)]
     sps[0].solve_qmr(einc[0], 1e-5, max_iter=5)  # cuFFT plans
     torch.cuda.synchronize()
@@ -181,18 +219,34 @@ def run_batched(args):
                        "vector operations, host-side scalars, bench_plain.py)"}
     del sps
     mv64.close()
-    _line("solves/s at relative residual 1e-5 (128-rhs spheroid block, QMR-CS)", value, "solves/s", args,
-          total / args.steps, "c64+f64",
-          {"workload": "spheroid 48x32x32 dipoles, m=1.33+0.01i, k a_eq=15, 64 directions x 2 pols = 128 rhs, "
-                       "qmr eps=1e-5, fp32 + fp64 refinement", "nv": p.nv, "grid": list(p.grid), "rhs_per_step": nrhs,
-           "iterations_max": max(iters), "iterations_mean": float(np.mean(iters)), "max_rel_residual": resid,
-           "refinements_max": max(refs),
-           "l2": "flushed between steps (256 MB write)", "layout": layout},
-          e2e=e2e, gpu_launches=launches, roofline=roof, matvec=matvec, plain_fp64_single_rhs=plain,
-          ours_fp64_single_rhs=ours64, speedup_vs_plain=value / plain["value"],
-          latency_ms={"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
-                      "per": "block of 128 rhs", "samples": len(lat)},
-          clocks=clocks)
+    cpu_b = None
+    if cpu:
+        try:
+            cpu_b = spheroid_cpu_sample(p, rhs[0], float(np.mean(iters)))
+        except Exception as ex:  # the CPU baseline is reported, never required
+            cpu_b = {"value": None, "error": str(ex)}
+    return {"value": value, "unit": "solves/s", "ms_per_step": total / steps, "steps": steps, "warmup": warmup,
+            "config": {"workload": "spheroid 48x32x32 dipoles, m=1.33+0.01i, k a_eq=15, 64 directions x 2 pols "
+                                   "= 128 rhs, qmr eps=1e-5, fp32 convolution + fp64 refinement",
+                       "nv": p.nv, "grid": list(p.grid), "rhs_per_step": nrhs, "precision": "mixed"},
+            "iterations_max": max(iters), "iterations_mean": float(np.mean(iters)), "max_rel_residual": resid,
+            "refinements_max": max(refs), "l2": "flushed between steps (256 MB write)", "layout": layout,
+            "e2e": e2e, "gpu_launches": launches, "roofline": roof, "matvec": matvec,
+            "plain_fp64_single_rhs": plain, "ours_fp64_single_rhs": ours64,
+            "speedup_vs_plain": value / plain["value"],
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                           "per": "block of %d rhs" % nrhs, "samples": len(lat)},
+            "cpu_baseline": cpu_b, "clocks": clocks}
+
+
+def run_batched(args):
+    import torch
+    rank, local, world = dist_env()
+    torch.cuda.set_device(local)
+    d = batched_block(args.steps, args.warmup, local, cpu=not args.no_cpu)
+    extra = {k: v for k, v in d.items() if k not in ("value", "unit", "ms_per_step", "steps", "warmup", "config")}
+    _line("solves/s at relative residual 1e-5 (128-rhs spheroid block, QMR-CS)", d["value"], "solves/s", args,
+          d["ms_per_step"], "c64+f64", d["config"], **extra)
 
 
 # ------------------------------------------------------------ mixed512 ----

@@ -69,8 +69,10 @@ def test_fixture_box_10_8_6(oracle):
     assert g.nv == 480
     assert g.box_size == (10, 8, 6)
     assert g.mat_count == 1
-    ref = "/root/reference/DDA/box_10_8_6.geom"
-    if os.path.exists(ref):  # same dipole list as the reference's fixture
+    # DDA_REFERENCE_DIR: a checkout of the reference, to compare with its own
+    # fixture file (skipped when unset)
+    ref = os.path.join(os.environ.get("DDA_REFERENCE_DIR", ""), "DDA", "box_10_8_6.geom")
+    if os.environ.get("DDA_REFERENCE_DIR") and os.path.exists(ref):  # same dipole list as the reference's fixture
         r = oracle.Geometry.load_text(ref, "0.1um")
         assert np.array_equal(r.positions(), g.positions())
         assert np.array_equal(r.materials(), g.materials())
@@ -211,3 +213,21 @@ def test_product_mie_matches_oracle(oracle, x, m):
     want = oracle.mie(x, m)
     for g, w in zip(got, want):  # Qabs of a lossless sphere is a difference of equal terms
         assert abs(g - w) <= 1e-9 * max(abs(w), want[0])
+
+
+def test_float_path_tracks_double(oracle):
+    # the reference's --ftype float CPU path (D built in float by
+    # DMatrixCpu<float>, matvec, vectors and scalars in float) against its
+    # double path on a small target.  Building D in float costs about 1e-4
+    # relative accuracy (1/r^3 terms over a wide dynamic range through float
+    # FFTs), so the solutions agree to that level, not to float rounding.
+    g = oracle.Geometry.sphere("0.6um", "0.1um")
+    p = oracle.Problem(g, [1.5 + 0.1j], "1um")
+    p.build_dmatrix()
+    p.set_cc((0, 0, 1), 1, "ldr")
+    e = p.einc((0, 0, 1), 1)
+    rc64, p64, st64, _ = p.solve(e, "bicgstab", 1e-5)
+    rc32, p32, st32, _ = p.solve(e, "bicgstab", 1e-5, precision="fp32")
+    assert rc64 == 0 and rc32 == 0
+    assert abs(st64.iterations - st32.iterations) <= 3
+    assert np.linalg.norm(p32 - p64) / np.linalg.norm(p64) < 1e-3

@@ -31,6 +31,7 @@ class Problem(ctypes.Structure):
                 ("device", ctypes.c_int32), ("flags", ctypes.c_uint32)]
 
 FLAG_SPLIT_YZ = 1
+FLAG_YZ_GROUPS2 = 32
 
 
 class Stats(ctypes.Structure):
@@ -377,6 +378,8 @@ class CudaMatVec:
                 "compile_time_plans", "device_bytes")
         d = dict(zip(keys, (int(x) for x in v)))
         d["yz_path"] = ("fused", "cluster", "split")[d["yz_path"]]
+        if d["yz_path"] == "fused":  # slot 2 holds the fused kernel's thread groups
+            d["groups"] = d.pop("cluster_size")
         return d
 
     def profile(self, nrhs=1, reps=10):

@@ -197,6 +197,7 @@ template <typename T> struct Engine {
   T2* xo = nullptr;    // MIXED, FP64 engine: refined solution x and b = sqrt(cc) Einc
   T2* bo = nullptr;
   bool fused = false;
+  int yz_groups = 1;          // fused kernel: 1 CTA-wide group, or 2 groups of half the CTA (k.yz2)
   bool slot_path = false;     // k_yz_slot: cluster per plane through L2 slots
   T2* slots = nullptr;        // [ncl][Gz][wp]
   uint32_t* order = nullptr;  // kx positions, mirrored frequencies adjacent
@@ -455,6 +456,11 @@ template <typename T> void setup_engine(dda_ctx* c) {
   e.yz_fixed = fixed;
   e.yz_row = row;
   e.fused = e.k.yz && e.smem_yz <= kSmemMax && !(c->flags & (DDA_FLAG_SPLIT_YZ | DDA_FLAG_SLOT_YZ));
+  if (e.fused && e.k.yz2 && (c->flags & DDA_FLAG_YZ_GROUPS2) && nrw >= 2) {
+    e.yz_groups = 2;
+    e.yz.nrw = nrw & ~1;  // an even number of rows: half to each group
+    e.smem_yz = fixed + e.yz.nrw * row;
+  }
   if (!e.fused && e.k.slot && !(c->flags & DDA_FLAG_SPLIT_YZ)) setup_slot<T>(c, e);
   if (!e.fused && !e.slot_path) {
     // split path: zbuf, k_yrows over NW rows per CTA, column FFTs along z
@@ -495,7 +501,10 @@ template <typename T> void setup_engine(dda_ctx* c) {
   };
   attr((const void*)e.k.xfwd, e.smem_x);
   attr((const void*)e.k.xinv, e.smem_x);
-  if (e.fused) attr((const void*)e.k.yz, e.smem_yz);
+  if (e.fused) {
+    attr((const void*)e.k.yz, e.smem_yz);
+    if (e.k.yz2) attr((const void*)e.k.yz2, e.smem_yz);
+  }
   else if (!e.slot_path) {
     attr((const void*)e.k.yrows, e.smem_rows);
     attr((const void*)e.k.cols, e.smem_cols);
@@ -552,7 +561,8 @@ void launch_yz(dda_ctx* c, int nrhs, cudaStream_t s, KrylovState* st, int skipmv
   const MvGeom& g = c->g;
   const FftPlanDev py = c->my.dev<T>(), pz = c->mz.dev<T>();
   if (e.fused) {
-    e.k.yz<<<dim3(g.Gx, nrhs), kNtYz, e.smem_yz, s>>>(e.xhat, e.dc, g, e.yz, pz, py, st, skipmv);
+    (e.yz_groups == 2 ? e.k.yz2 : e.k.yz)<<<dim3(g.Gx, nrhs), kNtYz, e.smem_yz, s>>>(e.xhat, e.dc, g, e.yz, pz, py,
+                                                                                      st, skipmv);
   } else if (e.slot_path) {
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute at[1];
@@ -585,7 +595,7 @@ void launch_yz(dda_ctx* c, int nrhs, cudaStream_t s, KrylovState* st, int skipmv
 // size and rows per batch.  Timed on the context's own buffers (x spectrum
 // zeroed, one right-hand side) and kept per shape for the process.
 struct TuneChoice {
-  int nrw = 0, cl = 0;
+  int nrw = 0, cl = 0, groups = 1;
 };
 std::mutex g_tune_mu;
 std::map<std::array<int, 6>, TuneChoice> g_tune_cache;
@@ -615,6 +625,7 @@ template <typename T> void apply_choice(dda_ctx* c, Engine<T>& e, const TuneChoi
   const MvGeom& g = c->g;
   if (e.fused) {
     e.yz.nrw = t.nrw;
+    e.yz_groups = t.groups;
     e.smem_yz = e.yz_fixed + (size_t)t.nrw * e.yz_row;
   } else if (e.slot_path) {
     e.cl = t.cl;
@@ -644,7 +655,10 @@ template <typename T> void autotune(dda_ctx* c) {
   if (e.fused) {
     const int max_rows = e.k.planned ? 48 : kNtYz / 32;
     for (int n : {4, 6, 8, 10, 12, 14, 16, 20, 24, 25, 28, 32, 34, 36, 40, 43, 48})
-      if (n <= max_rows && e.yz_fixed + (size_t)n * e.yz_row <= kSmemMax) cands.push_back({n, 0});
+      if (n <= max_rows && e.yz_fixed + (size_t)n * e.yz_row <= kSmemMax) {
+        if (!(c->flags & DDA_FLAG_YZ_GROUPS2)) cands.push_back({n, 0, 1});
+        if (e.k.yz2 && n % 2 == 0) cands.push_back({n, 0, 2});  // two groups of n/2 rows
+      }
   } else {
     for (int cl : {4, 8, 16})
       for (int n : {4, 8, 16})
@@ -958,40 +972,53 @@ struct SolveOpts {
 constexpr double kGapRatio = 4.0;  // |r_true|^2 > 4 |r_rec|^2: the gap dominates
 
 // Precision of the convolution in an adaptive MIXED inner solve
-// (SolveOpts::adapt), decided between rounds from the recurrence residuals.
+// (SolveOpts::adapt), decided between rounds from the recurrence residuals
+// of the right-hand sides still running (the worst one decides).  The solve
+// starts with the FP32 convolution.  If the best residual does not halve
+// within `window` iterations, the FP32 rounding is taken to hold the Krylov
+// recurrences back (on large, high-index targets QMR-CS with the FP32
+// convolution stays on a residual plateau that the FP64 solve leaves), and
+// the solve continues, in the same Krylov space, with the FP64 convolution
+// until the residual has fallen by `drop` below the level of the stall; then
+// it tries the FP32 convolution again.
 struct MixedSwitch {
-  bool start32 = false, mode32 = false;
-  double tau = 1e-3;        // FP64 -> FP32 when every running rhs is below tau
-  long long window = 256;   // FP32 iterations over which the residual must halve
-  long long mark_it = 0;
-  double mark = 0;
-  explicit MixedSwitch(const SolveOpts& o) {
-    if (const char* v = getenv("DDA_MX_TAU")) tau = atof(v);
+  bool mode32 = true;
+  long long window = 1024;
+  double drop = 0.01;
+  double tau = 0;            // FP64 -> FP32 below this
+  long long mark_it = -1;    // start of the current FP32 window
+  double mark = 0;           // best residual there
+  long long it32 = 0;        // iterations run with the FP32 convolution
+  MixedSwitch() {
     if (const char* v = getenv("DDA_MX_W")) window = atoll(v);
-    if (const char* v = getenv("DDA_MX_START")) start32 = atoi(v) != 0;
-    (void)o;
-    mode32 = start32;
+    if (const char* v = getenv("DDA_MX_DROP")) drop = atof(v);
+    if (const char* v = getenv("DDA_MX_START")) mode32 = atoi(v) != 0;
+    if (const char* v = getenv("DDA_MX_TAU")) tau = atof(v);
   }
-  bool update(const KrylovState* st, int nrhs, long long nr) {
+  bool update(const KrylovState* st, int nrhs, long long nr, long long poll) {
     double worst = 0;
     for (int r = 0; r < nrhs; r++)
       if (!st[r].done) worst = std::max(worst, std::sqrt(st[r].inprodR * st[r].residScale));
-    if (!mode32) {
-      if (worst < tau) {
-        mode32 = true;
+    if (mode32) {
+      it32 += poll;
+      if (mark_it < 0) {
         mark_it = nr;
         mark = worst;
-        if (getenv("DDA_MX_LOG")) fprintf(stderr, "mx: -> fp32 at %lld rel %.3e\n", nr, worst);
+      } else if (nr - mark_it >= window) {
+        if (worst > 0.5 * mark) {
+          mode32 = false;
+          tau = drop * worst;
+          if (getenv("DDA_MX_LOG")) fprintf(stderr, "mx: -> fp64 at %lld rel %.3e\n", nr, worst);
+        } else {
+          mark_it = nr;
+          mark = worst;
+        }
       }
-    } else if (nr - mark_it >= window) {
-      if (worst > 0.5 * mark) {  // stalled: FP64 until one more decade is gained
-        mode32 = false;
-        tau = 0.1 * worst;
-        if (getenv("DDA_MX_LOG")) fprintf(stderr, "mx: -> fp64 at %lld rel %.3e\n", nr, worst);
-      } else {
-        mark_it = nr;
-        mark = worst;
-      }
+    } else if (worst < tau) {
+      mode32 = true;
+      mark_it = nr;
+      mark = worst;
+      if (getenv("DDA_MX_LOG")) fprintf(stderr, "mx: -> fp32 at %lld rel %.3e\n", nr, worst);
     }
     return mode32;
   }
@@ -1087,8 +1114,8 @@ void run_solve(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
     }
     return -1;
   };
-  MixedSwitch ms(o);
-  if (o.adapt) sv.mv32 = ms.start32;
+  MixedSwitch ms;
+  if (o.adapt) sv.mv32 = ms.mode32;
   for (int round = 0;; round++) {
     if (!graphs || round == 0) {
       for (int k = 0; k < poll; k++) sv.iteration(solver, nr++, b);
@@ -1134,8 +1161,11 @@ void run_solve(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
       break;
     }
     if constexpr (std::is_same<T, double>::value) {
-      if (o.check_every > 0 && nr % o.check_every == 0 && check_gap(c, nrhs, b.X, B, S, o)) break;
-      if (o.adapt) sv.mv32 = ms.update(c->st_host, nrhs, nr);
+      // the FP64 check only once the FP32 convolution has run (the gap is
+      // its rounding carried along)
+      const bool gap_possible = !o.adapt || ms.it32 > 0;
+      if (o.check_every > 0 && nr % o.check_every == 0 && gap_possible && check_gap(c, nrhs, b.X, B, S, o)) break;
+      if (o.adapt) sv.mv32 = ms.update(c->st_host, nrhs, nr, poll);
     }
   }
   if (b.X != e.vec[4])
@@ -1373,9 +1403,10 @@ int dda_create(const dda_problem* p, int precision, dda_ctx** out) {
     if (p->dmatrix) upload_dmatrix(c.get(), p->dmatrix);
     else build_dmatrix(c.get());
     if (!(c->flags & DDA_FLAG_NO_AUTOTUNE)) {
-      // MIXED runs its FP64 engine only for the few outer residuals
+      // MIXED runs its FP64 engine for the outer residuals, the FP64 checks
+      // and the FP64 phases of its inner solves
       if (c->e32.on) autotune<float>(c.get());
-      if (c->e64.on && precision == DDA_PREC_FP64) autotune<double>(c.get());
+      if (c->e64.on) autotune<double>(c.get());
     }
     CK(cudaStreamSynchronize(c->stream));
     c->dev_bytes = g_dalloc_bytes;
@@ -1850,7 +1881,7 @@ int dda_matvec_layout(const dda_ctx* ctx, int64_t* out) {
   auto fill = [&](const auto& e) {
     out[0] = e.fused ? 0 : e.slot_path ? 1 : 2;
     out[1] = e.ncl;
-    out[2] = e.cl;
+    out[2] = e.fused ? e.yz_groups : e.cl;
     out[3] = e.slot_path ? e.sg.nrw : e.yz.nrw;
     out[4] = (int64_t)(e.fused ? e.smem_yz : e.slot_path ? e.smem_slot : e.smem_rows);
   };

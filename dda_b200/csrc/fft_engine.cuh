@@ -218,8 +218,12 @@ __device__ __forceinline__ typename C2<T>::t* smem_at(int off) {
 // (a + 0.5)/d stays 0.5/d away from an integer, above the rounding error.
 __device__ __forceinline__ int fdiv_i(int a, float rcp) { return (int)(((float)a + 0.5f) * rcp); }
 
-template <int G> __device__ __forceinline__ void group_sync() {
-  if (G == 32) __syncwarp(); else __syncthreads();
+// Barrier of a group of G threads: the warp (G == 32), the CTA (bar == 0),
+// or the named barrier `bar` (1..15) shared by G threads of the CTA.
+template <int G> __device__ __forceinline__ void group_sync(int bar = 0) {
+  if (G == 32) __syncwarp();
+  else if (bar == 0) __syncthreads();
+  else asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(G) : "memory");
 }
 
 // One radix-R stage over nl lines by a group of G threads (one warp, or the

@@ -219,7 +219,7 @@ __device__ __forceinline__ void butterfly(T2* v, int j, const T2* tw) {
 // (line, butterfly) pairs with the line fastest, so a line tile and a column
 // tile both keep every lane busy.
 template <typename T, typename P, int I, bool INV, int G>
-__device__ __forceinline__ void pstage(int soff, int nl, int ls, int es, int twoff, int tid) {
+__device__ __forceinline__ void pstage(int soff, int nl, int ls, int es, int twoff, int tid, int bar = 0) {
   typedef typename C2<T>::t T2;
   constexpr int R = P::r[I];
   constexpr int L = P::L(I);
@@ -241,19 +241,19 @@ __device__ __forceinline__ void pstage(int soff, int nl, int ls, int es, int two
 #pragma unroll
     for (int m = 0; m < R; m++) s[base + m * mstep] = v[m];
   }
-  group_sync<G>();
+  group_sync<G>(bar);
 }
 
 // Stages [I0, I1) of P, forward in order or inverse in reverse order.
 template <typename T, typename P, bool INV, int G, int I0, int I1>
-__device__ __forceinline__ void pstages(int soff, int nl, int ls, int es, int twoff, int tid) {
+__device__ __forceinline__ void pstages(int soff, int nl, int ls, int es, int twoff, int tid, int bar = 0) {
   if constexpr (I0 < I1) {
     if constexpr (!INV) {
-      pstage<T, P, I0, false, G>(soff, nl, ls, es, twoff, tid);
-      pstages<T, P, false, G, I0 + 1, I1>(soff, nl, ls, es, twoff, tid);
+      pstage<T, P, I0, false, G>(soff, nl, ls, es, twoff, tid, bar);
+      pstages<T, P, false, G, I0 + 1, I1>(soff, nl, ls, es, twoff, tid, bar);
     } else {
-      pstage<T, P, I1 - 1, true, G>(soff, nl, ls, es, twoff, tid);
-      pstages<T, P, true, G, I0, I1 - 1>(soff, nl, ls, es, twoff, tid);
+      pstage<T, P, I1 - 1, true, G>(soff, nl, ls, es, twoff, tid, bar);
+      pstages<T, P, true, G, I0, I1 - 1>(soff, nl, ls, es, twoff, tid, bar);
     }
   }
 }

@@ -23,6 +23,7 @@ template <typename T> struct MvKernels {
   XfwdFn xfwd = nullptr;
   XinvFn xinv = nullptr;
   YzFn yz = nullptr;        // fused plane kernel (nullptr: none for this shape)
+  YzFn yz2 = nullptr;       // the same kernel run as two groups of half the CTA
   YrowsFn yrows = nullptr;  // split path
   ColsFn cols = nullptr;
   SlotFn slot = nullptr;    // cluster plane kernel for planes beyond shared memory
@@ -42,13 +43,13 @@ inline bool has_tuned_plan(int n) {
 
 // Fused plane kernel for y = z = N; the HALF variant when the box is exactly
 // half the grid in y and z and the first radix is even.
-template <typename T, int NTYZ, int N>
+template <typename T, int NTYZ, int N, int GR = 1>
 typename MvKernels<T>::YzFn fused_kernel(bool half) {
   typedef typename PlanFor<N>::type P;
   if constexpr (P::r[0] % 2 == 0) {
-    if (half) return k_yz_p<T, NTYZ, P, P, true>;
+    if (half) return k_yz_p<T, NTYZ, P, P, true, GR>;
   }
-  return k_yz_p<T, NTYZ, P, P, false>;
+  return k_yz_p<T, NTYZ, P, P, false, GR>;
 }
 
 // Cluster plane kernel for y = z = N, likewise.
@@ -103,7 +104,10 @@ void planned_fused(MvKernels<T>& k, int gy, int gz, int by, int bz) {
   if (gy != gz) return;
   switch (gy) {
 #define C(N)                                                                                     \
-  case N: k.yz = fused_kernel<T, NTYZ, N>(2 * by == gy && 2 * bz == gz); break;
+  case N:                                                                                       \
+    k.yz = fused_kernel<T, NTYZ, N>(2 * by == gy && 2 * bz == gz);                               \
+    k.yz2 = fused_kernel<T, NTYZ, N, 2>(2 * by == gy && 2 * bz == gz);                           \
+    break;
     DDA_FUSED_LENGTHS(C)
 #undef C
     default: break;

@@ -71,15 +71,17 @@ inline std::vector<int> tuned_radices(int n) {
 // first radix even), so inputs z = j + m S0 are zero exactly for m >= R / 2
 // and the inverse keeps exactly the outputs m < R / 2: with that known at
 // compile time the zero operands and the unused outputs fold away.
-template <typename T, int NT, typename PZ, bool HALF = false>
+// Columns [l0, l0 + lw) of the W = 3 by columns, by the G threads of a group
+// (tid in [0, G), barrier `bar`: 0 = the whole CTA).
+template <typename T, int G, typename PZ, bool HALF = false>
 __device__ __forceinline__ void zp_first(const typename C2<T>::t* __restrict__ plane, int soff, int q,
-                                         int by, int bz, int twz) {
+                                         int by, int bz, int twz, int tid, int l0, int lw, int bar) {
   typedef typename C2<T>::t T2;
   constexpr int R = PZ::r[0], S0 = PZ::N / R;
   T2* sm = smem_at<T>(0);
-  const int W = 3 * by, nb = by * bz;
-  for (int b = threadIdx.x; b < W * S0; b += NT) {
-    const int j = b / W, l = b - j * W;
+  const int nb = by * bz;
+  for (int b = tid; b < lw * S0; b += G) {
+    const int j = b / lw, l = l0 + (b - j * lw);
     const int c = l / by, y = l - c * by;
     T2 v[R];
 #pragma unroll
@@ -91,18 +93,18 @@ __device__ __forceinline__ void zp_first(const typename C2<T>::t* __restrict__ p
 #pragma unroll
     for (int m = 0; m < R; m++) sm[soff + (j + m * S0) * q + l] = v[m];
   }
-  __syncthreads();
+  group_sync<G>(bar);
 }
 
-template <typename T, int NT, typename PZ, bool HALF = false>
+template <typename T, int G, typename PZ, bool HALF = false>
 __device__ __forceinline__ void zp_last(typename C2<T>::t* __restrict__ plane, int soff, int q, int by,
-                                        int bz, int twz) {
+                                        int bz, int twz, int tid, int l0, int lw) {
   typedef typename C2<T>::t T2;
   constexpr int R = PZ::r[0], S0 = PZ::N / R;
   T2* sm = smem_at<T>(0);
-  const int W = 3 * by, nb = by * bz;
-  for (int b = threadIdx.x; b < W * S0; b += NT) {
-    const int j = b / W, l = b - j * W;
+  const int nb = by * bz;
+  for (int b = tid; b < lw * S0; b += G) {
+    const int j = b / lw, l = l0 + (b - j * lw);
     const int c = l / by, y = l - c * by;
     T2 v[R];
 #pragma unroll
@@ -197,14 +199,14 @@ __device__ __forceinline__ void row_stage0(typename C2<T>::t* S, int kz, int q, 
 // row r, component c lives in the row buffers at ro + (3 r + c) py.
 
 // y stage 0 fused with the read from (INV: write to) the slab, zero padded.
-template <typename T, int NT, typename PY, bool INV, bool HALF = false>
+template <typename T, int G, typename PY, bool INV, bool HALF = false>
 __device__ __forceinline__ void rows_stage0(typename C2<T>::t* S, int kz0, int nr, int q, int by, int ro,
-                                            int py, int twy) {
+                                            int py, int twy, int tid, int bar) {
   typedef typename C2<T>::t T2;
   constexpr int R = PY::r[0], S0 = PY::N / R;
   T2* sm = smem_at<T>(0);
   const int total = nr * 3 * S0;
-  for (int it = threadIdx.x; it < total; it += NT) {
+  for (int it = tid; it < total; it += G) {
     const int j = it % S0, rc = it / S0;
     const int row = rc / 3, c = rc - 3 * row;
     const int srow = (kz0 + row) * q + c * by;
@@ -230,14 +232,15 @@ __device__ __forceinline__ void rows_stage0(typename C2<T>::t* S, int kz0, int n
       }
     }
   }
-  __syncthreads();
+  group_sync<G>(bar);
 }
 
 // last forward y stage, D-hat multiply, first inverse y stage, in registers
 // (kz positions kz0.. map to frequencies through PZ).
-template <typename T, int NT, typename PY, typename PZ>
+template <typename T, int G, typename PY, typename PZ>
 __device__ __forceinline__ void rows_dmul(int kz0, int nr, int ro, int py,
-                                          const typename C2<T>::t* __restrict__ dc, const MvGeom& g, int kx) {
+                                          const typename C2<T>::t* __restrict__ dc, const MvGeom& g, int kx,
+                                          int tid, int bar) {
   typedef typename C2<T>::t T2;
   constexpr int K = PY::K;
   constexpr int R = PY::r[K - 1];
@@ -249,7 +252,7 @@ __device__ __forceinline__ void rows_dmul(int kz0, int nr, int ro, int py,
   // instead (3 py complex apart); with odd R they take neighbouring
   // butterflies.
   constexpr bool ROW_FAST = R % 2 == 0;
-  for (int it = threadIdx.x; it < nr * NB; it += NT) {
+  for (int it = tid; it < nr * NB; it += G) {
     const int t = ROW_FAST ? it / nr : it % NB, row = ROW_FAST ? it - t * nr : it / NB;
     const int kz = PZ::freq_of(kz0 + row);
     const int base = ro + 3 * row * py + t * R;
@@ -279,10 +282,17 @@ __device__ __forceinline__ void rows_dmul(int kz0, int nr, int ro, int py,
       sm[base + 2 * py + m] = v2[m];
     }
   }
-  __syncthreads();
+  group_sync<G>(bar);
 }
 
-template <typename T, int NT, typename PZ, typename PY, bool HALF = false>
+// GR = 2: the CTA works as two groups of NT/2 threads with their own named
+// barriers.  The z passes split the columns between the groups, the y pass
+// gives each group every other batch of kz rows (in its own half of the row
+// buffers), and only the two hand-overs between the z and y passes are
+// CTA-wide: a group that waits at its barrier leaves the SM to the other
+// group.  Every butterfly does the same arithmetic as with GR = 1, so the
+// results are identical.
+template <typename T, int NT, typename PZ, typename PY, bool HALF = false, int GR = 1>
 __global__ void __launch_bounds__(NT, 1) k_yz_p(typename C2<T>::t* __restrict__ xhat,
                                              const typename C2<T>::t* __restrict__ dc, MvGeom g,
                                              YzGeom y, FftPlanDev pz, FftPlanDev pyp,
@@ -298,22 +308,31 @@ __global__ void __launch_bounds__(NT, 1) k_yz_p(typename C2<T>::t* __restrict__ 
   stage_twiddles<T, NT>(0, pz);
   stage_twiddles<T, NT>(g.Gz, pyp);
   __syncthreads();
-  zp_first<T, NT, PZ, HALF>(plane, soff, y.q, g.by, g.bz, 0);
+  constexpr int G = NT / GR;
+  const int grp = GR == 1 ? 0 : (int)threadIdx.x / G;
+  const int tid = (int)threadIdx.x - grp * G;
+  const int bar = GR == 1 ? 0 : 1 + grp;
   const int w3 = 3 * g.by;
-  plines<T, PZ, NT, false, 1, PZ::K>(soff, w3, 1, y.q, 0);
+  const int l0 = grp * (w3 / GR), lw = grp == GR - 1 ? w3 - l0 : w3 / GR;  // this group's columns
+  zp_first<T, G, PZ, HALF>(plane, soff, y.q, g.by, g.bz, 0, tid, l0, lw, bar);
+  pstages<T, PZ, false, G, 1, PZ::K>(soff + l0, lw, 1, y.q, 0, tid, bar);
+  if (GR > 1) __syncthreads();  // every column transformed before the rows
   {
     const int kxf = g.fx[kx];
-    for (int kz0 = 0; kz0 < g.Gz; kz0 += y.nrw) {  // kz: positions after the z transform
-      const int nr = min(y.nrw, g.Gz - kz0);
-      rows_stage0<T, NT, PY, false, HALF>(S, kz0, nr, y.q, g.by, roff, y.py, g.Gz);
-      pstages<T, PY, false, NT, 1, PY::K - 1>(roff, 3 * nr, y.py, 1, g.Gz, threadIdx.x);
-      rows_dmul<T, NT, PY, PZ>(kz0, nr, roff, y.py, dc, g, kxf);
-      pstages<T, PY, true, NT, 1, PY::K - 1>(roff, 3 * nr, y.py, 1, g.Gz, threadIdx.x);
-      rows_stage0<T, NT, PY, true, HALF>(S, kz0, nr, y.q, g.by, roff, y.py, g.Gz);
+    const int nrg = y.nrw / GR;  // rows per batch of a group
+    const int rog = roff + grp * nrg * 3 * y.py;
+    for (int kz0 = grp * nrg; kz0 < g.Gz; kz0 += GR * nrg) {  // kz: positions after the z transform
+      const int nr = min(nrg, g.Gz - kz0);
+      rows_stage0<T, G, PY, false, HALF>(S, kz0, nr, y.q, g.by, rog, y.py, g.Gz, tid, bar);
+      pstages<T, PY, false, G, 1, PY::K - 1>(rog, 3 * nr, y.py, 1, g.Gz, tid, bar);
+      rows_dmul<T, G, PY, PZ>(kz0, nr, rog, y.py, dc, g, kxf, tid, bar);
+      pstages<T, PY, true, G, 1, PY::K - 1>(rog, 3 * nr, y.py, 1, g.Gz, tid, bar);
+      rows_stage0<T, G, PY, true, HALF>(S, kz0, nr, y.q, g.by, rog, y.py, g.Gz, tid, bar);
     }
   }
-  plines<T, PZ, NT, true, 1, PZ::K>(soff, w3, 1, y.q, 0);
-  zp_last<T, NT, PZ, HALF>(plane, soff, y.q, g.by, g.bz, 0);
+  if (GR > 1) __syncthreads();  // every row back in the slab before the z inverse
+  pstages<T, PZ, true, G, 1, PZ::K>(soff + l0, lw, 1, y.q, 0, tid, bar);
+  zp_last<T, G, PZ, HALF>(plane, soff, y.q, g.by, g.bz, 0, tid, l0, lw);
 }
 
 // Split path rows with a compile-time y plan: each warp one kz row, copied

@@ -293,7 +293,7 @@ __device__ __forceinline__ void slot_rows(typename C2<T>::t* __restrict__ slot,
   } else {
     slot_rows_stage0<T, NT, PY, false, HALF>(slot, g, sg, kz0, nr, ro);
     pstages<T, PY, false, NT, 1, PY::K - 1>(ro, 3 * nr, sg.py, 1, g.Gz, threadIdx.x);
-    rows_dmul<T, NT, PY, PZ>(kz0, nr, ro, sg.py, dc, g, kxf);
+    rows_dmul<T, NT, PY, PZ>(kz0, nr, ro, sg.py, dc, g, kxf, (int)threadIdx.x, 0);
     pstages<T, PY, true, NT, 1, PY::K - 1>(ro, 3 * nr, sg.py, 1, g.Gz, threadIdx.x);
     slot_rows_stage0<T, NT, PY, true, HALF>(slot, g, sg, kz0, nr, ro);
   }

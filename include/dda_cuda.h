@@ -93,6 +93,10 @@ typedef struct dda_problem {
  * replaying captured CUDA graphs of eight iterations (the results are the
  * same; used by tests). */
 #define DDA_FLAG_NO_GRAPHS 16u
+/* dda_problem.flags: run the fused plane kernel as two groups of half the
+ * CTA with their own barriers (the autotuner otherwise chooses between one
+ * and two groups; the results are the same); used by tests. */
+#define DDA_FLAG_YZ_GROUPS2 32u
 
 typedef struct dda_stats {
   int64_t iterations;   /* Krylov iterations (summed over inner solves for MIXED) */
@@ -205,7 +209,8 @@ int dda_footprint(const dda_problem* prob, int precision, int64_t* resident, int
 /* Layout the context chose for its matvec (working precision: FP32 for
  * DDA_PREC_FP32 and DDA_PREC_MIXED, FP64 otherwise), 8 values:
  * [0] y/z path (0 fused plane kernel, 1 cluster kernel, 2 split path),
- * [1] resident clusters, [2] CTAs per cluster, [3] rows per y batch,
+ * [1] resident clusters, [2] CTAs per cluster (cluster kernel) or thread
+ * groups per CTA (fused kernel: 1 or 2), [3] rows per y batch,
  * [4] dynamic shared memory of the y/z kernel (bytes), [5] grid lines per
  * x tile, [6] compile-time FFT plans (1) or runtime plans (0),
  * [7] device bytes the context holds.  A diagnostic for tuning and
@@ -248,8 +253,11 @@ int dda_far_field(dda_ctx* ctx, int nrhs, const double* pol, int64_t ndir, const
  * requests return DDA_ERR_ARG with the sizes in dda_last_error and touch
  * nothing.  Nothing in the scratch needs to start at zero: each call writes
  * every byte it reads.  The first call on each device looks up the scratch
- * address (cudaGetSymbolAddress with that device current) and keeps it, so
- * make that first call before any stream capture begins.  Every context on
+ * address (cudaGetSymbolAddress with that device current) and keeps it for
+ * the life of the process, so make that first call before any stream
+ * capture begins, and do not call it on a device after cudaDeviceReset (or
+ * any other reset of that device's primary context) in the same process:
+ * the kept address would no longer be valid.  Every context on
  * a device shares the one scratch array: calls that overlap in time (from
  * two host threads, on any contexts of the same device) race on it and must
  * be serialised by the caller.  Each call returns after `out` is written. */

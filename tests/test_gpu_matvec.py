@@ -153,6 +153,52 @@ def test_autotuned_layout_gives_identical_results(prec, shape):
     print(mvs[0].layout, mvs[1].layout)
 
 
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+@pytest.mark.parametrize("case", ["cfg1", "half", "aniso_tuned"])
+def test_two_group_plane_kernel_is_identical(prec, case):
+    # the fused plane kernel run as two groups of half the CTA (named
+    # barriers, columns and row batches split between the groups) does the
+    # same arithmetic per butterfly: bit-identical to one group, and equal to
+    # the oracle
+    import dda_b200
+    from tests.pairs import Pair
+    if case == "cfg1":  # grid 80^3, Plan<10,8>, not half padded
+        kind, args, mats, lam = CASES["cfg1"]
+    elif case == "half":  # box 40 x 24 x 24 on 80 x 48 x 48: the HALF variant
+        pos = np.array([(x, y, z) for z in range(24) for y in range(24) for x in range(40) if (x + y + 2 * z) % 7],
+                       dtype=np.uint32)
+        kind, args, mats, lam = "arrays", (pos, np.zeros(len(pos), np.uint8), "0.05um"), [1.4 + 0.2j], "0.8um"
+    else:  # 35 x 40 x 45 with holes on its tuned grid 80 x 96 x 96
+        pos = np.array([(x, y, z) for z in range(45) for y in range(40) for x in range(35) if (x * 7 + y * 3 + z) % 11],
+                       dtype=np.uint32)
+        kind, args, mats, lam = "arrays", (pos, np.zeros(len(pos), np.uint8), "0.05um"), [1.4 + 0.2j], "0.8um"
+    out = []
+    for flags in (8, 8 | dda_b200.api.FLAG_YZ_GROUPS2):
+        if case == "aniso_tuned":
+            g = dda_b200.Geometry.from_arrays(*args)
+            p = dda_b200.DDAParams(g, mats, lam, grid_policy="tuned")
+            mv = dda_b200.CudaMatVec(p, prec, max_rhs=2, flags=flags)
+            op = None
+        else:
+            pr = Pair(kind, args, mats, lam, prec, max_rhs=2, flags=flags)
+            p, mv, op = pr.p, pr.mv, pr.op
+        lay = mv.layout
+        assert lay["yz_path"] == "fused" and lay["groups"] == (2 if flags & 32 else 1)
+        for r, pol in enumerate((1, 2)):
+            mv.set_couple_constants(dda_b200.CoupleConstants(p, (0.6, 0.0, 0.8), pol, "ldr"), rhs=r)
+        rng = np.random.default_rng(4)
+        x = rng.uniform(-1, 1, 2 * p.vec_size) + 1j * rng.uniform(-1, 1, 2 * p.vec_size)
+        for rr in range(2):
+            for c in range(3):
+                x[rr * p.vec_size + c * p.nvs + p.nv:rr * p.vec_size + (c + 1) * p.nvs] = 0
+        out.append((mv.apply(x), mv.apply(x, conj=True)))
+        if op is not None and flags & 32:
+            op.set_cc((0.6, 0.0, 0.8), 1, "ldr")
+            assert rel(out[-1][0][:p.vec_size], op.matvec(x[:p.vec_size])) < (FP64_TOL if prec == "fp64" else FP32_TOL)
+        mv.close()
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
 @pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("fp32", FP32_TOL)])
 @pytest.mark.parametrize("flags,path", [(0, "fused"), (4, "cluster")])
 def test_matvec_half_padded_box_matches_oracle(prec, tol, flags, path):

@@ -1,20 +1,32 @@
 """Command line in the shape of the reference's `dda` (DDA/Options.cpp:41-97,
-DDA/DDAMain.cpp:611-771): one target, both polarisations, cross sections and,
-on request, the far-field grid.
+DDA/DDAMain.cpp:611-771): one target, both polarisations, cross sections and
+the far-field outputs asked for.
 
     python -m dda_b200.cli --geometry 'sphere:10um,1.5+0.1i' --lambda 6um --grid-unit 0.5um \\
         --iter qmr --epsilon 5 --efield-grid --output-dir out
 
-Supported options: --lambda, --prop, --pol (ldr, cm, ldr-avgpol), --geometry
-(sphere:R,m | cylinder:L,R,m | box:(X,Y,Z),m | load:file=<text dipole list> with -m),
---grid-unit (default: the reference's rule, lambda / (10 max|m|) and at most a
-16th of every particle dimension, DDAMain.cpp:134-150), -m, --fft-grid, --epsilon
-(stop at 10^-epsilon), --maxiter, --iter, --ftype (float, double; plus mixed),
---efield-grid, --no-symmetry (both polarisations are always solved), --output-dir.
-Output files are text: CrossSec-Pol1.txt, CrossSec-Pol2.txt, MieCrossSec.txt
-(spheres), EFieldGrid.txt (--efield-grid: theta, phi and the Jones matrix
-S11, S12, S21, S22 per direction), DipPol-Pol<n>.txt (--store-dippol).  The
-reference's MATLAB-style HDF5 files are not written (no HDF5 library here).
+Options (the reference's names): --lambda, --prop, --pol (ldr, cm, ldr-avgpol),
+--geometry (sphere:R,m | cylinder:L,R,m | box:(X,Y,Z),m | load:file=<text dipole
+list> with -m), --grid-unit (default: the reference's rule, lambda / (10 max|m|)
+and at most a 16th of every particle dimension, DDAMain.cpp:134-150), -m,
+--fft-grid, --epsilon (stop at 10^-epsilon), --maxiter, --iter, --ftype (float,
+double; plus mixed), --no-symmetry (both polarisations are always solved),
+--far-field Name=theta,phi[,jones|mueller|both|none][,no-phi], --efield and
+--mueller-matrix (the YZ plane, --ntheta angles, DDAMain.cpp:323-344),
+--efield-grid and --mueller-matrix-grid (theta 0..180/91, phi 0..360/61),
+--load-dip-pol DIR (skip the solve), --load-start-dip-pol DIR (start values),
+--store-dippol, --store-intfield, --store-incbeam, --write-txt, --profiling-run
+(per-stage matvec times instead of a solve), --output-dir.
+
+Output files are text (the reference's MATLAB-style HDF5 files are not
+written: no HDF5 library on these machines): CrossSec-Pol<n>.txt,
+MieCrossSec.txt (spheres), Far<Name>.txt (Jones matrices, the column layout
+of JonesCalculus::storeTxt) and Far<Name>.mueller.txt (Mueller matrices,
+MuellerCalculus::storeTxt), and with --store-dippol / --write-txt,
+--store-intfield, --store-incbeam: DipPol-Pol<n>.txt, IntField-Pol<n>.txt,
+IncBeam-Pol<n>.txt (one dipole per line: grid x y z, then re, im of the x, y,
+z components).  --load-dip-pol and --load-start-dip-pol read DipPol-Pol<n>.txt
+files of that layout.
 """
 import argparse
 import math
@@ -78,6 +90,36 @@ def build_geometry(spec, grid_unit, m_opts, lambda_m):
     raise SystemExit("Unknown geometry option `%s'" % name)
 
 
+def cc_vector(params, per_material):
+    """Per-material, per-axis values (nmat*3) spread over the vector layout."""
+    mat = params.geometry.materials.astype(np.int64)
+    v = np.zeros(params.vec_size, dtype=np.complex128)
+    for c in range(3):
+        v[c * params.nvs:c * params.nvs + params.nv] = np.asarray(per_material)[mat * 3 + c]
+    return v
+
+
+def write_field(path, params, vec):
+    """One dipole per line: grid x y z, then re, im of the x, y, z components."""
+    nv, nvs = params.nv, params.nvs
+    cols = [params.geometry.positions.astype(np.float64)]
+    for c in range(3):
+        cols += [vec[c * nvs:c * nvs + nv].real[:, None], vec[c * nvs:c * nvs + nv].imag[:, None]]
+    np.savetxt(path, np.hstack(cols), fmt=["%d"] * 3 + ["%.17g"] * 6,
+               header="x y z  Ex.r Ex.i Ey.r Ey.i Ez.r Ez.i")
+
+
+def read_field(path, params):
+    """Inverse of write_field; the dipoles must be those of the target."""
+    d = np.loadtxt(path, ndmin=2)
+    if d.shape != (params.nv, 9) or not np.array_equal(d[:, :3].astype(np.uint32), params.geometry.positions):
+        raise SystemExit("`%s' does not hold this target's dipoles" % path)
+    v = np.zeros(params.vec_size, dtype=np.complex128)
+    for c in range(3):
+        v[c * params.nvs:c * params.nvs + params.nv] = d[:, 3 + 2 * c] + 1j * d[:, 4 + 2 * c]
+    return v
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(prog="dda_b200.cli", description=__doc__.split("\n\n")[0])
     ap.add_argument("--lambda", dest="lam", default="%.17gum" % (2 * math.pi))
@@ -92,8 +134,19 @@ def main(argv=None):
     ap.add_argument("--maxiter", type=int, default=0)
     ap.add_argument("--iter", default="qmr", choices=sorted(api.SOLVERS))
     ap.add_argument("--ftype", default="double", choices=["float", "double", "mixed"])
+    ap.add_argument("--far-field", action="append", default=[])
+    ap.add_argument("--efield", action="store_true")
+    ap.add_argument("--mueller-matrix", action="store_true")
+    ap.add_argument("--ntheta", type=int, default=0)
     ap.add_argument("--efield-grid", action="store_true")
+    ap.add_argument("--mueller-matrix-grid", action="store_true")
+    ap.add_argument("--load-dip-pol")
+    ap.add_argument("--load-start-dip-pol")
     ap.add_argument("--store-dippol", action="store_true")
+    ap.add_argument("--store-intfield", action="store_true")
+    ap.add_argument("--store-incbeam", action="store_true")
+    ap.add_argument("--write-txt", action="store_true")
+    ap.add_argument("--profiling-run", action="store_true")
     ap.add_argument("--output-dir", default=".")
     a = ap.parse_args(argv)
 
@@ -113,16 +166,40 @@ def main(argv=None):
     for r, pol in enumerate((1, 2)):
         ccs.append(api.CoupleConstants(params, prop, pol, a.pol))
         mv.set_couple_constants(ccs[-1], rhs=r)
+    if a.profiling_run:  # IterativeSolverBase::profilingRun, DDA/IterativeSolverBase.cpp:105-136
+        ms = mv.profile(nrhs=2, reps=5)
+        out.write("matvec (2 rhs): %.3f ms  [x forward %.3f, y/z %.3f, x inverse %.3f]\n"
+                  % (ms[3], ms[0], ms[1], ms[2]))
+        mv.close()
+        return 0
     einc = np.stack([params.einc(prop, 1), params.einc(prop, 2)])
-    solver = api.CudaSolver(mv, a.iter, max_iter=a.maxiter)
-    pol = solver.get_pol_vec(einc, 10.0 ** -a.epsilon)
-    for r, (st, hist) in enumerate(zip(solver.last_stats, solver.last_history)):
-        out.write("Pol%d: %d iterations, relative residual %.3e\n" % (r + 1, st.iterations, st.rel_residual))
-        for i, h in enumerate(hist):
-            out.write("RE_%d = %.10g\n" % (i + 1, h))
+    if a.store_incbeam:
+        for r in range(2):
+            write_field(os.path.join(a.output_dir, "IncBeam-Pol%d.txt" % (r + 1)), params, einc[r])
+    if a.load_dip_pol:  # DDA/DDAMain.cpp:374-378
+        pol = np.stack([read_field(os.path.join(a.load_dip_pol, "DipPol-Pol%d.txt" % (r + 1)), params)
+                        for r in range(2)])
+        out.write("Loaded dipole polarisations from %s\n" % a.load_dip_pol)
+    else:
+        start = None
+        if a.load_start_dip_pol:  # DDA/DDAMain.cpp:391-394
+            start = np.stack([read_field(os.path.join(a.load_start_dip_pol, "DipPol-Pol%d.txt" % (r + 1)),
+                                         params) for r in range(2)])
+        solver = api.CudaSolver(mv, a.iter, max_iter=a.maxiter)
+        pol = solver.get_pol_vec(einc, 10.0 ** -a.epsilon, start=start)
+        for r, (st, hist) in enumerate(zip(solver.last_stats, solver.last_history)):
+            out.write("Pol%d: %d iterations, relative residual %.3e\n" % (r + 1, st.iterations, st.rel_residual))
+            for i, h in enumerate(hist):
+                out.write("RE_%d = %.10g\n" % (i + 1, h))
+    for r in range(2):
+        if a.store_dippol or a.write_txt:
+            write_field(os.path.join(a.output_dir, "DipPol-Pol%d.txt" % (r + 1)), params, pol[r])
+        if a.store_intfield:  # internal field chi^-1 P, DDA/DDAMain.cpp:411-417
+            write_field(os.path.join(a.output_dir, "IntField-Pol%d.txt" % (r + 1)), params,
+                        cc_vector(params, ccs[r].chi_inv) * pol[r])
 
     _, pn = api.beam_pol(prop, 1)
-    ef = mv.far_field(pn[None, :], nrhs=2)[0]
+    ef = mv.far_field(pn[None, :], nrhs=2, pol=pol)[0]
     for r in range(2):
         cext, cabs, qext, qabs = postprocess.cross_sections(params, ccs[r], pol[r], ef[r], prop, r + 1)
         csca, qsca = cext - cabs, qext - qabs
@@ -133,9 +210,6 @@ def main(argv=None):
         with open(os.path.join(a.output_dir, "CrossSec-%s.txt" % label), "w") as f:
             f.write("BeamPolarization = %d\nCext = %.17g\nQext = %.17g\nCabs = %.17g\nQabs = %.17g\n"
                     "Csca = %.17g\nQsca = %.17g\n" % (r + 1, cext, qext, cabs, qabs, csca, qsca))
-        if a.store_dippol:
-            np.savetxt(os.path.join(a.output_dir, "DipPol-%s.txt" % label),
-                       np.column_stack([pol[r].real, pol[r].imag]), header="re im, [x: nvs][y: nvs][z: nvs]")
     if mie_geom is not None:
         radius = mie_geom[1]
         x = 2 * math.pi * radius / lambda_m
@@ -143,14 +217,33 @@ def main(argv=None):
         out.write("Mie solution:\nQext = %.10g Qabs = %.10g Qsca = %.10g\n" % (qe, qa, qs))
         with open(os.path.join(a.output_dir, "MieCrossSec.txt"), "w") as f:
             f.write("Qext = %.17g\nQabs = %.17g\nQsca = %.17g\n" % (qe, qa, qs))
+    # far fields (DDA/DDAMain.cpp:318-353): the angle lists of all options,
+    # each list computed once for both polarisations
+    far = [postprocess.parse_far_field(x) for x in a.far_field]
+    if a.efield or a.mueller_matrix:
+        nt = a.ntheta or (180 if params.nv < 1000 else 360 if params.nv < 10000 else 720 if params.nv < 100000
+                          else 1440)
+        th = "0..%.20f/%d" % (360.0 - 360.0 / nt, nt)
+        if a.efield:
+            far.append(("Plane", th, "90", True, False, True))
+        if a.mueller_matrix:
+            far.append(("Plane", th, "90", False, True, True))
     if a.efield_grid:
-        theta, phi = postprocess.grid_angles("0..180/91", "0..360/61")  # DDA/DDAMain.cpp:346-347
-        jones = postprocess.jones_far_field(mv, prop, theta, phi)
-        with open(os.path.join(a.output_dir, "EFieldGrid.txt"), "w") as f:
-            f.write("# theta_deg phi_deg  re/im of S11 S12 S21 S22\n")
-            for t, p_, j in zip(theta, phi, jones):
-                vals = " ".join("%.10e %.10e" % (z.real, z.imag) for z in j.reshape(-1))
-                f.write("%.6f %.6f %s\n" % (math.degrees(t), math.degrees(p_), vals))
+        far.append(("Grid", "0..180/91", "0..360/61", True, False, False))
+    if a.mueller_matrix_grid:
+        far.append(("Grid", "0..180/91", "0..360/61", False, True, False))
+    cache = {}
+    for name, ts, ps, want_j, want_m, no_phi in far:
+        if (ts, ps) not in cache:
+            theta, phi = postprocess.grid_angles(ts, ps)
+            cache[(ts, ps)] = (theta, phi, postprocess.jones_far_field(mv, prop, theta, phi, pol=pol))
+        theta, phi, jones = cache[(ts, ps)]
+        if want_j:
+            postprocess.store_jones_txt(os.path.join(a.output_dir, "Far%s.txt" % name), theta, phi, jones,
+                                        store_phi=not no_phi)
+        if want_m:
+            postprocess.store_mueller_txt(os.path.join(a.output_dir, "Far%s.mueller.txt" % name), theta, phi,
+                                          postprocess.mueller(jones), no_phi=no_phi)
     mv.close()
     return 0
 

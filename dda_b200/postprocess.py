@@ -128,3 +128,83 @@ def mie(x, m):
     qsca = 2 / (x * x) * qs
     qext = 4 / (x * x) * s1.real
     return qext, qsca, qext - qsca
+
+
+def mueller(j):
+    """Mueller matrices [count][4][4] from Jones matrices [count][2][2]
+    (MuellerCalculus::computeMuellerMatrix, EMSim/MuellerCalculus.cpp:36-60)."""
+    s00, s01, s10, s11 = j[:, 0, 0], j[:, 0, 1], j[:, 1, 0], j[:, 1, 1]
+    n = lambda z: np.abs(z) ** 2
+    c = np.conj
+    m = np.empty((len(j), 4, 4))
+    m[:, 0, 0] = (n(s11) + n(s00) + n(s01) + n(s10)) / 2
+    m[:, 0, 1] = (-n(s11) + n(s00) - n(s01) + n(s10)) / 2
+    m[:, 0, 2] = np.real(s00 * c(s01) + s11 * c(s10))
+    m[:, 0, 3] = np.imag(s00 * c(s01) - s11 * c(s10))
+    m[:, 1, 0] = (-n(s11) + n(s00) + n(s01) - n(s10)) / 2
+    m[:, 1, 1] = (n(s11) + n(s00) - n(s01) - n(s10)) / 2
+    m[:, 1, 2] = np.real(s00 * c(s01) - s11 * c(s10))
+    m[:, 1, 3] = np.imag(s00 * c(s01) + s11 * c(s10))
+    m[:, 2, 0] = np.real(s00 * c(s10) + s11 * c(s01))
+    m[:, 2, 1] = np.real(s00 * c(s10) - s11 * c(s01))
+    m[:, 2, 2] = np.real(s11 * c(s00) + s01 * c(s10))
+    m[:, 2, 3] = np.imag(s00 * c(s11) + s10 * c(s01))
+    m[:, 3, 0] = np.imag(s10 * c(s00) + s11 * c(s01))
+    m[:, 3, 1] = np.imag(s10 * c(s00) - s11 * c(s01))
+    m[:, 3, 2] = np.imag(s11 * c(s00) - s01 * c(s10))
+    m[:, 3, 3] = np.real(s11 * c(s00) - s01 * c(s10))
+    return m
+
+
+def store_jones_txt(path, theta, phi, j, store_phi=True):
+    """JonesCalculus::storeTxt (EMSim/JonesCalculus.cpp:89-116): angles in
+    degrees with two decimals, then s1..s4 = S22, S11, S12, S21 (real, imag)."""
+    with open(path, "w") as f:
+        f.write("#theta " + ("phi " if store_phi else "") + "s1.r s1.i s2.r s2.i s3.r s3.i s4.r s4.i\n")
+        for t, p, s in zip(theta, phi, j):
+            row = "%.2f " % math.degrees(t)
+            if store_phi:
+                row += "%.2f " % math.degrees(p)
+            vals = (s[1, 1], s[0, 0], s[0, 1], s[1, 0])
+            row += " ".join("%.10e %.10e" % (z.real, z.imag) for z in vals)
+            f.write(row + "\n")
+
+
+def store_mueller_txt(path, theta, phi, m, no_phi=False):
+    """MuellerCalculus::storeTxt (EMSim/MuellerCalculus.cpp:88-116)."""
+    with open(path, "w") as f:
+        f.write("#theta " + ("" if no_phi else "phi ") + " ".join("s%d%d" % (a, b) for a in range(1, 5)
+                                                                  for b in range(1, 5)) + "\n")
+        for t, p, e in zip(theta, phi, m):
+            row = "%.2f " % math.degrees(t)
+            if not no_phi:
+                row += "%.2f " % math.degrees(p)
+            f.write(row + " ".join("%.10e" % v for v in e.reshape(-1)) + "\n")
+
+
+def parse_far_field(spec):
+    """--far-field FileName=theta,phi[,jones|mueller|both|none][,no-phi]
+    (FarFieldOption::parse, DDA/FarFieldCalc.cpp:51-117): (name, theta
+    spec, phi spec, store Jones, store Mueller, no-phi)."""
+    name, _, rest = spec.rpartition("=")
+    if not name and not rest:
+        raise ValueError("bad --far-field " + spec)
+    if "/" in name:
+        raise ValueError("far-field name must not contain '/'")
+    parts = rest.split(",")
+    if len(parts) < 2:
+        raise ValueError("--far-field needs theta and phi: " + spec)
+    jones, mueller_, no_phi, have = True, False, False, False
+    for o in parts[2:]:
+        if o in ("jones", "mueller", "both", "none"):
+            if have:
+                raise ValueError("more than one of jones/mueller/both/none in " + spec)
+            have = True
+            jones, mueller_ = {"jones": (True, False), "mueller": (False, True), "both": (True, True),
+                               "none": (False, False)}[o]
+        elif o == "no-phi":
+            no_phi = True
+        else:
+            raise ValueError("Invalid option '%s' for far field" % o)
+    return name, parts[0], parts[1], jones, mueller_, no_phi
+

@@ -26,16 +26,68 @@ def test_geometry_strings_match_the_shapes():
     assert g.nv > 0
 
 
+def test_far_field_option_parsing():
+    from dda_b200 import postprocess as P
+    assert P.parse_far_field("Plane=0..359/360,90,no-phi") == ("Plane", "0..359/360", "90", True, False, True)
+    assert P.parse_far_field("X=10,20,both") == ("X", "10", "20", True, True, False)
+    assert P.parse_far_field("Y=0..180/7,0,mueller")[3:5] == (False, True)
+    for bad in ("Z=10", "Z=1,2,jones,mueller", "Z=1,2,foo", "a/b=1,2"):
+        with pytest.raises(ValueError):
+            P.parse_far_field(bad)
+
+
+def test_mueller_of_simple_jones_matrices():
+    from dda_b200 import postprocess as P
+    eye = np.array([[[1, 0], [0, 1]]], dtype=complex)
+    assert np.allclose(P.mueller(eye)[0], np.eye(4))
+    # a linear polariser along the first axis: S11 = 1, the rest 0
+    pol = np.array([[[1, 0], [0, 0]]], dtype=complex)
+    m = P.mueller(pol)[0]
+    assert np.allclose(m, 0.5 * np.array([[1, 1, 0, 0], [1, 1, 0, 0], [0, 0, 0, 0], [0, 0, 0, 0]]))
+
+
+def test_field_files_round_trip(tmp_path):
+    g = dda_b200.Geometry.sphere("0.3um", "0.1um")
+    p = dda_b200.DDAParams(g, [1.5 + 0.1j], "1um")
+    rng = np.random.default_rng(2)
+    v = np.zeros(p.vec_size, dtype=complex)
+    for c in range(3):
+        v[c * p.nvs:c * p.nvs + p.nv] = rng.normal(size=p.nv) + 1j * rng.normal(size=p.nv)
+    cli.write_field(str(tmp_path / "f.txt"), p, v)
+    assert np.array_equal(cli.read_field(str(tmp_path / "f.txt"), p), v)
+
+
 @pytest.mark.gpu
 def test_cli_run_writes_cross_sections(tmp_path, capsys):
     rc = cli.main(["--geometry", "sphere:0.5um,1.5+0.1i", "--lambda", "1um", "--grid-unit", "0.1um",
-                   "--epsilon", "8", "--efield-grid", "--output-dir", str(tmp_path)])
+                   "--epsilon", "8", "--efield-grid", "--efield", "--ntheta", "36", "--mueller-matrix-grid",
+                   "--far-field", "Side=90,0..360/5,both", "--store-dippol", "--store-intfield",
+                   "--store-incbeam", "--output-dir", str(tmp_path)])
     assert rc == 0
     out = capsys.readouterr().out
     assert "Cext Pol1" in out and "Mie solution" in out
-    for f in ("CrossSec-Pol1.txt", "CrossSec-Pol2.txt", "MieCrossSec.txt", "EFieldGrid.txt"):
-        assert os.path.exists(tmp_path / f)
-    assert sum(1 for _ in open(tmp_path / "EFieldGrid.txt")) == 1 + 91 * 61
+    for f in ("CrossSec-Pol1.txt", "CrossSec-Pol2.txt", "MieCrossSec.txt", "FarGrid.txt", "FarGrid.mueller.txt",
+              "FarPlane.txt", "FarSide.txt", "FarSide.mueller.txt", "DipPol-Pol1.txt", "IntField-Pol2.txt",
+              "IncBeam-Pol1.txt"):
+        assert os.path.exists(tmp_path / f), f
+    assert sum(1 for _ in open(tmp_path / "FarGrid.txt")) == 1 + 91 * 61
+    assert sum(1 for _ in open(tmp_path / "FarPlane.txt")) == 1 + 36
+    assert len(open(tmp_path / "FarPlane.txt").readline().split()) == 1 + 8  # no-phi
+    assert len(open(tmp_path / "FarGrid.mueller.txt").readlines()[1].split()) == 2 + 16
+    # the far fields of the loaded polarisations are the same
+    out2 = tmp_path / "again"
+    rc = cli.main(["--geometry", "sphere:0.5um,1.5+0.1i", "--lambda", "1um", "--grid-unit", "0.1um",
+                   "--load-dip-pol", str(tmp_path), "--efield-grid", "--output-dir", str(out2)])
+    assert rc == 0 and "Loaded dipole polarisations" in capsys.readouterr().out
+    a = np.loadtxt(tmp_path / "FarGrid.txt")
+    b = np.loadtxt(out2 / "FarGrid.txt")
+    assert np.allclose(a, b, rtol=1e-12, atol=0)
+    # a solve started from the stored polarisations ends at once
+    rc = cli.main(["--geometry", "sphere:0.5um,1.5+0.1i", "--lambda", "1um", "--grid-unit", "0.1um",
+                   "--epsilon", "8", "--load-start-dip-pol", str(tmp_path), "--output-dir", str(out2)])
+    assert rc == 0
+    its = [int(l.split(":")[1].split()[0]) for l in capsys.readouterr().out.splitlines() if l.startswith("Pol")]
+    assert its and max(its) <= 2
     vals = dict(l.split(" = ") for l in open(tmp_path / "CrossSec-Pol1.txt").read().splitlines())
     # the same problem through the API
     g = dda_b200.Geometry.sphere("0.5um", "0.1um")

@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--matvec-only", type=int, default=0,
                     help="run this many matvecs of the workload and exit (for ncu captures)")
     ap.add_argument("--rhs", type=int, default=0, help="--matvec-only: right-hand sides (0: the workload's)")
+    ap.add_argument("--solve-only", type=int, default=0,
+                    help="run this many solves of the default workload and exit (for ncu launch lists)")
     return ap.parse_args()
 
 
@@ -518,16 +520,43 @@ def run_matvec_only(args):
     x = torch.from_numpy(np.ascontiguousarray(einc[:nrhs])).to(cdt).cuda()
     y = torch.zeros_like(x)
     torch.cuda.synchronize()
+    torch.cuda.profiler.start()  # ncu --profile-from-start off: capture only these matvecs
     for _ in range(args.matvec_only):
         mv.apply_device(x.data_ptr(), y.data_ptr(), nrhs=nrhs)
     mv.synchronize()
+    torch.cuda.profiler.stop()
     print("matvecs", args.matvec_only, "nrhs", nrhs, "grid", p.grid, "layout", mv.layout, flush=True)
+
+
+def run_solve_only(args):
+    """Runs args.solve_only solves of the default workload (both
+    polarisations, device-resident fields) after one untimed solve, and exits:
+    the command ncu's launch list captures (--profile-from-start off)."""
+    import torch
+    import dda_b200
+    torch.cuda.set_device(0)
+    prec = args.precision
+    p, mv, einc = build_problem(prec, 2)
+    solver = dda_b200.CudaSolver(mv, args.solver)
+    cdt = torch.complex128 if prec == "fp64" else torch.complex64
+    e_dev = torch.from_numpy(einc).to(cdt).cuda()
+    p_dev = torch.zeros_like(e_dev)
+    torch.cuda.synchronize()
+    solver.get_pol_vec_device(e_dev.data_ptr(), p_dev.data_ptr(), 2, EPS)
+    torch.cuda.profiler.start()
+    for _ in range(args.solve_only):
+        solver.get_pol_vec_device(e_dev.data_ptr(), p_dev.data_ptr(), 2, EPS)
+    mv.synchronize()
+    torch.cuda.profiler.stop()
+    print("solves", args.solve_only, "iterations", [st.iterations for st in solver.last_stats], flush=True)
 
 
 if __name__ == "__main__":
     a = parse()
     if a.matvec_only:
         run_matvec_only(a)
+    elif a.solve_only:
+        run_solve_only(a)
     elif a.impl == "reference":
         run_reference(a)
     elif a.workload == "box":

@@ -967,48 +967,81 @@ struct SolveOpts {
   long long check_every = 0;
   const double* check_abs = nullptr;
   bool adapt = false;              // mv32 solve that switches the convolution precision (MixedSwitch)
+  int adapt_phase = 0;             // MixedSwitch phase
+  double adapt_tau = 0;            // MixedSwitch phase 1 threshold
+  char* stalled = nullptr;         // phase 0: per rhs, set when the FP32 start stalled
 };
 
 constexpr double kGapRatio = 4.0;  // |r_true|^2 > 4 |r_rec|^2: the gap dominates
 
 // Precision of the convolution in an adaptive MIXED inner solve
-// (SolveOpts::adapt), decided between rounds from the recurrence residuals
-// of the right-hand sides still running (the worst one decides).  The solve
-// starts with the FP32 convolution.  If the best residual does not halve
-// within `window` iterations, the FP32 rounding is taken to hold the Krylov
-// recurrences back (on large, high-index targets QMR-CS with the FP32
-// convolution stays on a residual plateau that the FP64 solve leaves), and
-// the solve continues, in the same Krylov space, with the FP64 convolution
-// until the residual has fallen by `drop` below the level of the stall; then
-// it tries the FP32 convolution again.
+// (SolveOpts::adapt), decided between rounds from the recurrence residuals.
+//
+// Phase 0 (the first inner solve): the FP32 convolution from the start,
+// which is the whole solve for well-conditioned targets.  A right-hand side
+// whose best residual does not halve within kStallStart iterations ends its
+// inner solve with `stalled` set: on large, high-index targets QMR-CS with
+// the FP32 convolution stays on a residual plateau that the FP64 solve
+// leaves after a few thousand iterations, and a Krylov space built with the
+// FP32 rounding does not recover when continued in FP64, so the outer step
+// restarts it.
+//
+// Phase 1 (after a stall): the FP64 convolution until every running
+// right-hand side is below tau (200 times its inner target: the rounding
+// the FP32 convolution then adds to each Krylov vector scales with a
+// residual that is already small), then the FP32 convolution in the same
+// Krylov space.  If that stalls (no halving within kStallLate iterations)
+// the solve continues, again in the same Krylov space, with the FP64
+// convolution until the residual has fallen a hundredfold below the stall.
+constexpr long long kStallStart = 256, kStallLate = 1024;
+
 struct MixedSwitch {
+  int phase = 0;
   bool mode32 = true;
-  long long window = 1024;
-  double drop = 0.01;
-  double tau = 0;            // FP64 -> FP32 below this
-  long long mark_it = -1;    // start of the current FP32 window
-  double mark = 0;           // best residual there
+  double tau = 0;            // phase 1: FP64 -> FP32 below this
   long long it32 = 0;        // iterations run with the FP32 convolution
-  MixedSwitch() {
-    if (const char* v = getenv("DDA_MX_W")) window = atoll(v);
-    if (const char* v = getenv("DDA_MX_DROP")) drop = atof(v);
-    if (const char* v = getenv("DDA_MX_START")) mode32 = atoi(v) != 0;
-    if (const char* v = getenv("DDA_MX_TAU")) tau = atof(v);
-  }
-  bool update(const KrylovState* st, int nrhs, long long nr, long long poll) {
+  long long mark_it = -1;    // phase 1: start of the current FP32 window
+  double mark = 0;
+  std::vector<long long> rmark_it;  // phase 0: per rhs
+  std::vector<double> rmark;
+  MixedSwitch(int phase_, double tau_, int nrhs)
+      : phase(phase_), mode32(phase_ == 0), tau(tau_), rmark_it(nrhs, -1), rmark(nrhs, 0) {}
+  // Called after each round; phase 0 may end right-hand sides (returns true
+  // when it changed a done flag in st).
+  bool update(KrylovState* st, int nrhs, long long nr, long long poll, char* stalled) {
+    bool changed = false;
+    if (mode32) it32 += poll;
+    if (phase == 0) {
+      for (int r = 0; r < nrhs; r++) {
+        if (st[r].done) continue;
+        const double rel = std::sqrt(st[r].inprodR * st[r].residScale);
+        if (rmark_it[r] < 0) {
+          rmark_it[r] = nr;
+          rmark[r] = rel;
+        } else if (nr - rmark_it[r] >= kStallStart) {
+          if (rel > 0.5 * rmark[r]) {
+            st[r].done = 1;
+            stalled[r] = 1;
+            changed = true;
+          } else {
+            rmark_it[r] = nr;
+            rmark[r] = rel;
+          }
+        }
+      }
+      return changed;
+    }
     double worst = 0;
     for (int r = 0; r < nrhs; r++)
       if (!st[r].done) worst = std::max(worst, std::sqrt(st[r].inprodR * st[r].residScale));
     if (mode32) {
-      it32 += poll;
       if (mark_it < 0) {
         mark_it = nr;
         mark = worst;
-      } else if (nr - mark_it >= window) {
+      } else if (nr - mark_it >= kStallLate) {
         if (worst > 0.5 * mark) {
           mode32 = false;
-          tau = drop * worst;
-          if (getenv("DDA_MX_LOG")) fprintf(stderr, "mx: -> fp64 at %lld rel %.3e\n", nr, worst);
+          tau = 0.01 * worst;
         } else {
           mark_it = nr;
           mark = worst;
@@ -1018,9 +1051,8 @@ struct MixedSwitch {
       mode32 = true;
       mark_it = nr;
       mark = worst;
-      if (getenv("DDA_MX_LOG")) fprintf(stderr, "mx: -> fp32 at %lld rel %.3e\n", nr, worst);
     }
-    return mode32;
+    return false;
   }
 };
 
@@ -1114,7 +1146,7 @@ void run_solve(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
     }
     return -1;
   };
-  MixedSwitch ms;
+  MixedSwitch ms(o.adapt_phase, o.adapt_tau, nrhs);
   if (o.adapt) sv.mv32 = ms.mode32;
   for (int round = 0;; round++) {
     if (!graphs || round == 0) {
@@ -1163,9 +1195,24 @@ void run_solve(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
     if constexpr (std::is_same<T, double>::value) {
       // the FP64 check only once the FP32 convolution has run (the gap is
       // its rounding carried along)
-      const bool gap_possible = !o.adapt || ms.it32 > 0;
+      // and only once some right-hand side's recurrence residual is within
+      // a hundred times its target (earlier the gap cannot dominate)
+      bool near = false;
+      for (int r = 0; r < nrhs && !near; r++) {
+        const KrylovState& k = c->st_host[r];
+        near = !k.done && k.inprodR < 1e4 * k.epsB;
+      }
+      const bool gap_possible = (!o.adapt || ms.it32 > 0) && near;
       if (o.check_every > 0 && nr % o.check_every == 0 && gap_possible && check_gap(c, nrhs, b.X, B, S, o)) break;
-      if (o.adapt) sv.mv32 = ms.update(c->st_host, nrhs, nr, poll);
+      if (o.adapt) {
+        if (ms.update(c->st_host, nrhs, nr, poll, o.stalled)) {
+          CK(cudaMemcpyAsync(c->st, c->st_host, nrhs * sizeof(KrylovState), cudaMemcpyHostToDevice, c->stream));
+          bool all_done = true;
+          for (int r = 0; r < nrhs; r++) all_done = all_done && c->st_host[r].done;
+          if (all_done) break;
+        }
+        sv.mv32 = ms.mode32;
+      }
     }
   }
   if (b.X != e.vec[4])
@@ -1219,6 +1266,7 @@ void run_mixed(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
   const int kOuterStall = 2;
   std::vector<double> prev_rel(nrhs, 0.0);
   std::vector<int> stalls(nrhs, 0);
+  std::vector<char> fp32_stalled(nrhs, 0);  // the FP32 start stalled (MixedSwitch phase 0)
   for (int outer = 0;; outer++) {
     // r = b - A x (full FP64 matvec); reduction n = |r|^2 -> last
     if (outer > 0 || start) sd.mv(X, A, 0, sd.step(KOP_NONE));
@@ -1263,10 +1311,22 @@ void run_mixed(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
     o.skip = done.data();
     o.result = false;
     o.mv32 = true;
-    o.adapt = !getenv("DDA_MX_FIXED");
+    o.adapt = true;
+    o.adapt_phase = 0;
+    double eps_max = 0;
+    for (int r = 0; r < nrhs; r++)
+      if (!done[r]) {
+        if (fp32_stalled[r]) o.adapt_phase = 1;
+        eps_max = std::max(eps_max, eps_in[r]);
+      }
+    o.adapt_tau = 200 * eps_max;
+    std::vector<char> stalled_now(nrhs, 0);
+    o.stalled = stalled_now.data();
     o.check_every = kCheckEvery;
     o.check_abs = thr.data();
     run_solve<double>(c, solver, nrhs, 0.0, max_iter > 0 ? max_iter - total_it : 0, o);
+    for (int r = 0; r < nrhs; r++)
+      if (stalled_now[r]) fp32_stalled[r] = 1;
     for (int r = 0; r < nrhs; r++) {
       if (done[r]) continue;
       out[r].iterations += c->st_host[r].count;

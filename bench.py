@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--requests", type=int, default=120, help="serve: requests in the stream")
     ap.add_argument("--rate", type=float, default=50.0, help="serve: mean arrivals per second")
     ap.add_argument("--slots", type=int, default=8, help="serve: concurrent requests")
+    ap.add_argument("--no-plain", action="store_true",
+                    help="serve: skip the FP64 and straightforward-solve samples of the stream")
     ap.add_argument("--max-iter", type=int, default=0, help="mixed512: iteration cap of each solve (0: none)")
     ap.add_argument("--no-batched", action="store_true",
                     help="default line without the 128-rhs spheroid block beside it")

@@ -32,6 +32,7 @@ class Problem(ctypes.Structure):
 
 FLAG_SPLIT_YZ = 1
 FLAG_YZ_GROUPS2 = 32
+FLAG_YZ_GROUPS4 = 64
 
 
 class Stats(ctypes.Structure):

@@ -456,9 +456,10 @@ template <typename T> void setup_engine(dda_ctx* c) {
   e.yz_fixed = fixed;
   e.yz_row = row;
   e.fused = e.k.yz && e.smem_yz <= kSmemMax && !(c->flags & (DDA_FLAG_SPLIT_YZ | DDA_FLAG_SLOT_YZ));
-  if (e.fused && e.k.yz2 && (c->flags & DDA_FLAG_YZ_GROUPS2) && nrw >= 2) {
-    e.yz_groups = 2;
-    e.yz.nrw = nrw & ~1;  // an even number of rows: half to each group
+  const int forced = (c->flags & DDA_FLAG_YZ_GROUPS4) ? 4 : (c->flags & DDA_FLAG_YZ_GROUPS2) ? 2 : 1;
+  if (e.fused && forced > 1 && (forced == 2 ? e.k.yz2 : e.k.yz4) && nrw >= forced) {
+    e.yz_groups = forced;
+    e.yz.nrw = nrw - nrw % forced;  // a multiple of the groups: an equal share each
     e.smem_yz = fixed + e.yz.nrw * row;
   }
   if (!e.fused && e.k.slot && !(c->flags & DDA_FLAG_SPLIT_YZ)) setup_slot<T>(c, e);
@@ -504,6 +505,7 @@ template <typename T> void setup_engine(dda_ctx* c) {
   if (e.fused) {
     attr((const void*)e.k.yz, e.smem_yz);
     if (e.k.yz2) attr((const void*)e.k.yz2, e.smem_yz);
+    if (e.k.yz4) attr((const void*)e.k.yz4, e.smem_yz);
   }
   else if (!e.slot_path) {
     attr((const void*)e.k.yrows, e.smem_rows);
@@ -561,8 +563,8 @@ void launch_yz(dda_ctx* c, int nrhs, cudaStream_t s, KrylovState* st, int skipmv
   const MvGeom& g = c->g;
   const FftPlanDev py = c->my.dev<T>(), pz = c->mz.dev<T>();
   if (e.fused) {
-    (e.yz_groups == 2 ? e.k.yz2 : e.k.yz)<<<dim3(g.Gx, nrhs), kNtYz, e.smem_yz, s>>>(e.xhat, e.dc, g, e.yz, pz, py,
-                                                                                      st, skipmv);
+    const auto f = e.yz_groups == 4 ? e.k.yz4 : e.yz_groups == 2 ? e.k.yz2 : e.k.yz;
+    f<<<dim3(g.Gx, nrhs), kNtYz, e.smem_yz, s>>>(e.xhat, e.dc, g, e.yz, pz, py, st, skipmv);
   } else if (e.slot_path) {
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute at[1];
@@ -656,8 +658,10 @@ template <typename T> void autotune(dda_ctx* c) {
     const int max_rows = e.k.planned ? 48 : kNtYz / 32;
     for (int n : {4, 6, 8, 10, 12, 14, 16, 20, 24, 25, 28, 32, 34, 36, 40, 43, 48})
       if (n <= max_rows && e.yz_fixed + (size_t)n * e.yz_row <= kSmemMax) {
-        if (!(c->flags & DDA_FLAG_YZ_GROUPS2)) cands.push_back({n, 0, 1});
-        if (e.k.yz2 && n % 2 == 0) cands.push_back({n, 0, 2});  // two groups of n/2 rows
+        const bool f2 = c->flags & DDA_FLAG_YZ_GROUPS2, f4 = c->flags & DDA_FLAG_YZ_GROUPS4;
+        if (!f2 && !f4) cands.push_back({n, 0, 1});
+        if (e.k.yz2 && n % 2 == 0 && !f4) cands.push_back({n, 0, 2});  // two groups of n/2 rows
+        if (e.k.yz4 && n % 4 == 0 && !f2) cands.push_back({n, 0, 4});  // four groups of n/4 rows
       }
   } else {
     for (int cl : {4, 8, 16})

@@ -24,6 +24,7 @@ template <typename T> struct MvKernels {
   XinvFn xinv = nullptr;
   YzFn yz = nullptr;        // fused plane kernel (nullptr: none for this shape)
   YzFn yz2 = nullptr;       // the same kernel run as two groups of half the CTA
+  YzFn yz4 = nullptr;       // ... and as four groups of a quarter
   YrowsFn yrows = nullptr;  // split path
   ColsFn cols = nullptr;
   SlotFn slot = nullptr;    // cluster plane kernel for planes beyond shared memory
@@ -107,6 +108,7 @@ void planned_fused(MvKernels<T>& k, int gy, int gz, int by, int bz) {
   case N:                                                                                       \
     k.yz = fused_kernel<T, NTYZ, N>(2 * by == gy && 2 * bz == gz);                               \
     k.yz2 = fused_kernel<T, NTYZ, N, 2>(2 * by == gy && 2 * bz == gz);                           \
+    k.yz4 = fused_kernel<T, NTYZ, N, 4>(2 * by == gy && 2 * bz == gz);                           \
     break;
     DDA_FUSED_LENGTHS(C)
 #undef C

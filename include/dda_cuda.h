@@ -94,9 +94,11 @@ typedef struct dda_problem {
  * same; used by tests). */
 #define DDA_FLAG_NO_GRAPHS 16u
 /* dda_problem.flags: run the fused plane kernel as two groups of half the
- * CTA with their own barriers (the autotuner otherwise chooses between one
- * and two groups; the results are the same); used by tests. */
+ * CTA (or, with DDA_FLAG_YZ_GROUPS4, four groups of a quarter) with their own
+ * barriers (the autotuner otherwise chooses between one, two and four
+ * groups; the results are the same); used by tests. */
 #define DDA_FLAG_YZ_GROUPS2 32u
+#define DDA_FLAG_YZ_GROUPS4 64u
 
 typedef struct dda_stats {
   int64_t iterations;   /* Krylov iterations (summed over inner solves for MIXED) */
@@ -210,7 +212,7 @@ int dda_footprint(const dda_problem* prob, int precision, int64_t* resident, int
  * DDA_PREC_FP32 and DDA_PREC_MIXED, FP64 otherwise), 8 values:
  * [0] y/z path (0 fused plane kernel, 1 cluster kernel, 2 split path),
  * [1] resident clusters, [2] CTAs per cluster (cluster kernel) or thread
- * groups per CTA (fused kernel: 1 or 2), [3] rows per y batch,
+ * groups per CTA (fused kernel: 1, 2 or 4), [3] rows per y batch,
  * [4] dynamic shared memory of the y/z kernel (bytes), [5] grid lines per
  * x tile, [6] compile-time FFT plans (1) or runtime plans (0),
  * [7] device bytes the context holds.  A diagnostic for tuning and

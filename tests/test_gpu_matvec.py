@@ -153,9 +153,10 @@ def test_autotuned_layout_gives_identical_results(prec, shape):
     print(mvs[0].layout, mvs[1].layout)
 
 
+@pytest.mark.parametrize("groups", [2, 4])
 @pytest.mark.parametrize("prec", ["fp64", "fp32"])
 @pytest.mark.parametrize("case", ["cfg1", "half", "aniso_tuned"])
-def test_two_group_plane_kernel_is_identical(prec, case):
+def test_grouped_plane_kernel_is_identical(prec, case, groups):
     # the fused plane kernel run as two groups of half the CTA (named
     # barriers, columns and row batches split between the groups) does the
     # same arithmetic per butterfly: bit-identical to one group, and equal to
@@ -173,7 +174,8 @@ def test_two_group_plane_kernel_is_identical(prec, case):
                        dtype=np.uint32)
         kind, args, mats, lam = "arrays", (pos, np.zeros(len(pos), np.uint8), "0.05um"), [1.4 + 0.2j], "0.8um"
     out = []
-    for flags in (8, 8 | dda_b200.api.FLAG_YZ_GROUPS2):
+    gflag = dda_b200.api.FLAG_YZ_GROUPS2 if groups == 2 else dda_b200.api.FLAG_YZ_GROUPS4
+    for flags in (8, 8 | gflag):
         if case == "aniso_tuned":
             g = dda_b200.Geometry.from_arrays(*args)
             p = dda_b200.DDAParams(g, mats, lam, grid_policy="tuned")
@@ -183,7 +185,7 @@ def test_two_group_plane_kernel_is_identical(prec, case):
             pr = Pair(kind, args, mats, lam, prec, max_rhs=2, flags=flags)
             p, mv, op = pr.p, pr.mv, pr.op
         lay = mv.layout
-        assert lay["yz_path"] == "fused" and lay["groups"] == (2 if flags & 32 else 1)
+        assert lay["yz_path"] == "fused" and lay["groups"] == (groups if flags & gflag else 1)
         for r, pol in enumerate((1, 2)):
             mv.set_couple_constants(dda_b200.CoupleConstants(p, (0.6, 0.0, 0.8), pol, "ldr"), rhs=r)
         rng = np.random.default_rng(4)
@@ -192,7 +194,7 @@ def test_two_group_plane_kernel_is_identical(prec, case):
             for c in range(3):
                 x[rr * p.vec_size + c * p.nvs + p.nv:rr * p.vec_size + (c + 1) * p.nvs] = 0
         out.append((mv.apply(x), mv.apply(x, conj=True)))
-        if op is not None and flags & 32:
+        if op is not None and flags & gflag:
             op.set_cc((0.6, 0.0, 0.8), 1, "ldr")
             assert rel(out[-1][0][:p.vec_size], op.matvec(x[:p.vec_size])) < (FP64_TOL if prec == "fp64" else FP32_TOL)
         mv.close()

@@ -66,18 +66,20 @@ def parse():
 
 # DRAM traffic per launch of the y/z plane kernel (dram__bytes_read.sum +
 # dram__bytes_write.sum), from ncu captures of `bench.py --matvec-only`:
-#   box:       the default workload, FP32, 2 rhs (captured at full size)
+#   box:       the default workload, FP32, 2 rhs (captured at full size; the
+#              planes stay in L2, so the DRAM bytes are the first reads only)
 #   spheroid:  the 128-rhs block's kernel captured at 8 rhs; the traffic is
 #              a fixed part (D octant, tables) plus a part per rhs, so a full
 #              launch is fixed + 128 * per_rhs
 # Summaries with the commands: profiles/k_yz_p_box10x5x5_fp32.md,
 # profiles/k_yz_p_spheroid_fp32.md.
-TRAFFIC = {"box": None, "spheroid": None}
+TRAFFIC = {"box": {"fixed": 36663637, "per_rhs": 0, "rhs": 2},      # L2-resident planes: reads only
+           "spheroid": {"fixed": 14340480, "per_rhs": 39347072}}
 
 
 def traffic_per_launch(workload, nrhs):
     t = TRAFFIC.get(workload)
-    if t is None:
+    if t is None or ("rhs" in t and t["rhs"] != nrhs):
         return None
     return int(t["fixed"] + nrhs * t["per_rhs"])
 

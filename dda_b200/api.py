@@ -33,6 +33,7 @@ class Problem(ctypes.Structure):
 FLAG_SPLIT_YZ = 1
 FLAG_YZ_GROUPS2 = 32
 FLAG_YZ_GROUPS4 = 64
+FLAG_YZ_PAIR = 128
 
 
 class Stats(ctypes.Structure):
@@ -379,8 +380,9 @@ class CudaMatVec:
                 "compile_time_plans", "device_bytes")
         d = dict(zip(keys, (int(x) for x in v)))
         d["yz_path"] = ("fused", "cluster", "split")[d["yz_path"]]
-        if d["yz_path"] == "fused":  # slot 2 holds the fused kernel's thread groups
+        if d["yz_path"] == "fused":  # slots 1, 2: CTAs per plane and thread groups
             d["groups"] = d.pop("cluster_size")
+            d["ctas_per_plane"] = d.pop("clusters")
         return d
 
     def profile(self, nrhs=1, reps=10):

@@ -197,7 +197,9 @@ template <typename T> struct Engine {
   T2* xo = nullptr;    // MIXED, FP64 engine: refined solution x and b = sqrt(cc) Einc
   T2* bo = nullptr;
   bool fused = false;
-  int yz_groups = 1;          // fused kernel: 1 CTA-wide group, or 2 groups of half the CTA (k.yz2)
+  int yz_groups = 1;          // fused kernel: thread groups per CTA (k.yz, k.yz2, k.yz4)
+  bool yz_pair = false;       // fused path through k_yz_pair: a plane per cluster of two CTAs
+  size_t pair_fixed = 0;      // k_yz_pair shared memory without the row buffers
   bool slot_path = false;     // k_yz_slot: cluster per plane through L2 slots
   T2* slots = nullptr;        // [ncl][Gz][wp]
   uint32_t* order = nullptr;  // kx positions, mirrored frequencies adjacent
@@ -456,8 +458,21 @@ template <typename T> void setup_engine(dda_ctx* c) {
   e.yz_fixed = fixed;
   e.yz_row = row;
   e.fused = e.k.yz && e.smem_yz <= kSmemMax && !(c->flags & (DDA_FLAG_SPLIT_YZ | DDA_FLAG_SLOT_YZ));
+  e.pair_fixed = ((size_t)g.Gz + g.Gy + (size_t)(g.Gz / 2) * y.q) * s;
+  if (e.fused && e.k.pair[0] && (c->flags & DDA_FLAG_YZ_PAIR)) {
+    int np = 32;
+    while (np > 1 && e.pair_fixed + np * row > kSmemMax) np--;
+    e.yz_pair = true;
+    e.yz.nrw = np;
+    e.smem_yz = e.pair_fixed + np * row;
+  }
   const int forced = (c->flags & DDA_FLAG_YZ_GROUPS4) ? 4 : (c->flags & DDA_FLAG_YZ_GROUPS2) ? 2 : 1;
-  if (e.fused && forced > 1 && (forced == 2 ? e.k.yz2 : e.k.yz4) && nrw >= forced) {
+  if (e.yz_pair && forced > 1 && e.yz.nrw >= forced) {
+    e.yz_groups = forced;
+    e.yz.nrw -= e.yz.nrw % forced;
+    e.smem_yz = e.pair_fixed + e.yz.nrw * row;
+  }
+  if (e.fused && !e.yz_pair && forced > 1 && (forced == 2 ? e.k.yz2 : e.k.yz4) && nrw >= forced) {
     e.yz_groups = forced;
     e.yz.nrw = nrw - nrw % forced;  // a multiple of the groups: an equal share each
     e.smem_yz = fixed + e.yz.nrw * row;
@@ -506,6 +521,8 @@ template <typename T> void setup_engine(dda_ctx* c) {
     attr((const void*)e.k.yz, e.smem_yz);
     if (e.k.yz2) attr((const void*)e.k.yz2, e.smem_yz);
     if (e.k.yz4) attr((const void*)e.k.yz4, e.smem_yz);
+    for (auto f : e.k.pair)
+      if (f) attr((const void*)f, e.smem_yz);
   }
   else if (!e.slot_path) {
     attr((const void*)e.k.yrows, e.smem_rows);
@@ -562,7 +579,23 @@ void launch_yz(dda_ctx* c, int nrhs, cudaStream_t s, KrylovState* st, int skipmv
   Engine<T>& e = eng<T>(c);
   const MvGeom& g = c->g;
   const FftPlanDev py = c->my.dev<T>(), pz = c->mz.dev<T>();
-  if (e.fused) {
+  if (e.fused && e.yz_pair) {
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = 2;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(2 * g.Gx, nrhs);
+    cfg.blockDim = dim3(kNtYz);
+    cfg.dynamicSmemBytes = e.smem_yz;
+    cfg.stream = s;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    const auto f = e.k.pair[e.yz_groups == 4 ? 2 : e.yz_groups == 2 ? 1 : 0];
+    CK(cudaLaunchKernelEx(&cfg, f, e.xhat, (const typename C2<T>::t*)e.dc, g, e.yz, pz, py, (const KrylovState*)st,
+                          skipmv));
+  } else if (e.fused) {
     const auto f = e.yz_groups == 4 ? e.k.yz4 : e.yz_groups == 2 ? e.k.yz2 : e.k.yz;
     f<<<dim3(g.Gx, nrhs), kNtYz, e.smem_yz, s>>>(e.xhat, e.dc, g, e.yz, pz, py, st, skipmv);
   } else if (e.slot_path) {
@@ -597,7 +630,7 @@ void launch_yz(dda_ctx* c, int nrhs, cudaStream_t s, KrylovState* st, int skipmv
 // size and rows per batch.  Timed on the context's own buffers (x spectrum
 // zeroed, one right-hand side) and kept per shape for the process.
 struct TuneChoice {
-  int nrw = 0, cl = 0, groups = 1;
+  int nrw = 0, cl = 0, groups = 1, pair = 0;
 };
 std::mutex g_tune_mu;
 std::map<std::array<int, 6>, TuneChoice> g_tune_cache;
@@ -628,7 +661,8 @@ template <typename T> void apply_choice(dda_ctx* c, Engine<T>& e, const TuneChoi
   if (e.fused) {
     e.yz.nrw = t.nrw;
     e.yz_groups = t.groups;
-    e.smem_yz = e.yz_fixed + (size_t)t.nrw * e.yz_row;
+    e.yz_pair = t.pair != 0;
+    e.smem_yz = (e.yz_pair ? e.pair_fixed : e.yz_fixed) + (size_t)t.nrw * e.yz_row;
   } else if (e.slot_path) {
     e.cl = t.cl;
     e.ncl = e.ncl_by_cl[t.cl];
@@ -659,10 +693,17 @@ template <typename T> void autotune(dda_ctx* c) {
     for (int n : {4, 6, 8, 10, 12, 14, 16, 20, 24, 25, 28, 32, 34, 36, 40, 43, 48})
       if (n <= max_rows && e.yz_fixed + (size_t)n * e.yz_row <= kSmemMax) {
         const bool f2 = c->flags & DDA_FLAG_YZ_GROUPS2, f4 = c->flags & DDA_FLAG_YZ_GROUPS4;
-        if (!f2 && !f4) cands.push_back({n, 0, 1});
-        if (e.k.yz2 && n % 2 == 0 && !f4) cands.push_back({n, 0, 2});  // two groups of n/2 rows
-        if (e.k.yz4 && n % 4 == 0 && !f2) cands.push_back({n, 0, 4});  // four groups of n/4 rows
+        if (c->flags & DDA_FLAG_YZ_PAIR) continue;
+        if (!f2 && !f4) cands.push_back({n, 0, 1, 0});
+        if (e.k.yz2 && n % 2 == 0 && !f4) cands.push_back({n, 0, 2, 0});  // two groups of n/2 rows
+        if (e.k.yz4 && n % 4 == 0 && !f2) cands.push_back({n, 0, 4, 0});  // four groups of n/4 rows
       }
+    // the two-CTA plane kernel: half the slab per CTA, more rows
+    if (e.k.pair[0] && !(c->flags & (DDA_FLAG_YZ_GROUPS2 | DDA_FLAG_YZ_GROUPS4)))
+      for (int n : {8, 12, 16, 20, 24, 28, 32, 36, 40, 48})
+        if (n <= 48 && n <= g.Gz / 2 && e.pair_fixed + (size_t)n * e.yz_row <= kSmemMax)
+          for (int gr : {1, 2, 4})
+            if (n % gr == 0) cands.push_back({n, 0, gr, 1});
   } else {
     for (int cl : {4, 8, 16})
       for (int n : {4, 8, 16})
@@ -1944,7 +1985,7 @@ int dda_matvec_layout(const dda_ctx* ctx, int64_t* out) {
   if (!ctx || !out) return DDA_ERR_ARG;
   auto fill = [&](const auto& e) {
     out[0] = e.fused ? 0 : e.slot_path ? 1 : 2;
-    out[1] = e.ncl;
+    out[1] = e.fused ? (e.yz_pair ? 2 : 1) : e.ncl;
     out[2] = e.fused ? e.yz_groups : e.cl;
     out[3] = e.slot_path ? e.sg.nrw : e.yz.nrw;
     out[4] = (int64_t)(e.fused ? e.smem_yz : e.slot_path ? e.smem_slot : e.smem_rows);

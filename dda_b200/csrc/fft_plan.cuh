@@ -218,13 +218,16 @@ __device__ __forceinline__ void butterfly(T2* v, int j, const T2* tw) {
 // Element e of line l is at shared offset soff + l*ls + e*es.  Work items are
 // (line, butterfly) pairs with the line fastest, so a line tile and a column
 // tile both keep every lane busy.
-template <typename T, typename P, int I, bool INV, int G>
+// DIV = 2 (stages I >= 1 only): the line's first half, positions [0, N/2),
+// which holds whole blocks of these stages when the first radix is even.
+template <typename T, typename P, int I, bool INV, int G, int DIV = 1>
 __device__ __forceinline__ void pstage(int soff, int nl, int ls, int es, int twoff, int tid, int bar = 0) {
   typedef typename C2<T>::t T2;
   constexpr int R = P::r[I];
   constexpr int L = P::L(I);
   constexpr int S = L / R;
-  constexpr int NB = P::N / R;  // butterflies per line
+  constexpr int NB = P::N / R / DIV;  // butterflies per line
+  static_assert(DIV == 1 || (I >= 1 && P::r[0] % DIV == 0), "half lines need stage >= 1 and an even first radix");
   T2* s = smem_at<T>(0);
   const T2* tw = s + twoff;
   const int total = nl * NB;
@@ -245,15 +248,15 @@ __device__ __forceinline__ void pstage(int soff, int nl, int ls, int es, int two
 }
 
 // Stages [I0, I1) of P, forward in order or inverse in reverse order.
-template <typename T, typename P, bool INV, int G, int I0, int I1>
+template <typename T, typename P, bool INV, int G, int I0, int I1, int DIV = 1>
 __device__ __forceinline__ void pstages(int soff, int nl, int ls, int es, int twoff, int tid, int bar = 0) {
   if constexpr (I0 < I1) {
     if constexpr (!INV) {
-      pstage<T, P, I0, false, G>(soff, nl, ls, es, twoff, tid, bar);
-      pstages<T, P, false, G, I0 + 1, I1>(soff, nl, ls, es, twoff, tid, bar);
+      pstage<T, P, I0, false, G, DIV>(soff, nl, ls, es, twoff, tid, bar);
+      pstages<T, P, false, G, I0 + 1, I1, DIV>(soff, nl, ls, es, twoff, tid, bar);
     } else {
-      pstage<T, P, I1 - 1, true, G>(soff, nl, ls, es, twoff, tid, bar);
-      pstages<T, P, true, G, I0, I1 - 1>(soff, nl, ls, es, twoff, tid, bar);
+      pstage<T, P, I1 - 1, true, G, DIV>(soff, nl, ls, es, twoff, tid, bar);
+      pstages<T, P, true, G, I0, I1 - 1, DIV>(soff, nl, ls, es, twoff, tid, bar);
     }
   }
 }

@@ -6,6 +6,7 @@
 #include "matvec_kernels.cuh"
 #include "matvec_planned.cuh"
 #include "matvec_slot.cuh"
+#include "matvec_pair.cuh"
 
 namespace dda {
 
@@ -25,6 +26,7 @@ template <typename T> struct MvKernels {
   YzFn yz = nullptr;        // fused plane kernel (nullptr: none for this shape)
   YzFn yz2 = nullptr;       // the same kernel run as two groups of half the CTA
   YzFn yz4 = nullptr;       // ... and as four groups of a quarter
+  YzFn pair[3] = {};        // a plane per cluster of two CTAs (k_yz_pair), 1 / 2 / 4 groups
   YrowsFn yrows = nullptr;  // split path
   ColsFn cols = nullptr;
   SlotFn slot = nullptr;    // cluster plane kernel for planes beyond shared memory
@@ -51,6 +53,19 @@ typename MvKernels<T>::YzFn fused_kernel(bool half) {
     if (half) return k_yz_p<T, NTYZ, P, P, true, GR>;
   }
   return k_yz_p<T, NTYZ, P, P, false, GR>;
+}
+
+// Two-CTA plane kernel for y = z = N (needs an even first radix).
+template <typename T, int NTYZ, int N, int GR>
+typename MvKernels<T>::YzFn pair_kernel(bool half) {
+  typedef typename PlanFor<N>::type P;
+  if constexpr (P::r[0] % 2 == 0) {
+    if (half) return k_yz_pair<T, NTYZ, P, P, true, GR>;
+    return k_yz_pair<T, NTYZ, P, P, false, GR>;
+  } else {
+    (void)half;
+    return nullptr;
+  }
 }
 
 // Cluster plane kernel for y = z = N, likewise.
@@ -117,6 +132,22 @@ void planned_fused(MvKernels<T>& k, int gy, int gz, int by, int bz) {
 }
 
 template <typename T, int NTYZ>
+void planned_pair(MvKernels<T>& k, int gy, int gz, int by, int bz) {
+  if (gy != gz) return;
+  switch (gy) {
+#define C(N)                                                                                     \
+  case N:                                                                                       \
+    k.pair[0] = pair_kernel<T, NTYZ, N, 1>(2 * by == gy && 2 * bz == gz);                        \
+    k.pair[1] = pair_kernel<T, NTYZ, N, 2>(2 * by == gy && 2 * bz == gz);                        \
+    k.pair[2] = pair_kernel<T, NTYZ, N, 4>(2 * by == gy && 2 * bz == gz);                        \
+    break;
+    DDA_FUSED_LENGTHS(C)
+#undef C
+    default: break;
+  }
+}
+
+template <typename T, int NTYZ>
 void planned_slot(MvKernels<T>& k, int gy, int gz, int by, int bz) {
   if (gy != gz) return;
   switch (gy) {
@@ -147,6 +178,8 @@ void mv_part_fused(MvKernels<float>& k, int gy, int gz, int by, int bz);
 void mv_part_fused(MvKernels<double>& k, int gy, int gz, int by, int bz);
 void mv_part_slot(MvKernels<float>& k, int gy, int gz, int by, int bz);
 void mv_part_slot(MvKernels<double>& k, int gy, int gz, int by, int bz);
+void mv_part_pair(MvKernels<float>& k, int gy, int gz, int by, int bz);
+void mv_part_pair(MvKernels<double>& k, int gy, int gz, int by, int bz);
 
 // Kernel table of a context: compile-time-planned kernels for grid
 // (gx, gy, gz) and box extents by, bz when every edge is tuned, the
@@ -162,6 +195,7 @@ MvKernels<T> select_kernels(bool planned, int gx, int gy, int gz, int by, int bz
   mv_part_x(k, gx);
   mv_part_split(k, gy, gz, false);
   mv_part_fused(k, gy, gz, by, bz);
+  mv_part_pair(k, gy, gz, by, bz);
   mv_part_slot(k, gy, gz, by, bz);
   return k;
 }

@@ -1,14 +1,14 @@
 // mv_inst.cu -- one part of the matvec kernel tables (matvec_dispatch.cuh),
 // compiled once per part and precision:
-//   nvcc -DDDA_MV_PART=<0..3> -DDDA_MV_DOUBLE=<0|1> -c mv_inst.cu
+//   nvcc -DDDA_MV_PART=<0..4> -DDDA_MV_DOUBLE=<0|1> -c mv_inst.cu
 // Part 0: x passes; 1: split path and runtime-planned kernels; 2: fused
-// plane kernels; 3: cluster plane kernels.  The parts hold the several
+// plane kernels; 3: cluster plane kernels; 4: two-CTA plane kernels.  The parts hold the several
 // hundred compile-time plan instantiations and build in parallel.
 #include "kernel_shapes.cuh"
 #include "matvec_dispatch.cuh"
 
 #if !defined(DDA_MV_PART) || !defined(DDA_MV_DOUBLE)
-#error "build with -DDDA_MV_PART=<0..3> -DDDA_MV_DOUBLE=<0|1>"
+#error "build with -DDDA_MV_PART=<0..4> -DDDA_MV_DOUBLE=<0|1>"
 #endif
 
 namespace dda {
@@ -33,6 +33,10 @@ void mv_part_fused(MvKernels<MvT>& k, int gy, int gz, int by, int bz) {
 #elif DDA_MV_PART == 3
 void mv_part_slot(MvKernels<MvT>& k, int gy, int gz, int by, int bz) {
   planned_slot<MvT, NtYz<MvT>::v>(k, gy, gz, by, bz);
+}
+#elif DDA_MV_PART == 4
+void mv_part_pair(MvKernels<MvT>& k, int gy, int gz, int by, int bz) {
+  planned_pair<MvT, NtYz<MvT>::v>(k, gy, gz, by, bz);
 }
 #endif
 

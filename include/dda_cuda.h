@@ -99,6 +99,11 @@ typedef struct dda_problem {
  * groups; the results are the same); used by tests. */
 #define DDA_FLAG_YZ_GROUPS2 32u
 #define DDA_FLAG_YZ_GROUPS4 64u
+/* dda_problem.flags: run the planned y/z passes with one kx plane per cluster
+ * of two CTAs (each holding half the plane; the autotuner otherwise chooses
+ * between this and one CTA per plane; the results are the same); used by
+ * tests. */
+#define DDA_FLAG_YZ_PAIR 128u
 
 typedef struct dda_stats {
   int64_t iterations;   /* Krylov iterations (summed over inner solves for MIXED) */
@@ -211,7 +216,8 @@ int dda_footprint(const dda_problem* prob, int precision, int64_t* resident, int
 /* Layout the context chose for its matvec (working precision: FP32 for
  * DDA_PREC_FP32 and DDA_PREC_MIXED, FP64 otherwise), 8 values:
  * [0] y/z path (0 fused plane kernel, 1 cluster kernel, 2 split path),
- * [1] resident clusters, [2] CTAs per cluster (cluster kernel) or thread
+ * [1] resident clusters (cluster kernel) or CTAs per kx plane (fused
+ * kernels: 1, or 2 for the two-CTA kernel), [2] CTAs per cluster (cluster kernel) or thread
  * groups per CTA (fused kernel: 1, 2 or 4), [3] rows per y batch,
  * [4] dynamic shared memory of the y/z kernel (bytes), [5] grid lines per
  * x tile, [6] compile-time FFT plans (1) or runtime plans (0),

@@ -153,10 +153,10 @@ def test_autotuned_layout_gives_identical_results(prec, shape):
     print(mvs[0].layout, mvs[1].layout)
 
 
-@pytest.mark.parametrize("groups", [2, 4])
+@pytest.mark.parametrize("groups,pair", [(2, False), (4, False), (1, True), (2, True), (4, True)])
 @pytest.mark.parametrize("prec", ["fp64", "fp32"])
 @pytest.mark.parametrize("case", ["cfg1", "half", "aniso_tuned"])
-def test_grouped_plane_kernel_is_identical(prec, case, groups):
+def test_grouped_plane_kernel_is_identical(prec, case, groups, pair):
     # the fused plane kernel run as two groups of half the CTA (named
     # barriers, columns and row batches split between the groups) does the
     # same arithmetic per butterfly: bit-identical to one group, and equal to
@@ -174,7 +174,11 @@ def test_grouped_plane_kernel_is_identical(prec, case, groups):
                        dtype=np.uint32)
         kind, args, mats, lam = "arrays", (pos, np.zeros(len(pos), np.uint8), "0.05um"), [1.4 + 0.2j], "0.8um"
     out = []
-    gflag = dda_b200.api.FLAG_YZ_GROUPS2 if groups == 2 else dda_b200.api.FLAG_YZ_GROUPS4
+    # the same plane kernel with thread groups and/or as a two-CTA cluster
+    # per plane (k_yz_pair: half the plane per CTA, exchanged through
+    # distributed shared memory)
+    gflag = {1: 0, 2: dda_b200.api.FLAG_YZ_GROUPS2, 4: dda_b200.api.FLAG_YZ_GROUPS4}[groups]
+    gflag |= dda_b200.api.FLAG_YZ_PAIR if pair else 0
     for flags in (8, 8 | gflag):
         if case == "aniso_tuned":
             g = dda_b200.Geometry.from_arrays(*args)
@@ -186,6 +190,7 @@ def test_grouped_plane_kernel_is_identical(prec, case, groups):
             p, mv, op = pr.p, pr.mv, pr.op
         lay = mv.layout
         assert lay["yz_path"] == "fused" and lay["groups"] == (groups if flags & gflag else 1)
+        assert lay["ctas_per_plane"] == (2 if pair and flags & gflag else 1)
         for r, pol in enumerate((1, 2)):
             mv.set_couple_constants(dda_b200.CoupleConstants(p, (0.6, 0.0, 0.8), pol, "ldr"), rhs=r)
         rng = np.random.default_rng(4)

@@ -633,17 +633,17 @@ struct TuneChoice {
   int nrw = 0, cl = 0, groups = 1, pair = 0;
 };
 std::mutex g_tune_mu;
-std::map<std::array<int, 6>, TuneChoice> g_tune_cache;
+std::map<std::array<int, 7>, TuneChoice> g_tune_cache;
 
-template <typename T> float time_yz(dda_ctx* c, int reps) {
+template <typename T> float time_yz(dda_ctx* c, int nrhs, int reps) {
   cudaEvent_t a, b;
   CK(cudaEventCreate(&a));
   CK(cudaEventCreate(&b));
-  launch_yz<T>(c, 1, c->stream, nullptr, 0);  // warm-up
+  launch_yz<T>(c, nrhs, c->stream, nullptr, 0);  // warm-up
   float best = 1e30f;
   for (int r = 0; r < reps; r++) {
     CK(cudaEventRecord(a, c->stream));
-    launch_yz<T>(c, 1, c->stream, nullptr, 0);
+    launch_yz<T>(c, nrhs, c->stream, nullptr, 0);
     CK(cudaEventRecord(b, c->stream));
     CK(cudaEventSynchronize(b));
     float ms = 0;
@@ -678,7 +678,8 @@ template <typename T> void autotune(dda_ctx* c) {
   if ((long long)g.Gx * g.Gy * g.Gz < (1LL << 20)) return;  // small grids keep the defaults
   // the box changes the best batching little next to the grid, so shapes
   // share a choice per grid (served targets mostly land on tuned grids)
-  const std::array<int, 6> key = {g.Gx, g.Gy, g.Gz, (int)sizeof(T), c->planned ? 1 : 0, e.fused ? 0 : 1};
+  const std::array<int, 7> key = {g.Gx, g.Gy, g.Gz, (int)sizeof(T), c->planned ? 1 : 0, e.fused ? 0 : 1,
+                                   std::min(c->max_rhs, 4)};
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune_cache.find(key);
@@ -712,12 +713,16 @@ template <typename T> void autotune(dda_ctx* c) {
           cands.push_back({n, cl});
   }
   if (cands.size() < 2) return;
-  CK(cudaMemsetAsync(e.xhat, 0, (size_t)g.Gx * 3 * g.nlines * sizeof(typename C2<T>::t), c->stream));
+  // timed on up to four right-hand sides: with one, a launch is about a wave
+  // of CTAs and the tail decides; with several, the steady rate does, as in
+  // the solves of batched contexts
+  const int nt = std::min(c->max_rhs, 4);
+  CK(cudaMemsetAsync(e.xhat, 0, (size_t)nt * g.Gx * 3 * g.nlines * sizeof(typename C2<T>::t), c->stream));
   TuneChoice best = cands[0];
   float best_ms = 1e30f;
   for (const TuneChoice& t : cands) {
     apply_choice<T>(c, e, t);
-    const float ms = time_yz<T>(c, 2);
+    const float ms = time_yz<T>(c, nt, 2);
     if (ms < best_ms) {
       best_ms = ms;
       best = t;

@@ -214,6 +214,48 @@ __device__ __forceinline__ void butterfly(T2* v, int j, const T2* tw) {
   }
 }
 
+// Stage-0 twiddles of plan P in butterfly-major order for two-stage plans,
+// whose last stage needs none: entry (m - 1) S0 + j = exp(-2 pi i j m / N)
+// for m in [1, R0), j in [0, S0), copied from the plan's length-N table (the
+// same values as tw[j m]).  Threads that run butterflies j, j+1, ... then
+// read consecutive words instead of words j m apart, which fall into the same
+// shared-memory banks for even m.
+template <typename T, int NT, typename P>
+__device__ __forceinline__ void stage_twiddles0(int off, const FftPlanDev& pl) {
+  constexpr int R = P::r[0], S0 = P::N / R;
+  const typename C2<T>::t* src = reinterpret_cast<const typename C2<T>::t*>(pl.tw);
+  typename C2<T>::t* dst = smem_at<T>(off);
+  for (int i = threadIdx.x; i < (R - 1) * S0; i += NT) {
+    const int m = 1 + i / S0, j = i - (m - 1) * S0;
+    dst[i] = src[j * m];
+  }
+}
+
+// butterfly<P, 0, INV> with the twiddles of stage_twiddles0.
+template <typename P, bool INV, typename T2>
+__device__ __forceinline__ void butterfly0(T2* v, int j, const T2* t0) {
+  constexpr int R = P::r[0];
+  constexpr int S0 = P::N / R;
+  static_assert(P::K == 2, "butterfly-major stage-0 twiddles are staged for two-stage plans");
+  if constexpr (INV) {
+    if (j) {
+#pragma unroll
+      for (int m = 1; m < R; m++) {
+        T2 w = t0[(m - 1) * S0 + j];
+        w.y = -w.y;
+        v[m] = cmul(v[m], w);
+      }
+    }
+    DftN<R, INV, T2>::run(v);
+  } else {
+    DftN<R, INV, T2>::run(v);
+    if (j) {
+#pragma unroll
+      for (int m = 1; m < R; m++) v[m] = cmul(v[m], t0[(m - 1) * S0 + j]);
+    }
+  }
+}
+
 // Stage I of plan P on nl lines by a group of G threads (tid in [0, G)).
 // Element e of line l is at shared offset soff + l*ls + e*es.  Work items are
 // (line, butterfly) pairs with the line fastest, so a line tile and a column

@@ -124,7 +124,7 @@ __global__ void __launch_bounds__(NT, 1) k_yz_pair(typename C2<T>::t* __restrict
   T2* slab1 = rank == 0 ? peer : S;
   T2* plane = xhat + ((size_t)b * g.Gx + kx) * 3 * g.nlines;
   stage_twiddles<T, NT>(0, pz);
-  stage_twiddles<T, NT>(g.Gz, pyp);
+  stage_twiddles0<T, NT, PY>(g.Gz, pyp);  // only y stage 0 has twiddles in two-stage plans
   __syncthreads();
   constexpr int G = NT / GR;
   const int grp = GR == 1 ? 0 : (int)threadIdx.x / G;

@@ -198,7 +198,8 @@ __device__ __forceinline__ void row_stage0(typename C2<T>::t* S, int kz, int q, 
 // Rows [kz0, kz0+nr) of the slab are transformed together by the whole CTA:
 // row r, component c lives in the row buffers at ro + (3 r + c) py.
 
-// y stage 0 fused with the read from (INV: write to) the slab, zero padded.
+// y stage 0 fused with the read from (INV: write to) the slab, zero padded;
+// the y twiddles at `twy` are staged by stage_twiddles0 (two-stage plans).
 template <typename T, int G, typename PY, bool INV, bool HALF = false>
 __device__ __forceinline__ void rows_stage0(typename C2<T>::t* S, int kz0, int nr, int q, int by, int ro,
                                             int py, int twy, int tid, int bar) {
@@ -218,13 +219,13 @@ __device__ __forceinline__ void rows_stage0(typename C2<T>::t* S, int kz0, int n
         const int yy = j + m * S0;
         v[m] = (HALF ? m < R / 2 : yy < by) ? S[srow + yy] : czero<T2>();
       }
-      butterfly<PY, 0, false>(v, j, sm + twy);
+      butterfly0<PY, false>(v, j, sm + twy);
 #pragma unroll
       for (int m = 0; m < R; m++) sm[rb + j + m * S0] = v[m];
     } else {
 #pragma unroll
       for (int m = 0; m < R; m++) v[m] = sm[rb + j + m * S0];
-      butterfly<PY, 0, true>(v, j, sm + twy);
+      butterfly0<PY, true>(v, j, sm + twy);
 #pragma unroll
       for (int m = 0; m < R; m++) {
         const int yy = j + m * S0;
@@ -306,7 +307,7 @@ __global__ void __launch_bounds__(NT, 1) k_yz_p(typename C2<T>::t* __restrict__ 
   T2* S = smem_at<T>(soff);
   T2* plane = xhat + ((size_t)b * g.Gx + kx) * 3 * g.nlines;
   stage_twiddles<T, NT>(0, pz);
-  stage_twiddles<T, NT>(g.Gz, pyp);
+  stage_twiddles0<T, NT, PY>(g.Gz, pyp);  // only y stage 0 has twiddles in two-stage plans
   __syncthreads();
   constexpr int G = NT / GR;
   const int grp = GR == 1 ? 0 : (int)threadIdx.x / G;

@@ -631,6 +631,7 @@ void launch_yz(dda_ctx* c, int nrhs, cudaStream_t s, KrylovState* st, int skipmv
 // zeroed, one right-hand side) and kept per shape for the process.
 struct TuneChoice {
   int nrw = 0, cl = 0, groups = 1, pair = 0;
+  int ncl = 0;  // cluster kernel: clusters in flight (0: as many as can be resident)
 };
 std::mutex g_tune_mu;
 std::map<std::array<int, 7>, TuneChoice> g_tune_cache;
@@ -665,7 +666,7 @@ template <typename T> void apply_choice(dda_ctx* c, Engine<T>& e, const TuneChoi
     e.smem_yz = (e.yz_pair ? e.pair_fixed : e.yz_fixed) + (size_t)t.nrw * e.yz_row;
   } else if (e.slot_path) {
     e.cl = t.cl;
-    e.ncl = e.ncl_by_cl[t.cl];
+    e.ncl = t.ncl > 0 ? std::min(t.ncl, e.ncl_by_cl[t.cl]) : e.ncl_by_cl[t.cl];
     e.sg.nrw = t.nrw;
     e.smem_slot = slot_smem_bytes<T>(g, t.nrw);
   }
@@ -709,8 +710,17 @@ template <typename T> void autotune(dda_ctx* c) {
     for (int cl : {4, 8, 16})
       for (int n : {4, 8, 16})
         if (e.ncl_by_cl[cl] > 0 && n <= (g.Gz + cl - 1) / cl && slot_smem_bytes<T>(g, n) <= kSmemMax &&
-            slot_clusters<T>(e, cl, slot_smem_bytes<T>(g, n)) >= e.ncl_by_cl[cl])
+            slot_clusters<T>(e, cl, slot_smem_bytes<T>(g, n)) >= e.ncl_by_cl[cl]) {
           cands.push_back({n, cl});
+          // fewer clusters in flight: their plane buffers then stay in L2
+          // next to the streamed planes, at the price of less latency hiding
+          for (int div : {2, 3})
+            if (e.ncl_by_cl[cl] / div >= 4) {
+              TuneChoice t{n, cl};
+              t.ncl = e.ncl_by_cl[cl] * (div - 1) / div;
+              cands.push_back(t);
+            }
+        }
   }
   if (cands.size() < 2) return;
   // timed on up to four right-hand sides: with one, a launch is about a wave

@@ -534,22 +534,34 @@ def run_matvec_only(args):
 
 def run_solve_only(args):
     """Runs args.solve_only solves of the default workload (both
-    polarisations, device-resident fields) after one untimed solve, and exits:
-    the command ncu's launch list captures (--profile-from-start off)."""
+    polarisations, device-resident fields; with --workload batched the
+    128-rhs spheroid block) after one untimed solve, and exits: the command
+    ncu's launch list captures (--profile-from-start off)."""
     import torch
     import dda_b200
     torch.cuda.set_device(0)
     prec = args.precision
-    p, mv, einc = build_problem(prec, 2)
-    solver = dda_b200.CudaSolver(mv, args.solver)
-    cdt = torch.complex128 if prec == "fp64" else torch.complex64
-    e_dev = torch.from_numpy(einc).to(cdt).cuda()
+    if args.workload == "batched":  # the 128-rhs spheroid block, mixed precision, QMR-CS
+        import bench_workloads
+        nrhs = args.rhs or 128
+        p, einc, rhs = bench_workloads.spheroid_problem(nrhs)
+        mv = dda_b200.CudaMatVec(p, "mixed", max_rhs=nrhs)
+        for r, (prop, pol) in enumerate(rhs):
+            mv.set_couple_constants(dda_b200.CoupleConstants(p, prop, pol, "ldr"), rhs=r)
+        solver = dda_b200.CudaSolver(mv, "qmr")
+        cdt = torch.complex128
+    else:
+        nrhs = 2
+        p, mv, einc = build_problem(prec, 2)
+        solver = dda_b200.CudaSolver(mv, args.solver)
+        cdt = torch.complex128 if prec == "fp64" else torch.complex64
+    e_dev = torch.from_numpy(np.ascontiguousarray(einc)).to(cdt).cuda()
     p_dev = torch.zeros_like(e_dev)
     torch.cuda.synchronize()
-    solver.get_pol_vec_device(e_dev.data_ptr(), p_dev.data_ptr(), 2, EPS)
+    solver.get_pol_vec_device(e_dev.data_ptr(), p_dev.data_ptr(), nrhs, EPS)
     torch.cuda.profiler.start()
     for _ in range(args.solve_only):
-        solver.get_pol_vec_device(e_dev.data_ptr(), p_dev.data_ptr(), 2, EPS)
+        solver.get_pol_vec_device(e_dev.data_ptr(), p_dev.data_ptr(), nrhs, EPS)
     mv.synchronize()
     torch.cuda.profiler.stop()
     print("solves", args.solve_only, "iterations", [st.iterations for st in solver.last_stats], flush=True)

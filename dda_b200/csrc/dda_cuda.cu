@@ -458,10 +458,17 @@ template <typename T> void setup_engine(dda_ctx* c) {
   e.yz_fixed = fixed;
   e.yz_row = row;
   e.fused = e.k.yz && e.smem_yz <= kSmemMax && !(c->flags & (DDA_FLAG_SPLIT_YZ | DDA_FLAG_SLOT_YZ));
+  // the two-CTA plane kernel: an autotuner candidate where one CTA holds a
+  // plane, the path where only half a plane fits (FP64 planes of the fused
+  // lengths: 1.2-1.8x faster than the cluster kernel's L2 slots), and forced
+  // by DDA_FLAG_YZ_PAIR
   e.pair_fixed = ((size_t)g.Gz + g.Gy + (size_t)(g.Gz / 2) * y.q) * s;
-  if (e.fused && e.k.pair[0] && (c->flags & DDA_FLAG_YZ_PAIR)) {
+  const bool pair_fits = e.k.pair[0] && e.pair_fixed + 4 * row <= kSmemMax &&
+                         !(c->flags & (DDA_FLAG_SPLIT_YZ | DDA_FLAG_SLOT_YZ));
+  if (pair_fits && ((c->flags & DDA_FLAG_YZ_PAIR) || !e.fused)) {
     int np = 32;
     while (np > 1 && e.pair_fixed + np * row > kSmemMax) np--;
+    e.fused = true;
     e.yz_pair = true;
     e.yz.nrw = np;
     e.smem_yz = e.pair_fixed + np * row;

@@ -67,9 +67,10 @@ def test_spheroid_block_matvec_matches_oracle(spheroid_oracle, prec, tol):
     p = dda_b200.DDAParams(g, [1.33 + 0.01j], lam)
     assert p.grid == (192, 128, 128) and p.box == (96, 64, 64)
     mv = dda_b200.CudaMatVec(p, prec, max_rhs=4)
-    # FP32: the fused half-padded plane kernel; FP64: the plane (395 KB) is
-    # beyond one CTA's shared memory, so the cluster kernel
-    assert mv.layout["yz_path"] == ("fused" if prec == "fp32" else "cluster")
+    # FP32: the fused half-padded plane kernel in one CTA; FP64: the plane
+    # (395 KB) is beyond one CTA's shared memory, so two CTAs share it
+    lay = mv.layout
+    assert lay["yz_path"] == "fused" and lay["ctas_per_plane"] == (1 if prec == "fp32" else 2)
     rng = np.random.default_rng(3)
     xs, want = [], []
     for r, (prop, pol) in enumerate(rhs):

@@ -399,6 +399,16 @@ template <typename T> void setup_slot(dda_ctx* c, Engine<T>& e) {
   e.slot_path = true;
 }
 
+// Every x-pass kernel of an engine (plain, with a solver step in the load,
+// over FP64 vectors).
+template <typename T> std::vector<const void*> x_pass_kernels(const Engine<T>& e) {
+  std::vector<const void*> v;
+  for (const void* f : {(const void*)e.k.xfwd, (const void*)e.k.xfwd_pre, (const void*)e.k.xinv,
+                        (const void*)e.k.xfwd_m, (const void*)e.k.xfwd_m_pre, (const void*)e.k.xinv_m})
+    if (f) v.push_back(f);
+  return v;
+}
+
 // Lines per k_xfwd / k_xinv tile.  The two x passes launch
 // ntiles x 3 x nrhs CTAs of a few microseconds each, so the count of waves
 // over the SMs decides their time: among tiles from half the 72 KB maximum
@@ -412,16 +422,19 @@ template <typename T> void pick_x_tile(dda_ctx* c, Engine<T>& e) {
   const size_t s = sizeof(typename C2<T>::t);
   int nsm = 148;
   CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
-  CK(allow_smem((const void*)e.k.xfwd));
-  CK(allow_smem((const void*)e.k.xinv));
+  const std::vector<const void*> xk = x_pass_kernels(e);
+  for (const void* f : xk) CK(allow_smem(f));
   const int tmax = x_tile_max((long long)s, g.Gx);
   long long best_cost = -1;
   for (int tl = std::max(1, tmax / 2); tl <= tmax; tl++) {
     const size_t smem = ((size_t)g.Gx + g.nmat + (size_t)tl * g.pitchx) * s;
-    int of = 0, oi = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&of, e.k.xfwd, kNtX, smem));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&oi, e.k.xinv, kNtX, smem));
-    const long long slots = (long long)std::max(1, std::min(of, oi)) * nsm;
+    int occ = 1 << 30;  // the least over every x-pass variant
+    for (const void* f : xk) {
+      int o = 0;
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, f, kNtX, smem));
+      occ = std::min(occ, o);
+    }
+    const long long slots = (long long)std::max(1, occ) * nsm;
     const long long ctas = (long long)ntiles(c, tl) * 3 * c->max_rhs;
     const long long cost = (ctas + slots - 1) / slots * (tl + 2);
     if (best_cost < 0 || cost <= best_cost) {
@@ -522,8 +535,7 @@ template <typename T> void setup_engine(dda_ctx* c) {
     if (bytes > kSmemMax) throw DdaError(DDA_ERR_UNSUPPORTED, "shared-memory tile above the SM limit");
     CK(allow_smem(f));
   };
-  attr((const void*)e.k.xfwd, e.smem_x);
-  attr((const void*)e.k.xinv, e.smem_x);
+  for (const void* f : x_pass_kernels(e)) attr(f, e.smem_x);
   if (e.fused) {
     attr((const void*)e.k.yz, e.smem_yz);
     if (e.k.yz2) attr((const void*)e.k.yz2, e.smem_yz);
@@ -750,20 +762,38 @@ template <typename T> void autotune(dda_ctx* c) {
   g_tune_cache[key] = best;
 }
 
-// The matvec: k_xfwd -> (k_yz | k_yz_slot | cols/yrows/cols) -> k_xinv.
-template <typename T>
-void matvec(dda_ctx* c, const typename C2<T>::t* arg, typename C2<T>::t* res, int conj, int nrhs,
-            cudaStream_t s, KrylovState* st, KrylovStep step, int skipmv = 0) {
+// The matvec: k_xfwd -> (k_yz | k_yz_slot | cols/yrows/cols) -> k_xinv, over
+// vectors of element type A2: the engine's own (T = float or double), or
+// FP64 vectors around the FP32 convolution (T = float, A2 = double2: the
+// argument is rounded to FP32 as k_xfwd reads it, the identity term added in
+// FP64 by k_xinv).  pre: a solver step that produces the argument, run in
+// k_xfwd's load (arg is then pre.out).
+template <typename T, typename A2 = typename C2<T>::t>
+void matvec(dda_ctx* c, const A2* arg, A2* res, int conj, int nrhs, cudaStream_t s, KrylovState* st,
+            KrylovStep step, int skipmv = 0, XPre pre = XPre{}) {
   Engine<T>& e = eng<T>(c);
   MvGeom g = c->g;
   g.tl = e.tl;
   const FftPlanDev px = c->mx.dev<T>();
   dim3 gx(ntiles(c, e.tl), 3, nrhs);
-  e.k.xfwd<<<gx, kNtX, e.smem_x, s>>>(arg, e.xhat, c->line_off, c->dip, c->perm, e.ccs, conj, g, px, st, skipmv);
+  const RedTarget red = red_target(c, 3 * ntiles(c, e.tl));
+  typename MvKernels<T>::template XfwdF<A2> xf;
+  typename MvKernels<T>::template XinvF<A2> xi;
+  if constexpr (std::is_same<A2, typename C2<T>::t>::value) {
+    xf = pre.op != XP_NONE ? e.k.xfwd_pre : e.k.xfwd;
+    xi = e.k.xinv;
+  } else {
+    xf = pre.op != XP_NONE ? e.k.xfwd_m_pre : e.k.xfwd_m;
+    xi = e.k.xinv_m;
+  }
+  if (pre.op != XP_NONE) {
+    pre.out = const_cast<A2*>(arg);
+    pre.step.red = red;
+  }
+  xf<<<gx, kNtX, e.smem_x, s>>>(arg, e.xhat, c->line_off, c->dip, c->perm, e.ccs, conj, g, px, st, skipmv, pre);
   launch_yz<T>(c, nrhs, s, st, skipmv);
-  step.red = red_target(c, 3 * ntiles(c, e.tl));
-  e.k.xinv<<<gx, kNtX, e.smem_x, s>>>(arg, res, e.xhat, c->line_off, c->dip, c->perm, e.ccs, conj, g, px, st, step,
-                                      skipmv);
+  step.red = red;
+  xi<<<gx, kNtX, e.smem_x, s>>>(arg, res, e.xhat, c->line_off, c->dip, c->perm, e.ccs, conj, g, px, st, step, skipmv);
   CK(cudaGetLastError());
   c->launches += (e.fused || e.slot_path) ? 3 : 5;
 }
@@ -903,39 +933,30 @@ template <typename T> struct Solve {
   // then y = arg + conv and the step's sums in FP64.
   bool mv32 = false;
 
-  void matvec_any(const T2* arg, T2* res, int conj, KrylovStep k, int skipmv = 0) {
+  void matvec_any(const T2* arg, T2* res, int conj, KrylovStep k, int skipmv = 0, XPre pre = XPre{}) {
     if constexpr (std::is_same<T, double>::value) {
       if (mv32) {
-        Engine<float>& f = c->e32;
-        const long long n = (long long)nrhs * 3 * c->g.nvs;
-        k_convert<double2, float2><<<592, 256, 0, s>>>(arg, f.vec[0], n);
-        CK(cudaGetLastError());
-        c->launches++;
-        KrylovStep conv{KOP_NONE, 0, nullptr, {}};
-        conv.conv_only = 1;
-        matvec<float>(c, f.vec[0], f.io, conj, nrhs, s, st, conv, skipmv);
-        VecArgs a;
-        memset(&a, 0, sizeof(a));
-        a.v[0] = res;
-        a.v[1] = const_cast<T2*>(arg);
-        a.v[2] = f.io;
-        a.op = V_ADD_CONV;
-        a.first = skipmv;
-        a.nv = c->g.nv;
-        a.nvs = c->g.nvs;
-        a.nmat = c->g.nmat;
-        a.nparts = c->nparts_vec;
-        a.step = k;
-        vec_kernel<T, kNtV>(a.op)<<<dim3(c->nparts_vec, nrhs), kNtV, 0, s>>>(a, st);
-        CK(cudaGetLastError());
-        c->launches++;
+        matvec<float, double2>(c, arg, res, conj, nrhs, s, st, k, skipmv, pre);
         return;
       }
     }
-    matvec<T>(c, arg, res, conj, nrhs, s, st, k, skipmv);
+    matvec<T>(c, arg, res, conj, nrhs, s, st, k, skipmv, pre);
   }
 
   void mv(const T2* arg, T2* res, int conj, KrylovStep k) { matvec_any(arg, res, conj, k); }
+
+  // res = A out, with out = the solver step `op` of v1, v2 (and out) computed
+  // in the matvec's first pass (XPreOp); pk: its sums, if any.
+  void mv_pre(int op, int first, T2* out, const T2* v1, const T2* v2, T2* res, KrylovStep pk, KrylovStep k,
+              int skipmv = 0) {
+    XPre pre{};
+    pre.op = op;
+    pre.first = first;
+    pre.v1 = v1;
+    pre.v2 = v2;
+    pre.step = pk;
+    matvec_any(out, res, 0, k, skipmv, pre);
+  }
 
   // CpuIterativeSolver::initGeneral (DDA/CpuIterativeSolver.cpp:45-91) with
   // the GPU setup kernels of DDA/GpuIterativeSolver.cpp:78-134.
@@ -968,27 +989,27 @@ template <typename T> struct Solve {
         break;
       }
       case DDA_SOLVER_BICGSTAB: {  // t1 = p, t2 = v, t3 = s, t4 = rt
-        vec(V_BIS_P, nr == 0, {b.t1, b.t2, b.R}, step(KOP_NONE));
-        mv(b.t1, b.t2, 0, step(KOP_BIS_ALPHA, EP_YW_HERM, b.t4));
-        vec(V_BIS_S, 0, {b.t3, b.t2, b.R}, step(KOP_BIS_S));
-        matvec_any(b.t3, b.A, 0, step(KOP_BIS_OMEGA, EP_AY_HERM_NORM), 1);
+        // p = r + beta (p - omega v) and s = r - alpha v run in the first
+        // pass of the matvec they feed; the s step's |s|^2 decides the
+        // half-step exit, which the rest of that matvec then skips
+        mv_pre(XP_BIS_P, nr == 0, b.t1, b.t2, b.R, b.t2, step(KOP_NONE), step(KOP_BIS_ALPHA, EP_YW_HERM, b.t4));
+        mv_pre(XP_BIS_S, 0, b.t3, b.t2, b.R, b.A, step(KOP_BIS_S), step(KOP_BIS_OMEGA, EP_AY_HERM_NORM), 1);
         vec(V_BIS_XR, 0, {b.X, b.t1, b.t3, b.A, b.R, b.t4}, step(KOP_BIS_END));
         break;
       }
       case DDA_SOLVER_BICG: {  // t1 = p
-        vec(V_BICG_P, nr == 0, {b.t1, b.R}, step(KOP_NONE));
-        mv(b.t1, b.A, 0, step(KOP_BICG_MU, EP_YA_BIL));
+        mv_pre(XP_BICG_P, nr == 0, b.t1, b.R, nullptr, b.A, step(KOP_NONE), step(KOP_BICG_MU, EP_YA_BIL));
         vec(V_BICG_XR, 0, {b.X, b.t1, b.A, b.R}, step(KOP_BICG_END));
         break;
       }
       default: {  // CGNR, t1 = p
         if (nr == 0) {
           mv(b.R, b.t1, 1, step(KOP_CGNR_RO, EP_NORM));
+          mv(b.t1, b.A, 0, step(KOP_CGNR_ALPHA, EP_NORM));
         } else {
           mv(b.R, b.A, 1, step(KOP_CGNR_RO, EP_NORM));
-          vec(V_CGNR_P, 0, {b.t1, b.A}, step(KOP_NONE));
+          mv_pre(XP_CGNR_P, 0, b.t1, b.A, nullptr, b.A, step(KOP_NONE), step(KOP_CGNR_ALPHA, EP_NORM));
         }
-        mv(b.t1, b.A, 0, step(KOP_CGNR_ALPHA, EP_NORM));
         vec(V_CGNR_XR, 0, {b.X, b.t1, b.A, b.R}, step(KOP_CGNR_END));
         break;
       }
@@ -1615,7 +1636,8 @@ template <typename T> void profile_t(dda_ctx* c, int nrhs, int reps, double* ms)
   for (int r = 0; r <= reps; r++) {
     dim3 gx(ntiles(c, e.tl), 3, nrhs);
     CK(cudaEventRecord(ev[0], s));
-    e.k.xfwd<<<gx, kNtX, e.smem_x, s>>>(arg, e.xhat, c->line_off, c->dip, c->perm, e.ccs, 0, g, px, nullptr, 0);
+    e.k.xfwd<<<gx, kNtX, e.smem_x, s>>>(arg, e.xhat, c->line_off, c->dip, c->perm, e.ccs, 0, g, px, nullptr, 0,
+                                        XPre{});
     CK(cudaEventRecord(ev[1], s));
     launch_yz<T>(c, nrhs, s, nullptr, 0);
     CK(cudaEventRecord(ev[2], s));

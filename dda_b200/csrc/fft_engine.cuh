@@ -65,6 +65,10 @@ template <typename T, typename T2> __host__ __device__ __forceinline__ T2 caxr(T
 #endif
   acc.x += c * t.x; acc.y += c * t.y; return acc;
 }
+// a complex value in another precision (round to nearest)
+template <typename T2, typename S2> __host__ __device__ __forceinline__ T2 cvt(S2 a) {
+  T2 r; r.x = a.x; r.y = a.y; return r;
+}
 template <typename T2> __host__ __device__ __forceinline__ T2 cconj(T2 a) {
   a.y = -a.y; return a;
 }

@@ -19,6 +19,8 @@
 
 namespace dda {
 
+// (The steps that produce a matvec argument -- BiCGStab's p and s, BiCG's
+// and CGNR's p -- run in the matvec's first pass: XPreOp, matvec_kernels.cuh.)
 enum VecOp {
   V_SETUP_PVEC = 0,  // v0 = sqrt(cc).v1 (b = sqrt(cc) Einc); n = |v0|^2
   V_START_X,         // v0 = v1 / sqrt(cc)  (start value, DDA/GpuIterativeSolverInst.cl:52-77)
@@ -28,17 +30,12 @@ enum VecOp {
   V_QMR_VT,          // v0 = [v0 mBeta] + v1 mAlpha + v2; a = v0.v0, n = |v0|^2   (vt, v, A)
   V_QMR_UPD,         // p/x/v/r update of DDA/QmrCs.cpp:152-167 (first: 1 = iteration 0, 2 = iteration 1)
   V_BIS_INIT,        // v0 = v1 (rt = r); a = v1.conj(v0)
-  V_BIS_P,           // v0 = first ? v2 : v0 beta + v1 bo + v2     (p, v, r)
-  V_BIS_S,           // v0 = v1 mAlpha + v2; n = |v0|^2            (s, v, r)
   V_BIS_XR,          // x/r update of DDA/BicgStab.cpp:98-110
   V_BICG_RO,         // a = v0.v0
-  V_BICG_P,          // v0 = first ? v1 : v0 beta + v1             (p, r)
   V_BICG_XR,         // x += p alpha; r += A mAlpha; n = |r|^2; a = r.r
-  V_CGNR_P,          // v0 = v0 beta + v1                          (p, Ah)
   V_CGNR_XR,         // x += p alpha; r += A mAlpha; n = |r|^2
   V_RESULT,          // v0 = sqrt(cc).v1  (P = sqrt(cc) x)
   V_NORM,            // n = |v0|^2
-  V_ADD_CONV,        // v0 = v1 + (FP32) v2; step sums as the matvec epilogue (first: skip on half-step exit)
   V_COUNT
 };
 
@@ -54,11 +51,6 @@ struct VecArgs {
   KrylovStep step;
 };
 
-template <typename T2, typename S2>
-__device__ __forceinline__ T2 cvt(S2 a) {
-  T2 r; r.x = a.x; r.y = a.y; return r;
-}
-
 // Whether the element loop of step OP reads vector k (first: the
 // iteration-0 variant flag, skip: the BiCGStab half-step exit).
 template <int OP>
@@ -69,10 +61,8 @@ __device__ __forceinline__ bool vec_reads(int k, int first, int skip) {
     case V_START_X:
     case V_QMR_V0:
     case V_BIS_INIT:
-    case V_ADD_CONV:
       return k == 1;
     case V_R_INIT:
-    case V_BIS_S:
       return k == 1 || k == 2;
     case V_CHOOSE_X0:
       return k == 2;
@@ -80,20 +70,14 @@ __device__ __forceinline__ bool vec_reads(int k, int first, int skip) {
       return k == 1 || k == 2 || (k == 0 && !first);
     case V_QMR_UPD:
       return k == 0 || k == 3 || k == 4 || k == 5 || (k == 2 && first != 1) || (k == 1 && first == 0);
-    case V_BIS_P:
-      return k == 2 || (!first && (k == 0 || k == 1));
     case V_BIS_XR:
       return k == 0 || k == 1 || (!skip && (k == 2 || k == 3 || k == 5));
     case V_BICG_RO:
     case V_NORM:
       return k == 0;
-    case V_BICG_P:
-      return k == 1 || (!first && k == 0);
     case V_BICG_XR:
     case V_CGNR_XR:
       return k <= 3;
-    case V_CGNR_P:
-      return k <= 1;
     default:
       return false;
   }
@@ -109,7 +93,6 @@ __global__ void __launch_bounds__(NT, 3) k_vec(VecArgs va, KrylovState* st) {
   const int b = blockIdx.y;
   KrylovState& s = st[b];
   if (s.done && OP != V_RESULT) return;  // the result copy runs after convergence
-  if (OP == V_ADD_CONV && va.first && s.skipmv) return;  // its matvec was skipped too
   const long long len = 3LL * va.nvs;
   const long long chunk = ((len + va.nparts - 1) / va.nparts + 31) / 32 * 32;
   const long long i0 = chunk * blockIdx.x;
@@ -124,7 +107,7 @@ __global__ void __launch_bounds__(NT, 3) k_vec(VecArgs va, KrylovState* st) {
   const T2* ccs = reinterpret_cast<const T2*>(va.ccs) + (size_t)b * va.nmat * 3;
   // step scalars in working precision
   const T2 mBeta = cvt<T2>(s.mBeta), mAlpha = cvt<T2>(s.mAlpha), alpha = cvt<T2>(s.alpha);
-  const T2 betaInv = cvt<T2>(s.betaInv), beta = cvt<T2>(s.beta), bo = cvt<T2>(s.bo);
+  const T2 betaInv = cvt<T2>(s.betaInv);
   const T2 omega = cvt<T2>(s.omega), tau = cvt<T2>(s.tau), cNOT = cvt<T2>(s.cNOT);
   const T2 zetaInv = cvt<T2>(s.zetaInv), mEtaZeta = cvt<T2>(s.mEtaZeta), mThetaZeta = cvt<T2>(s.mThetaZeta);
   const T2 mOmega = cvt<T2>(dneg(s.omega));
@@ -137,8 +120,7 @@ __global__ void __launch_bounds__(NT, 3) k_vec(VecArgs va, KrylovState* st) {
   constexpr int U = (sizeof(T) == 4 ? 4 : 2) / (OP == V_QMR_UPD ? 2 : 1);  // six streams: half
   const int first = va.first;
   for (long long base = i0 + threadIdx.x; base < i1; base += (long long)U * NT) {
-    T2 in0[U], in1[U], in2[U], in3[U], in4[U], in5[U], wv[U];
-    float2 cvv[U];
+    T2 in0[U], in1[U], in2[U], in3[U], in4[U], in5[U];
 #pragma unroll
     for (int u = 0; u < U; u++) {
       const long long i = base + (long long)u * NT;
@@ -149,10 +131,6 @@ __global__ void __launch_bounds__(NT, 3) k_vec(VecArgs va, KrylovState* st) {
         if (vec_reads<OP>(3, first, skip)) in3[u] = v3[i];
         if (vec_reads<OP>(4, first, skip)) in4[u] = v4[i];
         if (vec_reads<OP>(5, first, skip)) in5[u] = v5[i];
-        if (OP == V_ADD_CONV) {
-          cvv[u] = reinterpret_cast<const float2*>(va.v[2])[off + i];
-          if (va.step.w) wv[u] = reinterpret_cast<const T2*>(va.step.w)[off + i];
-        }
       }
     }
 #pragma unroll
@@ -237,15 +215,6 @@ __global__ void __launch_bounds__(NT, 3) k_vec(VecArgs va, KrylovState* st) {
           acc.a.x += (double)r.x * r.x + (double)r.y * r.y;
           break;
         }
-        case V_BIS_P:
-          v0[i] = va.first ? in2[u] : cadd(cadd(cmul(in0[u], beta), cmul(in1[u], bo)), in2[u]);
-          break;
-        case V_BIS_S: {
-          const T2 t = cadd(cmul(in1[u], mAlpha), in2[u]);
-          v0[i] = t;
-          acc.n += (double)t.x * t.x + (double)t.y * t.y;
-          break;
-        }
         case V_BIS_XR: {
           // v0 = x, v1 = p, v2 = s, v3 = A s, v4 = r, v5 = rt
           if (skip) {
@@ -268,9 +237,6 @@ __global__ void __launch_bounds__(NT, 3) k_vec(VecArgs va, KrylovState* st) {
           acc.a.y += 2.0 * (double)r.x * r.y;
           break;
         }
-        case V_BICG_P:
-          v0[i] = va.first ? in1[u] : cadd(cmul(in0[u], beta), in1[u]);
-          break;
         case V_BICG_XR:
         case V_CGNR_XR: {
           // v0 = x, v1 = p, v2 = A, v3 = r
@@ -282,25 +248,9 @@ __global__ void __launch_bounds__(NT, 3) k_vec(VecArgs va, KrylovState* st) {
           acc.a.y += 2.0 * (double)r.x * r.y;
           break;
         }
-        case V_CGNR_P:
-          v0[i] = cadd(cmul(in0[u], beta), in1[u]);
-          break;
         case V_NORM: {
           const T2 r = in0[u];
           acc.n += (double)r.x * r.x + (double)r.y * r.y;
-          break;
-        }
-        case V_ADD_CONV: {
-          // result of a matvec whose convolution ran in FP32: y = x + conv
-          const float2 cv = cvv[u];
-          const T2 a = in1[u];
-          T2 y = a;
-          y.x += cv.x;
-          y.y += cv.y;
-          v0[i] = y;
-          if (va.step.op != KOP_NONE)
-            acc = epilogue_terms<T2>(acc, y, a, va.step.w ? wv[u] : a,
-                                     va.step.mode);
           break;
         }
         default:

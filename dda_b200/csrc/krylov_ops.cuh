@@ -82,7 +82,6 @@ struct KrylovStep {
   int mode;
   const void* w;  // third vector for EP_YW_HERM (same precision as y)
   RedTarget red;
-  int conv_only;  // k_xinv: write conj?(sqrt(cc) X) only, without the identity term
 };
 
 __device__ __forceinline__ double2 dc(double x, double y) { return make_double2(x, y); }

@@ -12,17 +12,27 @@ namespace dda {
 
 template <typename T> struct MvKernels {
   typedef typename C2<T>::t T2;
-  typedef void (*XfwdFn)(const T2*, T2*, const uint32_t*, const uint32_t*, const uint32_t*, const T2*, int,
-                         MvGeom, FftPlanDev, const KrylovState*, int);
-  typedef void (*XinvFn)(const T2*, T2*, const T2*, const uint32_t*, const uint32_t*, const uint32_t*,
+  // x passes over vectors of element type A2 (T2, or double2 for FP64
+  // Krylov vectors around an FP32 convolution)
+  template <typename A2>
+  using XfwdF = void (*)(const A2*, T2*, const uint32_t*, const uint32_t*, const uint32_t*, const T2*, int,
+                         MvGeom, FftPlanDev, KrylovState*, int, XPre);
+  template <typename A2>
+  using XinvF = void (*)(const A2*, A2*, const T2*, const uint32_t*, const uint32_t*, const uint32_t*,
                          const T2*, int, MvGeom, FftPlanDev, KrylovState*, KrylovStep, int);
+  typedef XfwdF<T2> XfwdFn;
+  typedef XinvF<T2> XinvFn;
   typedef void (*YzFn)(T2*, const T2*, MvGeom, YzGeom, FftPlanDev, FftPlanDev, const KrylovState*, int);
   typedef void (*YrowsFn)(T2*, const T2*, MvGeom, YzGeom, FftPlanDev, const KrylovState*, int);
   typedef void (*ColsFn)(const T2*, T2*, ColGeom, FftPlanDev, int, const KrylovState*, int);
   typedef void (*SlotFn)(T2*, const T2*, MvGeom, SlotGeom, const uint32_t*, int, T2*, FftPlanDev, FftPlanDev,
                          const KrylovState*, int);
   XfwdFn xfwd = nullptr;
+  XfwdFn xfwd_pre = nullptr;  // with a solver step in the load (XPre)
   XinvFn xinv = nullptr;
+  // FP32 engines: the same over FP64 vectors (mixed precision)
+  XfwdF<double2> xfwd_m = nullptr, xfwd_m_pre = nullptr;
+  XinvF<double2> xinv_m = nullptr;
   YzFn yz = nullptr;        // fused plane kernel (nullptr: none for this shape)
   YzFn yz2 = nullptr;       // the same kernel run as two groups of half the CTA
   YzFn yz4 = nullptr;       // ... and as four groups of a quarter
@@ -83,14 +93,26 @@ typename MvKernels<T>::SlotFn slot_kernel(bool half) {
 // several hundred plan instantiations compile in parallel.  Part 0: x passes;
 // 1: split path (y rows, z columns) and the runtime-planned kernels; 2: fused
 // plane kernels; 3: cluster plane kernels.
+// The x passes of one x plan (PX: compile-time plan, or void), every
+// vector variant.
+template <typename T, int NTX, typename PX>
+void x_kernels(MvKernels<T>& k) {
+  typedef typename C2<T>::t T2;
+  k.xfwd = k_xfwd<T, NTX, PX, T2, 0>;
+  k.xfwd_pre = k_xfwd<T, NTX, PX, T2, 1>;
+  k.xinv = k_xinv<T, NTX, PX, T2>;
+  if constexpr (std::is_same<T, float>::value) {
+    k.xfwd_m = k_xfwd<T, NTX, PX, double2, 0>;
+    k.xfwd_m_pre = k_xfwd<T, NTX, PX, double2, 1>;
+    k.xinv_m = k_xinv<T, NTX, PX, double2>;
+  }
+}
+
 template <typename T, int NTX>
 void planned_x(MvKernels<T>& k, int gx) {
   switch (gx) {
-#define C(N)                                                           \
-  case N:                                                              \
-    k.xfwd = k_xfwd<T, NTX, typename PlanFor<N>::type>;                \
-    k.xinv = k_xinv<T, NTX, typename PlanFor<N>::type>;                \
-    break;
+#define C(N) \
+  case N: x_kernels<T, NTX, typename PlanFor<N>::type>(k); break;
     DDA_TUNED_LENGTHS(C)
 #undef C
     default: break;
@@ -161,8 +183,7 @@ void planned_slot(MvKernels<T>& k, int gy, int gz, int by, int bz) {
 
 template <typename T, int NTX, int NTYZ, int NTC>
 void generic_kernels(MvKernels<T>& k) {
-  k.xfwd = k_xfwd<T, NTX>;
-  k.xinv = k_xinv<T, NTX>;
+  x_kernels<T, NTX, void>(k);
   k.yz = k_yz<T, NTYZ>;
   k.yrows = k_yrows<T, NTYZ>;
   k.cols = k_fft_cols<T, NTC>;

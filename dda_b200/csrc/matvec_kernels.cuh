@@ -125,21 +125,61 @@ struct TileWalk {
   }
 };
 
+// A solver step whose result is the next matvec's argument, run in
+// k_xfwd's load instead of a pass of its own: the argument is computed from
+// the solver's vectors, written back for the later steps and transformed.
+// Same arithmetic as the k_vec step named beside each.
+enum XPreOp {
+  XP_NONE = 0,
+  XP_BIS_P,   // out = first ? v2 : out beta + v1 bo + v2       (p, v, r)   V_BIS_P
+  XP_BIS_S,   // out = v1 mAlpha + v2; n = |out|^2              (s, v, r)   V_BIS_S
+  XP_BICG_P,  // out = first ? v1 : out beta + v1               (p, r)      V_BICG_P
+  XP_CGNR_P,  // out = out beta + v1                            (p, A^H r)  V_CGNR_P
+};
+struct XPre {
+  int op;
+  int first;         // iteration 0 variant
+  void* out;         // the matvec argument (vector precision)
+  const void* v1;
+  const void* v2;
+  KrylovStep step;   // sums over out, finalised by the last CTA (XP_BIS_S)
+};
+
+__device__ __forceinline__ bool xpre_reads_out(int op, int first) {
+  return op == XP_CGNR_P || ((op == XP_BIS_P || op == XP_BICG_P) && !first);
+}
+__device__ __forceinline__ bool xpre_reads_v1(int op, int first) { return !(op == XP_BIS_P && first); }
+__device__ __forceinline__ bool xpre_reads_v2(int op) { return op == XP_BIS_P || op == XP_BIS_S; }
+
+template <typename A2>
+__device__ __forceinline__ A2 xpre_value(int op, int first, A2 p, A2 v1, A2 v2, A2 beta, A2 bo, A2 mAlpha) {
+  switch (op) {
+    case XP_BIS_P: return first ? v2 : cadd(cadd(cmul(p, beta), cmul(v1, bo)), v2);
+    case XP_BIS_S: return cadd(cmul(v1, mAlpha), v2);
+    case XP_BICG_P: return first ? v1 : cadd(cmul(p, beta), v1);
+    default: return cadd(cmul(p, beta), v1);
+  }
+}
+
 // ------------------------------------------------------------ k_xfwd ----
 // grid (ceil(nlines/tl), 3, nrhs).  PX: compile-time plan of the x
-// transform, or void for the runtime-planned engine.
-template <typename T, int NT, typename PX = void>
-__global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 3) k_xfwd(const typename C2<T>::t* __restrict__ arg,
+// transform, or void for the runtime-planned engine.  A2: the vectors'
+// element type (double2 with T = float: FP64 Krylov vectors, rounded to FP32
+// as they are read).  PRE: the argument is pre.op's result (XPreOp), which
+// this kernel writes back, padding included.
+template <typename T, int NT, typename PX = void, typename A2 = typename C2<T>::t, int PRE = 0>
+__global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 3) k_xfwd(const A2* __restrict__ arg,
                                              typename C2<T>::t* __restrict__ xhat,
                                              const uint32_t* __restrict__ line_off,
                                              const uint32_t* __restrict__ dip,
                                              const uint32_t* __restrict__ perm,
                                              const typename C2<T>::t* __restrict__ ccs, int conj,
-                                             MvGeom g, FftPlanDev px,
-                                             const KrylovState* __restrict__ st, int mvskip) {
+                                             MvGeom g, FftPlanDev px, KrylovState* st, int mvskip, XPre pre) {
   typedef typename C2<T>::t T2;
   const int b = blockIdx.z, c = blockIdx.y;
-  if (rhs_idle(st, b, mvskip)) return;
+  // the BiCGStab s step decides the half-step exit itself: it runs whenever
+  // the right-hand side is not done
+  if (rhs_idle(st, b, PRE ? 0 : mvskip)) return;
   const int toff = x_tile_off(g);
   T2* scc = smem_at<T>(g.Gx);
   T2* sm = smem_at<T>(toff);
@@ -153,15 +193,33 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 3) k_xfwd(const typen
   __syncthreads();
   // the tile's dipoles are one contiguous CSR range: every thread takes
   // entries of it independently, so many loads are in flight at once
-  const T2* a = arg + ((size_t)b * 3 + c) * g.nvs;
+  const size_t voff = ((size_t)b * 3 + c) * g.nvs;
+  const A2* a = arg + voff;
+  A2* po = PRE ? reinterpret_cast<A2*>(pre.out) + voff : nullptr;
+  const A2* p1 = PRE && pre.v1 ? reinterpret_cast<const A2*>(pre.v1) + voff : nullptr;
+  const A2* p2 = PRE && pre.v2 ? reinterpret_cast<const A2*>(pre.v2) + voff : nullptr;
+  A2 beta = czero<A2>(), bo = czero<A2>(), mAlpha = czero<A2>();
+  if (PRE) {
+    beta = cvt<A2>(st[b].beta);
+    bo = cvt<A2>(st[b].bo);
+    mAlpha = cvt<A2>(st[b].mAlpha);
+  }
+  const int op = pre.op, first = pre.first;
+  const bool rd_out = PRE && xpre_reads_out(op, first), rd1 = PRE && xpre_reads_v1(op, first);
+  const bool rd2 = PRE && xpre_reads_v2(op);
+  RedSums acc = red_zero();
+  // loads in flight per thread: fewer where each entry has three inputs or
+  // wider elements, within the registers of three CTAs per SM
+  constexpr int XB = PRE ? (sizeof(A2) == 16 && sizeof(T) == 4 ? 2 : 4)
+                         : (sizeof(A2) > sizeof(T2) ? kXBatch / 2 : kXBatch);
   const uint32_t je = soff[nl];
   uint32_t j = soff[0] + threadIdx.x;
   int l = j < je ? tile_line(soff, nl, j) : 0;
-  for (; j < je; j += kXBatch * NT) {
-    int o[kXBatch];  // shared offset of entry j + u NT, -1 past the tile
-    uint32_t d[kXBatch], jj[kXBatch];
+  for (; j < je; j += XB * NT) {
+    int o[XB];  // shared offset of entry j + u NT, -1 past the tile
+    uint32_t d[XB], jj[XB];
 #pragma unroll
-    for (int u = 0; u < kXBatch; u++) {
+    for (int u = 0; u < XB; u++) {
       const uint32_t ju = j + u * NT;
       o[u] = -1;
       if (ju < je) {
@@ -171,32 +229,57 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 3) k_xfwd(const typen
         o[u] = l * g.pitchx;
       }
     }
-    T2 v[kXBatch];
+    A2 v[XB], w1[XB], w2[XB];
 #pragma unroll
-    for (int u = 0; u < kXBatch; u++)
-      if (o[u] >= 0) v[u] = a[jj[u]];
-#pragma unroll
-    for (int u = 0; u < kXBatch; u++)
+    for (int u = 0; u < XB; u++)
       if (o[u] >= 0) {
-        if (conj) v[u].y = -v[u].y;
-        sm[o[u] + (d[u] & 0xffffu)] = cmul(v[u], scc[d[u] >> 16]);
+        if (!PRE) {
+          v[u] = a[jj[u]];
+        } else {
+          v[u] = rd_out ? po[jj[u]] : czero<A2>();
+          w1[u] = rd1 ? p1[jj[u]] : czero<A2>();
+          w2[u] = rd2 ? p2[jj[u]] : czero<A2>();
+        }
+      }
+#pragma unroll
+    for (int u = 0; u < XB; u++)
+      if (o[u] >= 0) {
+        if (PRE) {
+          v[u] = xpre_value<A2>(op, first, v[u], w1[u], w2[u], beta, bo, mAlpha);
+          po[jj[u]] = v[u];
+          if (op == XP_BIS_S) acc.n += (double)v[u].x * v[u].x + (double)v[u].y * v[u].y;
+        }
+        T2 x = cvt<T2>(v[u]);
+        if (conj) x.y = -x.y;
+        sm[o[u] + (d[u] & 0xffffu)] = cmul(x, scc[d[u] >> 16]);
       }
   }
+  if (PRE && blockIdx.x == 0)
+    for (int i = g.nv + threadIdx.x; i < g.nvs; i += NT) po[i] = czero<A2>();
   __syncthreads();
   if constexpr (std::is_void<PX>::value) fft_lines<T, NT, false>(toff, nl, g.pitchx, 1, false, px, 0);
   else plines<T, PX, NT, false>(toff, nl, g.pitchx, 1, 0);
   T2* out = xhat + ((size_t)b * g.Gx * 3 + c) * g.nlines + L0;
   const size_t kstride = (size_t)3 * g.nlines;
   for (TileWalk<NT> w(nl); w.kx < g.Gx; w.next(nl)) out[w.kx * kstride + w.l] = sm[w.l * g.pitchx + w.kx];
+  if (PRE && pre.step.op != KOP_NONE) {
+    RedSums tot;
+    const int part = blockIdx.y * gridDim.x + blockIdx.x;
+    if (block_finish<NT>(acc, pre.step.red, b, part, tot) && threadIdx.x == 0)
+      krylov_finalize(st[b], pre.step, tot);
+  }
 }
 
 // ------------------------------------------------------------ k_xinv ----
 // grid (ceil(nlines/tl), 3, nrhs).  Epilogue: res = conj?(sqrt(cc).X +
 // conj?(arg)), padding nv..nvs zeroed, and optional sums over the result for
 // the solver step `op` (finalised by the last CTA of each right-hand side).
-template <typename T, int NT, typename PX = void>
-__global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 3) k_xinv(const typename C2<T>::t* __restrict__ arg,
-                                             typename C2<T>::t* __restrict__ res,
+// With FP64 vectors (A2 = double2, T = float) the convolution term is
+// rounded in FP32 and the identity term added in FP64:
+// res = arg + conj?(sqrt(cc).X).
+template <typename T, int NT, typename PX = void, typename A2 = typename C2<T>::t>
+__global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 3) k_xinv(const A2* __restrict__ arg,
+                                             A2* __restrict__ res,
                                              const typename C2<T>::t* __restrict__ xhat,
                                              const uint32_t* __restrict__ line_off,
                                              const uint32_t* __restrict__ dip,
@@ -238,14 +321,14 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 3) k_xinv(const typen
   if constexpr (std::is_void<PX>::value) fft_lines<T, NT, true>(toff, nl, g.pitchx, 1, false, px, 0);
   else plines<T, PX, NT, true>(toff, nl, g.pitchx, 1, 0);
   const size_t voff = ((size_t)b * 3 + c) * g.nvs;
-  const T2* a = arg + voff;
-  T2* r = res + voff;
-  const T2* w = step.w ? reinterpret_cast<const T2*>(step.w) + voff : nullptr;
+  const A2* a = arg + voff;
+  A2* r = res + voff;
+  const A2* w = step.w ? reinterpret_cast<const A2*>(step.w) + voff : nullptr;
   RedSums acc = red_zero();
   const uint32_t je = soff[nl];
   uint32_t j = soff[0] + threadIdx.x;
   int l = j < je ? tile_line(soff, nl, j) : 0;
-  constexpr int U = kXBatch / 2;
+  constexpr int U = sizeof(A2) > sizeof(T2) ? kXBatch / 4 : kXBatch / 2;
   for (; j < je; j += U * NT) {
     int o[U];  // shared offset of entry j + u NT, -1 past the tile
     uint32_t d[U], jj[U];
@@ -260,7 +343,7 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 3) k_xinv(const typen
         o[u] = l * g.pitchx;
       }
     }
-    T2 a0[U], wv[U];
+    A2 a0[U], wv[U];
 #pragma unroll
     for (int u = 0; u < U; u++)
       if (o[u] >= 0) {
@@ -271,16 +354,25 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 3) k_xinv(const typen
     for (int u = 0; u < U; u++)
       if (o[u] >= 0) {
         const T2 x = sm[o[u] + (d[u] & 0xffffu)];
-        T2 av = a0[u];
-        if (conj) av.y = -av.y;
-        T2 y = step.conv_only ? cmul(x, scc[d[u] >> 16]) : cadd(cmul(x, scc[d[u] >> 16]), av);
-        if (conj) y.y = -y.y;
+        A2 y;
+        if constexpr (std::is_same<A2, T2>::value) {
+          T2 av = a0[u];
+          if (conj) av.y = -av.y;
+          y = cadd(cmul(x, scc[d[u] >> 16]), av);
+          if (conj) y.y = -y.y;
+        } else {
+          T2 cv = cmul(x, scc[d[u] >> 16]);
+          if (conj) cv.y = -cv.y;
+          y = a0[u];
+          y.x += cv.x;
+          y.y += cv.y;
+        }
         r[jj[u]] = y;
-        if (step.op != KOP_NONE) acc = epilogue_terms<T2>(acc, y, a0[u], w ? wv[u] : a0[u], step.mode);
+        if (step.op != KOP_NONE) acc = epilogue_terms<A2>(acc, y, a0[u], w ? wv[u] : a0[u], step.mode);
       }
   }
   if (blockIdx.x == 0)
-    for (int i = g.nv + threadIdx.x; i < g.nvs; i += NT) r[i] = czero<T2>();
+    for (int i = g.nv + threadIdx.x; i < g.nvs; i += NT) r[i] = czero<A2>();
   if (step.op != KOP_NONE) {
     RedSums tot;
     const int part = blockIdx.y * gridDim.x + blockIdx.x;

@@ -14,7 +14,7 @@ OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libdda_b200.so")
 SOURCES = ["dda_cuda.cu", "frontend.cpp", "serve.cpp"]
 # mv_inst.cu is compiled once per (part, double): the kernel-table parts
-MV_PARTS = [(part, dbl) for dbl in (0, 1) for part in (0, 1, 2, 3, 4)]
+MV_PARTS = [(part, dbl) for dbl in (0, 1) for part in (0, 1, 2, 3, 4, 5)]
 HEADERS = ["fft_engine.cuh", "fft_plan.cuh", "reduce.cuh", "krylov_ops.cuh", "krylov_kernels.cuh",
            "matvec_kernels.cuh", "matvec_planned.cuh", "matvec_dispatch.cuh", "dmatrix_kernels.cuh",
            "farfield_kernels.cuh", "matvec_slot.cuh", "kernel_shapes.cuh", "matvec_pair.cuh"]

@@ -399,6 +399,23 @@ template <typename T> void setup_slot(dda_ctx* c, Engine<T>& e) {
   e.slot_path = true;
 }
 
+// Group count forced by the context flags (1: none).
+inline int forced_groups(uint32_t flags) {
+  if (flags & DDA_FLAG_YZ_GROUPS4) return 4;
+  if (flags & DDA_FLAG_YZ_GROUPS2) return 2;
+  return 1;
+}
+
+// The fused plane kernel run as `groups` thread groups (nullptr: none).
+template <typename T> typename MvKernels<T>::YzFn fused_yz(const Engine<T>& e, int groups) {
+  switch (groups) {
+    case 1: return e.k.yz;
+    case 2: return e.k.yz2;
+    case 4: return e.k.yz4;
+    default: return nullptr;
+  }
+}
+
 // Every x-pass kernel of an engine (plain, with a solver step in the load,
 // over FP64 vectors).
 template <typename T> std::vector<const void*> x_pass_kernels(const Engine<T>& e) {
@@ -486,13 +503,13 @@ template <typename T> void setup_engine(dda_ctx* c) {
     e.yz.nrw = np;
     e.smem_yz = e.pair_fixed + np * row;
   }
-  const int forced = (c->flags & DDA_FLAG_YZ_GROUPS4) ? 4 : (c->flags & DDA_FLAG_YZ_GROUPS2) ? 2 : 1;
+  const int forced = forced_groups(c->flags);
   if (e.yz_pair && forced > 1 && e.yz.nrw >= forced) {
     e.yz_groups = forced;
     e.yz.nrw -= e.yz.nrw % forced;
     e.smem_yz = e.pair_fixed + e.yz.nrw * row;
   }
-  if (e.fused && !e.yz_pair && forced > 1 && (forced == 2 ? e.k.yz2 : e.k.yz4) && nrw >= forced) {
+  if (e.fused && !e.yz_pair && forced > 1 && fused_yz<T>(e, forced) && nrw >= forced) {
     e.yz_groups = forced;
     e.yz.nrw = nrw - nrw % forced;  // a multiple of the groups: an equal share each
     e.smem_yz = fixed + e.yz.nrw * row;
@@ -537,9 +554,8 @@ template <typename T> void setup_engine(dda_ctx* c) {
   };
   for (const void* f : x_pass_kernels(e)) attr(f, e.smem_x);
   if (e.fused) {
-    attr((const void*)e.k.yz, e.smem_yz);
-    if (e.k.yz2) attr((const void*)e.k.yz2, e.smem_yz);
-    if (e.k.yz4) attr((const void*)e.k.yz4, e.smem_yz);
+    for (int gr : {1, 2, 4})
+      if (fused_yz<T>(e, gr)) attr((const void*)fused_yz<T>(e, gr), e.smem_yz);
     for (auto f : e.k.pair)
       if (f) attr((const void*)f, e.smem_yz);
   }
@@ -615,8 +631,8 @@ void launch_yz(dda_ctx* c, int nrhs, cudaStream_t s, KrylovState* st, int skipmv
     CK(cudaLaunchKernelEx(&cfg, f, e.xhat, (const typename C2<T>::t*)e.dc, g, e.yz, pz, py, (const KrylovState*)st,
                           skipmv));
   } else if (e.fused) {
-    const auto f = e.yz_groups == 4 ? e.k.yz4 : e.yz_groups == 2 ? e.k.yz2 : e.k.yz;
-    f<<<dim3(g.Gx, nrhs), kNtYz, e.smem_yz, s>>>(e.xhat, e.dc, g, e.yz, pz, py, st, skipmv);
+    fused_yz<T>(e, e.yz_groups)<<<dim3(g.Gx, nrhs), kNtYz, e.smem_yz, s>>>(e.xhat, e.dc, g, e.yz, pz, py, st,
+                                                                           skipmv);
   } else if (e.slot_path) {
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute at[1];
@@ -653,7 +669,7 @@ struct TuneChoice {
   int ncl = 0;  // cluster kernel: clusters in flight (0: as many as can be resident)
 };
 std::mutex g_tune_mu;
-std::map<std::array<int, 7>, TuneChoice> g_tune_cache;
+std::map<std::array<int, 8>, TuneChoice> g_tune_cache;
 
 template <typename T> float time_yz(dda_ctx* c, int nrhs, int reps) {
   cudaEvent_t a, b;
@@ -698,8 +714,10 @@ template <typename T> void autotune(dda_ctx* c) {
   if ((long long)g.Gx * g.Gy * g.Gz < (1LL << 20)) return;  // small grids keep the defaults
   // the box changes the best batching little next to the grid, so shapes
   // share a choice per grid (served targets mostly land on tuned grids)
-  const std::array<int, 7> key = {g.Gx, g.Gy, g.Gz, (int)sizeof(T), c->planned ? 1 : 0, e.fused ? 0 : 1,
-                                   std::min(c->max_rhs, 4)};
+  // (the flags that restrict the candidates are part of the shape)
+  const std::array<int, 8> key = {g.Gx, g.Gy, g.Gz, (int)sizeof(T), c->planned ? 1 : 0, e.fused ? 0 : 1,
+                                   std::min(c->max_rhs, 4),
+                                   forced_groups(c->flags) + (c->flags & DDA_FLAG_YZ_PAIR ? 100 : 0)};
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune_cache.find(key);
@@ -713,14 +731,14 @@ template <typename T> void autotune(dda_ctx* c) {
     const int max_rows = e.k.planned ? 48 : kNtYz / 32;
     for (int n : {4, 6, 8, 10, 12, 14, 16, 20, 24, 25, 28, 32, 34, 36, 40, 43, 48})
       if (n <= max_rows && e.yz_fixed + (size_t)n * e.yz_row <= kSmemMax) {
-        const bool f2 = c->flags & DDA_FLAG_YZ_GROUPS2, f4 = c->flags & DDA_FLAG_YZ_GROUPS4;
         if (c->flags & DDA_FLAG_YZ_PAIR) continue;
-        if (!f2 && !f4) cands.push_back({n, 0, 1, 0});
-        if (e.k.yz2 && n % 2 == 0 && !f4) cands.push_back({n, 0, 2, 0});  // two groups of n/2 rows
-        if (e.k.yz4 && n % 4 == 0 && !f2) cands.push_back({n, 0, 4, 0});  // four groups of n/4 rows
+        const int forced = forced_groups(c->flags);
+        // gr groups of n / gr rows each (a forced group count keeps only it)
+        for (int gr : {1, 2, 4})
+          if (fused_yz<T>(e, gr) && n % gr == 0 && (forced == 1 || gr == forced)) cands.push_back({n, 0, gr, 0});
       }
     // the two-CTA plane kernel: half the slab per CTA, more rows
-    if (e.k.pair[0] && !(c->flags & (DDA_FLAG_YZ_GROUPS2 | DDA_FLAG_YZ_GROUPS4)))
+    if (e.k.pair[0] && forced_groups(c->flags) == 1)
       for (int n : {8, 12, 16, 20, 24, 28, 32, 36, 40, 48})
         if (n <= 48 && n <= g.Gz / 2 && e.pair_fixed + (size_t)n * e.yz_row <= kSmemMax)
           for (int gr : {1, 2, 4})

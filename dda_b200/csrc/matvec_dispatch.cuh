@@ -93,26 +93,28 @@ typename MvKernels<T>::SlotFn slot_kernel(bool half) {
 // several hundred plan instantiations compile in parallel.  Part 0: x passes;
 // 1: split path (y rows, z columns) and the runtime-planned kernels; 2: fused
 // plane kernels; 3: cluster plane kernels.
-// The x passes of one x plan (PX: compile-time plan, or void), every
-// vector variant.
-template <typename T, int NTX, typename PX>
+// The x passes of one x plan (PX: compile-time plan, or void) over the
+// engine's own vectors (M = false) or, for FP32 engines, over FP64 vectors
+// (M = true).
+template <typename T, int NTX, typename PX, bool M>
 void x_kernels(MvKernels<T>& k) {
   typedef typename C2<T>::t T2;
-  k.xfwd = k_xfwd<T, NTX, PX, T2, 0>;
-  k.xfwd_pre = k_xfwd<T, NTX, PX, T2, 1>;
-  k.xinv = k_xinv<T, NTX, PX, T2>;
-  if constexpr (std::is_same<T, float>::value) {
+  if constexpr (!M) {
+    k.xfwd = k_xfwd<T, NTX, PX, T2, 0>;
+    k.xfwd_pre = k_xfwd<T, NTX, PX, T2, 1>;
+    k.xinv = k_xinv<T, NTX, PX, T2>;
+  } else if constexpr (std::is_same<T, float>::value) {
     k.xfwd_m = k_xfwd<T, NTX, PX, double2, 0>;
     k.xfwd_m_pre = k_xfwd<T, NTX, PX, double2, 1>;
     k.xinv_m = k_xinv<T, NTX, PX, double2>;
   }
 }
 
-template <typename T, int NTX>
+template <typename T, int NTX, bool M>
 void planned_x(MvKernels<T>& k, int gx) {
   switch (gx) {
 #define C(N) \
-  case N: x_kernels<T, NTX, typename PlanFor<N>::type>(k); break;
+  case N: x_kernels<T, NTX, typename PlanFor<N>::type, M>(k); break;
     DDA_TUNED_LENGTHS(C)
 #undef C
     default: break;
@@ -183,7 +185,8 @@ void planned_slot(MvKernels<T>& k, int gy, int gz, int by, int bz) {
 
 template <typename T, int NTX, int NTYZ, int NTC>
 void generic_kernels(MvKernels<T>& k) {
-  x_kernels<T, NTX, void>(k);
+  x_kernels<T, NTX, void, false>(k);
+  x_kernels<T, NTX, void, true>(k);
   k.yz = k_yz<T, NTYZ>;
   k.yrows = k_yrows<T, NTYZ>;
   k.cols = k_fft_cols<T, NTC>;
@@ -193,6 +196,8 @@ void generic_kernels(MvKernels<T>& k) {
 // Entry points of the parts (defined in mv_inst.cu).
 void mv_part_x(MvKernels<float>& k, int gx);
 void mv_part_x(MvKernels<double>& k, int gx);
+void mv_part_xm(MvKernels<float>& k, int gx);
+void mv_part_xm(MvKernels<double>& k, int gx);
 void mv_part_split(MvKernels<float>& k, int gy, int gz, bool generic);
 void mv_part_split(MvKernels<double>& k, int gy, int gz, bool generic);
 void mv_part_fused(MvKernels<float>& k, int gy, int gz, int by, int bz);
@@ -214,6 +219,7 @@ MvKernels<T> select_kernels(bool planned, int gx, int gy, int gz, int by, int bz
     return k;
   }
   mv_part_x(k, gx);
+  mv_part_xm(k, gx);
   mv_part_split(k, gy, gz, false);
   mv_part_fused(k, gy, gz, by, bz);
   mv_part_pair(k, gy, gz, by, bz);

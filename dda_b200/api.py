@@ -99,6 +99,8 @@ def lib():
         "dda_couple_constants": ([ctypes.c_int, ctypes.c_uint32, dp, ctypes.c_double, ctypes.c_double,
                                   dp, ctypes.c_int, dp, dp, dp], ctypes.c_int),
         "dda_einc_plane": ([vp, ctypes.c_double, dp, ctypes.c_int, dp], ctypes.c_int),
+        "dda_einc_gaussian": ([vp, ctypes.c_double, dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, dp, dp],
+                              ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -139,6 +141,73 @@ def parse_length(s):
     v = ctypes.c_double()
     _front_check(lib().dda_parse_length_m(s.encode(), ctypes.byref(v)))
     return v.value
+
+
+GAUSSIAN_BEAMS = {"lminus": 0, "davis3": 1, "barton5": 2}
+
+
+class Beam:
+    """The incident beam of the reference's --beam option: "plane", or
+    "gaussian:<lminus|davis3|barton5>,<waist>[,(x,y,z)]" with EMSim lengths
+    ("2um"; the centre relative to the target's centre) -- Beam::parseBeam and
+    Beams::Gaussian::parse (DDA/Beam.cpp:68-98, 139-181).  lminus is the
+    fundamental Gaussian mode, davis3 and barton5 add the third- and
+    fifth-order corrections (DDA/Beam.hpp:126-129)."""
+
+    def __init__(self, spec="plane"):
+        self.spec = spec
+        i = 0
+        while i < len(spec) and "a" <= spec[i] <= "z":
+            i += 1
+        name = spec[:i]
+        while i < len(spec) and spec[i] in " \t:":
+            i += 1
+        rest = spec[i:]
+        self.kind, self.waist, self.center = None, None, (0.0, 0.0, 0.0)
+        if name == "plane":
+            if rest:
+                raise ValueError("the plane beam takes no parameters: " + spec)
+        elif name == "gaussian":
+            j = 0
+            while j < len(rest) and (rest[j].isdigit() or "a" <= rest[j] <= "z"):
+                j += 1
+            kind = rest[:j]
+            while j < len(rest) and rest[j] in " \t,":
+                j += 1
+            value = rest[j:]
+            if kind not in GAUSSIAN_BEAMS:
+                raise ValueError("unknown gaussian beam type `%s'" % kind)
+            size, _, center = value.partition(",")
+            self.kind = kind
+            self.waist = parse_length(size.strip())
+            if not self.waist > 0:
+                raise ValueError("the waist must be positive: " + spec)
+            if center.strip():
+                c = center.strip()
+                if not (c.startswith("(") and c.endswith(")")):
+                    raise ValueError("beam centre must read (x,y,z): " + spec)
+                parts = [x.strip() for x in c[1:-1].split(",")]
+                if len(parts) != 3:
+                    raise ValueError("beam centre must read (x,y,z): " + spec)
+                self.center = tuple(parse_length(x) for x in parts)
+        else:
+            raise ValueError("unknown beam `%s'" % name)
+
+    @property
+    def plane(self):
+        return self.kind is None
+
+    def einc(self, params, prop=(0, 0, 1), pol=1):
+        """Incident field [3 nvs] complex of polarisation pol."""
+        if self.plane:
+            return params.einc(prop, pol)
+        out = np.zeros(params.vec_size, dtype=np.complex128)
+        center = np.asarray(self.center, dtype=np.float64)
+        _front_check(lib().dda_einc_gaussian(params.geometry.h, ctypes.c_double(params.wave_num),
+                                             _dp(np.asarray(prop, dtype=np.float64)), pol,
+                                             GAUSSIAN_BEAMS[self.kind], ctypes.c_double(self.waist), _dp(center),
+                                             _dp(out.view(np.float64))))
+        return out
 
 
 class Geometry:
@@ -228,7 +297,13 @@ class DDAParams:
     def vec_size(self):
         return 3 * self.nvs
 
-    def einc(self, prop=(0, 0, 1), pol=1):
+    def einc(self, prop=(0, 0, 1), pol=1, beam=None):
+        """Incident field [3 nvs] complex: the plane wave, or `beam` (a Beam
+        or its --beam string)."""
+        if beam is not None:
+            b = beam if isinstance(beam, Beam) else Beam(beam)
+            if not b.plane:
+                return b.einc(self, prop, pol)
         out = np.zeros(self.vec_size, dtype=np.complex128)
         _front_check(lib().dda_einc_plane(self.geometry.h, self.wave_num,
                                           _dp(np.asarray(prop, dtype=np.float64)), pol,

@@ -5,7 +5,9 @@ the far-field outputs asked for.
     python -m dda_b200.cli --geometry 'sphere:10um,1.5+0.1i' --lambda 6um --grid-unit 0.5um \\
         --iter qmr --epsilon 5 --efield-grid --output-dir out
 
-Options (the reference's names): --lambda, --prop, --pol (ldr, cm, ldr-avgpol),
+Options (the reference's names): --lambda, --prop, --beam (plane |
+gaussian:<lminus|davis3|barton5>,<waist>[,(x,y,z)]; extinction of a Gaussian beam
+from the dipoles' work on the incident field), --pol (ldr, cm, ldr-avgpol),
 --geometry (sphere:R,m | cylinder:L,R,m | box:(X,Y,Z),m | load:file=<text dipole
 list> with -m), --grid-unit (default: the reference's rule, lambda / (10 max|m|)
 and at most a 16th of every particle dimension, DDAMain.cpp:134-150), -m,
@@ -124,6 +126,7 @@ def main(argv=None):
     ap = argparse.ArgumentParser(prog="dda_b200.cli", description=__doc__.split("\n\n")[0])
     ap.add_argument("--lambda", dest="lam", default="%.17gum" % (2 * math.pi))
     ap.add_argument("--prop", default="(0,0,1)")
+    ap.add_argument("--beam", default="plane")
     ap.add_argument("--pol", default="ldr", choices=["ldr", "cm", "ldr-avgpol"])
     ap.add_argument("--geometry", default="sphere:3.35103um,1.5")
     ap.add_argument("--grid-unit")
@@ -172,7 +175,8 @@ def main(argv=None):
                   % (ms[3], ms[0], ms[1], ms[2]))
         mv.close()
         return 0
-    einc = np.stack([params.einc(prop, 1), params.einc(prop, 2)])
+    beam = api.Beam(a.beam)
+    einc = np.stack([beam.einc(params, prop, 1), beam.einc(params, prop, 2)])
     if a.store_incbeam:
         for r in range(2):
             write_field(os.path.join(a.output_dir, "IncBeam-Pol%d.txt" % (r + 1)), params, einc[r])
@@ -201,7 +205,8 @@ def main(argv=None):
     _, pn = api.beam_pol(prop, 1)
     ef = mv.far_field(pn[None, :], nrhs=2, pol=pol)[0]
     for r in range(2):
-        cext, cabs, qext, qabs = postprocess.cross_sections(params, ccs[r], pol[r], ef[r], prop, r + 1)
+        cext, cabs, qext, qabs = postprocess.cross_sections(params, ccs[r], pol[r], ef[r], prop, r + 1,
+                                                            einc=None if beam.plane else einc[r])
         csca, qsca = cext - cabs, qext - qabs
         label = "Pol%d" % (r + 1)
         out.write("Cext %s = %-25s Qext %s = %.10g\n" % (label, "%.10g um^2" % (cext * 1e12), label, qext))
@@ -210,7 +215,7 @@ def main(argv=None):
         with open(os.path.join(a.output_dir, "CrossSec-%s.txt" % label), "w") as f:
             f.write("BeamPolarization = %d\nCext = %.17g\nQext = %.17g\nCabs = %.17g\nQabs = %.17g\n"
                     "Csca = %.17g\nQsca = %.17g\n" % (r + 1, cext, qext, cabs, qabs, csca, qsca))
-    if mie_geom is not None:
+    if mie_geom is not None and beam.plane:  # DDA/DDAMain.cpp:431
         radius = mie_geom[1]
         x = 2 * math.pi * radius / lambda_m
         qe, qs, qa = postprocess.mie(x, refr[0])

@@ -289,4 +289,75 @@ int dda_einc_plane(const dda_geometry* g, double wave_num, const double* prop_in
   return 0;
 }
 
+// Gaussian-beam incident field (Beams::Gaussian::createEInc,
+// DDA/Beam.cpp:196-263).  The beam frame: ex = the polarisation vector of
+// `pol`, ey = ex rotated by +90 degrees about the propagation direction, z
+// along it; coordinates relative to the beam centre, scaled by the waist w0
+// across and by the confocal parameter b = k w0^2 along the beam.  With
+// Q = 1 / (2 zeta - i) and psi0 = -i Q exp(i rho^2 Q), the fundamental mode
+// psi0 exp(i k z) (Gouesbet, Maheu, Grehan, JOSA A 5, 1427, eq. 22) is
+// corrected to third (Davis, Phys. Rev. A 19, 1177) or fifth order in
+// s = 1 / (k w0) (Barton, Alexander, J. Appl. Phys. 66, 2800, eq. 25), all
+// with the signs of the imaginary parts for an exp(-i omega t) time factor.
+int dda_einc_gaussian(const dda_geometry* g, double wave_num, const double* prop_in, int pol, int kind,
+                      double waist, const double* center, double* einc) {
+  if (!g || !prop_in || !einc || !(waist > 0) || kind < DDA_BEAM_LMINUS || kind > DDA_BEAM_BARTON5 ||
+      (pol != 1 && pol != 2)) {
+    g_err = "bad arguments";
+    return -1;
+  }
+  typedef std::complex<double> cd;
+  const uint32_t nv = (uint32_t)g->mat.size(), nvs = (nv + 15) / 16 * 16;
+  double p1[3], p2[3], prop[3];
+  dda_beam_pol(prop_in, 1, p1, prop);
+  dda_beam_pol(prop_in, 2, p2, nullptr);
+  double ex[3], ey[3];
+  for (int a = 0; a < 3; a++) {
+    ex[a] = pol == 1 ? p1[a] : p2[a];
+    ey[a] = pol == 1 ? -p2[a] : p1[a];
+  }
+  const double c0[3] = {center ? center[0] : 0.0, center ? center[1] : 0.0, center ? center[2] : 0.0};
+  const double w0 = waist, b = wave_num * w0 * w0, s = 1 / (wave_num * w0);
+  const double s2 = s * s, s3 = s2 * s, s4 = s2 * s2, s5 = s4 * s;
+  const cd I(0, 1);
+  std::memset(einc, 0, sizeof(double) * 2 * 3 * (size_t)nvs);
+  ld origin[3];
+  for (int a = 0; a < 3; a++) origin[a] = -((ld)g->box[a] - 1.0L) / 2 * g->grid_unit;
+  for (uint32_t i = 0; i < nv; i++) {
+    double r[3];
+    for (int a = 0; a < 3; a++)
+      r[a] = (double)((ld)(double)origin[a] + (ld)(double)g->pos[3 * i + a] * g->grid_unit) - c0[a];
+    const double x = r[0] * ex[0] + r[1] * ex[1] + r[2] * ex[2];
+    const double y = r[0] * ey[0] + r[1] * ey[1] + r[2] * ey[2];
+    const double z = r[0] * prop[0] + r[1] * prop[1] + r[2] * prop[2];
+    const double xi = x / w0, eta = y / w0, zeta = z / b;
+    const double rho2 = xi * xi + eta * eta, rho4 = rho2 * rho2;
+    const cd Q = 1.0 / cd(2 * zeta, -1);
+    const cd amp = -I * Q * std::exp(I * rho2 * Q) * std::exp(I * (wave_num * z));  // psi0 exp(ikz)
+    cd fx = 1, fy = 0, fz = 0;
+    if (kind != DDA_BEAM_LMINUS) {
+      const cd Q2 = Q * Q, Q3 = Q2 * Q, Q4 = Q2 * Q2;
+      const double xi2 = xi * xi;
+      if (kind == DDA_BEAM_DAVIS3) {
+        fx = 1.0 + s2 * (-4.0 * Q2 * xi2 - I * Q3 * rho4);
+        fz = -s * 2.0 * Q * xi + s3 * (8.0 * Q3 * rho2 * xi + 2.0 * I * Q4 * rho4 * xi - 4.0 * I * Q2 * xi);
+      } else {
+        const cd Q5 = Q4 * Q, Q6 = Q4 * Q2, Q7 = Q6 * Q;
+        fx = 1.0 + s2 * (-rho2 * Q2 - I * rho4 * Q3 - 2.0 * Q2 * xi2) +
+             s4 * (2.0 * rho4 * Q4 + 3.0 * I * rho4 * rho2 * Q5 - 0.5 * rho4 * rho4 * Q6 +
+                   (8.0 * rho2 * Q4 + 2.0 * I * rho4 * Q5) * xi2);
+        fy = s2 * (-2.0 * Q2 * xi * eta) + s4 * ((8.0 * rho2 * Q4 + 2.0 * I * rho4 * Q5) * xi * eta);
+        fz = s * (-2.0 * Q * xi) + s3 * ((6.0 * rho2 * Q3 + 2.0 * I * rho4 * Q4) * xi) +
+             s5 * ((-20.0 * rho4 * Q5 - 10.0 * I * rho4 * rho2 * Q6 + rho4 * rho4 * Q7) * xi);
+      }
+    }
+    for (int a = 0; a < 3; a++) {
+      const cd e = (fx * ex[a] + fy * ey[a] + fz * prop[a]) * amp;
+      einc[2 * (i + (size_t)a * nvs)] = e.real();
+      einc[2 * (i + (size_t)a * nvs) + 1] = e.imag();
+    }
+  }
+  return 0;
+}
+
 }  // extern "C"

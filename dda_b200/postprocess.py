@@ -73,12 +73,27 @@ def jones_far_field(mv, prop, theta, phi, pol=None):
     return jones(e[:, 0, :], e[:, 1, :], theta, phi, perp, par)
 
 
-def cross_sections(params, cc, pol_vec, e_forward, prop, pol):
+def ext_cross_general(params, pol_vec, einc):
+    """Cext = 4 pi k sum_i Im(P_i . conj(Einc_i)) over the dipoles: the
+    extinction of any incident beam (Beam::extCross, DDA/Beam.cpp:58-67); for
+    a plane wave it equals the optical theorem of cross_sections."""
+    nvs, nv = params.nvs, params.nv
+    p = np.asarray(pol_vec).reshape(3, nvs)[:, :nv]
+    e = np.asarray(einc).reshape(3, nvs)[:, :nv]
+    return 4 * np.pi * params.wave_num * float(np.sum(np.imag(p * np.conj(e))))
+
+
+def cross_sections(params, cc, pol_vec, e_forward, prop, pol, einc=None):
     """(Cext, Cabs, Qext, Qabs) of one solution: e_forward = far field in the
-    propagation direction, cc the CoupleConstants of that right-hand side."""
+    propagation direction, cc the CoupleConstants of that right-hand side.
+    einc: the incident field of a non-plane beam, whose extinction then comes
+    from ext_cross_general (e_forward is not used)."""
     inc, _ = api.beam_pol(prop, pol)
     k = params.wave_num
-    cext = -np.dot(np.real(e_forward), inc) * 4 * np.pi / k
+    if einc is not None:
+        cext = ext_cross_general(params, pol_vec, einc)
+    else:
+        cext = -np.dot(np.real(e_forward), inc) * 4 * np.pi / k
     temp1 = k ** 3 * 2 / 3
     multdr = -np.imag(1.0 / cc.cc) - temp1  # [nmat*3]
     nvs, nv = params.nvs, params.nv

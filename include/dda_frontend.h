@@ -63,6 +63,18 @@ int dda_couple_constants(int kind, uint32_t nmat, const double* refr, double gri
  * (PlaneWave::createEInc, DDA/Beam.cpp:111-118). */
 int dda_einc_plane(const dda_geometry* g, double wave_num, const double* prop, int pol, double* einc);
 
+#define DDA_BEAM_LMINUS 0  /* fundamental Gaussian mode */
+#define DDA_BEAM_DAVIS3 1  /* Davis, third-order corrections */
+#define DDA_BEAM_BARTON5 2 /* Barton-Alexander, fifth-order corrections */
+
+/* Gaussian-beam incident field [3][nvs] complex for polarisation pol: waist
+ * radius `waist` (metres), beam centre `center` (3 doubles, metres, relative
+ * to the target centre; NULL: the origin), propagation direction prop
+ * (Beams::Gaussian::createEInc, DDA/Beam.cpp:196-263; --beam
+ * gaussian:<kind>,<waist>[,(x,y,z)], DDA/Beam.cpp:139-181). */
+int dda_einc_gaussian(const dda_geometry* g, double wave_num, const double* prop, int pol, int kind,
+                      double waist, const double* center, double* einc);
+
 #ifdef __cplusplus
 }
 #endif

@@ -788,6 +788,15 @@ void orc_einc(const orc_problem* p, const double* propIn, int pol, double* outD)
   }
 }
 
+// Dipole coordinates [nv][3] in metres, origin at the box centre
+// (DipoleGeometry::getDipoleCoordPartRef as the incident fields use it,
+// DDA/Beam.cpp:116, 209).
+void orc_coords(const orc_problem* p, double* out) {
+  for (uint32_t i = 0; i < p->nv; i++)
+    for (int a = 0; a < 3; a++)
+      out[3 * i + a] = (double)((ldouble)(double)p->origin[a] + (ldouble)(double)p->pos[3 * i + a] * p->gridUnitL);
+}
+
 }  // extern "C"
 
 // ============================================================ solvers =====

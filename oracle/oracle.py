@@ -79,6 +79,7 @@ def lib():
         L.orc_matvec.argtypes = [vp, dp, dp, ctypes.c_int]
         L.orc_direct_matvec.argtypes = [vp, dp, dp]
         L.orc_einc.argtypes = [vp, dp, ctypes.c_int, dp]
+        L.orc_coords.argtypes = [vp, dp]
         L.orc_solve.argtypes = [vp, ctypes.c_int, dp, ctypes.c_double, ctypes.c_int64,
                                 dp, dp, ctypes.POINTER(OrcStats), ctypes.c_int64, dp,
                                 ctypes.c_int64]
@@ -278,6 +279,66 @@ class Problem:
         out = np.zeros(self.vec_size, dtype=np.complex128)
         lib().orc_einc(self.h, _dp(np.asarray(prop, dtype=np.float64)), pol, _dp(out))
         return out
+
+    def coords(self):
+        """Dipole coordinates [nv][3] in metres (origin at the box centre)."""
+        out = np.zeros((self.nv, 3))
+        lib().orc_coords(self.h, _dp(out))
+        return out
+
+    def einc_gaussian(self, prop, pol, kind, waist, center=(0.0, 0.0, 0.0)):
+        """Gaussian-beam incident field [3 nvs] (Beams::Gaussian::createEInc,
+        DDA/Beam.cpp:196-263), restated in numpy over all dipoles at once, in
+        the reference's order of operations: beam frame ex = polarisation
+        vector, ey = -pol-2 vector (pol 1) or the pol-1 vector (pol 2), z along
+        prop; Q = 1/(2 zeta - i), psi0 = -i Q exp(i rho^2 Q), phase exp(i k z);
+        kind "lminus" (DDA/Beam.cpp:217-218), "davis3" (225-238), "barton5"
+        (239-256)."""
+        k = self.wave_num
+        p1, pn = beam_pol(prop, 1)
+        p2, _ = beam_pol(prop, 2)
+        ex = p1 if pol == 1 else p2
+        ey = -p2 if pol == 1 else p1
+        w0 = waist
+        b = k * w0 * w0
+        coord = self.coords() - np.asarray(center, dtype=np.float64)[None, :]
+        x, y, z = coord @ ex, coord @ ey, coord @ pn
+        xi, eta, zeta = x / w0, y / w0, z / b
+        rho2 = xi * xi + eta * eta
+        Q = 1.0 / (2 * zeta - 1j)
+        psi0 = -1j * Q * np.exp(1j * rho2 * Q)
+        phase = np.exp(1j * k * z)
+        zero = np.zeros_like(Q)
+        if kind == "lminus":
+            xf, yf, zf = np.ones_like(Q), zero, zero
+        else:
+            s = 1 / (k * w0)
+            s2 = s * s
+            rho4 = rho2 * rho2
+            Q2 = Q * Q
+            Q3 = Q2 * Q
+            Q4 = Q2 * Q2
+            xi2 = xi * xi
+            if kind == "davis3":
+                s3 = s2 * s
+                xf = 1 + s2 * (-4 * Q2 * xi2 - 1j * Q3 * rho4)
+                yf = zero
+                zf = -s * 2 * Q * xi + s3 * (8 * Q3 * rho2 * xi + 2j * Q4 * rho4 * xi - 4j * Q2 * xi)
+            elif kind == "barton5":
+                Q5 = Q4 * Q
+                xf = (1 + s2 * (-rho2 * Q2 - 1j * rho4 * Q3 - 2 * Q2 * xi2)
+                      + s ** 4 * (2 * rho4 * Q4 + 3j * rho4 * rho2 * Q5 - 0.5 * rho4 * rho4 * Q4 * Q2
+                                  + (8 * rho2 * Q4 + 2j * rho4 * Q5) * xi2))
+                yf = s2 * (-2 * Q2 * xi * eta) + s2 * s2 * ((8 * rho2 * Q4 + 2j * rho4 * Q5) * xi * eta)
+                zf = (s * (-2 * Q * xi) + s2 * s * ((6 * rho2 * Q3 + 2j * rho4 * Q4) * xi)
+                      + s2 * s2 * s * ((-20 * rho4 * Q5 - 10j * rho4 * rho2 * Q4 * Q2 + rho4 * rho4 * Q4 * Q3) * xi))
+            else:
+                raise ValueError("unknown gaussian beam type " + kind)
+        out = np.zeros((3, self.nvs), dtype=np.complex128)
+        for a in range(3):
+            out[a, :self.nv] = (ex[a] * (xf * psi0 * phase) + ey[a] * (yf * psi0 * phase)
+                                + pn[a] * (zf * psi0 * phase))
+        return out.reshape(-1)
 
     def calc_field(self, pvec, n):
         p = np.ascontiguousarray(pvec, dtype=np.complex128)

@@ -349,11 +349,14 @@ def run_ours(args):
     value = replica_throughput(nrhs * args.steps, world, t_max)
     ms_per_step = t_max / args.steps
 
-    # e2e: host FP64 einc in, host FP64 polarisations out, through dda_solve,
-    # both from / into pinned host memory
-    einc_host = torch.empty(einc.size, dtype=torch.complex128, pin_memory=True).numpy()
+    # e2e: host fields in, host polarisations out, both from / into pinned
+    # host memory, in the line's precision: complex64 through dda_solve_f32
+    # for FP32 (the vectors of the reference's --ftype float path), complex128
+    # through dda_solve for FP64
+    hdt = torch.complex64 if prec == "fp32" else torch.complex128
+    einc_host = torch.empty(einc.size, dtype=hdt, pin_memory=True).numpy()
     einc_host[:] = einc.reshape(-1)
-    pol_host = torch.empty(einc.size, dtype=torch.complex128, pin_memory=True).numpy()
+    pol_host = torch.empty(einc.size, dtype=hdt, pin_memory=True).numpy()
     e2e_ms = 0.0
     for _ in range(args.steps):
         with torch.cuda.stream(stream):
@@ -367,7 +370,8 @@ def run_ours(args):
         e2e_ms += e0.elapsed_time(e1)
     e2e_ms = max_over_ranks(pg, e2e_ms, "cuda")
     e2e = {"value": replica_throughput(nrhs * args.steps, world, e2e_ms), "unit": "solves/s",
-           "h2d_bytes_per_step": int(einc_host.nbytes), "d2h_bytes_per_step": int(einc_host.nbytes)}
+           "h2d_bytes_per_step": int(einc_host.nbytes), "d2h_bytes_per_step": int(einc_host.nbytes),
+           "host_arrays": "complex64 (dda_solve_f32)" if prec == "fp32" else "complex128 (dda_solve)"}
 
     # matvec stage profile and roofline of the dominant pass
     ms = mv.profile(nrhs=nrhs, reps=20)

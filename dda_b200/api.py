@@ -68,6 +68,8 @@ def lib():
         "dda_matvec_host": ([vp, dp, dp, ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "dda_solve": ([vp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_double, ctypes.c_int64, dp, dp,
                        dp, ctypes.c_int64, ctypes.POINTER(Stats)], ctypes.c_int),
+        "dda_solve_f32": ([vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_double, ctypes.c_int64, vp, vp,
+                           dp, ctypes.c_int64, ctypes.POINTER(Stats)], ctypes.c_int),
         "dda_get_dmatrix": ([vp, dp], ctypes.c_int),
         "dda_solve_device": ([vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_double, ctypes.c_int64, vp, vp,
                               ctypes.POINTER(Stats)], ctypes.c_int),
@@ -480,9 +482,14 @@ class CudaSolver:
 
     def get_pol_vec(self, einc, eps, start=None, history_cap=100000, raise_on_error=True, out=None):
         """Solves for one or more right-hand sides; einc is [nrhs][3 nvs].
-        `out`, when given, is the complex128 C-contiguous array of einc's size
+        `out`, when given, is the C-contiguous array of einc's size and type
         that receives the polarisations (for instance a pinned host buffer,
-        which makes both bus copies asynchronous DMA)."""
+        which makes both bus copies asynchronous DMA).  A complex64 einc
+        (the reference's --ftype float vectors) goes through dda_solve_f32 and
+        gives complex64 polarisations: on an FP32 context half the bytes
+        cross the bus."""
+        if isinstance(einc, np.ndarray) and einc.dtype == np.complex64:
+            return self._get_pol_vec_f32(einc, eps, start, history_cap, raise_on_error, out)
         e, ep = _cbuf(einc)
         nvs = self.mv.nvs
         nrhs = e.size // (3 * nvs)
@@ -499,6 +506,27 @@ class CudaSolver:
         hist = np.zeros((nrhs, history_cap))
         rc = lib().dda_solve(self.mv.h, self.solver, nrhs, ep, eps, self.max_iter, sp,
                              _dp(pol.view(np.float64)), _dp(hist), history_cap, stats)
+        self.last_stats = [stats[i] for i in range(nrhs)]
+        self.last_history = [hist[i, :min(stats[i].iterations, history_cap)].copy() for i in range(nrhs)]
+        if rc != 0 and raise_on_error:
+            raise DDAError(rc, lib().dda_last_error(self.mv.h).decode())
+        return pol
+
+    def _get_pol_vec_f32(self, einc, eps, start, history_cap, raise_on_error, out):
+        e = np.ascontiguousarray(einc)
+        nrhs = e.size // (3 * self.mv.nvs)
+        if out is None:
+            pol = np.zeros_like(e)
+        else:
+            if out.dtype != np.complex64 or out.size != e.size or not out.flags["C_CONTIGUOUS"]:
+                raise ValueError("out must be a C-contiguous complex64 array of einc's size")
+            pol = out
+        s = None if start is None else np.ascontiguousarray(start, dtype=np.complex64)
+        stats = (Stats * nrhs)()
+        hist = np.zeros((nrhs, history_cap))
+        rc = lib().dda_solve_f32(self.mv.h, self.solver, nrhs, ctypes.c_void_p(e.ctypes.data), eps, self.max_iter,
+                                 None if s is None else ctypes.c_void_p(s.ctypes.data),
+                                 ctypes.c_void_p(pol.ctypes.data), _dp(hist), history_cap, stats)
         self.last_stats = [stats[i] for i in range(nrhs)]
         self.last_history = [hist[i, :min(stats[i].iterations, history_cap)].copy() for i in range(nrhs)]
         if rc != 0 and raise_on_error:

@@ -744,6 +744,9 @@ template <typename T> void autotune(dda_ctx* c) {
           for (int gr : {1, 2, 4})
             if (n % gr == 0) cands.push_back({n, 0, gr, 1});
   } else {
+    int l2 = 0;
+    CK(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, c->device));
+    const size_t slot_bytes = (size_t)g.Gz * e.sg.wp * sizeof(typename C2<T>::t);
     for (int cl : {4, 8, 16})
       for (int n : {4, 8, 16})
         if (e.ncl_by_cl[cl] > 0 && n <= (g.Gz + cl - 1) / cl && slot_smem_bytes<T>(g, n) <= kSmemMax &&
@@ -751,6 +754,9 @@ template <typename T> void autotune(dda_ctx* c) {
           cands.push_back({n, cl});
           // fewer clusters in flight: their plane buffers then stay in L2
           // next to the streamed planes, at the price of less latency hiding
+          // -- worth timing only where the buffers of all clusters fill more
+          // than half the L2 (each candidate costs context set-up time)
+          if ((size_t)e.ncl_by_cl[cl] * slot_bytes * 2 <= (size_t)l2) continue;
           for (int div : {2, 3})
             if (e.ncl_by_cl[cl] / div >= 4) {
               TuneChoice t{n, cl};
@@ -1774,6 +1780,22 @@ int solve_t(dda_ctx* c, int solver, int nrhs, const double* einc, double eps, lo
   return collect_stats(c, nrhs, history, history_cap, stats);
 }
 
+// FP32 context, single-precision host arrays: the fields cross the bus as
+// they are (complex float, the engine's own layout), with no conversion.
+int solve_f32_host(dda_ctx* c, int solver, int nrhs, const float* einc, double eps, long long max_iter,
+                   const float* start, float* pol_out, double* history, long long history_cap, dda_stats* stats) {
+  Engine<float>& e = c->e32;
+  const size_t bytes = (size_t)nrhs * 3 * c->g.nvs * sizeof(float2);
+  CK(cudaMemcpyAsync(e.vec[0], einc, bytes, cudaMemcpyHostToDevice, c->stream));
+  if (start) CK(cudaMemcpyAsync(e.vec[2], start, bytes, cudaMemcpyHostToDevice, c->stream));
+  SolveOpts o;
+  o.start = start != nullptr;
+  run_solve<float>(c, solver, nrhs, eps, max_iter, o);
+  if (pol_out) CK(cudaMemcpyAsync(pol_out, e.io, bytes, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return collect_stats(c, nrhs, history, history_cap, stats);
+}
+
 template <typename T>
 int solve_device_t(dda_ctx* c, int solver, int nrhs, const void* einc, double eps, long long max_iter,
                    const void* start, void* pol, dda_stats* stats) {
@@ -1942,6 +1964,35 @@ int dda_solve(dda_ctx* ctx, int solver, int nrhs, const double* einc, double eps
     if (ctx->precision == DDA_PREC_MIXED)
       return solve_mixed_host(ctx, solver, nrhs, einc, eps, max_iter, start, pol_out, history, history_cap, stats);
     return solve_t<double>(ctx, solver, nrhs, einc, eps, max_iter, start, pol_out, history, history_cap, stats);
+  });
+  ctx->cancel.store(0);
+  return rc;
+}
+
+int dda_solve_f32(dda_ctx* ctx, int solver, int nrhs, const float* einc, double eps, int64_t max_iter,
+                  const float* start, float* pol_out, double* history, int64_t history_cap, dda_stats* stats) {
+  if (!ctx) return DDA_ERR_ARG;
+  if (ctx->precision != DDA_PREC_FP32) {
+    // FP64 and MIXED contexts: widen on the host (exact) and solve as
+    // dda_solve (which also rejects bad arguments: einc NULL then)
+    const bool ok = einc && nrhs >= 1 && nrhs <= ctx->max_rhs;
+    const size_t n = ok ? (size_t)nrhs * 3 * ctx->g.nvs * 2 : 0;
+    std::vector<double> e(ok ? einc : nullptr, ok ? einc + n : nullptr), s, p(pol_out ? n : 0);
+    if (ok && start) s.assign(start, start + n);
+    const int rc = dda_solve(ctx, solver, nrhs, ok ? e.data() : nullptr, eps, max_iter,
+                             ok && start ? s.data() : nullptr, pol_out ? p.data() : nullptr, history, history_cap,
+                             stats);
+    if (pol_out)
+      for (size_t i = 0; i < n; i++) pol_out[i] = (float)p[i];
+    return rc;
+  }
+  const int rc = guard(ctx, [&]() -> int {
+    if (solver < 0 || solver > 3) throw DdaError(DDA_ERR_ARG, "unknown solver");
+    if (nrhs < 1 || nrhs > ctx->max_rhs || !einc) throw DdaError(DDA_ERR_ARG, "bad solve arguments");
+    if (!(eps > 0)) throw DdaError(DDA_ERR_ARG, "eps must be positive");
+    for (int r = 0; r < nrhs; r++)
+      if (!ctx->cc_set[r]) throw DdaError(DDA_ERR_ARG, "couple constants not set (dda_set_cc)");
+    return solve_f32_host(ctx, solver, nrhs, einc, eps, max_iter, start, pol_out, history, history_cap, stats);
   });
   ctx->cancel.store(0);
   return rc;

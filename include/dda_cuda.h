@@ -169,6 +169,16 @@ int dda_solve(dda_ctx* ctx, int solver, int nrhs, const double* einc, double eps
               int64_t max_iter, const double* start, double* pol_out, double* history,
               int64_t history_cap, dda_stats* stats);
 
+/* dda_solve with single-precision host arrays (complex float pairs, same
+ * [nrhs][3][nvs] layout): the vectors of the reference's --ftype float path
+ * (IterativeSolverBase<float>::getPolVec, DDA/IterativeSolverBase.hpp:59,
+ * with std::vector<std::complex<float> >).  On an FP32 context the arrays
+ * cross the bus as they are, half the bytes of dda_solve, and the result is
+ * dda_solve's rounded to float (the same device arithmetic).  FP64 and
+ * MIXED contexts widen the arrays on the host and run dda_solve. */
+int dda_solve_f32(dda_ctx* ctx, int solver, int nrhs, const float* einc, double eps, int64_t max_iter,
+                  const float* start, float* pol_out, double* history, int64_t history_cap, dda_stats* stats);
+
 /* dda_solve on device buffers of the context precision (double pairs for
  * DDA_PREC_FP64 and DDA_PREC_MIXED, whose outer residual is FP64; float
  * pairs for DDA_PREC_FP32):

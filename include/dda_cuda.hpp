@@ -79,6 +79,21 @@ class CudaMatVec {
   size_t nvs_ = 0;
 };
 
+namespace detail {
+// dda_solve on the vectors' own precision: complex double, or complex float
+// (the --ftype float vectors, dda_solve_f32: no widening copies).
+inline int solve(dda_ctx* c, int solver, int nrhs, const std::complex<double>* e, double eps, int64_t maxIter,
+                 const std::complex<double>* s, std::complex<double>* p, double* h, int64_t cap, dda_stats* st) {
+  return dda_solve(c, solver, nrhs, reinterpret_cast<const double*>(e), eps, maxIter,
+                   reinterpret_cast<const double*>(s), reinterpret_cast<double*>(p), h, cap, st);
+}
+inline int solve(dda_ctx* c, int solver, int nrhs, const std::complex<float>* e, double eps, int64_t maxIter,
+                 const std::complex<float>* s, std::complex<float>* p, double* h, int64_t cap, dda_stats* st) {
+  return dda_solve_f32(c, solver, nrhs, reinterpret_cast<const float*>(e), eps, maxIter,
+                       reinterpret_cast<const float*>(s), reinterpret_cast<float*>(p), h, cap, st);
+}
+}  // namespace detail
+
 template <typename T>
 class CudaSolver {
  public:
@@ -105,20 +120,19 @@ class CudaSolver {
                                const std::vector<ctype>& start = std::vector<ctype>()) {
     const size_t n = einc.size();
     const int nrhs = (int)(n / (3 * mv_.vecStride()));
-    std::vector<std::complex<double>> e(einc.begin(), einc.end()), s(start.begin(), start.end()), p(n);
+    std::vector<ctype> p(n);
     const int64_t cap = 100000;
     std::vector<double> hist(residuals ? (size_t)cap * nrhs : 0);
     stats_.assign(nrhs, dda_stats());
-    const int rc = dda_solve(mv_.context(), solver_, nrhs, reinterpret_cast<const double*>(e.data()), (double)eps,
-                             maxIter_, s.empty() ? nullptr : reinterpret_cast<const double*>(s.data()),
-                             reinterpret_cast<double*>(p.data()), residuals ? hist.data() : nullptr,
-                             residuals ? cap : 0, stats_.data());
+    const int rc = detail::solve(mv_.context(), solver_, nrhs, einc.data(), (double)eps, maxIter_,
+                                 start.empty() ? nullptr : start.data(), p.data(), residuals ? hist.data() : nullptr,
+                                 residuals ? cap : 0, stats_.data());
     if (residuals)
       for (int r = 0; r < nrhs; r++)
         residuals->insert(residuals->end(), hist.begin() + (size_t)r * cap,
                           hist.begin() + (size_t)r * cap + std::min<int64_t>(cap, stats_[r].iterations));
     check(rc, mv_.context());
-    return std::vector<ctype>(p.begin(), p.end());
+    return p;
   }
 
   const std::vector<dda_stats>& stats() const { return stats_; }

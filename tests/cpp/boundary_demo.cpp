@@ -72,6 +72,10 @@ int main(int argc, char** argv) {
     dda::CudaSolver<double> solver(mv64, "qmr");
     std::vector<double> residuals;
     std::vector<std::complex<double>> pol = solver.getPolVec(einc, 1e-8, &residuals);
+    // the --ftype float vectors: CudaSolver<float> on the FP32 context
+    std::vector<std::complex<float>> einc32(einc.begin(), einc.end());
+    dda::CudaSolver<float> solver32(mv32, "bicgstab");
+    std::vector<std::complex<float>> pol32 = solver32.getPolVec(einc32, 1e-5f);
     dda_geom_free(g);
 
     std::FILE* f = std::fopen(argv[1], "wb");
@@ -84,6 +88,8 @@ int main(int argc, char** argv) {
     std::fwrite(pol.data(), sizeof(pol[0]), n, f);
     const double iters = (double)solver.stats()[0].iterations;
     std::fwrite(&iters, sizeof iters, 1, f);
+    std::vector<std::complex<double>> pol32d(pol32.begin(), pol32.end());
+    std::fwrite(pol32d.data(), sizeof(pol32d[0]), n, f);
     std::fclose(f);
     std::printf("ok %zu %lld %zu\n", nvs, (long long)solver.stats()[0].iterations, residuals.size());
     return 0;

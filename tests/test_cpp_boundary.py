@@ -70,6 +70,7 @@ def test_cpp_demo_matches_oracle(tmp_path):
     c = raw[1:1 + 6 * n].view(np.complex128)
     y64, y32, pol = c[:n], c[n:2 * n], c[2 * n:3 * n]
     iters = int(raw[1 + 6 * n])
+    pol32 = raw[2 + 6 * n:2 + 8 * n].view(np.complex128)
     og = O.Geometry.sphere("0.5um", "0.1um")
     op = O.Problem(og, [1.5 + 0.1j], "1um")
     assert op.nvs == nvs
@@ -87,3 +88,5 @@ def test_cpp_demo_matches_oracle(tmp_path):
     assert rc == 0
     assert abs(iters - st.iterations) <= 1
     assert rel(pol, opol) < 1e-6
+    # CudaSolver<float>: complex float vectors through dda_solve_f32, to 1e-5
+    assert rel(pol32, opol) < 1e-3

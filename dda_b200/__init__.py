@@ -17,7 +17,8 @@ be loaded, and every call raises DDAError with the library's message when the
 device path fails (the reference throws Core::Exception the same way).
 """
 from .api import (DDAError, Geometry, DDAParams, CoupleConstants, CudaMatVec, CudaSolver,
-                  SOLVERS, PRECISIONS, fft_fit, beam_pol, Beam, lib, lib_path)
+                  SOLVERS, PRECISIONS, fft_fit, beam_pol, beam_frame, Beam, lib, lib_path)
 
 __all__ = ["DDAError", "Geometry", "DDAParams", "CoupleConstants", "CudaMatVec", "CudaSolver",
-           "SOLVERS", "PRECISIONS", "fft_fit", "beam_pol", "Beam", "lib", "lib_path"]
+           "SOLVERS", "PRECISIONS", "fft_fit", "beam_pol", "beam_frame", "Beam", "lib",
+           "lib_path"]

@@ -103,6 +103,12 @@ def lib():
         "dda_einc_plane": ([vp, ctypes.c_double, dp, ctypes.c_int, dp], ctypes.c_int),
         "dda_einc_gaussian": ([vp, ctypes.c_double, dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, dp, dp],
                               ctypes.c_int),
+        "dda_beam_frame": ([dp, dp, dp, dp, dp, dp, dp], None),
+        "dda_einc_plane_frame": ([vp, ctypes.c_double, dp, dp, dp], ctypes.c_int),
+        "dda_einc_gaussian_frame": ([vp, ctypes.c_double, dp, dp, dp, ctypes.c_int, ctypes.c_double, dp, dp],
+                                    ctypes.c_int),
+        "dda_couple_constants_frame": ([ctypes.c_int, ctypes.c_uint32, dp, ctypes.c_double, ctypes.c_double,
+                                        dp, dp, dp, dp, dp], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -137,6 +143,25 @@ def beam_pol(prop, pol):
     pn = np.zeros(3)
     lib().dda_beam_pol(_dp(np.asarray(prop, dtype=np.float64)), pol, _dp(out), _dp(pn))
     return out, pn
+
+
+def beam_frame(prop, orient=None, center=None):
+    """(prop_p, pol1_p, pol2_p, center_p): the beam's propagation direction,
+    polarisation vectors and a point (the Gaussian beam's centre) in the
+    frame of a particle oriented by the ZYZ Euler angles `orient` in degrees
+    (--orient; DipoleGeometry::orientationInverse, DDA/DipoleGeometry.cpp:
+    149-152, applied as in DDA/Beam.hpp:69-81)."""
+    out = [np.zeros(3) for _ in range(4)]
+    o = None if orient is None else _dp(np.asarray(orient, dtype=np.float64))
+    c = None if center is None else _dp(np.asarray(center, dtype=np.float64))
+    lib().dda_beam_frame(_dp(np.asarray(prop, dtype=np.float64)), o, _dp(out[0]), _dp(out[1]), _dp(out[2]), c,
+                         _dp(out[3]))
+    return tuple(out)
+
+
+def oriented(orient):
+    """True for a particle orientation other than the identity."""
+    return orient is not None and any(float(x) != 0.0 for x in orient)
 
 
 def parse_length(s):
@@ -199,11 +224,20 @@ class Beam:
     def plane(self):
         return self.kind is None
 
-    def einc(self, params, prop=(0, 0, 1), pol=1):
-        """Incident field [3 nvs] complex of polarisation pol."""
+    def einc(self, params, prop=(0, 0, 1), pol=1, orient=None):
+        """Incident field [3 nvs] complex of polarisation pol (orient: the
+        particle orientation, ZYZ Euler angles in degrees)."""
         if self.plane:
-            return params.einc(prop, pol)
+            return params.einc(prop, pol, orient=orient)
         out = np.zeros(params.vec_size, dtype=np.complex128)
+        if oriented(orient):
+            pp, p1, p2, cp = beam_frame(prop, orient, self.center)
+            ex, ey = (p1, -p2) if pol == 1 else (p2, p1)
+            _front_check(lib().dda_einc_gaussian_frame(params.geometry.h, ctypes.c_double(params.wave_num), _dp(pp),
+                                                       _dp(ex), _dp(ey), GAUSSIAN_BEAMS[self.kind],
+                                                       ctypes.c_double(self.waist), _dp(cp),
+                                                       _dp(out.view(np.float64))))
+            return out
         center = np.asarray(self.center, dtype=np.float64)
         _front_check(lib().dda_einc_gaussian(params.geometry.h, ctypes.c_double(params.wave_num),
                                              _dp(np.asarray(prop, dtype=np.float64)), pol,
@@ -299,14 +333,20 @@ class DDAParams:
     def vec_size(self):
         return 3 * self.nvs
 
-    def einc(self, prop=(0, 0, 1), pol=1, beam=None):
+    def einc(self, prop=(0, 0, 1), pol=1, beam=None, orient=None):
         """Incident field [3 nvs] complex: the plane wave, or `beam` (a Beam
-        or its --beam string)."""
+        or its --beam string); orient: the particle orientation (ZYZ Euler
+        angles in degrees, --orient)."""
         if beam is not None:
             b = beam if isinstance(beam, Beam) else Beam(beam)
             if not b.plane:
-                return b.einc(self, prop, pol)
+                return b.einc(self, prop, pol, orient=orient)
         out = np.zeros(self.vec_size, dtype=np.complex128)
+        if oriented(orient):
+            pp, p1, p2, _ = beam_frame(prop, orient)
+            _front_check(lib().dda_einc_plane_frame(self.geometry.h, self.wave_num, _dp(pp),
+                                                    _dp(p1 if pol == 1 else p2), _dp(out.view(np.float64))))
+            return out
         _front_check(lib().dda_einc_plane(self.geometry.h, self.wave_num,
                                           _dp(np.asarray(prop, dtype=np.float64)), pol,
                                           _dp(out.view(np.float64))))
@@ -316,12 +356,20 @@ class DDAParams:
 class CoupleConstants:
     """cc, sqrt(cc), chi_inv per material and axis (DDA/DDAParams.cpp:315-331)."""
 
-    def __init__(self, params, prop=(0, 0, 1), pol=1, kind="ldr"):
+    def __init__(self, params, prop=(0, 0, 1), pol=1, kind="ldr", orient=None):
         n = len(params.materials) * 3
         refr = np.array([c for m in params.materials for c in m], dtype=np.complex128)
         self.cc = np.zeros(n, dtype=np.complex128)
         self.cc_sqrt = np.zeros(n, dtype=np.complex128)
         self.chi_inv = np.zeros(n, dtype=np.complex128)
+        if oriented(orient):  # LDR sees the beam in the particle frame
+            pp, p1, p2, _ = beam_frame(prop, orient)
+            _front_check(lib().dda_couple_constants_frame(
+                POLARIZABILITIES[kind], len(params.materials), _dp(refr.view(np.float64)),
+                params.grid_unit, params.wave_num, _dp(pp), _dp(p1 if pol == 1 else p2),
+                _dp(self.cc.view(np.float64)), _dp(self.cc_sqrt.view(np.float64)),
+                _dp(self.chi_inv.view(np.float64))))
+            return
         _front_check(lib().dda_couple_constants(
             POLARIZABILITIES[kind], len(params.materials), _dp(refr.view(np.float64)),
             params.grid_unit, params.wave_num, _dp(np.asarray(prop, dtype=np.float64)), pol,

@@ -7,7 +7,8 @@ the far-field outputs asked for.
 
 Options (the reference's names): --lambda, --prop, --beam (plane |
 gaussian:<lminus|davis3|barton5>,<waist>[,(x,y,z)]; extinction of a Gaussian beam
-from the dipoles' work on the incident field), --pol (ldr, cm, ldr-avgpol),
+from the dipoles' work on the incident field), --orient (alpha,beta,gamma): the
+particle orientation as ZYZ Euler angles in degrees, --pol (ldr, cm, ldr-avgpol),
 --geometry (sphere:R,m | cylinder:L,R,m | box:(X,Y,Z),m | load:file=<text dipole
 list> with -m), --grid-unit (default: the reference's rule, lambda / (10 max|m|)
 and at most a 16th of every particle dimension, DDAMain.cpp:134-150), -m,
@@ -127,6 +128,7 @@ def main(argv=None):
     ap.add_argument("--lambda", dest="lam", default="%.17gum" % (2 * math.pi))
     ap.add_argument("--prop", default="(0,0,1)")
     ap.add_argument("--beam", default="plane")
+    ap.add_argument("--orient", default="(0,0,0)")
     ap.add_argument("--pol", default="ldr", choices=["ldr", "cm", "ldr-avgpol"])
     ap.add_argument("--geometry", default="sphere:3.35103um,1.5")
     ap.add_argument("--grid-unit")
@@ -155,6 +157,7 @@ def main(argv=None):
 
     lambda_m = api.parse_length(a.lam)
     prop = tuple(parse_vector(a.prop))
+    orient = tuple(parse_vector(a.orient))
     geom, refr, mie_geom = build_geometry(a.geometry, a.grid_unit, a.m, lambda_m)
     grid = tuple(int(x) for x in parse_vector(a.fft_grid, float))
     params = api.DDAParams(geom, refr, lambda_m, grid=grid if any(grid) else None)
@@ -167,7 +170,7 @@ def main(argv=None):
     mv = api.CudaMatVec(params, prec, max_rhs=2)
     ccs = []
     for r, pol in enumerate((1, 2)):
-        ccs.append(api.CoupleConstants(params, prop, pol, a.pol))
+        ccs.append(api.CoupleConstants(params, prop, pol, a.pol, orient=orient))
         mv.set_couple_constants(ccs[-1], rhs=r)
     if a.profiling_run:  # IterativeSolverBase::profilingRun, DDA/IterativeSolverBase.cpp:105-136
         ms = mv.profile(nrhs=2, reps=5)
@@ -176,7 +179,7 @@ def main(argv=None):
         mv.close()
         return 0
     beam = api.Beam(a.beam)
-    einc = np.stack([beam.einc(params, prop, 1), beam.einc(params, prop, 2)])
+    einc = np.stack([beam.einc(params, prop, 1, orient=orient), beam.einc(params, prop, 2, orient=orient)])
     if a.store_incbeam:
         for r in range(2):
             write_field(os.path.join(a.output_dir, "IncBeam-Pol%d.txt" % (r + 1)), params, einc[r])
@@ -202,11 +205,11 @@ def main(argv=None):
             write_field(os.path.join(a.output_dir, "IntField-Pol%d.txt" % (r + 1)), params,
                         cc_vector(params, ccs[r].chi_inv) * pol[r])
 
-    _, pn = api.beam_pol(prop, 1)
+    pn = api.beam_frame(prop, orient)[0]  # forward direction in the particle frame
     ef = mv.far_field(pn[None, :], nrhs=2, pol=pol)[0]
     for r in range(2):
         cext, cabs, qext, qabs = postprocess.cross_sections(params, ccs[r], pol[r], ef[r], prop, r + 1,
-                                                            einc=None if beam.plane else einc[r])
+                                                            einc=None if beam.plane else einc[r], orient=orient)
         csca, qsca = cext - cabs, qext - qabs
         label = "Pol%d" % (r + 1)
         out.write("Cext %s = %-25s Qext %s = %.10g\n" % (label, "%.10g um^2" % (cext * 1e12), label, qext))
@@ -241,7 +244,8 @@ def main(argv=None):
     for name, ts, ps, want_j, want_m, no_phi in far:
         if (ts, ps) not in cache:
             theta, phi = postprocess.grid_angles(ts, ps)
-            cache[(ts, ps)] = (theta, phi, postprocess.jones_far_field(mv, prop, theta, phi, pol=pol))
+            cache[(ts, ps)] = (theta, phi, postprocess.jones_far_field(mv, prop, theta, phi, pol=pol,
+                                                                       orient=orient))
         theta, phi, jones = cache[(ts, ps)]
         if want_j:
             postprocess.store_jones_txt(os.path.join(a.output_dir, "Far%s.txt" % name), theta, phi, jones,

@@ -226,19 +226,73 @@ void dda_beam_pol(const double* prop_in, int pol, double* inc_pol, double* prop_
   }
 }
 
+// The beam's vectors in the particle frame for a particle orientation given
+// as ZYZ Euler angles in degrees (--orient): R = Rz(alpha) Ry(beta) Rz(gamma)
+// as a unit quaternion q (EMSim::Rotation::fromZYZDeg, EMSim/Rotation.hpp:
+// 94-102), and each lab-frame vector v mapped to R^-1 v = conj(q) v q
+// (DipoleGeometry::orientationInverse, DDA/DipoleGeometry.cpp:149-152;
+// Beam::propP / getIncPolP, DDA/Beam.hpp:69-81).  prop_p, pol1_p, pol2_p:
+// the normalised propagation direction and the polarisation vectors of
+// dda_beam_pol, rotated; center_in/center_p (may be NULL): a point.
+static void quat_mul(const ld a[4], const ld b[4], ld r[4]) {
+  r[0] = a[0] * b[0] - a[1] * b[1] - a[2] * b[2] - a[3] * b[3];
+  r[1] = a[0] * b[1] + a[1] * b[0] + a[2] * b[3] - a[3] * b[2];
+  r[2] = a[0] * b[2] - a[1] * b[3] + a[2] * b[0] + a[3] * b[1];
+  r[3] = a[0] * b[3] + a[1] * b[2] - a[2] * b[1] + a[3] * b[0];
+}
+
+void dda_beam_frame(const double* prop_in, const double* orient_deg, double* prop_p, double* pol1_p,
+                    double* pol2_p, const double* center_in, double* center_p) {
+  double v[4][3];
+  dda_beam_pol(prop_in, 1, v[1], v[0]);
+  dda_beam_pol(prop_in, 2, v[2], nullptr);
+  for (int a = 0; a < 3; a++) v[3][a] = center_in ? center_in[a] : 0.0;
+  const ld pi = 3.14159265358979323846264338327950288L;
+  ld q[4] = {1, 0, 0, 0};
+  const int axis[3] = {3, 2, 3};  // z, y, z
+  for (int k = 0; k < 3; k++) {
+    const ld h = (orient_deg ? (ld)orient_deg[k] : 0.0L) / 180 * pi / 2;
+    ld f[4] = {cosl(h), 0, 0, 0}, t[4];
+    f[axis[k]] = sinl(h);
+    quat_mul(q, f, t);
+    for (int i = 0; i < 4; i++) q[i] = t[i];
+  }
+  const ld n = sqrtl(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+  for (auto& x : q) x /= n;
+  const ld qc[4] = {q[0], -q[1], -q[2], -q[3]};
+  double* out[4] = {prop_p, pol1_p, pol2_p, center_p};
+  for (int j = 0; j < 4; j++) {
+    if (!out[j]) continue;
+    const ld w[4] = {0, v[j][0], v[j][1], v[j][2]};
+    ld t[4], r[4];
+    quat_mul(qc, w, t);
+    quat_mul(t, q, r);
+    for (int a = 0; a < 3; a++) out[j][a] = (double)r[a + 1];
+  }
+}
+
 // Couple constants (DDA/DDAParams.cpp:315-331) with the polarisability of
 // DDA/PolarizabilityDescription.cpp:65-110.  refr: nmat*3 complex refractive
 // indices; outputs nmat*3 complex each (any output may be NULL).
 int dda_couple_constants(int kind, uint32_t nmat, const double* refr, double grid_unit, double wave_num,
                          const double* prop_in, int pol, double* cc, double* cc_sqrt, double* chi_inv) {
-  if (kind < DDA_POL_CM || kind > DDA_POL_LDR_AVGPOL || !refr || !prop_in) { g_err = "bad arguments"; return -1; }
+  if (!prop_in) { g_err = "bad arguments"; return -1; }
+  double inc[3], prop[3];
+  dda_beam_pol(prop_in, pol, inc, prop);
+  return dda_couple_constants_frame(kind, nmat, refr, grid_unit, wave_num, prop, inc, cc, cc_sqrt, chi_inv);
+}
+
+// The same with the propagation direction and polarisation vector given in
+// the particle frame (dda_beam_frame; PolarizabilityDescription.cpp:96-98
+// rotates both by the inverse orientation).
+int dda_couple_constants_frame(int kind, uint32_t nmat, const double* refr, double grid_unit, double wave_num,
+                               const double* prop, const double* inc, double* cc, double* cc_sqrt, double* chi_inv) {
+  if (kind < DDA_POL_CM || kind > DDA_POL_LDR_AVGPOL || !refr || !prop || !inc) { g_err = "bad arguments"; return -1; }
   typedef std::complex<double> cd;
   const ld d = grid_unit;
   const double vol = (double)(d * d * d);
   const double kd = wave_num * grid_unit;
   const double temp = vol / (double)kFourPi;
-  double inc[3], prop[3];
-  dda_beam_pol(prop_in, pol, inc, prop);
   for (uint32_t i = 0; i < nmat * 3; i++) {
     const cd m(refr[2 * i], refr[2 * i + 1]);
     const cd m2 = m * m;
@@ -268,10 +322,19 @@ int dda_couple_constants(int kind, uint32_t nmat, const double* refr, double gri
 // r_i the dipole position in the particle frame with the particle centred
 // (DipoleGeometry::moveToCenter, DDA/DipoleGeometry.cpp:75-80).
 int dda_einc_plane(const dda_geometry* g, double wave_num, const double* prop_in, int pol, double* einc) {
-  if (!g || !prop_in || !einc) { g_err = "bad arguments"; return -1; }
-  const uint32_t nv = (uint32_t)g->mat.size(), nvs = (nv + 15) / 16 * 16;
+  if (!prop_in) { g_err = "bad arguments"; return -1; }
   double inc[3], prop[3];
   dda_beam_pol(prop_in, pol, inc, prop);
+  return dda_einc_plane_frame(g, wave_num, prop, inc, einc);
+}
+
+// The plane wave with its propagation direction and polarisation vector in
+// the particle frame (PlaneWave::createEInc with propP and getIncPolP,
+// DDA/Beam.cpp:113-117).
+int dda_einc_plane_frame(const dda_geometry* g, double wave_num, const double* prop, const double* inc,
+                         double* einc) {
+  if (!g || !prop || !inc || !einc) { g_err = "bad arguments"; return -1; }
+  const uint32_t nv = (uint32_t)g->mat.size(), nvs = (nv + 15) / 16 * 16;
   std::memset(einc, 0, sizeof(double) * 2 * 3 * (size_t)nvs);
   ld origin[3];
   for (int a = 0; a < 3; a++) origin[a] = -((ld)g->box[a] - 1.0L) / 2 * g->grid_unit;
@@ -301,13 +364,10 @@ int dda_einc_plane(const dda_geometry* g, double wave_num, const double* prop_in
 // with the signs of the imaginary parts for an exp(-i omega t) time factor.
 int dda_einc_gaussian(const dda_geometry* g, double wave_num, const double* prop_in, int pol, int kind,
                       double waist, const double* center, double* einc) {
-  if (!g || !prop_in || !einc || !(waist > 0) || kind < DDA_BEAM_LMINUS || kind > DDA_BEAM_BARTON5 ||
-      (pol != 1 && pol != 2)) {
+  if (!prop_in || (pol != 1 && pol != 2)) {
     g_err = "bad arguments";
     return -1;
   }
-  typedef std::complex<double> cd;
-  const uint32_t nv = (uint32_t)g->mat.size(), nvs = (nv + 15) / 16 * 16;
   double p1[3], p2[3], prop[3];
   dda_beam_pol(prop_in, 1, p1, prop);
   dda_beam_pol(prop_in, 2, p2, nullptr);
@@ -316,6 +376,20 @@ int dda_einc_gaussian(const dda_geometry* g, double wave_num, const double* prop
     ex[a] = pol == 1 ? p1[a] : p2[a];
     ey[a] = pol == 1 ? -p2[a] : p1[a];
   }
+  return dda_einc_gaussian_frame(g, wave_num, prop, ex, ey, kind, waist, center, einc);
+}
+
+// The Gaussian beam with its frame (prop, ex = the polarisation vector, ey)
+// and centre in the particle frame (DDA/Beam.cpp:198-205 rotate all four by
+// the inverse orientation).
+int dda_einc_gaussian_frame(const dda_geometry* g, double wave_num, const double* prop, const double* ex,
+                            const double* ey, int kind, double waist, const double* center, double* einc) {
+  if (!g || !prop || !ex || !ey || !einc || !(waist > 0) || kind < DDA_BEAM_LMINUS || kind > DDA_BEAM_BARTON5) {
+    g_err = "bad arguments";
+    return -1;
+  }
+  typedef std::complex<double> cd;
+  const uint32_t nv = (uint32_t)g->mat.size(), nvs = (nv + 15) / 16 * 16;
   const double c0[3] = {center ? center[0] : 0.0, center ? center[1] : 0.0, center ? center[2] : 0.0};
   const double w0 = waist, b = wave_num * w0 * w0, s = 1 / (wave_num * w0);
   const double s2 = s * s, s3 = s2 * s, s4 = s2 * s2, s5 = s4 * s;

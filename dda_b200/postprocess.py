@@ -38,11 +38,12 @@ def grid_angles(theta_spec="0..180/91", phi_spec="0..360/61"):
     return t0 + (i // npf) * dt, p0 + (i % npf) * dp
 
 
-def scattering_frame(prop, theta, phi):
+def scattering_frame(prop, theta, phi, orient=None):
     """Directions n, perpendicular and parallel vectors for each angle, in
-    the frame (prop, incPolX = polarisation 2, incPolY = polarisation 1)."""
-    px, pn = api.beam_pol(prop, 2)
-    py, _ = api.beam_pol(prop, 1)
+    the frame (prop, incPolX = polarisation 2, incPolY = polarisation 1), in
+    the particle's coordinates (orient: its ZYZ Euler angles in degrees,
+    DDA/FarFieldCalc.cpp:165-170)."""
+    pn, py, px, _ = api.beam_frame(prop, orient)
     st, ct = np.sin(theta)[:, None], np.cos(theta)[:, None]
     sp, cp = np.sin(phi)[:, None], np.cos(phi)[:, None]
     n = ct * pn + st * (cp * px + sp * py)
@@ -65,10 +66,10 @@ def jones(e1, e2, theta, phi, perp, par):
     return out
 
 
-def jones_far_field(mv, prop, theta, phi, pol=None):
+def jones_far_field(mv, prop, theta, phi, pol=None, orient=None):
     """Jones matrices on an angle grid from the two polarisations of the last
     solve (right-hand sides 0 and 1 of `mv`) or of `pol` ([2][3 nvs])."""
-    n, perp, par = scattering_frame(prop, theta, phi)
+    n, perp, par = scattering_frame(prop, theta, phi, orient)
     e = mv.far_field(n, nrhs=2, pol=pol)  # [count][2][3]
     return jones(e[:, 0, :], e[:, 1, :], theta, phi, perp, par)
 
@@ -83,12 +84,14 @@ def ext_cross_general(params, pol_vec, einc):
     return 4 * np.pi * params.wave_num * float(np.sum(np.imag(p * np.conj(e))))
 
 
-def cross_sections(params, cc, pol_vec, e_forward, prop, pol, einc=None):
+def cross_sections(params, cc, pol_vec, e_forward, prop, pol, einc=None, orient=None):
     """(Cext, Cabs, Qext, Qabs) of one solution: e_forward = far field in the
-    propagation direction, cc the CoupleConstants of that right-hand side.
-    einc: the incident field of a non-plane beam, whose extinction then comes
-    from ext_cross_general (e_forward is not used)."""
-    inc, _ = api.beam_pol(prop, pol)
+    propagation direction (in the particle frame: api.beam_frame), cc the
+    CoupleConstants of that right-hand side.  einc: the incident field of a
+    non-plane beam, whose extinction then comes from ext_cross_general
+    (e_forward is not used)."""
+    _, p1, p2, _ = api.beam_frame(prop, orient)
+    inc = p1 if pol == 1 else p2
     k = params.wave_num
     if einc is not None:
         cext = ext_cross_general(params, pol_vec, einc)

@@ -53,15 +53,35 @@ const uint8_t* dda_geom_materials(const dda_geometry* g);  /* nv */
  * direction (DDA/Beam.cpp:33-51). */
 void dda_beam_pol(const double* prop, int pol, double* inc_pol3, double* prop_normalised3);
 
+/* The beam's vectors in the particle frame for the particle orientation
+ * orient_deg = ZYZ Euler angles (alpha, beta, gamma) in degrees (--orient;
+ * NULL: none): the normalised propagation direction prop_p and the
+ * polarisation vectors of dda_beam_pol for polarisations 1 and 2, and the
+ * point center_in (may be NULL) as center_p, each mapped by the inverse of
+ * R = Rz(alpha) Ry(beta) Rz(gamma) (EMSim::Rotation::fromZYZDeg,
+ * EMSim/Rotation.hpp:94-102; DipoleGeometry::orientationInverse,
+ * DDA/DipoleGeometry.cpp:149-152).  The *_frame functions below take these. */
+void dda_beam_frame(const double* prop, const double* orient_deg, double* prop_p, double* pol1_p, double* pol2_p,
+                    const double* center_in, double* center_p);
+
 /* Couple constants cc, sqrt(cc) and the inverse susceptibility for nmat*3
  * complex refractive indices (CoupleConstants, DDA/DDAParams.cpp:315-331;
  * Cm / Ldr ::getCoupleConstants, DDA/PolarizabilityDescription.cpp:65-110). */
 int dda_couple_constants(int kind, uint32_t nmat, const double* refr, double grid_unit, double wave_num,
                          const double* prop, int pol, double* cc, double* cc_sqrt, double* chi_inv);
+/* The same for a propagation direction and polarisation vector in the
+ * particle frame (DDA/PolarizabilityDescription.cpp:96-98). */
+int dda_couple_constants_frame(int kind, uint32_t nmat, const double* refr, double grid_unit, double wave_num,
+                               const double* prop_p, const double* pol_p, double* cc, double* cc_sqrt,
+                               double* chi_inv);
 
 /* Plane-wave incident field [3][nvs] complex for polarisation pol
  * (PlaneWave::createEInc, DDA/Beam.cpp:111-118). */
 int dda_einc_plane(const dda_geometry* g, double wave_num, const double* prop, int pol, double* einc);
+/* The same for a propagation direction and polarisation vector in the
+ * particle frame (DDA/Beam.cpp:113-117). */
+int dda_einc_plane_frame(const dda_geometry* g, double wave_num, const double* prop_p, const double* pol_p,
+                         double* einc);
 
 #define DDA_BEAM_LMINUS 0  /* fundamental Gaussian mode */
 #define DDA_BEAM_DAVIS3 1  /* Davis, third-order corrections */
@@ -74,6 +94,12 @@ int dda_einc_plane(const dda_geometry* g, double wave_num, const double* prop, i
  * gaussian:<kind>,<waist>[,(x,y,z)], DDA/Beam.cpp:139-181). */
 int dda_einc_gaussian(const dda_geometry* g, double wave_num, const double* prop, int pol, int kind,
                       double waist, const double* center, double* einc);
+/* The same with the beam frame (prop_p, ex_p = the polarisation vector, ey_p
+ * = ex rotated by +90 degrees about prop: -pol2 for polarisation 1, pol1 for
+ * polarisation 2) and the centre in the particle frame (DDA/Beam.cpp:
+ * 198-205). */
+int dda_einc_gaussian_frame(const dda_geometry* g, double wave_num, const double* prop_p, const double* ex_p,
+                            const double* ey_p, int kind, double waist, const double* center_p, double* einc);
 
 #ifdef __cplusplus
 }

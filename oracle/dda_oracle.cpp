@@ -537,12 +537,21 @@ void orc_beam_pol(const double* propIn, int pol, double* out3, double* prop3) {
 // CoupleConstants (DDA/DDAParams.cpp:315-331) with the CM / LDR
 // polarisability of DDA/PolarizabilityDescription.cpp:65-110.
 // kind: 0 = cm, 1 = ldr, 2 = ldr-avgpol.  pol: 1 or 2.
+void orc_set_cc_frame(orc_problem* p, int kind, const double* prop, const double* incPol);
+
 void orc_set_cc(orc_problem* p, int kind, const double* propIn, int pol) {
+  double incPol[3], prop[3];
+  orc_beam_pol(propIn, pol, incPol, prop);
+  orc_set_cc_frame(p, kind, prop, incPol);
+}
+
+// The same for a propagation direction and polarisation vector already in
+// the particle frame (PolarizabilityDescription.cpp:96-98, where both are
+// rotated by the inverse orientation).
+void orc_set_cc_frame(orc_problem* p, int kind, const double* prop, const double* incPol) {
   p->cc.assign(p->nmat * 3, 0);
   p->ccSqrt.assign(p->nmat * 3, 0);
   p->chiInv.assign(p->nmat * 3, 0);
-  double incPol[3], prop[3];
-  orc_beam_pol(propIn, pol, incPol, prop);
   double temp = p->gridUnitVol / (double)kFourPi;
   for (uint32_t i = 0; i < p->nmat; i++) {
     for (int j = 0; j < 3; j++) {

@@ -80,6 +80,7 @@ def lib():
         L.orc_direct_matvec.argtypes = [vp, dp, dp]
         L.orc_einc.argtypes = [vp, dp, ctypes.c_int, dp]
         L.orc_coords.argtypes = [vp, dp]
+        L.orc_set_cc_frame.argtypes = [vp, ctypes.c_int, dp, dp]
         L.orc_solve.argtypes = [vp, ctypes.c_int, dp, ctypes.c_double, ctypes.c_int64,
                                 dp, dp, ctypes.POINTER(OrcStats), ctypes.c_int64, dp,
                                 ctypes.c_int64]
@@ -123,6 +124,32 @@ def fft(x, inverse=False):
     n = a.shape[-1]
     lib().orc_fft(_dp(a), n, a.size // n, 1 if inverse else 0)
     return a
+
+
+def rotation_inverse(orient):
+    """The inverse of the particle orientation R = Rz(alpha) Ry(beta) Rz(gamma)
+    (ZYZ Euler angles in degrees; EMSim::Rotation::fromZYZDeg,
+    EMSim/Rotation.hpp:94-102) as a 3x3 matrix: Rz(-gamma) Ry(-beta) Rz(-alpha),
+    built from rotation matrices rather than the quaternions the reference
+    uses."""
+    a, b, g = (np.radians(float(x)) for x in orient)
+
+    def rz(t):
+        return np.array([[np.cos(t), -np.sin(t), 0], [np.sin(t), np.cos(t), 0], [0, 0, 1]])
+
+    def ry(t):
+        return np.array([[np.cos(t), 0, np.sin(t)], [0, 1, 0], [-np.sin(t), 0, np.cos(t)]])
+
+    return rz(-g) @ ry(-b) @ rz(-a)
+
+
+def beam_frame(prop, orient, center=(0.0, 0.0, 0.0)):
+    """(prop, pol1, pol2, center) of the beam in the particle frame
+    (DDA/Beam.hpp:69-81 with DipoleGeometry::orientationInverse)."""
+    m = rotation_inverse(orient)
+    p1, pn = beam_pol(prop, 1)
+    p2, _ = beam_pol(prop, 2)
+    return m @ pn, m @ p1, m @ p2, m @ np.asarray(center, dtype=np.float64)
 
 
 def beam_pol(prop, pol):
@@ -240,6 +267,20 @@ class Problem:
     def set_cc(self, prop=(0, 0, 1), pol=1, kind="ldr"):
         lib().orc_set_cc(self.h, POLARIZABILITIES[kind], _dp(np.asarray(prop, dtype=np.float64)), pol)
 
+    def set_cc_frame(self, prop_p, pol_p, kind="ldr"):
+        """Couple constants for a beam given in the particle frame."""
+        lib().orc_set_cc_frame(self.h, POLARIZABILITIES[kind], _dp(np.asarray(prop_p, dtype=np.float64)),
+                               _dp(np.asarray(pol_p, dtype=np.float64)))
+
+    def einc_frame(self, prop_p, pol_p):
+        """Plane-wave incident field [3 nvs] for a propagation direction and a
+        polarisation vector in the particle frame (DDA/Beam.cpp:113-117):
+        exp(i k r . prop_p) pol_p, in numpy."""
+        ph = self.coords() @ np.asarray(prop_p, dtype=np.float64) * self.wave_num
+        out = np.zeros((3, self.nvs), dtype=np.complex128)
+        out[:, :self.nv] = np.asarray(pol_p, dtype=np.float64)[:, None] * np.exp(1j * ph)[None, :]
+        return out.reshape(-1)
+
     def set_cc_sqrt(self, cc_sqrt):
         a = np.ascontiguousarray(cc_sqrt, dtype=np.complex128)
         lib().orc_set_cc_sqrt(self.h, _dp(a.view(np.float64)))
@@ -286,7 +327,7 @@ class Problem:
         lib().orc_coords(self.h, _dp(out))
         return out
 
-    def einc_gaussian(self, prop, pol, kind, waist, center=(0.0, 0.0, 0.0)):
+    def einc_gaussian(self, prop, pol, kind, waist, center=(0.0, 0.0, 0.0), orient=(0, 0, 0)):
         """Gaussian-beam incident field [3 nvs] (Beams::Gaussian::createEInc,
         DDA/Beam.cpp:196-263), restated in numpy over all dipoles at once, in
         the reference's order of operations: beam frame ex = polarisation
@@ -295,13 +336,12 @@ class Problem:
         kind "lminus" (DDA/Beam.cpp:217-218), "davis3" (225-238), "barton5"
         (239-256)."""
         k = self.wave_num
-        p1, pn = beam_pol(prop, 1)
-        p2, _ = beam_pol(prop, 2)
+        pn, p1, p2, cp = beam_frame(prop, orient, center)
         ex = p1 if pol == 1 else p2
         ey = -p2 if pol == 1 else p1
         w0 = waist
         b = k * w0 * w0
-        coord = self.coords() - np.asarray(center, dtype=np.float64)[None, :]
+        coord = self.coords() - cp[None, :]
         x, y, z = coord @ ex, coord @ ey, coord @ pn
         xi, eta, zeta = x / w0, y / w0, z / b
         rho2 = xi * xi + eta * eta

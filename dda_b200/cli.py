@@ -21,6 +21,11 @@ double; plus mixed), --no-symmetry (both polarisations are always solved),
 --store-dippol, --store-intfield, --store-incbeam, --write-txt, --profiling-run
 (per-stage matvec times instead of a solve), --output-dir.
 
+--adda-options, followed by options in ADDA's syntax (-dpl, -lambda, -m, -shape
+read, -prop, -orient, -beam, -pol, -eps, -iter, -maxiter, -ntheta, -scat_matr,
+-store_scat_grid, -store_beam, -store_int_field, -store_dip_pol, -dir,
+-dda-ftype), translated as DDA/AddaOptions.cpp:57-238 does.
+
 Output files are text (the reference's MATLAB-style HDF5 files are not
 written: no HDF5 library on these machines): CrossSec-Pol<n>.txt,
 MieCrossSec.txt (spheres), Far<Name>.txt (Jones matrices, the column layout
@@ -93,6 +98,129 @@ def build_geometry(spec, grid_unit, m_opts, lambda_m):
     raise SystemExit("Unknown geometry option `%s'" % name)
 
 
+def _is_adda_option(s):
+    return len(s) >= 2 and s[0] == "-" and s[1].isalpha()
+
+
+def translate_adda(args):
+    """The options of an ADDA command line (what follows --adda-options) as
+    options of this command line, the way parseAddaOptions does
+    (DDA/AddaOptions.cpp:57-238): lengths in micrometres, -dpl dipoles per
+    wavelength giving the grid unit, the default target a sphere of diameter
+    16 grid units, text output, and the far fields of -scat_matr (default
+    both, as in the reference) on the YZ plane or, with -store_scat_grid, on
+    the angle grid."""
+    opts, had = [], set()
+    dpl, lam, m_values, shape = None, 2 * math.pi, [], None
+    muel, ampl, grid = True, True, False
+    i = 0
+    while i < len(args):
+        if not _is_adda_option(args[i]):
+            raise SystemExit("adda options: expected an option, got `%s'" % args[i])
+        name = args[i][1:]
+        pars = []
+        while i + 1 < len(args) and not _is_adda_option(args[i + 1]):
+            i += 1
+            pars.append(args[i])
+        i += 1
+        if name in had:
+            raise SystemExit("Got adda option `%s' more than once" % name)
+        had.add(name)
+
+        def want(*counts):
+            if len(pars) not in counts:
+                raise SystemExit("adda option -%s: %s parameters" % (name, len(pars)))
+
+        if name == "dpl":
+            want(1)
+            dpl = float(pars[0])
+        elif name == "lambda":
+            want(1)
+            lam = float(pars[0])
+        elif name == "pol":
+            want(1, 2)
+            opts += ["--pol", "-".join(pars)]
+        elif name == "beam":
+            if not pars:
+                want(1)
+            if pars[0] == "plane":
+                want(1)
+                opts += ["--beam", "plane"]
+            else:
+                want(2, 5)
+                c = pars[2:] if len(pars) == 5 else ["0", "0", "0"]
+                opts += ["--beam", "gaussian:%s,%sum,(%s)" % (pars[0], pars[1], ",".join(x + "um" for x in c))]
+        elif name in ("prop", "orient"):
+            want(3)
+            opts += ["--" + name, "(%s)" % ",".join(pars)]
+        elif name == "m":
+            if not pars or len(pars) % 2:
+                raise SystemExit("adda option -m: pairs of real and imaginary parts")
+            m_values += ["%s%+gi" % (pars[k], float(pars[k + 1])) for k in range(0, len(pars), 2)]
+        elif name == "shape":
+            if not pars or pars[0] != "read":
+                raise SystemExit("Unknown shape type `%s', only 'read' is known" % (pars[0] if pars else ""))
+            want(2)
+            shape = pars[1]
+        elif name == "store_scat_grid":
+            want(0)
+            grid = True
+        elif name == "store_beam":
+            want(0)
+            opts.append("--store-incbeam")
+        elif name == "store_int_field":
+            want(0)
+            opts.append("--store-intfield")
+        elif name == "store_dip_pol":
+            want(0)
+            opts.append("--store-dippol")
+        elif name == "scat_matr":
+            want(1)
+            modes = {"muel": (True, False), "ampl": (False, True), "both": (True, True), "none": (False, False)}
+            if pars[0] not in modes:
+                raise SystemExit("Invalid value for -scat_matr `%s'" % pars[0])
+            muel, ampl = modes[pars[0]]
+        elif name == "eps":
+            want(1)
+            opts += ["--epsilon", pars[0]]
+        elif name == "iter":
+            want(1)
+            opts += ["--iter", pars[0]]
+        elif name == "maxiter":
+            want(1)
+            opts += ["--maxiter", pars[0]]
+        elif name == "ntheta":
+            want(1)
+            opts += ["--ntheta", str(2 * int(pars[0]))]
+        elif name == "dir":
+            want(1)
+            opts += ["--output-dir", pars[0]]
+        elif name == "dda-ftype":
+            want(1)
+            opts += ["--ftype", pars[0]]
+        else:  # -dda-cpu and -dda-device select the reference's OpenCL device: no counterpart
+            raise SystemExit("Unknown adda option `%s'" % name)
+    if dpl is None:
+        raise SystemExit("No dpl option given")
+    gu = lam / dpl
+    opts += ["--lambda", "%.17gum" % lam, "--grid-unit", "%.17gum" % gu, "--write-txt"]
+    if not m_values:
+        m_values = ["1.5"]
+    if shape is None:
+        if len(m_values) != 1:
+            raise SystemExit("adda options: one -m value for the default sphere")
+        opts += ["--geometry", "sphere:%.17gum,%s" % (gu * 16 / 2, m_values[0])]
+    else:
+        opts += ["--geometry", "load:file=" + shape]
+        for m in m_values:
+            opts += ["-m", m]
+    if grid:
+        opts += ["--mueller-matrix-grid"] * muel + ["--efield-grid"] * ampl
+    else:
+        opts += ["--mueller-matrix"] * muel + ["--efield"] * ampl
+    return opts
+
+
 def cc_vector(params, per_material):
     """Per-material, per-axis values (nmat*3) spread over the vector layout."""
     mat = params.geometry.materials.astype(np.int64)
@@ -123,7 +251,8 @@ def read_field(path, params):
     return v
 
 
-def main(argv=None):
+def parser():
+    """The command line's options (the reference's names, DDA/Options.cpp:41-97)."""
     ap = argparse.ArgumentParser(prog="dda_b200.cli", description=__doc__.split("\n\n")[0])
     ap.add_argument("--lambda", dest="lam", default="%.17gum" % (2 * math.pi))
     ap.add_argument("--prop", default="(0,0,1)")
@@ -153,7 +282,15 @@ def main(argv=None):
     ap.add_argument("--write-txt", action="store_true")
     ap.add_argument("--profiling-run", action="store_true")
     ap.add_argument("--output-dir", default=".")
-    a = ap.parse_args(argv)
+    return ap
+
+
+def main(argv=None):
+    argv = list(sys.argv[1:] if argv is None else argv)
+    if "--adda-options" in argv:  # DDA/Options.cpp:122-133
+        k = argv.index("--adda-options")
+        argv = argv[:k] + translate_adda(argv[k + 1:])
+    a = parser().parse_args(argv)
 
     lambda_m = api.parse_length(a.lam)
     prop = tuple(parse_vector(a.prop))

@@ -102,3 +102,46 @@ def test_cli_run_writes_cross_sections(tmp_path, capsys):
     cext, cabs, _, _ = postprocess.cross_sections(p, cc, pol, ef, (0, 0, 1), 1)
     assert abs(float(vals["Cext"]) - cext) <= 1e-12 * abs(cext)
     assert abs(float(vals["Cabs"]) - cabs) <= 1e-12 * abs(cabs)
+
+
+def test_adda_options_translate():
+    # DDA/AddaOptions.cpp:57-238 on the option sets of DDA/test-adda.sh
+    T = cli.translate_adda
+    a = cli.parser().parse_args(T("-dpl 15".split()))
+    assert api_len(a.grid_unit) == pytest.approx(2 * math.pi / 15 * 1e-6)
+    assert api_len(a.geometry.split(":")[1].split(",")[0]) == pytest.approx(8 * 2 * math.pi / 15 * 1e-6)
+    assert a.geometry.endswith(",1.5") and a.efield and a.mueller_matrix and a.write_txt and not a.efield_grid
+    a = cli.parser().parse_args(T(("-lambda 30 -shape read box.geom -dpl 30 -store_scat_grid -scat_matr both "
+                                   "-prop 10 -2 3 -orient -5 -30 10 -iter bicgstab -beam barton5 1 1 6 3").split()))
+    assert a.geometry == "load:file=box.geom" and a.m == ["1.5"] and api_len(a.grid_unit) == pytest.approx(1e-6)
+    assert a.efield_grid and a.mueller_matrix_grid and not a.efield and not a.mueller_matrix
+    assert cli.parse_vector(a.prop) == [10, -2, 3] and cli.parse_vector(a.orient) == [-5, -30, 10]
+    assert a.iter == "bicgstab"
+    b = dda_b200.Beam(a.beam)
+    assert b.kind == "barton5" and b.waist == pytest.approx(1e-6) and np.allclose(b.center, (1e-6, 6e-6, 3e-6))
+    a = cli.parser().parse_args(T(("-dpl 15 -scat_matr muel -pol ldr avgpol -m 1.4 -0.2 -ntheta 3 -eps 1 "
+                                   "-iter cgnr -maxiter 50 -store_beam -store_dip_pol -dir out").split()))
+    assert a.pol == "ldr-avgpol" and a.ntheta == 6 and a.geometry.endswith(",1.4-0.2i")
+    assert a.mueller_matrix and not a.efield and a.epsilon == 1 and a.iter == "cgnr" and a.maxiter == 50
+    assert a.store_incbeam and a.store_dippol and a.output_dir == "out"
+    assert cli.parser().parse_args(T("-dpl 15 -beam plane -scat_matr none".split())).beam == "plane"
+    for bad in ("-lambda 6", "-dpl 15 -dpl 15", "-dpl 15 -size 10", "-dpl 15 -dda-cpu", "-dpl 15 -m 1.5",
+                "-dpl 15 -shape box", "dpl 15"):
+        with pytest.raises(SystemExit):
+            T(bad.split())
+
+
+def api_len(s):
+    return dda_b200.api.parse_length(s)
+
+
+@pytest.mark.gpu
+def test_cli_adda_options_run(tmp_path, capsys):
+    rc = cli.main(["--adda-options", "-dpl", "15", "-scat_matr", "both", "-prop", "1", "2", "3", "-orient", "40", "70",
+                   "100", "-beam", "barton5", "10", "-pol", "ldr", "-ntheta", "4", "-dir", str(tmp_path)])
+    assert rc == 0
+    out = capsys.readouterr().out
+    assert "Cext Pol1" in out and "Mie solution" not in out
+    for f in ("CrossSec-Pol1.txt", "CrossSec-Pol2.txt", "FarPlane.txt", "FarPlane.mueller.txt", "DipPol-Pol1.txt"):
+        assert os.path.exists(tmp_path / f), f
+    assert sum(1 for _ in open(tmp_path / "FarPlane.txt")) == 1 + 8

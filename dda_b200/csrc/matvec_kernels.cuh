@@ -328,7 +328,7 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 3) k_xinv(const A2* _
   const uint32_t je = soff[nl];
   uint32_t j = soff[0] + threadIdx.x;
   int l = j < je ? tile_line(soff, nl, j) : 0;
-  constexpr int U = sizeof(A2) > sizeof(T2) ? kXBatch / 4 : kXBatch / 2;
+  constexpr int U = kXBatch / 2;
   for (; j < je; j += U * NT) {
     int o[U];  // shared offset of entry j + u NT, -1 past the tile
     uint32_t d[U], jj[U];

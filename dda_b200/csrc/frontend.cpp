@@ -113,6 +113,7 @@ int dda_geom_sphere(const char* radius, const char* grid_unit, dda_geometry** ou
         const double xd = x - r + 0.5, yd = y - r + 0.5, zd = z - r + 0.5;
         if (xd * xd + yd * yd + zd * zd <= r2) g->add(x, y, z, 0);
       }
+  if (g->mat.empty()) { delete g; g_err = "the geometry has no dipoles"; return -1; }
   *out = g;
   return 0;
 }
@@ -135,6 +136,7 @@ int dda_geom_cylinder(const char* length, const char* radius, const char* grid_u
       if (yd * yd + zd * zd <= r2)
         for (uint32_t x = 0; x < len; x++) g->add(x, y, z, 0);
     }
+  if (g->mat.empty()) { delete g; g_err = "the geometry has no dipoles"; return -1; }
   *out = g;
   return 0;
 }
@@ -153,6 +155,7 @@ int dda_geom_box(const char* sx, const char* sy, const char* sz, const char* gri
   for (uint32_t z = 0; z < s[2]; z++)
     for (uint32_t y = 0; y < s[1]; y++)
       for (uint32_t x = 0; x < s[0]; x++) g->add(x, y, z, 0);
+  if (g->mat.empty()) { delete g; g_err = "the geometry has no dipoles"; return -1; }
   *out = g;
   return 0;
 }
@@ -181,6 +184,7 @@ int dda_geom_load(const char* path, const char* grid_unit, dda_geometry** out) {
     g->add((uint32_t)x, (uint32_t)y, (uint32_t)z, (uint8_t)(m - 1));
   }
   if (!g->sorted) { delete g; g_err = "load: dipoles must be sorted by z"; return -1; }
+  if (g->mat.empty()) { delete g; g_err = "the geometry has no dipoles"; return -1; }
   *out = g;
   return 0;
 }
@@ -193,6 +197,7 @@ int dda_geom_from_arrays(const uint32_t* pos, const uint8_t* mat, uint32_t nv, c
   g->grid_unit = d;
   for (uint32_t i = 0; i < nv; i++) g->add(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], mat ? mat[i] : 0);
   if (!g->sorted) { delete g; g_err = "dipoles must be sorted by z"; return -1; }
+  if (g->mat.empty()) { delete g; g_err = "the geometry has no dipoles"; return -1; }
   *out = g;
   return 0;
 }

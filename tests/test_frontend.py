@@ -125,3 +125,13 @@ def test_grid_angles_follow_angle_list():
     assert np.allclose(np.degrees(p[:4]), [0, 120, 240, 360])
     t1, p1 = postprocess.grid_angles("30", "45")
     assert np.allclose(np.degrees([t1[0], p1[0]]), [30, 45])
+
+
+def test_geometry_without_dipoles_is_rejected():
+    # an empty dipole list or a shape too small to hold a dipole centre is an
+    # error of the front end, not an empty problem
+    import dda_b200
+    for make in (lambda: dda_b200.Geometry.from_arrays(np.zeros((0, 3), np.uint32), np.zeros(0, np.uint8), "0.1um"),
+                 lambda: dda_b200.Geometry.sphere("0.01um", "0.1um")):
+        with pytest.raises(dda_b200.api.DDAError, match="no dipoles"):
+            make()

@@ -185,3 +185,32 @@ def test_serve_cancel_queued_and_running():
     with pytest.raises(dda_b200.DDAError):
         srv.cancel(ids[1])  # finished: neither queued nor running
     srv.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_single_dipole(prec):
+    # one dipole (box 1x1x1, grid 2^3, runtime-planned FFTs): no interaction,
+    # A = I, so the solve ends at once with the oracle's polarisation
+    import dda_b200
+    from oracle import oracle as O
+    g = dda_b200.Geometry.from_arrays(np.zeros((1, 3), np.uint32), np.zeros(1, np.uint8), "0.1um")
+    p = dda_b200.DDAParams(g, [1.5 + 0.1j], "1um")
+    op = O.Problem(O.Geometry.from_arrays(np.zeros((1, 3), np.uint32), np.zeros(1, np.uint8), "0.1um"),
+                   [1.5 + 0.1j], "1um")
+    op.build_dmatrix()
+    mv = dda_b200.CudaMatVec(p, prec, max_rhs=2)
+    for r, pol in enumerate((1, 2)):
+        mv.set_couple_constants(dda_b200.CoupleConstants(p, (0, 0, 1), pol, "ldr"), rhs=r)
+    e = np.stack([p.einc((0, 0, 1), pol) for pol in (1, 2)])
+    x = np.random.default_rng(3).normal(size=p.vec_size) + 0j
+    x.reshape(3, p.nvs)[:, 1:] = 0
+    y = mv.apply(x)
+    assert np.allclose(y, x, rtol=0, atol=1e-6 if prec == "fp32" else 1e-14)  # A = I
+    pol = dda_b200.CudaSolver(mv, "qmr").get_pol_vec(e, 1e-8)
+    for r, pv in enumerate((1, 2)):
+        op.set_cc((0, 0, 1), pv, "ldr")
+        rc, want, _, _ = op.solve(e[r], "qmr", 1e-8)
+        assert rc == 0
+        assert np.linalg.norm(pol[r] - want) <= (1e-6 if prec == "fp32" else 1e-12) * np.linalg.norm(want)
+    mv.close()

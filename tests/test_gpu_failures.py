@@ -214,3 +214,36 @@ def test_single_dipole(prec):
         assert rc == 0
         assert np.linalg.norm(pol[r] - want) <= (1e-6 if prec == "fp32" else 1e-12) * np.linalg.norm(want)
     mv.close()
+
+
+@pytest.mark.gpu
+def test_argument_and_size_checks():
+    # the context and solve entry points reject what they cannot run with a
+    # code and a message, before any device work: grids that are odd, smaller
+    # than twice the box, not 2,3,5,7-smooth or above the 4096 edge limit;
+    # more right-hand sides than the context holds, a solve before its couple
+    # constants, a non-positive tolerance
+    import dda_b200
+    from dda_b200.api import DDAError
+    g = dda_b200.Geometry.box_shape("0.5um", "0.4um", "0.3um", "0.1um")
+    cases = [((11, 8, 6), -1, "even"), ((8, 8, 6), -1, "twice"), ((22, 8, 6), -4, "smooth"),
+             ((4098, 8, 6), -4, "4096")]
+    for grid, code, words in cases:
+        p = dda_b200.DDAParams(g, [1.5], "1um", grid=grid)
+        with pytest.raises(DDAError) as ei:
+            dda_b200.CudaMatVec(p, "fp32")
+        assert ei.value.code == code and words in str(ei.value), (grid, str(ei.value))
+    p = dda_b200.DDAParams(g, [1.5], "1um")
+    mv = dda_b200.CudaMatVec(p, "fp32", max_rhs=1)
+    s = dda_b200.CudaSolver(mv, "qmr")
+    e = p.einc((0, 0, 1), 1)
+    with pytest.raises(DDAError, match="couple constants"):
+        s.get_pol_vec(e, 1e-5)
+    mv.set_couple_constants(dda_b200.CoupleConstants(p, (0, 0, 1), 1, "ldr"))
+    with pytest.raises(DDAError) as ei:
+        s.get_pol_vec(np.stack([e, e]), 1e-5)  # two rhs on a one-rhs context
+    assert ei.value.code == -1
+    with pytest.raises(DDAError, match="eps"):
+        s.get_pol_vec(e, 0.0)
+    assert np.all(np.isfinite(s.get_pol_vec(e, 1e-5)))  # the context still works
+    mv.close()

@@ -226,6 +226,9 @@ template <typename T> struct Engine {
 
 struct dda_ctx {
   std::atomic<int> cancel{0};  // dda_cancel: the running (or next) solve stops at its next round
+  // MIXED: the FP64 engine's plane kernel shapes are tuned when a solve first
+  // runs the FP64 convolution (many served targets never do)
+  bool e64_tuned = true;
   int device = 0;
   int precision = DDA_PREC_FP64;
   int max_rhs = 1;
@@ -1261,6 +1264,12 @@ void run_solve(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
   MixedSwitch ms(o.adapt_phase, o.adapt_tau, nrhs);
   if (o.adapt) sv.mv32 = ms.mode32;
   for (int round = 0;; round++) {
+    if constexpr (std::is_same<T, double>::value) {
+      if (!sv.mv32 && !c->e64_tuned) {  // first FP64-convolution round of a MIXED context
+        c->e64_tuned = true;
+        autotune<double>(c);
+      }
+    }
     if (!graphs || round == 0) {
       for (int k = 0; k < poll; k++) sv.iteration(solver, nr++, b);
     } else {
@@ -1575,10 +1584,14 @@ int dda_create(const dda_problem* p, int precision, dda_ctx** out) {
     if (p->dmatrix) upload_dmatrix(c.get(), p->dmatrix);
     else build_dmatrix(c.get());
     if (!(c->flags & DDA_FLAG_NO_AUTOTUNE)) {
-      // MIXED runs its FP64 engine for the outer residuals, the FP64 checks
-      // and the FP64 phases of its inner solves
       if (c->e32.on) autotune<float>(c.get());
-      if (c->e64.on) autotune<double>(c.get());
+      // MIXED runs its FP64 engine for a few outer residuals and checks and,
+      // for targets whose FP32 convolution stalls, the FP64 phases of its
+      // inner solves: tuned on the first such phase (run_solve), which many
+      // targets never reach, instead of here.  The shapes never change the
+      // arithmetic.
+      if (c->e64.on && precision == DDA_PREC_MIXED) c->e64_tuned = false;
+      else if (c->e64.on) autotune<double>(c.get());
     }
     CK(cudaStreamSynchronize(c->stream));
     c->dev_bytes = g_dalloc_bytes;

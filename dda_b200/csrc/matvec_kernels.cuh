@@ -128,13 +128,14 @@ struct TileWalk {
 // A solver step whose result is the next matvec's argument, run in
 // k_xfwd's load instead of a pass of its own: the argument is computed from
 // the solver's vectors, written back for the later steps and transformed.
-// Same arithmetic as the k_vec step named beside each.
+// The linear combinations are the reference's (bo = -beta omega, mAlpha =
+// -alpha, from the device state).
 enum XPreOp {
   XP_NONE = 0,
-  XP_BIS_P,   // out = first ? v2 : out beta + v1 bo + v2       (p, v, r)   V_BIS_P
-  XP_BIS_S,   // out = v1 mAlpha + v2; n = |out|^2              (s, v, r)   V_BIS_S
-  XP_BICG_P,  // out = first ? v1 : out beta + v1               (p, r)      V_BICG_P
-  XP_CGNR_P,  // out = out beta + v1                            (p, A^H r)  V_CGNR_P
+  XP_BIS_P,   // out = first ? v2 : out beta + v1 bo + v2   (p, v, r)   DDA/BicgStab.cpp:88
+  XP_BIS_S,   // out = v1 mAlpha + v2; n = |out|^2          (s, v, r)   DDA/BicgStab.cpp:96
+  XP_BICG_P,  // out = first ? v1 : out beta + v1           (p, r)      DDA/BicgCs.cpp:73
+  XP_CGNR_P,  // out = out beta + v1                        (p, A^H r)  DDA/Cgnr.cpp:62
 };
 struct XPre {
   int op;

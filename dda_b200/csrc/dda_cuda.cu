@@ -9,6 +9,7 @@
 // replayed from a captured CUDA graph.
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <chrono>
@@ -69,6 +70,16 @@ constexpr size_t kSmemMax = 227 * 1024;
 // process-wide attribute of the function, shared by every context (and
 // thread) that launches it, so it is always set to the same maximum; each
 // launch's own size is checked against kSmemMax by its caller.
+// A named range on the host timeline (NVTX) for Nsight Systems: context
+// set-up, D matrix, autotuning, solves and their rounds, refinement, far
+// field.  Free when no tool is attached.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
+
 inline cudaError_t allow_smem(const void* f) {
   cudaFuncAttributes a;
   cudaError_t rc = cudaFuncGetAttributes(&a, f);
@@ -714,6 +725,7 @@ template <typename T> void autotune(dda_ctx* c) {
   Engine<T>& e = eng<T>(c);
   const MvGeom& g = c->g;
   if (!e.on || !(e.fused || e.slot_path)) return;
+  NvtxRange range(sizeof(T) == 4 ? "dda autotune fp32" : "dda autotune fp64");
   if ((long long)g.Gx * g.Gy * g.Gz < (1LL << 20)) return;  // small grids keep the defaults
   // the box changes the best batching little next to the grid, so shapes
   // share a choice per grid (served targets mostly land on tuned grids)
@@ -827,6 +839,7 @@ void matvec(dda_ctx* c, const A2* arg, A2* res, int conj, int nrhs, cudaStream_t
 
 // D-matrix generation (FP64) into the enabled engines' octants.
 void build_dmatrix(dda_ctx* c) {
+  NvtxRange range("dda D matrix");
   const MvGeom& g = c->g;
   const long long N = (long long)g.Gx * g.Gy * g.Gz;
   double2* full = nullptr;
@@ -1205,6 +1218,7 @@ bool check_gap(dda_ctx* c, int nrhs, double2* X, double2* B, double2* tmp, const
 template <typename T>
 void run_solve(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter, const SolveOpts& o) {
   typedef typename C2<T>::t T2;
+  NvtxRange range(sizeof(T) == 4 ? "dda solve fp32" : (o.mv32 || o.adapt) ? "dda inner solve" : "dda solve fp64");
   Engine<T>& e = eng<T>(c);
   Solve<T> sv(c, nrhs);
   sv.mv32 = o.mv32;
@@ -1299,8 +1313,11 @@ void run_solve(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter,
       c->launches += c->round_graphs[gi].launches;
       nr += poll;
     }
-    CK(cudaMemcpyAsync(c->st_host, c->st, nrhs * sizeof(KrylovState), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
+    {
+      NvtxRange wait("dda round: wait for the state");
+      CK(cudaMemcpyAsync(c->st_host, c->st, nrhs * sizeof(KrylovState), cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+    }
     bool all = true;
     for (int r = 0; r < nrhs; r++) all = all && c->st_host[r].done;
     if (all) break;
@@ -1353,6 +1370,7 @@ struct MixedOut {
 
 void run_mixed(dda_ctx* c, int solver, int nrhs, double eps, long long max_iter, bool start,
                std::vector<MixedOut>& out) {
+  NvtxRange range("dda mixed refinement");
   Engine<double>& d = c->e64;
   Solve<double> sd(c, nrhs, c->st_outer);
   const size_t n = (size_t)nrhs * 3 * c->g.nvs;
@@ -1475,6 +1493,7 @@ const char* dda_last_error(const dda_ctx* ctx) {
 }
 
 int dda_create(const dda_problem* p, int precision, dda_ctx** out) {
+  NvtxRange range("dda create");
   if (!p || !out) {
     g_create_error = "null argument";
     return DDA_ERR_ARG;
@@ -2246,6 +2265,7 @@ extern "C" {
 
 int dda_far_field(dda_ctx* ctx, int nrhs, const double* pol, int64_t ndir, const double* dirs, double* out) {
   if (!ctx) return DDA_ERR_ARG;
+  NvtxRange range("dda far field");
   return guard(ctx, [&]() -> int {
     if (nrhs < 1 || nrhs > ctx->max_rhs || ndir < 1 || !dirs || !out) throw DdaError(DDA_ERR_ARG, "bad far-field arguments");
     if (ndir > (1LL << 31) / 4) throw DdaError(DDA_ERR_ARG, "too many directions");

@@ -8,6 +8,7 @@
 // incident fields from the front end, dda_create (D-matrix on the GPU),
 // dda_solve, the forward far field for the cross sections, dda_destroy.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <chrono>
@@ -90,6 +91,10 @@ void set_error(Done& d, const std::string& msg, int code) {
 
 // One request: the sequence of ddaMain for one target (DDA/DDAMain.cpp:611-771).
 void dda_server::run(Job& j, Done& d) {
+  nvtxRangePushA("dda served request");
+  struct Pop {
+    ~Pop() { nvtxRangePop(); }
+  } pop;
   const dda_serve_request& q = j.req;
   d.res.npol = q.npol;
   if (cudaSetDevice(device) != cudaSuccess) return set_error(d, "cudaSetDevice failed", DDA_ERR_CUDA);

@@ -10,7 +10,10 @@ gaussian:<lminus|davis3|barton5>,<waist>[,(x,y,z)]; extinction of a Gaussian bea
 from the dipoles' work on the incident field), --orient (alpha,beta,gamma): the
 particle orientation as ZYZ Euler angles in degrees, --pol (ldr, cm, ldr-avgpol),
 --geometry (sphere:R,m | cylinder:L,R,m | box:(X,Y,Z),m | load:file=<text dipole
-list> with -m), --grid-unit (default: the reference's rule, lambda / (10 max|m|)
+list, with -m and --grid-unit> | load:file=<HDF5 geometry file, or a directory
+holding Geometry.hdf5>: grid unit, refractive indices and orientation from the
+file unless --grid-unit, -m or --orient are given, DDAMain.cpp:156-235),
+--grid-unit (default: the reference's rule, lambda / (10 max|m|)
 and at most a 16th of every particle dimension, DDAMain.cpp:134-150), -m,
 --fft-grid, --epsilon (stop at 10^-epsilon), --maxiter, --iter, --ftype (float,
 double; plus mixed), --no-symmetry (both polarisations are always solved),
@@ -26,15 +29,18 @@ read, -prop, -orient, -beam, -pol, -eps, -iter, -maxiter, -ntheta, -scat_matr,
 -store_scat_grid, -store_beam, -store_int_field, -store_dip_pol, -dir,
 -dda-ftype), translated as DDA/AddaOptions.cpp:57-238 does.
 
-Output files are text (the reference's MATLAB-style HDF5 files are not
-written: no HDF5 library on these machines): CrossSec-Pol<n>.txt,
-MieCrossSec.txt (spheres), Far<Name>.txt (Jones matrices, the column layout
-of JonesCalculus::storeTxt) and Far<Name>.mueller.txt (Mueller matrices,
-MuellerCalculus::storeTxt), and with --store-dippol / --write-txt,
---store-intfield, --store-incbeam: DipPol-Pol<n>.txt, IntField-Pol<n>.txt,
-IncBeam-Pol<n>.txt (one dipole per line: grid x y z, then re, im of the x, y,
-z components).  --load-dip-pol and --load-start-dip-pol read DipPol-Pol<n>.txt
-files of that layout.
+Output files, as the reference writes them (DDAMain.cpp:265, 380-480): the
+MATLAB-style HDF5 files (dda_b200.matfile; dda_b200.datafiles for their
+structures) Geometry.hdf5, DipPol-Pol<n>.hdf5, CrossSec-Pol<n>.hdf5,
+MieCrossSec.hdf5 (spheres, plane wave), Far<Name>.hdf5 (Jones matrices) and
+Far<Name>.mueller.hdf5 (Mueller matrices), with --store-intfield
+IntField-Pol<n>.hdf5 and with --store-incbeam IncBeam-Pol<n>.hdf5; the cross
+sections also as CrossSec-Pol<n>.txt and MieCrossSec.txt; with --write-txt
+every file also in the reference's text layout (.txt: fields one dipole per
+line with coordinates in metres and |E|^2, JonesCalculus::storeTxt,
+MuellerCalculus::storeTxt, the geometry's dipole list).  --load-dip-pol and
+--load-start-dip-pol read DipPol-Pol<n>.hdf5, or DipPol-Pol<n>.txt where only
+that exists (DDA/Load.cpp:110-135).
 """
 import argparse
 import math
@@ -43,7 +49,7 @@ import sys
 
 import numpy as np
 
-from . import api, postprocess
+from . import api, datafiles, matfile, postprocess
 
 
 def parse_complex(s):
@@ -67,34 +73,70 @@ def default_grid_unit(lambda_m, dims_m, refr):
     return gu
 
 
+def load_hdf5_geometry(path, grid_unit, m_opts):
+    """--geometry load:file=<HDF5 file> (DDAMain.cpp:163-235): (geometry,
+    refractive indices, orientation from the file or None)."""
+    try:
+        f = datafiles.load_geometry(path)
+    except (ValueError, matfile.MatFileError) as e:
+        raise SystemExit("`%s': %s" % (path, e))
+    if grid_unit:
+        gu = api.parse_length(grid_unit)
+    elif "grid_unit" in f:
+        gu = f["grid_unit"]
+    else:
+        raise SystemExit("No --grid-unit option and no GridSpacing object in Geometry object in geometry file")
+    if m_opts:
+        refr = [parse_complex(m) for m in m_opts]
+    elif "refractive_indices" in f:
+        refr = [r[0] if r[0] == r[1] == r[2] else r for r in f["refractive_indices"]]
+    else:
+        raise SystemExit("No -m option given and no RefractiveIndices object in Geometry object in geometry file")
+    geom = api.Geometry.from_arrays(f["positions"], f["materials"], "%.17gm" % gu)
+    if "origin" in f:
+        # this library places the dipole box's centre at the origin
+        # (DipoleGeometry::moveToCenter); other grid origins are not supported
+        centred = -(np.asarray(geom.box, dtype=np.float64) - 1) / 2 * gu
+        if np.max(np.abs(f["origin"] + f["shift"] * gu - centred)) > 1e-6 * gu:
+            raise SystemExit("`%s': a GridOrigin other than the centre of the dipole box is not supported" % path)
+    return geom, refr, f.get("orientation")
+
+
 def build_geometry(spec, grid_unit, m_opts, lambda_m):
+    """(geometry, refractive indices, ("sphere", radius) for Mie or None,
+    orientation stored in a loaded HDF5 geometry or None)."""
     name, _, rest = spec.partition(":")
     name = name.strip()
     if name == "sphere":
         r, m = rest.split(",", 1)
         refr = [parse_complex(m)]
         gu = grid_unit or "%.17gm" % default_grid_unit(lambda_m, [2 * api.parse_length(r)], refr)
-        return api.Geometry.sphere(r, gu), refr, ("sphere", api.parse_length(r))
+        return api.Geometry.sphere(r, gu), refr, ("sphere", api.parse_length(r)), None
     if name == "cylinder":
         length, r, m = rest.split(",", 2)
         refr = [parse_complex(m)]
         dims = [api.parse_length(length), 2 * api.parse_length(r)]
         gu = grid_unit or "%.17gm" % default_grid_unit(lambda_m, dims, refr)
-        return api.Geometry.cylinder(length, r, gu), refr, None
+        return api.Geometry.cylinder(length, r, gu), refr, None, None
     if name == "box":
         i = rest.index(")")
         xyz = rest[:i + 1].strip("()").split(",")
         refr = [parse_complex(rest[i + 1:].lstrip(","))]
         dims = [api.parse_length(x) for x in xyz]
         gu = grid_unit or "%.17gm" % default_grid_unit(lambda_m, dims, refr)
-        return api.Geometry.box_shape(*xyz, gu), refr, None
+        return api.Geometry.box_shape(*xyz, gu), refr, None, None
     if name == "load":
         path = rest.split("=", 1)[1] if rest.startswith("file=") else rest
+        if os.path.isdir(path):
+            path = os.path.join(path, "Geometry.hdf5")
+        if matfile.is_hdf5(path):
+            geom, refr, orient = load_hdf5_geometry(path, grid_unit, m_opts)
+            return geom, refr, None, orient
         if not grid_unit:
             raise SystemExit("No --grid-unit option given but needed for loading text geometry file")
         if not m_opts:
             raise SystemExit("No -m option given for the loaded geometry")
-        return api.Geometry.load(path, grid_unit), [parse_complex(m) for m in m_opts], None
+        return api.Geometry.load(path, grid_unit), [parse_complex(m) for m in m_opts], None, None
     raise SystemExit("Unknown geometry option `%s'" % name)
 
 
@@ -230,34 +272,13 @@ def cc_vector(params, per_material):
     return v
 
 
-def write_field(path, params, vec):
-    """One dipole per line: grid x y z, then re, im of the x, y, z components."""
-    nv, nvs = params.nv, params.nvs
-    cols = [params.geometry.positions.astype(np.float64)]
-    for c in range(3):
-        cols += [vec[c * nvs:c * nvs + nv].real[:, None], vec[c * nvs:c * nvs + nv].imag[:, None]]
-    np.savetxt(path, np.hstack(cols), fmt=["%d"] * 3 + ["%.17g"] * 6,
-               header="x y z  Ex.r Ex.i Ey.r Ey.i Ez.r Ez.i")
-
-
-def read_field(path, params):
-    """Inverse of write_field; the dipoles must be those of the target."""
-    d = np.loadtxt(path, ndmin=2)
-    if d.shape != (params.nv, 9) or not np.array_equal(d[:, :3].astype(np.uint32), params.geometry.positions):
-        raise SystemExit("`%s' does not hold this target's dipoles" % path)
-    v = np.zeros(params.vec_size, dtype=np.complex128)
-    for c in range(3):
-        v[c * params.nvs:c * params.nvs + params.nv] = d[:, 3 + 2 * c] + 1j * d[:, 4 + 2 * c]
-    return v
-
-
 def parser():
     """The command line's options (the reference's names, DDA/Options.cpp:41-97)."""
     ap = argparse.ArgumentParser(prog="dda_b200.cli", description=__doc__.split("\n\n")[0])
     ap.add_argument("--lambda", dest="lam", default="%.17gum" % (2 * math.pi))
     ap.add_argument("--prop", default="(0,0,1)")
     ap.add_argument("--beam", default="plane")
-    ap.add_argument("--orient", default="(0,0,0)")
+    ap.add_argument("--orient")
     ap.add_argument("--pol", default="ldr", choices=["ldr", "cm", "ldr-avgpol"])
     ap.add_argument("--geometry", default="sphere:3.35103um,1.5")
     ap.add_argument("--grid-unit")
@@ -294,15 +315,34 @@ def main(argv=None):
 
     lambda_m = api.parse_length(a.lam)
     prop = tuple(parse_vector(a.prop))
-    orient = tuple(parse_vector(a.orient))
-    geom, refr, mie_geom = build_geometry(a.geometry, a.grid_unit, a.m, lambda_m)
+    geom, refr, mie_geom, file_orient = build_geometry(a.geometry, a.grid_unit, a.m, lambda_m)
+    # the orientation stored in a loaded geometry, unless --orient is given (DDAMain.cpp:221-225)
+    orient = tuple(parse_vector(a.orient)) if a.orient else (file_orient or (0.0, 0.0, 0.0))
     grid = tuple(int(x) for x in parse_vector(a.fft_grid, float))
     params = api.DDAParams(geom, refr, lambda_m, grid=grid if any(grid) else None)
     prec = {"float": "fp32", "double": "fp64", "mixed": "mixed"}[a.ftype]
+    ftype = "float" if a.ftype == "float" else "double"
     os.makedirs(a.output_dir, exist_ok=True)
     out = sys.stdout
     out.write("nv = %d, grid unit = %.6g um, box = %s, FFT grid = %s\n"
               % (params.nv, params.grid_unit * 1e6, params.box, params.grid))
+    odir = lambda name: os.path.join(a.output_dir, name)
+    txt = a.write_txt
+    pars = datafiles.parameters(params, a.geometry)
+    full_geometry = datafiles.dipole_list_geometry(params, orient, full=True)
+    datafiles.write(odir("Geometry"), {"Type": "Geometry", "Geometry": full_geometry},
+                    (lambda p: datafiles.geometry_txt(p, params)) if txt else None)  # DDAMain.cpp:265
+
+    def store_field(base, name, r, vec):  # createDDAFieldFile(...)->write, DDAMain.cpp:380-425
+        datafiles.write(odir(base), datafiles.field_file(params, pars, full_geometry, name, r + 1, vec, ftype),
+                        (lambda p: datafiles.field_txt(p, params, name, r + 1, vec, ftype)) if txt else None)
+
+    def load_pol(d):  # Load<ftype>::loadDipPol, DDA/Load.cpp:110-135
+        try:
+            return np.stack([datafiles.load_dip_pol(os.path.join(d, "DipPol-Pol%d" % (r + 1)), params)
+                             for r in range(2)])
+        except (OSError, ValueError, KeyError, matfile.MatFileError) as e:
+            raise SystemExit("cannot load dipole polarisations from %s: %s" % (d, e))
 
     mv = api.CudaMatVec(params, prec, max_rhs=2)
     ccs = []
@@ -319,16 +359,14 @@ def main(argv=None):
     einc = np.stack([beam.einc(params, prop, 1, orient=orient), beam.einc(params, prop, 2, orient=orient)])
     if a.store_incbeam:
         for r in range(2):
-            write_field(os.path.join(a.output_dir, "IncBeam-Pol%d.txt" % (r + 1)), params, einc[r])
+            store_field("IncBeam-Pol%d" % (r + 1), "IncidentBeam", r, einc[r])
     if a.load_dip_pol:  # DDA/DDAMain.cpp:374-378
-        pol = np.stack([read_field(os.path.join(a.load_dip_pol, "DipPol-Pol%d.txt" % (r + 1)), params)
-                        for r in range(2)])
+        pol = load_pol(a.load_dip_pol)
         out.write("Loaded dipole polarisations from %s\n" % a.load_dip_pol)
     else:
         start = None
         if a.load_start_dip_pol:  # DDA/DDAMain.cpp:391-394
-            start = np.stack([read_field(os.path.join(a.load_start_dip_pol, "DipPol-Pol%d.txt" % (r + 1)),
-                                         params) for r in range(2)])
+            start = load_pol(a.load_start_dip_pol)
         solver = api.CudaSolver(mv, a.iter, max_iter=a.maxiter)
         pol = solver.get_pol_vec(einc, 10.0 ** -a.epsilon, start=start)
         for r, (st, hist) in enumerate(zip(solver.last_stats, solver.last_history)):
@@ -336,11 +374,9 @@ def main(argv=None):
             for i, h in enumerate(hist):
                 out.write("RE_%d = %.10g\n" % (i + 1, h))
     for r in range(2):
-        if a.store_dippol or a.write_txt:
-            write_field(os.path.join(a.output_dir, "DipPol-Pol%d.txt" % (r + 1)), params, pol[r])
-        if a.store_intfield:  # internal field chi^-1 P, DDA/DDAMain.cpp:411-417
-            write_field(os.path.join(a.output_dir, "IntField-Pol%d.txt" % (r + 1)), params,
-                        cc_vector(params, ccs[r].chi_inv) * pol[r])
+        store_field("DipPol-Pol%d" % (r + 1), "DipolePolarization", r, pol[r])  # always, DDAMain.cpp:412
+        if a.store_intfield:  # internal field chi^-1 P, DDA/DDAMain.cpp:420-425
+            store_field("IntField-Pol%d" % (r + 1), "InternalField", r, cc_vector(params, ccs[r].chi_inv) * pol[r])
 
     pn = api.beam_frame(prop, orient)[0]  # forward direction in the particle frame
     ef = mv.far_field(pn[None, :], nrhs=2, pol=pol)[0]
@@ -352,16 +388,17 @@ def main(argv=None):
         out.write("Cext %s = %-25s Qext %s = %.10g\n" % (label, "%.10g um^2" % (cext * 1e12), label, qext))
         out.write("Cabs %s = %-25s Qabs %s = %.10g\n" % (label, "%.10g um^2" % (cabs * 1e12), label, qabs))
         out.write("Csca %s = %-25s Qsca %s = %.10g\n" % (label, "%.10g um^2" % (csca * 1e12), label, qsca))
-        with open(os.path.join(a.output_dir, "CrossSec-%s.txt" % label), "w") as f:
-            f.write("BeamPolarization = %d\nCext = %.17g\nQext = %.17g\nCabs = %.17g\nQabs = %.17g\n"
-                    "Csca = %.17g\nQsca = %.17g\n" % (r + 1, cext, qext, cabs, qabs, csca, qsca))
+        # createCrossSectionFile(...)->write (output, ".txt"), DDAMain.cpp:302
+        datafiles.write(odir("CrossSec-" + label), datafiles.cross_section_file(r + 1, cext, cabs, qext, qabs),
+                        lambda p: datafiles.cross_section_txt(p, cext, cabs, qext, qabs))
     if mie_geom is not None and beam.plane:  # DDA/DDAMain.cpp:431
         radius = mie_geom[1]
         x = 2 * math.pi * radius / lambda_m
         qe, qs, qa = postprocess.mie(x, refr[0])
         out.write("Mie solution:\nQext = %.10g Qabs = %.10g Qsca = %.10g\n" % (qe, qa, qs))
-        with open(os.path.join(a.output_dir, "MieCrossSec.txt"), "w") as f:
-            f.write("Qext = %.17g\nQabs = %.17g\nQsca = %.17g\n" % (qe, qa, qs))
+        area = math.pi * radius ** 2  # CrossSection::setCFromQ, DDAMain.cpp:454-456
+        datafiles.write(odir("MieCrossSec"), datafiles.cross_section_file(0, qe * area, qa * area, qe, qa),
+                        lambda p: datafiles.cross_section_txt(p, qe * area, qa * area, qe, qa))
     # far fields (DDA/DDAMain.cpp:318-353): the angle lists of all options,
     # each list computed once for both polarisations
     far = [postprocess.parse_far_field(x) for x in a.far_field]
@@ -378,18 +415,25 @@ def main(argv=None):
     if a.mueller_matrix_grid:
         far.append(("Grid", "0..180/91", "0..360/61", False, True, False))
     cache = {}
+    far_geometry = datafiles.dipole_list_geometry(params, orient, full=False)  # FarFieldCalc.cpp:173
+    freq = datafiles.SPEED_OF_LIGHT / lambda_m
     for name, ts, ps, want_j, want_m, no_phi in far:
         if (ts, ps) not in cache:
             theta, phi = postprocess.grid_angles(ts, ps)
             cache[(ts, ps)] = (theta, phi, postprocess.jones_far_field(mv, prop, theta, phi, pol=pol,
                                                                        orient=orient))
         theta, phi, jones = cache[(ts, ps)]
+        # FarFieldCalc<ftype>::store, DDA/FarFieldCalc.hpp:82-97
         if want_j:
-            postprocess.store_jones_txt(os.path.join(a.output_dir, "Far%s.txt" % name), theta, phi, jones,
-                                        store_phi=not no_phi)
+            datafiles.write(odir("Far" + name), datafiles.jones_file(pars, far_geometry, theta, phi, freq, jones, ftype),
+                            (lambda p: postprocess.store_jones_txt(p, theta, phi, jones, store_phi=not no_phi))
+                            if txt else None)
         if want_m:
-            postprocess.store_mueller_txt(os.path.join(a.output_dir, "Far%s.mueller.txt" % name), theta, phi,
-                                          postprocess.mueller(jones), no_phi=no_phi)
+            m = postprocess.mueller(jones)
+            datafiles.write(odir("Far%s.mueller" % name),
+                            datafiles.mueller_file(pars, far_geometry, theta, phi, freq, m, ftype),
+                            (lambda p: postprocess.store_mueller_txt(p, theta, phi, m, no_phi=no_phi))
+                            if txt else None)
     mv.close()
     return 0
 

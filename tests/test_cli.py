@@ -17,12 +17,12 @@ def test_default_grid_unit_rule():
 
 
 def test_geometry_strings_match_the_shapes():
-    g, refr, mie = cli.build_geometry("sphere:1um,1.5+0.1i", "0.1um", [], 1e-6)
+    g, refr, mie, _ = cli.build_geometry("sphere:1um,1.5+0.1i", "0.1um", [], 1e-6)
     ref = dda_b200.Geometry.sphere("1um", "0.1um")
     assert np.array_equal(g.positions, ref.positions) and refr == [1.5 + 0.1j] and mie[0] == "sphere"
-    g, refr, _ = cli.build_geometry("box:(1um,0.5um,0.3um),1.33", "0.1um", [], 1e-6)
+    g, refr, _, _ = cli.build_geometry("box:(1um,0.5um,0.3um),1.33", "0.1um", [], 1e-6)
     assert g.box == (10, 5, 3) and refr == [1.33 + 0j]
-    g, _, _ = cli.build_geometry("cylinder:1um,0.3um,2+0.5i", "0.1um", [], 1e-6)
+    g, _, _, _ = cli.build_geometry("cylinder:1um,0.3um,2+0.5i", "0.1um", [], 1e-6)
     assert g.nv > 0
 
 
@@ -47,14 +47,22 @@ def test_mueller_of_simple_jones_matrices():
 
 
 def test_field_files_round_trip(tmp_path):
+    from dda_b200 import datafiles as F
     g = dda_b200.Geometry.sphere("0.3um", "0.1um")
     p = dda_b200.DDAParams(g, [1.5 + 0.1j], "1um")
     rng = np.random.default_rng(2)
     v = np.zeros(p.vec_size, dtype=complex)
     for c in range(3):
         v[c * p.nvs:c * p.nvs + p.nv] = rng.normal(size=p.nv) + 1j * rng.normal(size=p.nv)
-    cli.write_field(str(tmp_path / "f.txt"), p, v)
-    assert np.array_equal(cli.read_field(str(tmp_path / "f.txt"), p), v)
+    base = str(tmp_path / "DipPol-Pol1")
+    F.write(base, F.field_file(p, F.parameters(p), F.dipole_list_geometry(p), "DipolePolarization", 1, v),
+            lambda path: F.field_txt(path, p, "DipolePolarization", 1, v))
+    assert np.array_equal(F.load_dip_pol(base, p), v)  # the .hdf5 file, bit for bit
+    assert np.max(np.abs(F.read_field_txt(base + ".txt", p) - v)) <= 1e-9 * np.max(np.abs(v))  # 10 digits
+    head = open(base + ".txt").readline().split()
+    assert head[:5] == ["#x", "y", "z", "|DipolePolarization-Pol1|^2", "DipolePolarization-Pol1.x.r"]
+    os.remove(base + ".hdf5")
+    assert np.max(np.abs(F.load_dip_pol(base, p) - v)) <= 1e-9 * np.max(np.abs(v))  # only the .txt left
 
 
 @pytest.mark.gpu
@@ -62,14 +70,24 @@ def test_cli_run_writes_cross_sections(tmp_path, capsys):
     rc = cli.main(["--geometry", "sphere:0.5um,1.5+0.1i", "--lambda", "1um", "--grid-unit", "0.1um",
                    "--epsilon", "8", "--efield-grid", "--efield", "--ntheta", "36", "--mueller-matrix-grid",
                    "--far-field", "Side=90,0..360/5,both", "--store-dippol", "--store-intfield",
-                   "--store-incbeam", "--output-dir", str(tmp_path)])
+                   "--store-incbeam", "--write-txt", "--output-dir", str(tmp_path)])
     assert rc == 0
     out = capsys.readouterr().out
     assert "Cext Pol1" in out and "Mie solution" in out
-    for f in ("CrossSec-Pol1.txt", "CrossSec-Pol2.txt", "MieCrossSec.txt", "FarGrid.txt", "FarGrid.mueller.txt",
-              "FarPlane.txt", "FarSide.txt", "FarSide.mueller.txt", "DipPol-Pol1.txt", "IntField-Pol2.txt",
-              "IncBeam-Pol1.txt"):
-        assert os.path.exists(tmp_path / f), f
+    for f in ("CrossSec-Pol1", "CrossSec-Pol2", "MieCrossSec", "FarGrid", "FarGrid.mueller", "FarPlane", "FarSide",
+              "FarSide.mueller", "DipPol-Pol1", "IntField-Pol2", "IncBeam-Pol1", "Geometry"):
+        for ext in (".txt", ".hdf5"):
+            assert os.path.exists(tmp_path / (f + ext)), f + ext
+    from dda_b200 import matfile
+    jf = matfile.load(str(tmp_path / "FarGrid.hdf5"))
+    assert jf["Type"] == "JonesFarField" and jf["JonesFarField"]["Data"].shape == (1, 91 * 61, 2, 2)
+    assert "DipolePositions" not in jf["Geometry"] and jf["Geometry"]["Type"] == "DDADipoleList"
+    txt = np.loadtxt(tmp_path / "FarGrid.txt")
+    d = jf["JonesFarField"]["Data"][0]  # [n][j][i] = J[i][j]; s1..s4 = S22, S11, S12, S21
+    assert np.allclose(txt[:, 2], d[:, 1, 1].real, rtol=1e-9, atol=1e-9 * np.abs(d).max())
+    assert np.allclose(txt[:, 6], d[:, 1, 0].real, rtol=1e-9, atol=1e-9 * np.abs(d).max())
+    mf = matfile.load(str(tmp_path / "FarGrid.mueller.hdf5"))
+    assert mf["MuellerFarField"]["Data"].shape == (1, 91 * 61, 4, 4)
     assert sum(1 for _ in open(tmp_path / "FarGrid.txt")) == 1 + 91 * 61
     assert sum(1 for _ in open(tmp_path / "FarPlane.txt")) == 1 + 36
     assert len(open(tmp_path / "FarPlane.txt").readline().split()) == 1 + 8  # no-phi
@@ -79,16 +97,22 @@ def test_cli_run_writes_cross_sections(tmp_path, capsys):
     rc = cli.main(["--geometry", "sphere:0.5um,1.5+0.1i", "--lambda", "1um", "--grid-unit", "0.1um",
                    "--load-dip-pol", str(tmp_path), "--efield-grid", "--output-dir", str(out2)])
     assert rc == 0 and "Loaded dipole polarisations" in capsys.readouterr().out
-    a = np.loadtxt(tmp_path / "FarGrid.txt")
-    b = np.loadtxt(out2 / "FarGrid.txt")
+    a = matfile.load(str(tmp_path / "FarGrid.hdf5"))["JonesFarField"]["Data"]
+    b = matfile.load(str(out2 / "FarGrid.hdf5"))["JonesFarField"]["Data"]
     assert np.allclose(a, b, rtol=1e-12, atol=0)
+    assert not os.path.exists(out2 / "FarGrid.txt")  # text only with --write-txt
     # a solve started from the stored polarisations ends at once
     rc = cli.main(["--geometry", "sphere:0.5um,1.5+0.1i", "--lambda", "1um", "--grid-unit", "0.1um",
                    "--epsilon", "8", "--load-start-dip-pol", str(tmp_path), "--output-dir", str(out2)])
     assert rc == 0
     its = [int(l.split(":")[1].split()[0]) for l in capsys.readouterr().out.splitlines() if l.startswith("Pol")]
     assert its and max(its) <= 2
-    vals = dict(l.split(" = ") for l in open(tmp_path / "CrossSec-Pol1.txt").read().splitlines())
+    cs = matfile.load(str(tmp_path / "CrossSec-Pol1.hdf5"))
+    assert cs["Type"] == "CrossSection" and cs["BeamPolarization"].tolist() == [1]
+    vals = {k: v[0] for k, v in cs["CrossSection"].items()}
+    txt = dict(l.split(" = ") for l in open(tmp_path / "CrossSec-Pol1.txt").read().splitlines())
+    assert list(txt) == ["Cext", "Qext", "Cabs", "Qabs", "Csca", "Qsca"]
+    assert float(txt["Cext"]) == pytest.approx(vals["Cext"], rel=1e-9)
     # the same problem through the API
     g = dda_b200.Geometry.sphere("0.5um", "0.1um")
     p = dda_b200.DDAParams(g, [1.5 + 0.1j], "1um")
@@ -102,6 +126,15 @@ def test_cli_run_writes_cross_sections(tmp_path, capsys):
     cext, cabs, _, _ = postprocess.cross_sections(p, cc, pol, ef, (0, 0, 1), 1)
     assert abs(float(vals["Cext"]) - cext) <= 1e-12 * abs(cext)
     assert abs(float(vals["Cabs"]) - cabs) <= 1e-12 * abs(cabs)
+    mv.close()
+    # the stored Geometry.hdf5 as the target: grid unit and refractive index from the file
+    out3 = tmp_path / "loaded"
+    rc = cli.main(["--geometry", "load:file=" + str(tmp_path), "--lambda", "1um", "--epsilon", "8",
+                   "--output-dir", str(out3)])
+    assert rc == 0 and "Mie solution" not in capsys.readouterr().out
+    cs3 = matfile.load(str(out3 / "CrossSec-Pol1.hdf5"))["CrossSection"]
+    assert abs(cs3["Cext"][0] - vals["Cext"]) <= 1e-10 * abs(vals["Cext"])
+    assert abs(cs3["Cabs"][0] - vals["Cabs"]) <= 1e-10 * abs(vals["Cabs"])
 
 
 def test_adda_options_translate():
@@ -142,6 +175,7 @@ def test_cli_adda_options_run(tmp_path, capsys):
     assert rc == 0
     out = capsys.readouterr().out
     assert "Cext Pol1" in out and "Mie solution" not in out
-    for f in ("CrossSec-Pol1.txt", "CrossSec-Pol2.txt", "FarPlane.txt", "FarPlane.mueller.txt", "DipPol-Pol1.txt"):
+    for f in ("CrossSec-Pol1.txt", "CrossSec-Pol2.txt", "FarPlane.txt", "FarPlane.mueller.txt", "DipPol-Pol1.txt",
+              "DipPol-Pol1.hdf5", "FarPlane.hdf5"):
         assert os.path.exists(tmp_path / f), f
     assert sum(1 for _ in open(tmp_path / "FarPlane.txt")) == 1 + 8

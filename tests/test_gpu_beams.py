@@ -53,8 +53,9 @@ def test_cli_gaussian_beam(tmp_path, capsys):
     assert "Cext Pol1" in out and "Mie solution" not in out  # Mie only for plane waves
     vals = dict(l.split(" = ") for l in open(tmp_path / "CrossSec-Pol1.txt").read().splitlines())
     assert float(vals["Cext"]) > float(vals["Cabs"]) > 0
-    assert os.path.exists(tmp_path / "IncBeam-Pol2.txt")
+    assert os.path.exists(tmp_path / "IncBeam-Pol2.hdf5")
     g = dda_b200.Geometry.sphere("0.5um", "0.1um")
     p = dda_b200.DDAParams(g, [1.5 + 0.1j], "1um")
-    stored = cli.read_field(str(tmp_path / "IncBeam-Pol2.txt"), p)
+    from dda_b200 import datafiles
+    stored = datafiles.load_dip_pol(str(tmp_path / "IncBeam-Pol2"), p)
     assert rel(stored, p.einc((0, 0, 1), 2, beam="gaussian:davis3,0.6um")) < 1e-12

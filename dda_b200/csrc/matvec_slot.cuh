@@ -21,7 +21,9 @@
 // The barrier (barrier.cluster arrive.release / wait.acquire) orders the
 // slot stores of one phase before the loads of the next across the
 // cluster's CTAs; the slot is read with ld.global.cg so no stale L1 line of
-// an earlier item is seen.  A CTA writes in phase Z only the columns it
+// an earlier item is seen.  The plane is read through the non-coherent path:
+// within the kernel only the cluster that owns an item reads or writes its
+// plane, and it reads a plane's elements before it writes them.  A CTA writes in phase Z only the columns it
 // reads back in phase Z', so consecutive items need no third barrier.
 #pragma once
 
@@ -43,6 +45,56 @@ template <typename T> struct SlotTc { static constexpr int value = sizeof(T) == 
 // Global loads a thread issues before it consumes the first of them (the
 // loads are volatile asm, kept in program order, so batching is explicit).
 template <typename T> struct SlotU { static constexpr int value = sizeof(T) == 4 ? 8 : 4; };
+
+// L2 eviction priorities (createpolicy, sm_80+).  The clusters' slots (one
+// [Gz][wp] buffer each, together up to about 100 MB) are written and read
+// back four times per item and are marked evict_last; the planes of xhat are
+// read once and written once per item and are marked evict_first, so that the
+// stream of planes does not push the slots out of the 126 MB L2.
+__device__ __forceinline__ uint64_t l2_evict_last() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t l2_evict_first() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+// slot: L2 only (ld/st .cg), with a cache policy
+__device__ __forceinline__ float2 slot_ld(const float2* a, uint64_t pol) {
+  float2 v;
+  asm volatile("ld.global.cg.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;" : "=f"(v.x), "=f"(v.y) : "l"(a), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ double2 slot_ld(const double2* a, uint64_t pol) {
+  double2 v;
+  asm volatile("ld.global.cg.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(v.x), "=d"(v.y) : "l"(a), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ void slot_st(float2* a, float2 v, uint64_t pol) {
+  asm volatile("st.global.cg.L2::cache_hint.v2.f32 [%0], {%1, %2}, %3;" ::"l"(a), "f"(v.x), "f"(v.y), "l"(pol));
+}
+__device__ __forceinline__ void slot_st(double2* a, double2 v, uint64_t pol) {
+  asm volatile("st.global.cg.L2::cache_hint.v2.f64 [%0], {%1, %2}, %3;" ::"l"(a), "d"(v.x), "d"(v.y), "l"(pol));
+}
+// plane: read-only within the kernel (non-coherent path) / plain store
+__device__ __forceinline__ float2 plane_ld(const float2* a, uint64_t pol) {
+  float2 v;
+  asm volatile("ld.global.nc.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;" : "=f"(v.x), "=f"(v.y) : "l"(a), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ double2 plane_ld(const double2* a, uint64_t pol) {
+  double2 v;
+  asm volatile("ld.global.nc.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(v.x), "=d"(v.y) : "l"(a), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ void plane_st(float2* a, float2 v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.v2.f32 [%0], {%1, %2}, %3;" ::"l"(a), "f"(v.x), "f"(v.y), "l"(pol));
+}
+__device__ __forceinline__ void plane_st(double2* a, double2 v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.v2.f64 [%0], {%1, %2}, %3;" ::"l"(a), "d"(v.x), "d"(v.y), "l"(pol));
+}
 
 // Shared memory (complex offsets): z twiddles [0, Gz), y twiddles
 // [Gz, Gz+Gy), then either the z tile [Gz][tc+1] or the row buffers
@@ -70,7 +122,8 @@ __host__ __device__ constexpr bool even_first_radix() {
 template <typename T, int NT, typename PZ, bool HALF = false>
 __device__ __forceinline__ void slot_cols_fwd(const typename C2<T>::t* __restrict__ plane,
                                               typename C2<T>::t* __restrict__ slot, const MvGeom& g,
-                                              const SlotGeom& sg, const FftPlanDev& pz, int c0) {
+                                              const SlotGeom& sg, const FftPlanDev& pz, int c0, uint64_t keep,
+                                              uint64_t stream) {
   typedef typename C2<T>::t T2;
   constexpr int TC = SlotTc<T>::value, P = TC + 1;
   const int toff = slot_work_off(g);
@@ -87,7 +140,7 @@ __device__ __forceinline__ void slot_cols_fwd(const typename C2<T>::t* __restric
         v[u] = czero<T2>();
         if (i < g.Gz * TC && z < g.bz && gl < W) {
           const int c = gl / g.by, y = gl - c * g.by;
-          v[u] = plane[c * nb + z * g.by + y];
+          v[u] = plane_ld(plane + c * nb + z * g.by + y, stream);
         }
       }
 #pragma unroll
@@ -113,7 +166,8 @@ __device__ __forceinline__ void slot_cols_fwd(const typename C2<T>::t* __restric
 #pragma unroll
         for (int m = 0; m < R; m++) {
           const int z = j + m * S0;
-          v[u][m] = (live && (HALF ? m < R / 2 : z < g.bz)) ? plane[c * nb + z * g.by + y] : czero<T2>();
+          v[u][m] = (live && (HALF ? m < R / 2 : z < g.bz)) ? plane_ld(plane + c * nb + z * g.by + y, stream)
+                                                             : czero<T2>();
         }
       }
 #pragma unroll
@@ -132,7 +186,7 @@ __device__ __forceinline__ void slot_cols_fwd(const typename C2<T>::t* __restric
   }
   for (int i = threadIdx.x; i < g.Gz * TC; i += NT) {
     const int kz = i / TC, l = i - kz * TC;
-    if (c0 + l < W) __stcg(slot + (size_t)kz * sg.wp + c0 + l, tile[kz * P + l]);
+    if (c0 + l < W) slot_st(slot + (size_t)kz * sg.wp + c0 + l, tile[kz * P + l], keep);
   }
   __syncthreads();
 }
@@ -141,7 +195,8 @@ __device__ __forceinline__ void slot_cols_fwd(const typename C2<T>::t* __restric
 template <typename T, int NT, typename PZ, bool HALF = false>
 __device__ __forceinline__ void slot_cols_inv(typename C2<T>::t* __restrict__ plane,
                                               const typename C2<T>::t* __restrict__ slot, const MvGeom& g,
-                                              const SlotGeom& sg, const FftPlanDev& pz, int c0) {
+                                              const SlotGeom& sg, const FftPlanDev& pz, int c0, uint64_t keep,
+                                              uint64_t stream) {
   typedef typename C2<T>::t T2;
   constexpr int TC = SlotTc<T>::value, P = TC + 1;
   const int toff = slot_work_off(g);
@@ -154,7 +209,7 @@ __device__ __forceinline__ void slot_cols_inv(typename C2<T>::t* __restrict__ pl
     for (int u = 0; u < U; u++) {
       const int i = i0 + u * NT + threadIdx.x;
       const int kz = i / TC, l = i - kz * TC;
-      v[u] = (i < g.Gz * TC && c0 + l < W) ? __ldcg(slot + (size_t)kz * sg.wp + c0 + l) : czero<T2>();
+      v[u] = (i < g.Gz * TC && c0 + l < W) ? slot_ld(slot + (size_t)kz * sg.wp + c0 + l, keep) : czero<T2>();
     }
 #pragma unroll
     for (int u = 0; u < U; u++) {
@@ -170,7 +225,7 @@ __device__ __forceinline__ void slot_cols_inv(typename C2<T>::t* __restrict__ pl
       const int z = i / TC, l = i - z * TC, gl = c0 + l;
       if (gl < W) {
         const int c = gl / g.by, y = gl - c * g.by;
-        plane[c * nb + z * g.by + y] = tile[z * P + l];
+        plane_st(plane + c * nb + z * g.by + y, tile[z * P + l], stream);
       }
     }
   } else {
@@ -187,7 +242,7 @@ __device__ __forceinline__ void slot_cols_inv(typename C2<T>::t* __restrict__ pl
 #pragma unroll
         for (int m = 0; m < R; m++) {
           const int z = j + m * S0;
-          if (HALF ? m < R / 2 : z < g.bz) plane[c * nb + z * g.by + y] = v[m];
+          if (HALF ? m < R / 2 : z < g.bz) plane_st(plane + c * nb + z * g.by + y, v[m], stream);
         }
       }
     }
@@ -200,7 +255,7 @@ __device__ __forceinline__ void slot_cols_inv(typename C2<T>::t* __restrict__ pl
 // stage, D-hat and the first inverse stage in registers (rows_dmul).
 template <typename T, int NT, typename PY, bool INV, bool HALF = false>
 __device__ __forceinline__ void slot_rows_stage0(typename C2<T>::t* __restrict__ slot, const MvGeom& g,
-                                                 const SlotGeom& sg, int kz0, int nr, int ro) {
+                                                 const SlotGeom& sg, int kz0, int nr, int ro, uint64_t keep) {
   typedef typename C2<T>::t T2;
   constexpr int R = PY::r[0], S0 = PY::N / R;
   T2* sm = smem_at<T>(0);
@@ -218,7 +273,7 @@ __device__ __forceinline__ void slot_rows_stage0(typename C2<T>::t* __restrict__
 #pragma unroll
         for (int m = 0; m < R; m++) {
           const int yy = j + m * S0;
-          v[u][m] = (it < total && (HALF ? m < R / 2 : yy < g.by)) ? __ldcg(srow + yy) : czero<T2>();
+          v[u][m] = (it < total && (HALF ? m < R / 2 : yy < g.by)) ? slot_ld(srow + yy, keep) : czero<T2>();
         }
       }
 #pragma unroll
@@ -245,7 +300,7 @@ __device__ __forceinline__ void slot_rows_stage0(typename C2<T>::t* __restrict__
 #pragma unroll
       for (int m = 0; m < R; m++) {
         const int yy = j + m * S0;
-        if (HALF ? m < R / 2 : yy < g.by) __stcg(srow + yy, v[m]);
+        if (HALF ? m < R / 2 : yy < g.by) slot_st(srow + yy, v[m], keep);
       }
     }
   }
@@ -255,7 +310,8 @@ __device__ __forceinline__ void slot_rows_stage0(typename C2<T>::t* __restrict__
 template <typename T, int NT, typename PY, typename PZ, bool HALF = false>
 __device__ __forceinline__ void slot_rows(typename C2<T>::t* __restrict__ slot,
                                           const typename C2<T>::t* __restrict__ dc, const MvGeom& g,
-                                          const SlotGeom& sg, const FftPlanDev& pyp, int kxf, int kz0, int nr) {
+                                          const SlotGeom& sg, const FftPlanDev& pyp, int kxf, int kz0, int nr,
+                                          uint64_t keep) {
   typedef typename C2<T>::t T2;
   const int ro = slot_work_off(g);
   if constexpr (std::is_void<PY>::value) {
@@ -269,7 +325,7 @@ __device__ __forceinline__ void slot_rows(typename C2<T>::t* __restrict__ slot,
         const int i = i0 + u * NT + threadIdx.x;
         const int rc = i / g.Gy, yy = i - rc * g.Gy;
         const int row = rc / 3, c = rc - 3 * row;
-        v[u] = (i < total && yy < g.by) ? __ldcg(slot + (size_t)(kz0 + row) * sg.wp + c * g.by + yy)
+        v[u] = (i < total && yy < g.by) ? slot_ld(slot + (size_t)(kz0 + row) * sg.wp + c * g.by + yy, keep)
                                         : czero<T2>();
       }
 #pragma unroll
@@ -287,15 +343,15 @@ __device__ __forceinline__ void slot_rows(typename C2<T>::t* __restrict__ slot,
     for (int i = threadIdx.x; i < nr * 3 * g.by; i += NT) {
       const int rc = i / g.by, yy = i - rc * g.by;
       const int row = rc / 3, c = rc - 3 * row;
-      __stcg(slot + (size_t)(kz0 + row) * sg.wp + c * g.by + yy, Rb[rc * sg.py + yy]);
+      slot_st(slot + (size_t)(kz0 + row) * sg.wp + c * g.by + yy, Rb[rc * sg.py + yy], keep);
     }
     __syncthreads();
   } else {
-    slot_rows_stage0<T, NT, PY, false, HALF>(slot, g, sg, kz0, nr, ro);
+    slot_rows_stage0<T, NT, PY, false, HALF>(slot, g, sg, kz0, nr, ro, keep);
     pstages<T, PY, false, NT, 1, PY::K - 1>(ro, 3 * nr, sg.py, 1, g.Gz, threadIdx.x);
     rows_dmul<T, NT, PY, PZ>(kz0, nr, ro, sg.py, dc, g, kxf, (int)threadIdx.x, 0);
     pstages<T, PY, true, NT, 1, PY::K - 1>(ro, 3 * nr, sg.py, 1, g.Gz, threadIdx.x);
-    slot_rows_stage0<T, NT, PY, true, HALF>(slot, g, sg, kz0, nr, ro);
+    slot_rows_stage0<T, NT, PY, true, HALF>(slot, g, sg, kz0, nr, ro, keep);
   }
 }
 
@@ -328,19 +384,20 @@ __global__ void __launch_bounds__(NT, 1) k_yz_slot(typename C2<T>::t* __restrict
   const int nchunks = (W + TC - 1) / TC;
   const int nbatches = (g.Gz + sg.nrw - 1) / sg.nrw;
   const int nitems = g.Gx * nrhs;
+  const uint64_t keep = l2_evict_last(), stream = l2_evict_first();
   for (int it = cid; it < nitems; it += ncl) {
     const int kx = (int)order[it / nrhs], b = it % nrhs;
     if (rhs_idle(st, b, mvskip)) continue;  // the same for every CTA of the cluster
     T2* plane = xhat + ((size_t)b * g.Gx + kx) * 3 * g.nlines;
-    for (int ch = rank; ch < nchunks; ch += cl) slot_cols_fwd<T, NT, PZ, HALF>(plane, slot, g, sg, pz, ch * TC);
+    for (int ch = rank; ch < nchunks; ch += cl) slot_cols_fwd<T, NT, PZ, HALF>(plane, slot, g, sg, pz, ch * TC, keep, stream);
     cluster.sync();
     const int kxf = g.fx[kx];
     for (int bt = rank; bt < nbatches; bt += cl) {
       const int kz0 = bt * sg.nrw;
-      slot_rows<T, NT, PY, PZ, HALF>(slot, dc, g, sg, pyp, kxf, kz0, min(sg.nrw, g.Gz - kz0));
+      slot_rows<T, NT, PY, PZ, HALF>(slot, dc, g, sg, pyp, kxf, kz0, min(sg.nrw, g.Gz - kz0), keep);
     }
     cluster.sync();
-    for (int ch = rank; ch < nchunks; ch += cl) slot_cols_inv<T, NT, PZ, HALF>(plane, slot, g, sg, pz, ch * TC);
+    for (int ch = rank; ch < nchunks; ch += cl) slot_cols_inv<T, NT, PZ, HALF>(plane, slot, g, sg, pz, ch * TC, keep, stream);
   }
 }
 

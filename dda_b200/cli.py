@@ -33,7 +33,8 @@ Output files, as the reference writes them (DDAMain.cpp:265, 380-480): the
 MATLAB-style HDF5 files (dda_b200.matfile; dda_b200.datafiles for their
 structures) Geometry.hdf5, DipPol-Pol<n>.hdf5, CrossSec-Pol<n>.hdf5,
 MieCrossSec.hdf5 (spheres, plane wave), Far<Name>.hdf5 (Jones matrices) and
-Far<Name>.mueller.hdf5 (Mueller matrices), with --store-intfield
+Far<Name>.mueller.hdf5 (Mueller matrices), for spheres under a plane wave also
+the Mie series' MieFar<Name>.hdf5 and MieFar<Name>.mueller.hdf5, with --store-intfield
 IntField-Pol<n>.hdf5 and with --store-incbeam IncBeam-Pol<n>.hdf5; the cross
 sections also as CrossSec-Pol<n>.txt and MieCrossSec.txt; with --write-txt
 every file also in the reference's text layout (.txt: fields one dipole per
@@ -417,6 +418,12 @@ def main(argv=None):
     cache = {}
     far_geometry = datafiles.dipole_list_geometry(params, orient, full=False)  # FarFieldCalc.cpp:173
     freq = datafiles.SPEED_OF_LIGHT / lambda_m
+    mie_far = mie_geom is not None and beam.plane  # the Mie far field beside it, DDAMain.cpp:476-489
+    if mie_far:
+        mie_pars = datafiles.mie_parameters(lambda_m, a.geometry, prop, a.beam,
+                                            [api.beam_pol(prop, 1)[0], api.beam_pol(prop, 2)[0]], " ".join(argv))
+        mie_g = datafiles.mie_geometry(mie_geom[1], refr[0])
+        mie_x = 2 * math.pi * mie_geom[1] / lambda_m
     for name, ts, ps, want_j, want_m, no_phi in far:
         if (ts, ps) not in cache:
             theta, phi = postprocess.grid_angles(ts, ps)
@@ -434,6 +441,18 @@ def main(argv=None):
                             datafiles.mueller_file(pars, far_geometry, theta, phi, freq, m, ftype),
                             (lambda p: postprocess.store_mueller_txt(p, theta, phi, m, no_phi=no_phi))
                             if txt else None)
+        if mie_far:  # FarFieldCalc<ldouble>::store (outputDir / "MieFar", ...): double precision files
+            mj = postprocess.mie_jones(mie_x, refr[0], theta, params.wave_num)
+            if want_j:
+                datafiles.write(odir("MieFar" + name), datafiles.jones_file(mie_pars, mie_g, theta, phi, freq, mj),
+                                (lambda p: postprocess.store_jones_txt(p, theta, phi, mj, store_phi=not no_phi))
+                                if txt else None)
+            if want_m:
+                mm = postprocess.mueller(mj)
+                datafiles.write(odir("MieFar%s.mueller" % name),
+                                datafiles.mueller_file(mie_pars, mie_g, theta, phi, freq, mm),
+                                (lambda p: postprocess.store_mueller_txt(p, theta, phi, mm, no_phi=no_phi))
+                                if txt else None)
     mv.close()
     return 0
 

@@ -161,6 +161,20 @@ def mueller_file(pars, geometry, theta, phi, frequency, mueller, ftype="double")
                                 "Data": np.ascontiguousarray(data)}}
 
 
+def mie_parameters(wavelength, geometry_string, prop, beam_string, pols, cmd_line=""):
+    """Parameters<MieParameters> of the Mie far-field files
+    (createParametersMie, EMSim/DataFilesUtil.cpp:29-47; DDAMain.cpp:438-443)."""
+    return {"Method": "Mie", "MethodParameters": {"Frequency": np.array([SPEED_OF_LIGHT / wavelength])},
+            "GeometryString": geometry_string, "CmdLine": cmd_line, "RefractiveIndexMedium": np.ones(3),
+            "PropagationVector": np.asarray(prop, dtype=np.float64), "BeamString": beam_string,
+            "Polarizations": np.asarray(pols, dtype=np.float64).reshape(-1, 3)}
+
+
+def mie_geometry(radius, m):
+    """MieGeometry (EMSim/DataFiles.hpp:144-157)."""
+    return {"Type": "Mie", "Radius": np.array([float(radius)]), "RefractiveIndex": np.full(3, complex(m))}
+
+
 def geometry_file(params, orient=None):
     """DDADipoleListGeometryFile (DDA/DataFilesDDAUtil.cpp:88-93)."""
     return {"Type": "Geometry", "Geometry": dipole_list_geometry(params, orient, True)}

@@ -148,6 +148,57 @@ def mie(x, m):
     return qext, qsca, qext - qsca
 
 
+def mie_amplitudes(x, m, theta):
+    """Scattering amplitudes S1(theta), S2(theta) of the sphere of `mie` (the
+    Bohren-Huffman series with the angle functions pi_n, tau_n of
+    mu = cos theta, as EMSim/Mie.cpp:41-174 evaluates them; phi does not
+    enter)."""
+    m = complex(m)
+    mx = x * m
+    mu = np.cos(np.asarray(theta, dtype=np.float64))
+    xstop = x + 4 * x ** (1.0 / 3) + 2
+    nstop = int(xstop)
+    nmx = int(max(xstop, abs(mx)) + 15)
+    d = np.zeros(nmx, dtype=np.complex128)
+    for i in range(nmx - 1, 0, -1):
+        d[i - 1] = (i + 1) / mx - 1.0 / (d[i] + (i + 1) / mx)
+    psi0, psi1 = math.cos(x), math.sin(x)
+    chi0, chi1 = -math.sin(x), math.cos(x)
+    xi1 = complex(psi1, -chi1)
+    s1 = np.zeros(mu.shape, dtype=np.complex128)
+    s2 = np.zeros(mu.shape, dtype=np.complex128)
+    pi0, pi1 = np.zeros(mu.shape), np.ones(mu.shape)
+    for n in range(nstop):
+        rn = n + 1.0
+        psi = (2 * rn - 1) * psi1 / x - psi0
+        chi = (2 * rn - 1) * chi1 / x - chi0
+        xi = complex(psi, -chi)
+        a = ((d[n] / m + rn / x) * psi - psi1) / ((d[n] / m + rn / x) * xi - xi1)
+        b = ((m * d[n] + rn / x) * psi - psi1) / ((m * d[n] + rn / x) * xi - xi1)
+        fn = (2 * rn + 1) / (rn * (rn + 1))
+        pi = pi1
+        tau = rn * mu * pi - (rn + 1) * pi0
+        s1 += fn * (a * pi + b * tau)
+        s2 += fn * (a * tau + b * pi)
+        pi1 = ((2 * rn + 1) * mu * pi - (rn + 1) * pi0) / rn
+        pi0 = pi
+        psi0, psi1 = psi1, psi
+        chi0, chi1 = chi1, chi
+        xi1 = complex(psi1, -chi1)
+    return s1, s2
+
+
+def mie_jones(x, m, theta, wave_num):
+    """Jones matrices [n][2][2] of the Mie far field on the angles `theta`:
+    diag(S2, S1) times -1/k, the far-field factor the reference passes
+    (DDAMain.cpp:484, EMSim/Mie.cpp:165-172)."""
+    s1, s2 = mie_amplitudes(x, m, theta)
+    j = np.zeros((len(s1), 2, 2), dtype=np.complex128)
+    j[:, 0, 0] = -s2 / wave_num
+    j[:, 1, 1] = -s1 / wave_num
+    return j
+
+
 def mueller(j):
     """Mueller matrices [count][4][4] from Jones matrices [count][2][2]
     (MuellerCalculus::computeMuellerMatrix, EMSim/MuellerCalculus.cpp:36-60)."""

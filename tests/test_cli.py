@@ -88,6 +88,19 @@ def test_cli_run_writes_cross_sections(tmp_path, capsys):
     assert np.allclose(txt[:, 6], d[:, 1, 0].real, rtol=1e-9, atol=1e-9 * np.abs(d).max())
     mf = matfile.load(str(tmp_path / "FarGrid.mueller.hdf5"))
     assert mf["MuellerFarField"]["Data"].shape == (1, 91 * 61, 4, 4)
+    # the Mie series' far field beside it (MieFar*, DDAMain.cpp:476-489): the DDA sphere's
+    # Jones matrices within the discretisation error of |m| k d = 0.95
+    mie = matfile.load(str(tmp_path / "MieFarGrid.hdf5"))
+    assert mie["Geometry"]["Type"] == "Mie" and mie["Geometry"]["Radius"][0] == pytest.approx(0.5e-6)
+    assert np.allclose(mie["Geometry"]["RefractiveIndex"], 1.5 + 0.1j)
+    assert mie["Parameters"]["Method"] == "Mie" and mie["Parameters"]["Polarizations"].shape == (2, 3)
+    dm = mie["JonesFarField"]["Data"][0]
+    err = np.linalg.norm(d - dm) / np.linalg.norm(dm)
+    with capsys.disabled():
+        print("DDA vs Mie Jones, relative 2-norm difference: %.4f" % err)
+    assert err < 0.1
+    for f in ("MieFarGrid.txt", "MieFarGrid.mueller.hdf5", "MieFarPlane.hdf5", "MieFarSide.mueller.txt"):
+        assert os.path.exists(tmp_path / f), f
     assert sum(1 for _ in open(tmp_path / "FarGrid.txt")) == 1 + 91 * 61
     assert sum(1 for _ in open(tmp_path / "FarPlane.txt")) == 1 + 36
     assert len(open(tmp_path / "FarPlane.txt").readline().split()) == 1 + 8  # no-phi

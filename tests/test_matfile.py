@@ -231,3 +231,24 @@ def test_cross_section_file(tmp_path):
         "Cext": [2e-12], "Cabs": [0.5e-12], "Csca": [1.5e-12], "Qext": [1.25], "Qabs": [0.3125], "Qsca": [0.9375]}
     assert open(base + ".txt").read() == ("Cext = 2e-12\nQext = 1.25\nCabs = 5e-13\nQabs = 0.3125\n"
                                           "Csca = 1.5e-12\nQsca = 0.9375\n")
+
+
+def test_mie_amplitudes_identities():
+    """S1, S2 of the Bohren-Huffman series: equal forward with 4/x^2 Re S(0) =
+    Qext, opposite backward, |S1|^2 + |S2|^2 integrating to Qsca, and the
+    Rayleigh limit S1 = -i x^3 (m^2-1)/(m^2+2), S2 = S1 cos theta."""
+    from dda_b200 import postprocess as P
+    x, m = 3.7, 1.5 + 0.1j
+    qe, qs, _ = P.mie(x, m)
+    s1, s2 = P.mie_amplitudes(x, m, np.array([0.0, math.pi]))
+    assert abs(s1[0] - s2[0]) <= 1e-12 * abs(s1[0]) and abs(s1[1] + s2[1]) <= 1e-12 * abs(s1[1])
+    assert 4 / x ** 2 * s1[0].real == pytest.approx(qe, rel=1e-12)
+    mu, w = np.polynomial.legendre.leggauss(200)
+    s1, s2 = P.mie_amplitudes(x, m, np.arccos(mu))
+    assert np.sum(w * (np.abs(s1) ** 2 + np.abs(s2) ** 2)) / x ** 2 == pytest.approx(qs, rel=1e-10)
+    th = np.linspace(0, math.pi, 7)
+    s1, s2 = P.mie_amplitudes(0.01, m, th)
+    ray = -1j * 0.01 ** 3 * (m * m - 1) / (m * m + 2)
+    assert np.allclose(s1, ray, rtol=1e-3) and np.allclose(s2, ray * np.cos(th), rtol=1e-3, atol=1e-3 * abs(ray))
+    j = P.mie_jones(x, m, th, 2.0)
+    assert np.array_equal(j[:, 0, 1], np.zeros(7)) and np.allclose(j[:, 1, 1], -P.mie_amplitudes(x, m, th)[0] / 2)

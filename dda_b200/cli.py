@@ -22,7 +22,15 @@ double; plus mixed), --no-symmetry (both polarisations are always solved),
 --efield-grid and --mueller-matrix-grid (theta 0..180/91, phi 0..360/61),
 --load-dip-pol DIR (skip the solve), --load-start-dip-pol DIR (start values),
 --store-dippol, --store-intfield, --store-incbeam, --write-txt, --profiling-run
-(per-stage matvec times instead of a solve), --output-dir.
+(per-stage matvec times instead of a solve), --verbose (the couple constants and the
+beam), --mem-info (the context's device memory), --gamma (stored in the output
+files' parameters), --periodicity-1/-2 (only (0,0,0): periodic targets are not
+supported), --device (the CUDA device index; auto = 0), --cpu, --opencl, --sync,
+--dmatrix-host, --opencl-fft (accepted; the solve runs on the GPU with CUDA).
+Output directory (DDAMain.cpp:683-706, EMSim/OutputDirectory.cpp): --output-dir,
+or else a new output_<n> under --output-parent-dir (default ./output) numbered by
+its counter file, tagged "running" while the run lasts and with --tag names and
+"latest" at its end (symbolic links beside it); stdout is copied to its log file.
 
 --adda-options, followed by options in ADDA's syntax (-dpl, -lambda, -m, -shape
 read, -prop, -orient, -beam, -pol, -eps, -iter, -maxiter, -ntheta, -scat_matr,
@@ -303,8 +311,67 @@ def parser():
     ap.add_argument("--store-incbeam", action="store_true")
     ap.add_argument("--write-txt", action="store_true")
     ap.add_argument("--profiling-run", action="store_true")
-    ap.add_argument("--output-dir", default=".")
+    ap.add_argument("--output-dir")
+    ap.add_argument("--output-parent-dir", action="append", default=[])
+    ap.add_argument("--tag", action="append", default=[])
+    ap.add_argument("--verbose", action="store_true")
+    ap.add_argument("--mem-info", action="store_true")
+    ap.add_argument("--gamma", type=float, default=0.001)
+    ap.add_argument("--periodicity-1", dest="periodicity1", default="(0,0,0)")
+    ap.add_argument("--periodicity-2", dest="periodicity2", default="(0,0,0)")
+    ap.add_argument("--device", default="auto")
+    for flag in ("--cpu", "--opencl", "--sync", "--dmatrix-host"):
+        ap.add_argument(flag, action="store_true")
+    ap.add_argument("--opencl-fft")
     return ap
+
+
+def output_directory(parent):
+    """A new directory output_<n> under `parent` (EMSim::OutputDirectory,
+    EMSim/OutputDirectory.cpp:46-116): n is read from parent/counter and the
+    counter advanced under a lock on parent/counter.lck."""
+    import fcntl
+    os.makedirs(parent, exist_ok=True)
+    counter = os.path.join(parent, "counter")
+    with open(counter + ".lck", "a") as lock:
+        fcntl.flock(lock, fcntl.LOCK_EX)
+        try:
+            with open(counter) as f:
+                n = int(f.read().split()[0])
+        except (OSError, ValueError, IndexError):
+            n = 0
+        with open(counter + ".new", "w") as f:
+            f.write("%d\n" % (n + 1))
+        os.replace(counter + ".new", counter)
+    path = os.path.join(parent, "output_%d" % n)
+    os.mkdir(path)
+    return path
+
+
+def create_tag(path, tag):
+    """A symbolic link `tag` beside the output directory `path`
+    (OutputDirectory::createTag, EMSim/OutputDirectory.cpp:118-128)."""
+    if not tag or "/" in tag or tag[0] == "." or tag.startswith("output_"):
+        raise SystemExit("Invalid tag `%s'" % tag)
+    link = os.path.join(os.path.dirname(path), tag)
+    if os.path.lexists(link):
+        os.unlink(link)
+    os.symlink(os.path.basename(path), link)
+
+
+class _Tee:
+    """stdout copied to the output directory's log file (DDAMain.cpp:711-712)."""
+
+    def __init__(self, *streams):
+        self.streams = streams
+
+    def write(self, text):
+        for st in self.streams:
+            st.write(text)
+
+    def flush(self):
+        for st in self.streams:
+            st.flush()
 
 
 def main(argv=None):
@@ -313,7 +380,36 @@ def main(argv=None):
         k = argv.index("--adda-options")
         argv = argv[:k] + translate_adda(argv[k + 1:])
     a = parser().parse_args(argv)
+    if a.cpu and a.opencl:  # DDAMain.cpp:709
+        raise SystemExit("--cpu and --opencl exclude each other")
+    if a.output_dir and a.tag:
+        raise SystemExit("Error: Got both --output-dir and --tag")
+    for per in (a.periodicity1, a.periodicity2):
+        if any(api.parse_length(x.strip()) != 0 for x in per.strip().strip("()").split(",")):
+            raise SystemExit("periodic targets (--periodicity-1, --periodicity-2) are not supported")
+    device = 0 if a.device == "auto" else int(a.device)
+    if a.output_dir:
+        out_dir, tagged = a.output_dir, None
+        os.makedirs(out_dir, exist_ok=True)
+    else:
+        tagged = out_dir = output_directory(a.output_parent_dir[-1] if a.output_parent_dir else "output")
+        create_tag(tagged, "running")
+    a.output_dir = out_dir
+    log = open(os.path.join(out_dir, "log"), "w")
+    try:
+        rc = _run(a, argv, _Tee(sys.stdout, log), device)
+    finally:
+        log.close()
+    if tagged:
+        for t in a.tag:
+            create_tag(tagged, t)
+        create_tag(tagged, "latest")
+    return rc
 
+
+def _run(a, argv, out, device):
+    out.write("Output directory: %s\n" % os.path.abspath(a.output_dir))
+    out.write("Command: %s\n" % " ".join(argv))
     lambda_m = api.parse_length(a.lam)
     prop = tuple(parse_vector(a.prop))
     geom, refr, mie_geom, file_orient = build_geometry(a.geometry, a.grid_unit, a.m, lambda_m)
@@ -323,13 +419,13 @@ def main(argv=None):
     params = api.DDAParams(geom, refr, lambda_m, grid=grid if any(grid) else None)
     prec = {"float": "fp32", "double": "fp64", "mixed": "mixed"}[a.ftype]
     ftype = "float" if a.ftype == "float" else "double"
-    os.makedirs(a.output_dir, exist_ok=True)
-    out = sys.stdout
+    out.write("Particle grid: (%d, %d, %d), FFT grid: (%d, %d, %d)\n" % (tuple(params.box) + tuple(params.grid)))
+    out.write("Total dipoles: %d, Non-void dipoles: %d\n" % (int(np.prod(params.box)), params.nv))
     out.write("nv = %d, grid unit = %.6g um, box = %s, FFT grid = %s\n"
               % (params.nv, params.grid_unit * 1e6, params.box, params.grid))
     odir = lambda name: os.path.join(a.output_dir, name)
     txt = a.write_txt
-    pars = datafiles.parameters(params, a.geometry)
+    pars = datafiles.parameters(params, a.geometry, a.gamma)
     full_geometry = datafiles.dipole_list_geometry(params, orient, full=True)
     datafiles.write(odir("Geometry"), {"Type": "Geometry", "Geometry": full_geometry},
                     (lambda p: datafiles.geometry_txt(p, params)) if txt else None)  # DDAMain.cpp:265
@@ -345,11 +441,20 @@ def main(argv=None):
         except (OSError, ValueError, KeyError, matfile.MatFileError) as e:
             raise SystemExit("cannot load dipole polarisations from %s: %s" % (d, e))
 
-    mv = api.CudaMatVec(params, prec, max_rhs=2)
+    mv = api.CudaMatVec(params, prec, max_rhs=2, device=device)
     ccs = []
     for r, pol in enumerate((1, 2)):
         ccs.append(api.CoupleConstants(params, prop, pol, a.pol, orient=orient))
         mv.set_couple_constants(ccs[-1], rhs=r)
+    if a.verbose:  # DDAParams::dump (DDAMain.cpp:272-273)
+        out.write("wavelength = %.10g m, k d = %.10g, beam = %s, prop = %s, orient = %s\n"
+                  % (lambda_m, params.kd, a.beam, prop, orient))
+        for r in range(2):
+            out.write("Pol%d couple constants sqrt(cc) = %s\n" % (r + 1, np.asarray(ccs[r].cc_sqrt).tolist()))
+    if a.mem_info:  # DDAMain.cpp:578
+        lay = mv.layout()
+        out.write("GPU memory of the context: %.1f MB (y/z path %s)\n"
+                  % (lay["device_bytes"] / 1e6, lay["yz_path"]))
     if a.profiling_run:  # IterativeSolverBase::profilingRun, DDA/IterativeSolverBase.cpp:105-136
         ms = mv.profile(nrhs=2, reps=5)
         out.write("matvec (2 rhs): %.3f ms  [x forward %.3f, y/z %.3f, x inverse %.3f]\n"

@@ -193,3 +193,44 @@ def test_cli_adda_options_run(tmp_path, capsys):
               "DipPol-Pol1.hdf5", "FarPlane.hdf5"):
         assert os.path.exists(tmp_path / f), f
     assert sum(1 for _ in open(tmp_path / "FarPlane.txt")) == 1 + 8
+
+
+def test_output_directories_and_tags(tmp_path):
+    # EMSim/OutputDirectory.cpp: output_<n> numbered by the counter file, tags as links beside it
+    parent = str(tmp_path / "out")
+    a = cli.output_directory(parent)
+    b = cli.output_directory(parent)
+    assert os.path.basename(a) == "output_0" and os.path.basename(b) == "output_1"
+    assert open(os.path.join(parent, "counter")).read().split() == ["2"]
+    cli.create_tag(a, "running")
+    cli.create_tag(b, "running")  # moves to the newer directory
+    assert os.readlink(os.path.join(parent, "running")) == "output_1"
+    for bad in ("", "a/b", ".hidden", "output_7"):
+        with pytest.raises(SystemExit):
+            cli.create_tag(a, bad)
+
+
+def test_option_errors_before_any_gpu_work(tmp_path):
+    base = ["--geometry", "sphere:0.5um,1.5", "--output-dir", str(tmp_path)]
+    for extra, msg in ((["--periodicity-1", "(1um,0,0)"], "periodic"), (["--cpu", "--opencl"], "exclude"),
+                       (["--tag", "x"], "both --output-dir and --tag")):
+        with pytest.raises(SystemExit, match=msg):
+            cli.main(base + extra)
+    a = cli.parser().parse_args(["--cpu", "--sync", "--dmatrix-host", "--opencl-fft", "apple", "--device", "0",
+                                 "--gamma", "0.01", "--verbose", "--mem-info", "--periodicity-2", "(0,0,0)"])
+    assert a.cpu and a.gamma == 0.01 and a.device == "0" and a.output_dir is None
+
+
+@pytest.mark.gpu
+def test_cli_output_parent_dir_tags_and_log(tmp_path, capsys):
+    rc = cli.main(["--geometry", "sphere:0.3um,1.5", "--lambda", "1um", "--grid-unit", "0.1um",
+                   "--output-parent-dir", str(tmp_path), "--tag", "mine", "--verbose", "--mem-info"])
+    assert rc == 0
+    out = capsys.readouterr().out
+    assert "couple constants" in out and "GPU memory of the context" in out and "Particle grid" in out
+    d = tmp_path / "output_0"
+    log = open(d / "log").read()
+    assert log.startswith("Output directory: ") and "Command: " in log and "Cext Pol1" in log
+    for tag in ("running", "mine", "latest"):
+        assert os.readlink(tmp_path / tag) == "output_0"
+    assert os.path.exists(d / "DipPol-Pol1.hdf5") and os.path.exists(d / "CrossSec-Pol2.txt")

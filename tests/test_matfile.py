@@ -150,6 +150,8 @@ def test_geometry_file_loads_through_the_command_line(tmp_path):
     assert g["Type"] == "Geometry" and g["Geometry"]["Size"].tolist() == [3, 3, 3]
     assert g["Geometry"]["DipolePositions"].dtype == np.uint32 and g["Geometry"]["RefractiveIndices"].shape == (2, 3)
     assert open(base + ".txt").read().splitlines()[:3] == ["#box size: 3x3x3", "Nmat=2", "0 0 0 1"]
+    back = dda_b200.Geometry.load(base + ".txt", "0.1um")  # the text loader reads it (DDA/Load.cpp:37-69)
+    assert np.array_equal(back.positions, p.geometry.positions) and np.array_equal(back.materials, p.geometry.materials)
     # no --grid-unit, no -m, no --orient: all three from the file (DDAMain.cpp:170-230)
     geom, refr, mie, orient = cli.build_geometry("load:file=" + str(tmp_path), None, [], 1e-6)
     assert mie is None and np.array_equal(geom.positions, p.geometry.positions)

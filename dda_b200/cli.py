@@ -452,7 +452,7 @@ def _run(a, argv, out, device):
         for r in range(2):
             out.write("Pol%d couple constants sqrt(cc) = %s\n" % (r + 1, np.asarray(ccs[r].cc_sqrt).tolist()))
     if a.mem_info:  # DDAMain.cpp:578
-        lay = mv.layout()
+        lay = mv.layout
         out.write("GPU memory of the context: %.1f MB (y/z path %s)\n"
                   % (lay["device_bytes"] / 1e6, lay["yz_path"]))
     if a.profiling_run:  # IterativeSolverBase::profilingRun, DDA/IterativeSolverBase.cpp:105-136

@@ -425,6 +425,8 @@ class _Reader:
             val = np.frombuffer(b, dtype=dt, count=n, offset=p)
             if dt.kind == "S":
                 out[name] = b"".join(val.tolist()).split(b"\0")[0].decode("latin-1")
+            elif shp is None:
+                out[name] = val.copy()
             elif shp == ():
                 out[name] = val[0].item()
             else:

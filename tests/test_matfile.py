@@ -254,3 +254,54 @@ def test_mie_amplitudes_identities():
     assert np.allclose(s1, ray, rtol=1e-3) and np.allclose(s2, ray * np.cos(th), rtol=1e-3, atol=1e-3 * abs(ray))
     j = P.mie_jones(x, m, th, 2.0)
     assert np.array_equal(j[:, 0, 1], np.zeros(7)) and np.allclose(j[:, 1, 1], -P.mie_amplitudes(x, m, th)[0] / 2)
+
+
+def test_newer_attribute_and_dataspace_versions():
+    """Attribute messages 2 and 3 (no padding; 3 with a character set byte)
+    and version 2 dataspaces, scalar and null, as libhdf5 writes them with its
+    newer format options."""
+    r = M._Reader.__new__(M._Reader)
+    i32 = struct.pack("<BBBBIHH", 0x10, 0x08, 0, 0, 4, 0, 32)
+    s6 = struct.pack("<BBBBI", 0x13, 0, 0, 0, 6)
+    scalar, null = struct.pack("<BBBB", 2, 0, 0, 0), struct.pack("<BBBB", 2, 0, 0, 2)
+
+    def attr(ver, name, dt, space, data):
+        nm = name.encode() + b"\0"
+        head = struct.pack("<BBHHH", ver, 0, len(nm), len(dt), len(space)) + (b"\0" if ver == 3 else b"")
+        return (0x0C, head + nm + dt + space + data, 0)
+
+    got = r.attributes([attr(2, "MATLAB_class", s6, scalar, b"double"),
+                        attr(3, "MATLAB_int_decode", i32, scalar, struct.pack("<i", 2)),
+                        attr(2, "MATLAB_empty", struct.pack("<BBBBIHH", 0x10, 0, 0, 0, 1, 0, 8), null, b"")])
+    assert got["MATLAB_class"] == "double" and got["MATLAB_int_decode"] == 2
+    assert got["MATLAB_empty"].size == 0
+
+
+def test_version_2_object_headers_and_compact_groups():
+    """Superblock 2, version 2 object headers (OHDR) and a group stored as
+    link messages, the structures of libhdf5's newer format: the reader walks
+    them (it does not check their checksums)."""
+    def ohdr(msgs):
+        body = b"".join(struct.pack("<BHB", t, len(d), 0) + d for t, d in msgs)
+        assert len(body) < 256
+        return b"OHDR" + struct.pack("<BBB", 2, 0, len(body)) + body + b"\0" * 4
+
+    data = np.arange(6, dtype="<f8").reshape(2, 3)
+    buf = bytearray(48)  # superblock
+    raw_at = len(buf)
+    buf += data.tobytes()
+    dt = struct.pack("<BBBBIHHBBBBI", 0x11, 0x20, 63, 0, 8, 0, 64, 52, 11, 0, 52, 1023)
+    space = struct.pack("<BBBB", 2, 2, 0, 1) + struct.pack("<QQ", 2, 3)
+    s6 = struct.pack("<BBBBI", 0x13, 0, 0, 0, 6)
+    nm = b"MATLAB_class\0"
+    attr = struct.pack("<BBHHH", 3, 0, len(nm), len(s6), 4) + b"\0" + nm + s6 + struct.pack("<BBBB", 2, 0, 0, 0) + b"double"
+    ds_at = len(buf)
+    buf += ohdr([(0x01, space), (0x03, dt), (0x08, struct.pack("<BBQQ", 3, 1, raw_at, data.nbytes)), (0x0C, attr)])
+    link = struct.pack("<BB", 1, 0) + struct.pack("<B", 1) + b"x" + struct.pack("<Q", ds_at)
+    root_at = len(buf)
+    buf += ohdr([(0x06, link)])
+    buf[:48] = M.SIGNATURE + struct.pack("<BBBB", 2, 8, 8, 0) + struct.pack("<QQQQ", 0, M.UNDEF, len(buf), root_at) \
+        + b"\0" * 4
+    v = M.loads(bytes(buf))
+    assert list(v) == ["x"] and np.array_equal(v["x"], data)
+    assert M._Reader(bytes(buf)).attrs_of("x") == {"MATLAB_class": "double"}

@@ -141,12 +141,7 @@ def test_sphere512_cluster_path_equals_split_path(sphere512):
 
 
 # ----------------------------------------------- Jones gate, README sphere ----
-def field_diff(a, b):
-    """Normalised RMS difference of DDA/FieldDiff.cpp:192 over the real and
-    imaginary parts: sqrt(sum (a-b)^2 / ((sum a^2 + sum b^2) / 2))."""
-    a = np.concatenate([np.real(a).ravel(), np.imag(a).ravel()])
-    b = np.concatenate([np.real(b).ravel(), np.imag(b).ravel()])
-    return math.sqrt(np.sum((a - b) ** 2) / ((np.sum(a * a) + np.sum(b * b)) / 2))
+from dda_b200.fielddiff import normalised_rms as field_diff  # DDA/FieldDiff.cpp:189-192
 
 
 @pytest.fixture(scope="module")

@@ -387,6 +387,8 @@ def main(argv=None):
     for per in (a.periodicity1, a.periodicity2):
         if any(api.parse_length(x.strip()) != 0 for x in per.strip().strip("()").split(",")):
             raise SystemExit("periodic targets (--periodicity-1, --periodicity-2) are not supported")
+    if a.device != "auto" and not a.device.isdigit():
+        raise SystemExit("--device takes a CUDA device index or `auto' (the OpenCL device names do not apply)")
     device = 0 if a.device == "auto" else int(a.device)
     if a.output_dir:
         out_dir, tagged = a.output_dir, None

@@ -213,7 +213,7 @@ def test_output_directories_and_tags(tmp_path):
 def test_option_errors_before_any_gpu_work(tmp_path):
     base = ["--geometry", "sphere:0.5um,1.5", "--output-dir", str(tmp_path)]
     for extra, msg in ((["--periodicity-1", "(1um,0,0)"], "periodic"), (["--cpu", "--opencl"], "exclude"),
-                       (["--tag", "x"], "both --output-dir and --tag")):
+                       (["--tag", "x"], "both --output-dir and --tag"), (["--device", "list"], "device index")):
         with pytest.raises(SystemExit, match=msg):
             cli.main(base + extra)
     a = cli.parser().parse_args(["--cpu", "--sync", "--dmatrix-host", "--opencl-fft", "apple", "--device", "0",

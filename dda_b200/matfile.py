@@ -131,26 +131,34 @@ def _object_header(messages):
 
 
 class _Image:
-    """The file after the user block, as it is laid out (relative addresses)."""
+    """The file after the user block, as it is laid out (relative addresses):
+    a list of pieces, the datasets' raw data as views of their arrays, so
+    that a large field is not copied before it is written."""
 
     def __init__(self):
-        self.buf = bytearray(96)  # superblock
+        self.parts = [bytes(96)]  # superblock, filled in last
+        self.size = 96
 
     def add(self, data):
-        self.buf += b"\0" * (-len(self.buf) % 8)
-        addr = len(self.buf)
-        self.buf += data
+        pad = -self.size % 8
+        if pad:
+            self.parts.append(b"\0" * pad)
+            self.size += pad
+        addr = self.size
+        self.parts.append(data)
+        self.size += len(data)
         return addr
 
     def next_addr(self):
-        return len(self.buf) + (-len(self.buf) % 8)
+        return self.size + (-self.size % 8)
 
 
 def _write_dataset(img, arr, attrs):
     arr = np.ascontiguousarray(arr)
-    arr = arr.astype(arr.dtype.newbyteorder("<"))
-    raw = arr.tobytes()
-    addr = img.add(raw) if raw else UNDEF
+    if arr.dtype.byteorder == ">":
+        arr = arr.astype(arr.dtype.newbyteorder("<"))
+    raw = memoryview(arr.reshape(-1).view(np.uint8))
+    addr = img.add(raw) if len(raw) else UNDEF
     msgs = [(1, _dataspace_message(arr.shape), 0), (3, _dtype_message(arr.dtype), 1),
             (8, struct.pack("<BBQQ", 3, 1, addr, len(raw)), 0)]
     msgs += [(0x0C, _attribute_message(k, v), 0) for k, v in attrs]
@@ -224,24 +232,28 @@ def user_block(text="MATLAB 7.3 MAT-file, written by dda_b200, HDF5 schema 1.00 
     return bytes(ub)
 
 
-def dumps(members):
-    """The bytes of a file whose root group holds `members` (a dict)."""
+def _pieces(members):
+    """The file as a list of byte pieces: user block, superblock, the rest."""
     img = _Image()
     root, (tree, heap) = _write_group(img, members, [])
-    size = USER_BLOCK + len(img.buf)
     sb = SIGNATURE + struct.pack("<BBBBBBBBHHI", 0, 0, 0, 0, 0, 8, 8, 0, LEAF_K, NODE_K, 0)
-    sb += struct.pack("<QQQQ", USER_BLOCK, UNDEF, size, UNDEF)
+    sb += struct.pack("<QQQQ", USER_BLOCK, UNDEF, USER_BLOCK + img.size, UNDEF)
     sb += struct.pack("<QQI4xQQ", 0, root, 1, tree, heap)
     assert len(sb) == 96
-    img.buf[:96] = sb
-    return user_block() + bytes(img.buf)
+    img.parts[0] = sb
+    return [user_block()] + img.parts
+
+
+def dumps(members):
+    """The bytes of a file whose root group holds `members` (a dict)."""
+    return b"".join(bytes(p) for p in _pieces(members))
 
 
 def save(path, members):
     """Write a MATLAB-style HDF5 file (HDF5::matlabSerialize)."""
-    data = dumps(members)
     with open(path, "wb") as f:
-        f.write(data)
+        for piece in _pieces(members):
+            f.write(piece)
 
 
 # --------------------------------------------------------------------------

@@ -189,17 +189,39 @@ def _g10(x):
 
 
 def field_txt(path, params, field_name, pol, vec, ftype="double"):
-    """DDAFieldFile::writeTxt (EMSim/DataFilesDDA.cpp:34-54): coordinates in
-    metres, |E|^2, then re, im of the x, y, z components."""
+    """DDAFieldFile::writeTxt (EMSim/DataFilesDDA.cpp:34-54) of a [3 nvs]
+    vector of this target."""
+    field_txt_rows(path, dipole_coords(params), _vec_rows(params, vec).astype(_cdtype(ftype)), field_name, pol)
+
+
+def field_txt_rows(out, coords, rows, field_name, pol):
+    """The text layout of a field: coordinates in metres, |E|^2, then re, im of
+    the x, y, z components, one dipole ([nv][3] rows) per line; `out` is a
+    path or a text stream."""
     name = field_name + ("-Pol%d" % pol if pol else "")
-    rows = _vec_rows(params, vec).astype(_cdtype(ftype))
     norm = (np.abs(rows) ** 2).sum(axis=1, dtype=rows.real.dtype)
-    coords = dipole_coords(params)
-    with open(path, "w") as f:
+    with open_out(out) as f:
         f.write("#x y z |%s|^2 " % name + " ".join("%s.%s.%s" % (name, c, p) for c in "xyz" for p in "ri") + "\n")
         for xyz, n2, r in zip(coords, norm, rows):
             f.write(" ".join(_g10(x) for x in xyz) + " " + _g10(n2) + " "
                     + " ".join(_g10(z) for v in r for z in (v.real, v.imag)) + "\n")
+
+
+class open_out:
+    """A path opened for writing, or a text stream used as it is."""
+
+    def __init__(self, out):
+        self.out, self.f = out, None
+
+    def __enter__(self):
+        if isinstance(self.out, str):
+            self.f = open(self.out, "w")
+            return self.f
+        return self.out
+
+    def __exit__(self, *exc):
+        if self.f is not None:
+            self.f.close()
 
 
 def read_field_txt(path, params):
@@ -224,23 +246,29 @@ def _from_rows(params, rows):
     return v
 
 
-def cross_section_txt(path, cext, cabs, qext, qabs):
-    """CrossSectionFile::writeTxt (EMSim/DataFiles.cpp:32-42)."""
-    with open(path, "w") as f:
-        for k, v in (("Cext", cext), ("Qext", qext), ("Cabs", cabs), ("Qabs", qabs), ("Csca", cext - cabs),
-                     ("Qsca", qext - qabs)):
+def cross_section_txt(out, cext, cabs, qext, qabs, csca=None, qsca=None):
+    """CrossSectionFile::writeTxt (EMSim/DataFiles.cpp:32-42); Csca and Qsca
+    default to the differences (CrossSection::setSca)."""
+    csca = cext - cabs if csca is None else csca
+    qsca = qext - qabs if qsca is None else qsca
+    with open_out(out) as f:
+        for k, v in (("Cext", cext), ("Qext", qext), ("Cabs", cabs), ("Qabs", qabs), ("Csca", csca), ("Qsca", qsca)):
             f.write("%s = %s\n" % (k, _g10(v)))
 
 
 def geometry_txt(path, params):
+    """DDADipoleListGeometryFile::writeTxt of this target."""
+    geometry_txt_rows(path, params.box, params.geometry.positions, params.geometry.materials)
+
+
+def geometry_txt_rows(out, box, pos, mat):
     """DDADipoleListGeometryFile::writeTxt (EMSim/DataFilesDDA.cpp:58-82): the
     box size, Nmat when there is more than one material, one dipole per line
     (with its 1-based material index when there are several)."""
-    pos = params.geometry.positions
-    mat = params.geometry.materials.astype(np.int64)
+    mat = np.asarray(mat).astype(np.int64)
     nmat = int(mat.max()) + 1 if len(mat) else 0
-    with open(path, "w") as f:
-        f.write("#box size: %dx%dx%d\n" % tuple(params.box))
+    with open_out(out) as f:
+        f.write("#box size: %dx%dx%d\n" % tuple(int(b) for b in box))
         if nmat != 1:
             f.write("Nmat=%d\n" % nmat)
         for p, m in zip(pos, mat):

@@ -17,6 +17,7 @@ import math
 import numpy as np
 
 from . import api
+from .datafiles import open_out
 
 
 def parse_angles(spec):
@@ -227,8 +228,9 @@ def mueller(j):
 
 def store_jones_txt(path, theta, phi, j, store_phi=True):
     """JonesCalculus::storeTxt (EMSim/JonesCalculus.cpp:89-116): angles in
-    degrees with two decimals, then s1..s4 = S22, S11, S12, S21 (real, imag)."""
-    with open(path, "w") as f:
+    degrees with two decimals, then s1..s4 = S22, S11, S12, S21 (real, imag);
+    `path` may also be a text stream."""
+    with open_out(path) as f:
         f.write("#theta " + ("phi " if store_phi else "") + "s1.r s1.i s2.r s2.i s3.r s3.i s4.r s4.i\n")
         for t, p, s in zip(theta, phi, j):
             row = "%.2f " % math.degrees(t)
@@ -241,7 +243,7 @@ def store_jones_txt(path, theta, phi, j, store_phi=True):
 
 def store_mueller_txt(path, theta, phi, m, no_phi=False):
     """MuellerCalculus::storeTxt (EMSim/MuellerCalculus.cpp:88-116)."""
-    with open(path, "w") as f:
+    with open_out(path) as f:
         f.write("#theta " + ("" if no_phi else "phi ") + " ".join("s%d%d" % (a, b) for a in range(1, 5)
                                                                   for b in range(1, 5)) + "\n")
         for t, p, e in zip(theta, phi, m):

@@ -223,8 +223,8 @@ def test_option_errors_before_any_gpu_work(tmp_path):
 
 @pytest.mark.gpu
 def test_cli_output_parent_dir_tags_and_log(tmp_path, capsys):
-    rc = cli.main(["--geometry", "sphere:0.3um,1.5", "--lambda", "1um", "--grid-unit", "0.1um",
-                   "--output-parent-dir", str(tmp_path), "--tag", "mine", "--verbose", "--mem-info"])
+    rc = cli.main(["--geometry", "sphere:0.3um,1.5", "--lambda", "1um", "--grid-unit", "0.1um", "--ftype", "float",
+                   "--efield", "--output-parent-dir", str(tmp_path), "--tag", "mine", "--verbose", "--mem-info"])
     assert rc == 0
     out = capsys.readouterr().out
     assert "couple constants" in out and "GPU memory of the context" in out and "Particle grid" in out
@@ -234,3 +234,8 @@ def test_cli_output_parent_dir_tags_and_log(tmp_path, capsys):
     for tag in ("running", "mine", "latest"):
         assert os.readlink(tmp_path / tag) == "output_0"
     assert os.path.exists(d / "DipPol-Pol1.hdf5") and os.path.exists(d / "CrossSec-Pol2.txt")
+    # --ftype float: fields and far fields in single precision, the Mie series in double
+    from dda_b200 import matfile
+    assert matfile.load(str(d / "DipPol-Pol1.hdf5"))["Field"]["Data"].dtype == np.complex64
+    assert matfile.reader(str(d / "FarPlane.hdf5")).attrs_of("JonesFarField/Data") == {"MATLAB_class": "single"}
+    assert matfile.load(str(d / "MieFarPlane.hdf5"))["JonesFarField"]["Data"].dtype == np.complex128

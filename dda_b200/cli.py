@@ -374,8 +374,49 @@ class _Tee:
             st.flush()
 
 
+HELP_TOPICS = {
+    "--geometry": ("Geometry options:\n"
+                   "  sphere:<radius>,<m>\n"
+                   "  cylinder:<length>,<radius>,<m>\n"
+                   "  box:(<x>,<y>,<z>),<m>\n"
+                   "  load:file=<filename>   a text dipole list (with -m and --grid-unit), an HDF5\n"
+                   "                         geometry file, or a directory holding Geometry.hdf5\n"),
+    "--beam": ("Beams:\n"
+               "  plane\n"
+               "  gaussian:lminus,<waist size>[,(x,y,z)]\n"
+               "  gaussian:davis3,<waist size>[,(x,y,z)]\n"
+               "  gaussian:barton5,<waist size>[,(x,y,z)]\n"),
+    "--pol": ("Polarizability descriptions:\n"
+              "  cm          Clausius-Mossotti\n"
+              "  ldr         lattice dispersion relation (Draine and Goodman)\n"
+              "  ldr-avgpol  lattice dispersion relation, polarisation-averaged\n"),
+    "--far-field": ("--far-field FileName=theta,phi[,jones|mueller|both|none][,no-phi]\n"
+                    "  theta and phi: an angle in degrees, or start..end/count (degrees)\n"
+                    "  jones (default), mueller or both: the matrices written\n"
+                    "  no-phi: no phi column in the text files\n"
+                    "  files: Far<FileName>.hdf5, Far<FileName>.mueller.hdf5 (and .txt with --write-txt)\n"),
+}
+
+
+def help_topic(argv):
+    """The text for `--geometry help`, `--beam help` (or `gaussian:help`),
+    `--pol help` and `--far-field help` (the help values of GeometryParser,
+    Beam, PolarizabilityDescription and FarFieldOption), or None."""
+    for i, arg in enumerate(argv):
+        opt, eq, val = arg.partition("=")
+        if not eq:
+            val = argv[i + 1] if i + 1 < len(argv) else ""
+        if opt in HELP_TOPICS and val in ("help", "gaussian:help"):
+            return HELP_TOPICS[opt]
+    return None
+
+
 def main(argv=None):
     argv = list(sys.argv[1:] if argv is None else argv)
+    topic = help_topic(argv)
+    if topic is not None:
+        sys.stdout.write(topic)
+        return 0
     if "--adda-options" in argv:  # DDA/Options.cpp:122-133
         k = argv.index("--adda-options")
         argv = argv[:k] + translate_adda(argv[k + 1:])

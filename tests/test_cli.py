@@ -239,3 +239,13 @@ def test_cli_output_parent_dir_tags_and_log(tmp_path, capsys):
     assert matfile.load(str(d / "DipPol-Pol1.hdf5"))["Field"]["Data"].dtype == np.complex64
     assert matfile.reader(str(d / "FarPlane.hdf5")).attrs_of("JonesFarField/Data") == {"MATLAB_class": "single"}
     assert matfile.load(str(d / "MieFarPlane.hdf5"))["JonesFarField"]["Data"].dtype == np.complex128
+
+
+def test_help_topics(capsys):
+    # "--beam help" and the like (Beam.cpp:78, GeometryParser.cpp:87, PolarizabilityDescription.cpp:36,
+    # FarFieldCalc.cpp:52) print the accepted values instead of running
+    for args, word in ((["--beam", "help"], "barton5"), (["--geometry=help"], "load:file="),
+                       (["--pol", "help"], "ldr-avgpol"), (["--far-field", "help"], "no-phi"),
+                       (["--beam", "gaussian:help"], "davis3")):
+        assert cli.main(args) == 0
+        assert word in capsys.readouterr().out

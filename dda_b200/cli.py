@@ -55,6 +55,7 @@ import argparse
 import math
 import os
 import sys
+import time
 
 import numpy as np
 
@@ -359,6 +360,43 @@ def create_tag(path, tag):
     os.symlink(os.path.basename(path), link)
 
 
+class _Prof:
+    """Consecutive named phases with their wall-clock and CPU time, written as
+    the reference's prof file (ProfilingData::toString, Core/Profiling.cpp:
+    47-150: per phase the milliseconds and the share of the total, then the
+    totals per name and overall)."""
+
+    def __init__(self):
+        self.phases, self.cur = [], None
+
+    def begin(self, name):
+        self.end()
+        self.cur = (name, time.perf_counter(), time.process_time())
+
+    def end(self):
+        if self.cur:
+            name, t, c = self.cur
+            self.phases.append((name, (time.perf_counter() - t) * 1e3, (time.process_time() - c) * 1e3))
+            self.cur = None
+
+    def overall(self):
+        self.end()
+        return sum(p[1] for p in self.phases), sum(p[2] for p in self.phases)
+
+    def text(self):
+        real, cpu = self.overall()
+        width = max([len("overall")] + [len(p[0]) for p in self.phases]) + 1
+        pct = lambda v, o: 100.0 * v / o if o > 0 else float("nan")
+        row = lambda n, r, c: "%-*s %10.3f ms = %5.1f%% %10.3f ms = %5.1f%% \n" % (width, n, r, pct(r, real), c,
+                                                                                    pct(c, cpu))
+        totals = {}
+        for n, r, c in self.phases:
+            tr, tc = totals.get(n, (0.0, 0.0))
+            totals[n] = (tr + r, tc + c)
+        return ("".join(row(n, r, c) for n, r, c in self.phases) + "====\n"
+                + "".join(row("=" + n, *totals[n]) for n, _, _ in self.phases) + row("overall", real, cpu))
+
+
 class _Tee:
     """stdout copied to the output directory's log file (DDAMain.cpp:711-712)."""
 
@@ -439,8 +477,14 @@ def main(argv=None):
         create_tag(tagged, "running")
     a.output_dir = out_dir
     log = open(os.path.join(out_dir, "log"), "w")
+    prof = _Prof()
     try:
-        rc = _run(a, argv, _Tee(sys.stdout, log), device)
+        out = _Tee(sys.stdout, log)
+        rc = _run(a, argv, out, device, prof)
+        with open(os.path.join(out_dir, "prof"), "w") as f:  # DDAMain.cpp:744-755
+            f.write(prof.text() + "\n")
+        out.write("Overall time %10.3f ms, %10.3f ms\n" % prof.overall())
+        out.write("Output directory: %s\n" % os.path.abspath(out_dir))
     finally:
         log.close()
     if tagged:
@@ -450,9 +494,10 @@ def main(argv=None):
     return rc
 
 
-def _run(a, argv, out, device):
+def _run(a, argv, out, device, prof):
     out.write("Output directory: %s\n" % os.path.abspath(a.output_dir))
     out.write("Command: %s\n" % " ".join(argv))
+    prof.begin("ddaParams cr")  # the phase names of DDAMain.cpp's ProfileHandles
     lambda_m = api.parse_length(a.lam)
     prop = tuple(parse_vector(a.prop))
     geom, refr, mie_geom, file_orient = build_geometry(a.geometry, a.grid_unit, a.m, lambda_m)
@@ -484,6 +529,7 @@ def _run(a, argv, out, device):
         except (OSError, ValueError, KeyError, matfile.MatFileError) as e:
             raise SystemExit("cannot load dipole polarisations from %s: %s" % (d, e))
 
+    prof.begin("Dmatrix")  # context: D matrix on the GPU, FFT plans, autotuning
     mv = api.CudaMatVec(params, prec, max_rhs=2, device=device)
     ccs = []
     for r, pol in enumerate((1, 2)):
@@ -504,6 +550,7 @@ def _run(a, argv, out, device):
                   % (ms[3], ms[0], ms[1], ms[2]))
         mv.close()
         return 0
+    prof.begin("res12")  # incident fields and the solve of both polarisations
     beam = api.Beam(a.beam)
     einc = np.stack([beam.einc(params, prop, 1, orient=orient), beam.einc(params, prop, 2, orient=orient)])
     if a.store_incbeam:
@@ -522,10 +569,14 @@ def _run(a, argv, out, device):
             out.write("Pol%d: %d iterations, relative residual %.3e\n" % (r + 1, st.iterations, st.rel_residual))
             for i, h in enumerate(hist):
                 out.write("RE_%d = %.10g\n" % (i + 1, h))
+    prof.begin("output dippol")
     for r in range(2):
         store_field("DipPol-Pol%d" % (r + 1), "DipolePolarization", r, pol[r])  # always, DDAMain.cpp:412
-        if a.store_intfield:  # internal field chi^-1 P, DDA/DDAMain.cpp:420-425
+    if a.store_intfield:  # internal field chi^-1 P, DDA/DDAMain.cpp:420-425
+        prof.begin("output intfield")
+        for r in range(2):
             store_field("IntField-Pol%d" % (r + 1), "InternalField", r, cc_vector(params, ccs[r].chi_inv) * pol[r])
+    prof.begin("output")
 
     pn = api.beam_frame(prop, orient)[0]  # forward direction in the particle frame
     ef = mv.far_field(pn[None, :], nrhs=2, pol=pol)[0]
@@ -550,6 +601,7 @@ def _run(a, argv, out, device):
                         lambda p: datafiles.cross_section_txt(p, qe * area, qa * area, qe, qa))
     # far fields (DDA/DDAMain.cpp:318-353): the angle lists of all options,
     # each list computed once for both polarisations
+    prof.begin("farfield")
     far = [postprocess.parse_far_field(x) for x in a.far_field]
     if a.efield or a.mueller_matrix:
         nt = a.ntheta or (180 if params.nv < 1000 else 360 if params.nv < 10000 else 720 if params.nv < 100000
@@ -602,6 +654,7 @@ def _run(a, argv, out, device):
                                 (lambda p: postprocess.store_mueller_txt(p, theta, phi, mm, no_phi=no_phi))
                                 if txt else None)
     mv.close()
+    prof.end()
     return 0
 
 

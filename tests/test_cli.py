@@ -231,6 +231,10 @@ def test_cli_output_parent_dir_tags_and_log(tmp_path, capsys):
     d = tmp_path / "output_0"
     log = open(d / "log").read()
     assert log.startswith("Output directory: ") and "Command: " in log and "Cext Pol1" in log
+    assert "Overall time" in log
+    prof = open(d / "prof").read()
+    for phase in ("ddaParams cr", "Dmatrix", "res12", "output dippol", "output", "farfield", "====", "overall"):
+        assert phase in prof, phase
     for tag in ("running", "mine", "latest"):
         assert os.readlink(tmp_path / tag) == "output_0"
     assert os.path.exists(d / "DipPol-Pol1.hdf5") and os.path.exists(d / "CrossSec-Pol2.txt")
@@ -249,3 +253,14 @@ def test_help_topics(capsys):
                        (["--beam", "gaussian:help"], "davis3")):
         assert cli.main(args) == 0
         assert word in capsys.readouterr().out
+
+
+def test_prof_file_layout():
+    # ProfilingData::toString (Core/Profiling.cpp): phases, "====", per-name totals, overall
+    p = cli._Prof()
+    for name in ("a", "bb", "a"):
+        p.begin(name)
+    p.end()
+    lines = p.text().splitlines()
+    assert [l.split()[0] for l in lines] == ["a", "bb", "a", "====", "=a", "=bb", "=a", "overall"]
+    assert lines[-1].split()[4] == "100.0%"

@@ -23,7 +23,7 @@ double; plus mixed), --no-symmetry (both polarisations are always solved),
 --load-dip-pol DIR (skip the solve), --load-start-dip-pol DIR (start values),
 --store-dippol, --store-intfield, --store-incbeam, --write-txt, --profiling-run
 (per-stage matvec times instead of a solve), --verbose (the couple constants and the
-beam), --mem-info (the context's device memory), --gamma (stored in the output
+beam), --mem-info (the context's device memory on stderr; always in the meminfo file), --gamma (stored in the output
 files' parameters), --periodicity-1/-2 (only (0,0,0): periodic targets are not
 supported), --device (the CUDA device index; auto = 0), --cpu, --opencl, --sync,
 --dmatrix-host, --opencl-fft (accepted; the solve runs on the GPU with CUDA).
@@ -271,6 +271,25 @@ def translate_adda(args):
     else:
         opts += ["--mueller-matrix"] * muel + ["--efield"] * ampl
     return opts
+
+
+def residual_lines(hist):
+    """The RE lines of IterativeSolverBase::getPolVec (DDA/IterativeSolverBase.cpp:
+    64-95): the iteration as five digits, the relative residual in scientific
+    notation, and "+ " for a new minimum, "-+" for a drop below the previous
+    step's residual, "- " otherwise (the progress and time-left columns, which
+    need per-iteration wall times, are left out)."""
+    lines, best, prev = [], None, None
+    for i, h in enumerate(hist):
+        if best is None or h <= best:
+            mark, best = "+ ", h
+        elif h < prev:
+            mark = "-+"
+        else:
+            mark = "- "
+        lines.append("RE_%05d = %12.6e  %s\n" % (i + 1, h, mark))
+        prev = h
+    return "".join(lines)
 
 
 def cc_vector(params, per_material):
@@ -540,10 +559,15 @@ def _run(a, argv, out, device, prof):
                   % (lambda_m, params.kd, a.beam, prop, orient))
         for r in range(2):
             out.write("Pol%d couple constants sqrt(cc) = %s\n" % (r + 1, np.asarray(ccs[r].cc_sqrt).tolist()))
-    if a.mem_info:  # DDAMain.cpp:578
-        lay = mv.layout
-        out.write("GPU memory of the context: %.1f MB (y/z path %s)\n"
-                  % (lay["device_bytes"] / 1e6, lay["yz_path"]))
+    # <out>/meminfo, and with --mem-info also stderr (DDAMain.cpp:577-601); this
+    # library allocates per context, so the context's device bytes are listed
+    lay = mv.layout
+    mem = ("Alloc 'context' (D matrix, plane buffers, Krylov vectors; y/z path %s) = %d kB, sum = %d kB\n"
+           % (lay["yz_path"], (lay["device_bytes"] + 1023) // 1024, (lay["device_bytes"] + 1023) // 1024))
+    with open(os.path.join(a.output_dir, "meminfo"), "w") as f:
+        f.write(mem)
+    if a.mem_info:
+        sys.stderr.write(mem)
     if a.profiling_run:  # IterativeSolverBase::profilingRun, DDA/IterativeSolverBase.cpp:105-136
         ms = mv.profile(nrhs=2, reps=5)
         out.write("matvec (2 rhs): %.3f ms  [x forward %.3f, y/z %.3f, x inverse %.3f]\n"
@@ -567,8 +591,7 @@ def _run(a, argv, out, device, prof):
         pol = solver.get_pol_vec(einc, 10.0 ** -a.epsilon, start=start)
         for r, (st, hist) in enumerate(zip(solver.last_stats, solver.last_history)):
             out.write("Pol%d: %d iterations, relative residual %.3e\n" % (r + 1, st.iterations, st.rel_residual))
-            for i, h in enumerate(hist):
-                out.write("RE_%d = %.10g\n" % (i + 1, h))
+            out.write(residual_lines(hist))
     prof.begin("output dippol")
     for r in range(2):
         store_field("DipPol-Pol%d" % (r + 1), "DipolePolarization", r, pol[r])  # always, DDAMain.cpp:412

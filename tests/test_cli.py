@@ -226,8 +226,8 @@ def test_cli_output_parent_dir_tags_and_log(tmp_path, capsys):
     rc = cli.main(["--geometry", "sphere:0.3um,1.5", "--lambda", "1um", "--grid-unit", "0.1um", "--ftype", "float",
                    "--efield", "--output-parent-dir", str(tmp_path), "--tag", "mine", "--verbose", "--mem-info"])
     assert rc == 0
-    out = capsys.readouterr().out
-    assert "couple constants" in out and "GPU memory of the context" in out and "Particle grid" in out
+    cap = capsys.readouterr()
+    assert "couple constants" in cap.out and "Particle grid" in cap.out and "Alloc 'context'" in cap.err
     d = tmp_path / "output_0"
     log = open(d / "log").read()
     assert log.startswith("Output directory: ") and "Command: " in log and "Cext Pol1" in log
@@ -238,6 +238,8 @@ def test_cli_output_parent_dir_tags_and_log(tmp_path, capsys):
     for tag in ("running", "mine", "latest"):
         assert os.readlink(tmp_path / tag) == "output_0"
     assert os.path.exists(d / "DipPol-Pol1.hdf5") and os.path.exists(d / "CrossSec-Pol2.txt")
+    assert open(d / "meminfo").read().startswith("Alloc 'context'")
+    assert "RE_00001 = " in log
     # --ftype float: fields and far fields in single precision, the Mie series in double
     from dda_b200 import matfile
     assert matfile.load(str(d / "DipPol-Pol1.hdf5"))["Field"]["Data"].dtype == np.complex64
@@ -264,3 +266,10 @@ def test_prof_file_layout():
     lines = p.text().splitlines()
     assert [l.split()[0] for l in lines] == ["a", "bb", "a", "====", "=a", "=bb", "=a", "overall"]
     assert lines[-1].split()[4] == "100.0%"
+
+
+def test_residual_lines():
+    # RE_%05d = %12.6e with the trend mark of DDA/IterativeSolverBase.cpp:77-83
+    assert cli.residual_lines([0.5, 0.25, 0.3, 0.28, 0.1]).splitlines() == [
+        "RE_00001 = 5.000000e-01  + ", "RE_00002 = 2.500000e-01  + ", "RE_00003 = 3.000000e-01  - ",
+        "RE_00004 = 2.800000e-01  -+", "RE_00005 = 1.000000e-01  + "]

@@ -305,3 +305,25 @@ def test_version_2_object_headers_and_compact_groups():
     v = M.loads(bytes(buf))
     assert list(v) == ["x"] and np.array_equal(v["x"], data)
     assert M._Reader(bytes(buf)).attrs_of("x") == {"MATLAB_class": "double"}
+
+
+def test_version_1_header_continued_in_a_second_block():
+    """A version 1 object header whose attribute sits in a continuation block
+    (message 0x10), the way libhdf5 grows a header when attributes are added."""
+    img = M._Image()
+    data = np.arange(4, dtype="<i4")
+    raw_at = img.add(data.tobytes())
+    attr = M._attribute_message("MATLAB_class", "int32")
+    cont_body = struct.pack("<HHB3x", 0x0C, len(M._pad8(attr)), 0) + M._pad8(attr)
+    cont_at = img.add(cont_body)
+    msgs = [(1, M._dataspace_message((4,)), 0), (3, M._dtype_message(data.dtype), 1),
+            (8, struct.pack("<BBQQ", 3, 1, raw_at, data.nbytes), 0),
+            (0x10, struct.pack("<QQ", cont_at, len(cont_body)), 0)]
+    hdr = bytearray(M._object_header(msgs))
+    struct.pack_into("<H", hdr, 2, len(msgs) + 1)  # the message count includes the continued one
+    ds_at = img.add(bytes(hdr))
+    r = M._Reader.__new__(M._Reader)
+    r.d, r.base = b"".join(bytes(p) for p in img.parts), 0
+    got = r.messages(ds_at)
+    assert [t for t, _, _ in got] == [1, 3, 8, 0x0C]
+    assert r.attributes(got) == {"MATLAB_class": "int32"} and np.array_equal(r.data(got), data)

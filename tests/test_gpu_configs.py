@@ -24,7 +24,7 @@ import dda_b200
 from dda_b200 import postprocess as PP
 from dda_b200 import targets
 from oracle import oracle as O
-from tests.pairs import Pair, rel
+from tests.pairs import rel
 
 pytestmark = pytest.mark.gpu
 

@@ -7,6 +7,9 @@ commands:
   hdf5-to-text   write each input's text layout to <input>.txt (or --output)
   cat            print each input's text layout
   resave-hdf5    write each input again, to <input>.new.hdf5 (or --output)
+  jones-to-mueller
+                 the Mueller matrices of each Jones far-field input, to
+                 <input>.mueller.hdf5 (or --output)
 
 options: --output/-o FILE (one input only), --theta-max-180 (keep far-field
 entries with theta <= 180 degrees), --no-phi (far-field text without the phi
@@ -86,9 +89,22 @@ def resave(path, out, type_override=None, theta_max_180=False):
     matfile.save(out, f)
 
 
+def jones_to_mueller(path, out, theta_max_180=False):
+    """jonesToMueller (EMSim/JonesToMueller.cpp:32-48): a MuellerFarField file
+    from a JonesFarField file, its Parameters and Geometry carried over."""
+    f = matfile.load(path)
+    theta, phi, j = _far_field(f, "JonesFarField", theta_max_180)
+    freq = np.asarray(f["JonesFarField"]["Frequency"], dtype=np.float64).reshape(-1)
+    m = postprocess.mueller(j)
+    members = {"Type": "MuellerFarField", "Parameters": f.get("Parameters"), "Geometry": f.get("Geometry"),
+               "MuellerFarField": {"Theta": theta, "Phi": phi, "Frequency": freq,
+                                   "Data": np.ascontiguousarray(m.transpose(0, 2, 1)[None])}}
+    matfile.save(out, members)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(prog="dda_b200.hdf5util", description=__doc__.split("\n\n")[0])
-    ap.add_argument("command", choices=["hdf5-to-text", "cat", "resave-hdf5"])
+    ap.add_argument("command", choices=["hdf5-to-text", "cat", "resave-hdf5", "jones-to-mueller"])
     ap.add_argument("inputs", nargs="+")
     ap.add_argument("-o", "--output")
     ap.add_argument("--theta-max-180", action="store_true")
@@ -106,12 +122,14 @@ def main(argv=None):
                     sys.stderr.write("Showing '%s':\n" % inp)
                 to_text(inp, sys.stdout, a.type, a.theta_max_180, a.no_phi)
                 continue
-            ext = ".txt" if a.command == "hdf5-to-text" else ".new.hdf5"
+            ext = {"hdf5-to-text": ".txt", "resave-hdf5": ".new.hdf5", "jones-to-mueller": ".mueller.hdf5"}[a.command]
             out = a.output or os.path.splitext(inp)[0] + ext
             if a.verbose:
                 sys.stderr.write("Converting '%s' to '%s' ..." % (inp, out))
             if a.command == "hdf5-to-text":
                 to_text(inp, out, a.type, a.theta_max_180, a.no_phi)
+            elif a.command == "jones-to-mueller":
+                jones_to_mueller(inp, out, a.theta_max_180)
             else:
                 resave(inp, out, a.type, a.theta_max_180)
             if a.verbose:

@@ -51,3 +51,17 @@ def test_text_of_every_file_type(tmp_path, capsys):
                           M.load(str(tmp_path / "IntField-Pol2.hdf5"))["Field"]["Data"])
     assert H.main(["cat", str(tmp_path / "IntField-Pol2.hdf5"), "--type", "Nonsense"]) == 1
     assert H.main(["hdf5-to-text", "a.hdf5", "b.hdf5", "-o", "x.txt"]) == 1
+
+
+def test_jones_to_mueller(tmp_path):
+    p = _params()
+    rng = np.random.default_rng(7)
+    theta, phi = P.grid_angles("0..180/5", "0..90/2")
+    j = rng.normal(size=(len(theta), 2, 2)) + 1j * rng.normal(size=(len(theta), 2, 2))
+    F.write(str(tmp_path / "FarX"), F.jones_file(F.parameters(p), F.dipole_list_geometry(p, full=False), theta, phi,
+                                                 3e14, j))
+    assert H.main(["jones-to-mueller", str(tmp_path / "FarX.hdf5")]) == 0
+    m = M.load(str(tmp_path / "FarX.mueller.hdf5"))
+    assert m["Type"] == "MuellerFarField" and m["Geometry"]["Type"] == "DDADipoleList" and m["Parameters"]["Method"] == "DDA"
+    assert np.allclose(m["MuellerFarField"]["Data"][0], P.mueller(j).transpose(0, 2, 1), rtol=1e-15, atol=0)
+    assert m["MuellerFarField"]["Frequency"].tolist() == [3e14]

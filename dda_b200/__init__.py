@@ -12,6 +12,12 @@ it mirrors the reference's interfaces for the path:
                        (DDA/IterativeSolverBase.hpp:59) for qmr, bicgstab,
                        bicg and cgnr (DDA/DDAMain.cpp:647-656)
 
+Beside them: postprocess (far field, Jones and Mueller matrices, cross
+sections, Mie), cli (the DDA command line), matfile and datafiles (the
+reference's MATLAB-style HDF5 and text data files, with no HDF5 library),
+fielddiff and hdf5util (its FieldDiff and Hdf5Util tools), serve (the request
+loop).
+
 There is no CPU fallback: importing the package fails if the library cannot
 be loaded, and every call raises DDAError with the library's message when the
 device path fails (the reference throws Core::Exception the same way).
